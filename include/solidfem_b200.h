@@ -1,0 +1,320 @@
+/*
+ * solidfem_b200 — C ABI of a B200-native (sm_100a) implementation of solidfem's solve path:
+ * 10-node tetrahedral elasticity, device FP64 stiffness assembly, and conjugate gradients
+ * preconditioned by a block smoothed-aggregation multigrid V-cycle that runs on the GPU.
+ *
+ * Every entry point replaces one call of the reference's Rust API (larsbrubaker/solidfem); the
+ * comment above each names the reference item (path:line inside that project) whose behaviour it
+ * keeps. Plain pointers and sizes only; no exceptions cross this boundary; every call returns an
+ * sf_status and leaves details in a thread-local sf_error (sf_last_error).
+ *
+ * Ownership follows the reference: a model moves into the builder (sf_builder_create consumes
+ * it, like StudyBuilder::new), a finished builder moves into the study (sf_builder_finish), and
+ * results are copied into caller buffers. Handles are not thread-safe: use one per host thread.
+ */
+#ifndef SOLIDFEM_B200_H
+#define SOLIDFEM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SF_ABI_VERSION 1
+
+/* Status codes. Named refusals mirror MeshError (crates/solidfem-mesh/src/error.rs),
+ * ModelError (crates/solidfem-elastic/src/error.rs:23-119), MultigridError
+ * (crates/solidfem-solve/src/multigrid/mod.rs:199-246) and PcgError
+ * (crates/solidfem-solve/src/pcg.rs:61-77). */
+typedef enum sf_status {
+  SF_OK = 0,
+  SF_MESH_EMPTY = 1,
+  SF_MESH_NON_FINITE_POSITION = 2,
+  SF_MESH_NODE_OUT_OF_RANGE = 3,
+  SF_MESH_DEGENERATE_TET = 4,
+  SF_MESH_FLAT_TET = 5,
+  SF_MESH_UNUSED_NODE = 6,
+  SF_MESH_NON_MANIFOLD_FACE = 7,
+  SF_MESH_INVALID_BOX = 8,
+  SF_NO_FIXED_NODES = 20,
+  SF_BODY_NOT_HELD = 21,
+  SF_NODE_OUT_OF_RANGE = 22,
+  SF_NON_FINITE_LOAD = 23,
+  SF_FACE_NOT_ON_BOUNDARY = 24,
+  SF_NO_EFFECTIVE_LOAD = 25,
+  SF_ELEMENT_INVERTED_JACOBIAN = 26,
+  SF_ELEMENT_INVALID_MATERIAL = 27,
+  SF_JACOBI_DIAGONAL = 28,
+  SF_CANCELLED = 29,
+  SF_NOT_FINISHED = 30,
+  SF_AXIS_OUT_OF_RANGE = 31,
+  SF_PRESCRIBED_ON_FIXED_NODE = 32,
+  SF_DOFS_DO_NOT_HOLD = 33,
+  SF_MG_BLOCK_STRUCTURE = 40,
+  SF_MG_NEAR_NULL_LENGTH = 41,
+  SF_MG_NOT_POSITIVE_DEFINITE = 42,
+  SF_MG_POSITION_LENGTH = 43,
+  SF_MG_COARSEST_NOT_FACTORED = 44,
+  SF_MG_COARSE_LENGTH = 45,
+  SF_PCG_NOT_POSITIVE_DEFINITE = 50,
+  SF_PCG_NOT_CONVERGED = 51,
+  SF_INVALID_ARGUMENT = 60,
+  SF_CUDA_ERROR = 61,
+  SF_DEVICE_MEMORY_BUDGET = 62,
+  SF_NO_DEVICE = 63,
+  SF_DEVICE_WAIT_TIMEOUT = 64
+} sf_status;
+
+/* Details of the last failure on this thread: the payloads of the reference's error variants. */
+typedef struct sf_error {
+  int32_t status;
+  uint32_t tet, node, face, point, axis;
+  uint64_t row, level, block, iteration, rank;
+  double pivot, curvature, relative_residual, determinant, value;
+  char message[256];
+} sf_error;
+
+/* The last failure on the calling thread. */
+sf_status sf_last_error(sf_error* out);
+/* A static English description of a status. */
+const char* sf_status_message(sf_status status);
+/* SF_ABI_VERSION of the loaded library. */
+int32_t sf_abi_version(void);
+
+/* ---------------------------------------------------------------- mesh --------------------- */
+typedef struct sf_mesh sf_mesh;
+
+/* A face on the mesh boundary: BoundaryFace, crates/solidfem-mesh/src/boundary.rs:15-24. */
+typedef struct sf_boundary_face {
+  uint32_t tet;
+  uint32_t face;     /* the corner it is opposite, 0..3 */
+  uint32_t nodes[6]; /* FACE_NODES order: three corners, then edge midpoints */
+} sf_boundary_face;
+
+/* box_tet_mesh (crates/solidfem-mesh/src/box_mesh.rs:22-80) upgraded by
+ * QuadraticTetMesh::from_linear (crates/solidfem-mesh/src/quadratic.rs:24-71). */
+sf_status sf_box_tet_mesh(const double origin[3], const double size[3],
+                          const uint64_t divisions[3], sf_mesh** out);
+/* TetMesh::new (crates/solidfem-mesh/src/tet.rs:59-109) then QuadraticTetMesh::from_linear.
+ * positions: n x 3, tets: ntets x 4. */
+sf_status sf_mesh_from_linear(const double* positions, uint64_t n, const uint32_t* tets,
+                              uint64_t ntets, sf_mesh** out);
+void sf_mesh_destroy(sf_mesh* mesh);
+uint64_t sf_mesh_node_count(const sf_mesh* mesh);
+uint64_t sf_mesh_tet_count(const sf_mesh* mesh);
+uint64_t sf_mesh_vertex_count(const sf_mesh* mesh);
+/* QuadraticTetMesh::nodes / tets (quadratic.rs:74-81): node_count x 3 and tet_count x 10. */
+sf_status sf_mesh_nodes(const sf_mesh* mesh, double* out);
+sf_status sf_mesh_tets(const sf_mesh* mesh, uint32_t* out);
+/* QuadraticTetMesh::boundary_faces (quadratic.rs:89-124), ascending by sorted corners. */
+uint64_t sf_mesh_boundary_face_count(const sf_mesh* mesh);
+sf_status sf_mesh_boundary_faces(const sf_mesh* mesh, sf_boundary_face* out);
+
+/* ---------------------------------------------------------------- model -------------------- */
+typedef struct sf_model sf_model;
+
+/* Material, crates/solidfem-elastic/src/material.rs:5-31. */
+typedef struct sf_material {
+  double youngs_modulus;
+  double poisson_ratio;
+} sf_material;
+
+/* A MaterialField (material.rs:35-50), evaluated in batches: write out[i] for positions[3i..3i+3],
+ * i < count. Called on the host with the integration points' physical positions. */
+typedef void (*sf_material_field_fn)(void* user, const double* positions, uint64_t count,
+                                     sf_material* out);
+
+enum { SF_QUADRATURE_FOUR_POINT = 0, SF_QUADRATURE_FOURTEEN_POINT = 1 };
+
+/* Model::new (crates/solidfem-elastic/src/study.rs:58-68): copies the mesh. */
+sf_status sf_model_create(const sf_mesh* mesh, sf_material material, sf_model** out);
+void sf_model_destroy(sf_model* model);
+/* A MaterialField callback in place of the uniform material. */
+sf_status sf_model_set_material_field(sf_model* model, sf_material_field_fn field, void* user);
+/* The printed-part field: points closer than `depth` to a face of the box [lo, hi] are `shell`,
+ * the rest `core`; evaluated per integration point like any MaterialField. */
+sf_status sf_model_set_shell_core(sf_model* model, sf_material shell, sf_material core,
+                                  const double lo[3], const double hi[3], double depth);
+/* Model::set_quadrature (study.rs:76-78). */
+sf_status sf_model_set_quadrature(sf_model* model, int32_t rule);
+/* Model::fix_node (study.rs:81-83); the array form fixes each listed node. */
+sf_status sf_model_fix_node(sf_model* model, uint32_t node);
+sf_status sf_model_fix_nodes(sf_model* model, const uint32_t* nodes, uint64_t count);
+/* Model::add_nodal_force (study.rs:86-88). */
+sf_status sf_model_add_nodal_force(sf_model* model, uint32_t node, const double force[3]);
+/* Model::add_traction (study.rs:101-103); the array form adds count faces, tractions count x 3. */
+sf_status sf_model_add_traction(sf_model* model, const sf_boundary_face* face,
+                                const double traction[3]);
+sf_status sf_model_add_tractions(sf_model* model, const sf_boundary_face* faces,
+                                 const double* tractions, uint64_t count);
+/* Model::prescribe_displacement (study.rs:96-98). */
+sf_status sf_model_prescribe_displacement(sf_model* model, uint32_t node, uint32_t axis,
+                                          double value);
+
+/* ---------------------------------------------------------------- options ------------------ */
+enum { SF_PRECONDITIONER_JACOBI = 0, SF_PRECONDITIONER_MULTIGRID = 1 };
+/* Precision (crates/solidfem-solve/src/multigrid/mod.rs:127-141) plus MIXED: the Single cycle
+ * (f32 storage and vectors) inside an FP64 flexible conjugate gradient. */
+enum {
+  SF_PRECISION_DOUBLE = 0,
+  SF_PRECISION_SINGLE_STORAGE = 1,
+  SF_PRECISION_SINGLE = 2,
+  SF_PRECISION_MIXED = 3
+};
+
+/* StudyOptions (study.rs:139-148) with PcgOptions (pcg.rs:14-33) and MultigridOptions
+ * (multigrid/mod.rs:143-182), plus device settings. */
+typedef struct sf_study_options {
+  double tolerance;        /* 1e-9 */
+  uint64_t max_iterations; /* 0: 10 n + 1000 */
+  int32_t preconditioner;  /* SF_PRECONDITIONER_* ; the reference's default is Jacobi */
+  double neighbour_reach;  /* 3.0 */
+  uint64_t coarse_dofs;    /* 1500 */
+  uint64_t max_levels;     /* 12 */
+  uint64_t smoother_degree;/* 3 */
+  double smoother_range;   /* 30.0 */
+  int32_t precision;       /* SF_PRECISION_* ; SINGLE_STORAGE */
+  uint64_t threads;        /* host threads for setup; 0: half the logical processors, at most 8 */
+  int32_t device;          /* CUDA device ordinal */
+  int32_t use_graphs;      /* capture each solver iteration in a CUDA graph (default 1) */
+  uint64_t device_memory_budget; /* bytes a study may hold on the device; 0: no limit */
+} sf_study_options;
+
+/* StudyOptions::default with the reference's defaults (Jacobi preconditioner). */
+void sf_study_options_default(sf_study_options* options);
+
+/* Returns nonzero to cancel. Read per element, per setup row and per solver iteration. */
+typedef int32_t (*sf_cancel_fn)(void* user);
+
+/* ---------------------------------------------------------------- build -------------------- */
+typedef struct sf_builder sf_builder;
+typedef struct sf_study sf_study;
+
+/* BuildProgress, study.rs:381-390. */
+typedef struct sf_build_progress {
+  uint64_t elements_done;
+  uint64_t elements_total;
+  int32_t setup_finished;
+} sf_build_progress;
+
+/* StudyBuilder::new (study.rs:419-474): validates, builds the load and the pattern. Consumes
+ * `model` whatever the outcome. */
+sf_status sf_builder_create(sf_model* model, const sf_study_options* options, sf_builder** out);
+/* StudyBuilder::step (study.rs:478-512): adds the stiffness of up to max_elements more elements
+ * (on the device), then advances the multigrid setup by up to max_elements block rows. Any
+ * slicing gives the bits of one call. */
+sf_status sf_builder_step(sf_builder* builder, uint64_t max_elements, sf_cancel_fn cancel,
+                          void* user, sf_build_progress* progress);
+/* StudyBuilder::finish (study.rs:601-656): on success consumes the builder. */
+sf_status sf_builder_finish(sf_builder* builder, sf_study** out);
+void sf_builder_destroy(sf_builder* builder);
+/* StaticStudy::new (study.rs:191-199): create + step(all) + finish. Consumes `model`. */
+sf_status sf_study_create(sf_model* model, const sf_study_options* options, sf_cancel_fn cancel,
+                          void* user, sf_study** out);
+
+/* ---------------------------------------------------------------- solve -------------------- */
+/* Progress, pcg.rs:36-45. */
+typedef struct sf_progress {
+  uint64_t iteration;
+  double relative_residual;
+  int32_t at_rounding_floor;
+} sf_progress;
+
+/* StepOutcome, pcg.rs:47-57. */
+enum { SF_OUTCOME_RUNNING = 0, SF_OUTCOME_CONVERGED = 1, SF_OUTCOME_CANCELLED = 2 };
+typedef struct sf_step_outcome {
+  int32_t kind;
+  sf_progress progress;
+} sf_step_outcome;
+
+/* StaticStudy::step (study.rs:202-215): up to max_iterations device iterations; the same bits
+ * however the solve is sliced. */
+sf_status sf_study_step(sf_study* study, uint64_t max_iterations, sf_cancel_fn cancel, void* user,
+                        sf_step_outcome* outcome);
+/* StaticStudy::displacements (study.rs:219-238): node_count x 3, zero at fixed nodes. */
+sf_status sf_study_displacements(const sf_study* study, double* out);
+
+/* Report, study.rs:151-176. */
+typedef struct sf_report {
+  uint64_t total_dofs;
+  uint64_t free_dofs;
+  uint64_t nonzeros;
+  int32_t at_rounding_floor;
+  uint64_t iterations;
+  double relative_residual;
+  double assembly_seconds;
+  double preconditioner_seconds;
+  double solve_seconds;
+  double recovery_seconds;
+  int32_t has_multigrid;
+  uint64_t mg_levels;
+  uint64_t mg_coarse_dofs;
+  double mg_operator_complexity;
+  uint64_t mg_memory_bytes;
+} sf_report;
+sf_status sf_study_report(const sf_study* study, sf_report* out);
+
+/* PointStress, crates/solidfem-elastic/src/results.rs:66-79. */
+typedef struct sf_point_stress {
+  uint32_t tet;
+  uint32_t point;
+  double position[3];
+  double stress[6];
+  double von_mises;
+} sf_point_stress;
+
+/* StaticStudy::solution (study.rs:246-260), recovered on the device: refuses with
+ * SF_NOT_FINISHED before convergence. Any output pointer may be NULL. displacements:
+ * node_count x 3; nodal_stress: node_count x 6; nodal_von_mises: node_count; points:
+ * tet_count x points_per_element. */
+sf_status sf_study_solution(sf_study* study, double* displacements, double* nodal_stress,
+                            double* nodal_von_mises, sf_point_stress* points);
+void sf_study_destroy(sf_study* study);
+
+/* ------------------------------------------------------------- inspection ----------------- */
+/* The assembled free-DOF system as scalar CSR (csr.rs:6-13), copied from the device:
+ * row_starts free_dofs + 1, columns and values nonzeros each. */
+sf_status sf_study_matrix(const sf_study* study, uint64_t* row_starts, uint32_t* columns,
+                          double* values);
+/* The right-hand side over the free DOFs (study.rs:444-449). */
+sf_status sf_study_rhs(const sf_study* study, double* out);
+
+/* Multigrid::level_sizes (cycle.rs:333-339) and MultigridStats (mod.rs:186-195). */
+uint64_t sf_study_level_count(const sf_study* study);
+typedef struct sf_level_info {
+  uint64_t rows, row_block, blocks;
+  double lambda_min, lambda_max;
+  int32_t has_prolongator;
+  uint64_t prolongator_blocks;
+  int32_t has_factor;
+} sf_level_info;
+sf_status sf_study_level_info(const sf_study* study, uint64_t level, sf_level_info* out);
+/* Multigrid::level_matrix / level_prolongator (cycle.rs:367-385): the level's f64 setup values
+ * (before any rounding to the stored precision). starts rows + 1, columns blocks. */
+sf_status sf_study_level_matrix(const sf_study* study, uint64_t level, int32_t prolongator,
+                                uint64_t* starts, uint32_t* columns, double* values);
+/* Multigrid::aggregates (cycle.rs:355-361): one per block row, empty on the coarsest level. */
+sf_status sf_study_aggregates(const sf_study* study, uint64_t level, uint32_t* out);
+/* Preconditioner::apply (preconditioner.rs:10-20): one device V-cycle (or Jacobi scaling) of
+ * `residual` into `output`, free_dofs each, host buffers. */
+sf_status sf_study_precondition(sf_study* study, const double* residual, double* output);
+/* CsrMatrix::multiply (csr.rs:112-120) on the device, FP64, host buffers. */
+sf_status sf_study_system_multiply(sf_study* study, const double* x, double* y);
+
+/* ------------------------------------------------------------- timing ---------------------- */
+/* Device time of the last sf_study_step call's kernels, measured with CUDA events on the
+ * study's stream; and the summed device time of the solver's SpMV-class kernels. */
+typedef struct sf_device_timing {
+  double step_ms;
+  double assembly_ms;
+  double setup_ms;
+  uint64_t kernel_launches;
+} sf_device_timing;
+sf_status sf_study_device_timing(const sf_study* study, sf_device_timing* out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,626 @@
+"""solidfem_b200: the solve path of solidfem (larsbrubaker/solidfem) on NVIDIA B200 (sm_100a).
+
+Python mirror of the reference's Rust API (crates/solidfem-elastic/src/study.rs and
+crates/solidfem-solve): ``box_tet_mesh`` / ``Mesh`` in, ``Model`` with material, supports and
+loads, ``StudyBuilder`` (resumable assembly and multigrid setup), ``StaticStudy`` (resumable,
+cancellable conjugate gradient) and the displacement field out. Every call goes through the C ABI
+of ``libsolidfem_b200.so`` (include/solidfem_b200.h); there is no CPU fallback: importing this
+package fails loudly when the library has not been built.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import enum
+import os
+from dataclasses import dataclass, field
+from typing import Callable, Optional, Sequence
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIBRARY_PATH = os.path.join(_HERE, "libsolidfem_b200.so")
+
+# ----------------------------------------------------------------------------- C structures
+
+
+class BoundaryFace(C.Structure):
+    """A boundary face: BoundaryFace, crates/solidfem-mesh/src/boundary.rs:15-24."""
+    _fields_ = [("tet", C.c_uint32), ("face", C.c_uint32), ("nodes", C.c_uint32 * 6)]
+
+    def key(self):
+        return (self.tet, self.face, tuple(self.nodes))
+
+    def __repr__(self):
+        return f"BoundaryFace(tet={self.tet}, face={self.face}, nodes={list(self.nodes)})"
+
+
+class _Material(C.Structure):
+    _fields_ = [("youngs_modulus", C.c_double), ("poisson_ratio", C.c_double)]
+
+
+class _Options(C.Structure):
+    _fields_ = [("tolerance", C.c_double), ("max_iterations", C.c_uint64), ("preconditioner", C.c_int32),
+                ("neighbour_reach", C.c_double), ("coarse_dofs", C.c_uint64), ("max_levels", C.c_uint64),
+                ("smoother_degree", C.c_uint64), ("smoother_range", C.c_double), ("precision", C.c_int32),
+                ("threads", C.c_uint64), ("device", C.c_int32), ("use_graphs", C.c_int32),
+                ("device_memory_budget", C.c_uint64)]
+
+
+class _BuildProgress(C.Structure):
+    _fields_ = [("elements_done", C.c_uint64), ("elements_total", C.c_uint64), ("setup_finished", C.c_int32)]
+
+
+class _Progress(C.Structure):
+    _fields_ = [("iteration", C.c_uint64), ("relative_residual", C.c_double), ("at_rounding_floor", C.c_int32)]
+
+
+class _StepOutcome(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("progress", _Progress)]
+
+
+class _Report(C.Structure):
+    _fields_ = [("total_dofs", C.c_uint64), ("free_dofs", C.c_uint64), ("nonzeros", C.c_uint64),
+                ("at_rounding_floor", C.c_int32), ("iterations", C.c_uint64), ("relative_residual", C.c_double),
+                ("assembly_seconds", C.c_double), ("preconditioner_seconds", C.c_double),
+                ("solve_seconds", C.c_double), ("recovery_seconds", C.c_double), ("has_multigrid", C.c_int32),
+                ("mg_levels", C.c_uint64), ("mg_coarse_dofs", C.c_uint64),
+                ("mg_operator_complexity", C.c_double), ("mg_memory_bytes", C.c_uint64)]
+
+
+class PointStress(C.Structure):
+    """PointStress, crates/solidfem-elastic/src/results.rs:66-79."""
+    _fields_ = [("tet", C.c_uint32), ("point", C.c_uint32), ("position", C.c_double * 3),
+                ("stress", C.c_double * 6), ("von_mises", C.c_double)]
+
+
+class _Error(C.Structure):
+    _fields_ = [("status", C.c_int32), ("tet", C.c_uint32), ("node", C.c_uint32), ("face", C.c_uint32),
+                ("point", C.c_uint32), ("axis", C.c_uint32), ("row", C.c_uint64), ("level", C.c_uint64),
+                ("block", C.c_uint64), ("iteration", C.c_uint64), ("rank", C.c_uint64), ("pivot", C.c_double),
+                ("curvature", C.c_double), ("relative_residual", C.c_double), ("determinant", C.c_double),
+                ("value", C.c_double), ("message", C.c_char * 256)]
+
+
+class _LevelInfo(C.Structure):
+    _fields_ = [("rows", C.c_uint64), ("row_block", C.c_uint64), ("blocks", C.c_uint64),
+                ("lambda_min", C.c_double), ("lambda_max", C.c_double), ("has_prolongator", C.c_int32),
+                ("prolongator_blocks", C.c_uint64), ("has_factor", C.c_int32)]
+
+
+class _DeviceTiming(C.Structure):
+    _fields_ = [("step_ms", C.c_double), ("assembly_ms", C.c_double), ("setup_ms", C.c_double),
+                ("kernel_launches", C.c_uint64)]
+
+
+_CANCEL = C.CFUNCTYPE(C.c_int32, C.c_void_p)
+_FIELD = C.CFUNCTYPE(None, C.c_void_p, C.POINTER(C.c_double), C.c_uint64, C.POINTER(_Material))
+
+# Every symbol include/solidfem_b200.h declares, with (restype, argtypes).
+_P = C.POINTER
+_V = C.c_void_p
+SIGNATURES = {
+    "sf_last_error": (C.c_int, [_P(_Error)]),
+    "sf_status_message": (C.c_char_p, [C.c_int]),
+    "sf_abi_version": (C.c_int32, []),
+    "sf_box_tet_mesh": (C.c_int, [_P(C.c_double), _P(C.c_double), _P(C.c_uint64), _P(_V)]),
+    "sf_mesh_from_linear": (C.c_int, [_P(C.c_double), C.c_uint64, _P(C.c_uint32), C.c_uint64, _P(_V)]),
+    "sf_mesh_destroy": (None, [_V]),
+    "sf_mesh_node_count": (C.c_uint64, [_V]),
+    "sf_mesh_tet_count": (C.c_uint64, [_V]),
+    "sf_mesh_vertex_count": (C.c_uint64, [_V]),
+    "sf_mesh_nodes": (C.c_int, [_V, _P(C.c_double)]),
+    "sf_mesh_tets": (C.c_int, [_V, _P(C.c_uint32)]),
+    "sf_mesh_boundary_face_count": (C.c_uint64, [_V]),
+    "sf_mesh_boundary_faces": (C.c_int, [_V, _P(BoundaryFace)]),
+    "sf_model_create": (C.c_int, [_V, _Material, _P(_V)]),
+    "sf_model_destroy": (None, [_V]),
+    "sf_model_set_material_field": (C.c_int, [_V, _FIELD, _V]),
+    "sf_model_set_shell_core": (C.c_int, [_V, _Material, _Material, _P(C.c_double), _P(C.c_double), C.c_double]),
+    "sf_model_set_quadrature": (C.c_int, [_V, C.c_int32]),
+    "sf_model_fix_node": (C.c_int, [_V, C.c_uint32]),
+    "sf_model_fix_nodes": (C.c_int, [_V, _P(C.c_uint32), C.c_uint64]),
+    "sf_model_add_nodal_force": (C.c_int, [_V, C.c_uint32, _P(C.c_double)]),
+    "sf_model_add_traction": (C.c_int, [_V, _P(BoundaryFace), _P(C.c_double)]),
+    "sf_model_add_tractions": (C.c_int, [_V, _P(BoundaryFace), _P(C.c_double), C.c_uint64]),
+    "sf_model_prescribe_displacement": (C.c_int, [_V, C.c_uint32, C.c_uint32, C.c_double]),
+    "sf_study_options_default": (None, [_P(_Options)]),
+    "sf_builder_create": (C.c_int, [_V, _P(_Options), _P(_V)]),
+    "sf_builder_step": (C.c_int, [_V, C.c_uint64, _CANCEL, _V, _P(_BuildProgress)]),
+    "sf_builder_finish": (C.c_int, [_V, _P(_V)]),
+    "sf_builder_destroy": (None, [_V]),
+    "sf_study_create": (C.c_int, [_V, _P(_Options), _CANCEL, _V, _P(_V)]),
+    "sf_study_step": (C.c_int, [_V, C.c_uint64, _CANCEL, _V, _P(_StepOutcome)]),
+    "sf_study_displacements": (C.c_int, [_V, _P(C.c_double)]),
+    "sf_study_report": (C.c_int, [_V, _P(_Report)]),
+    "sf_study_solution": (C.c_int, [_V, _P(C.c_double), _P(C.c_double), _P(C.c_double), _P(PointStress)]),
+    "sf_study_destroy": (None, [_V]),
+    "sf_study_matrix": (C.c_int, [_V, _P(C.c_uint64), _P(C.c_uint32), _P(C.c_double)]),
+    "sf_study_rhs": (C.c_int, [_V, _P(C.c_double)]),
+    "sf_study_level_count": (C.c_uint64, [_V]),
+    "sf_study_level_info": (C.c_int, [_V, C.c_uint64, _P(_LevelInfo)]),
+    "sf_study_level_matrix": (C.c_int, [_V, C.c_uint64, C.c_int32, _P(C.c_uint64), _P(C.c_uint32), _P(C.c_double)]),
+    "sf_study_aggregates": (C.c_int, [_V, C.c_uint64, _P(C.c_uint32)]),
+    "sf_study_precondition": (C.c_int, [_V, _P(C.c_double), _P(C.c_double)]),
+    "sf_study_system_multiply": (C.c_int, [_V, _P(C.c_double), _P(C.c_double)]),
+    "sf_study_device_timing": (C.c_int, [_V, _P(_DeviceTiming)]),
+}
+
+_lib = None
+
+
+def library() -> C.CDLL:
+    """The loaded C-ABI library. Raises when it has not been built (no fallback exists)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIBRARY_PATH):
+            raise ImportError(f"{LIBRARY_PATH} is missing: build it with `python -m solidfem_b200.build` "
+                              "(there is no CPU fallback)")
+        lib = C.CDLL(LIBRARY_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = lib
+    return _lib
+
+
+class Status(enum.IntEnum):
+    OK = 0
+    MESH_EMPTY = 1
+    MESH_NON_FINITE_POSITION = 2
+    MESH_NODE_OUT_OF_RANGE = 3
+    MESH_DEGENERATE_TET = 4
+    MESH_FLAT_TET = 5
+    MESH_UNUSED_NODE = 6
+    MESH_NON_MANIFOLD_FACE = 7
+    MESH_INVALID_BOX = 8
+    NO_FIXED_NODES = 20
+    BODY_NOT_HELD = 21
+    NODE_OUT_OF_RANGE = 22
+    NON_FINITE_LOAD = 23
+    FACE_NOT_ON_BOUNDARY = 24
+    NO_EFFECTIVE_LOAD = 25
+    ELEMENT_INVERTED_JACOBIAN = 26
+    ELEMENT_INVALID_MATERIAL = 27
+    JACOBI_DIAGONAL = 28
+    CANCELLED = 29
+    NOT_FINISHED = 30
+    AXIS_OUT_OF_RANGE = 31
+    PRESCRIBED_ON_FIXED_NODE = 32
+    DOFS_DO_NOT_HOLD = 33
+    MG_BLOCK_STRUCTURE = 40
+    MG_NEAR_NULL_LENGTH = 41
+    MG_NOT_POSITIVE_DEFINITE = 42
+    MG_POSITION_LENGTH = 43
+    MG_COARSEST_NOT_FACTORED = 44
+    MG_COARSE_LENGTH = 45
+    PCG_NOT_POSITIVE_DEFINITE = 50
+    PCG_NOT_CONVERGED = 51
+    INVALID_ARGUMENT = 60
+    CUDA_ERROR = 61
+    DEVICE_MEMORY_BUDGET = 62
+    NO_DEVICE = 63
+    DEVICE_WAIT_TIMEOUT = 64
+
+
+class SolidfemError(RuntimeError):
+    """A refusal or failure: the reference's ModelError / MultigridError / PcgError variants, named by
+    ``status`` with their payload in ``detail``."""
+
+    def __init__(self, status: int, detail: dict):
+        self.status = Status(status)
+        self.detail = detail
+        super().__init__(f"{self.status.name}: {detail.get('message', '')}")
+
+
+def _check(code: int) -> None:
+    if code != 0:
+        err = _Error()
+        library().sf_last_error(C.byref(err))
+        detail = {name: getattr(err, name) for name, _ in _Error._fields_ if name != "message"}
+        detail["message"] = err.message.decode(errors="replace")
+        raise SolidfemError(code, detail)
+
+
+def _dptr(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def _uptr(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_uint32))
+
+
+# ----------------------------------------------------------------------------- mesh
+
+
+class Mesh:
+    """A validated 10-node tetrahedral mesh (QuadraticTetMesh, crates/solidfem-mesh/src/quadratic.rs)."""
+
+    def __init__(self, handle):
+        self._h = handle
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            library().sf_mesh_destroy(self._h)
+            self._h = None
+
+    @property
+    def handle(self):
+        return self._h
+
+    def node_count(self) -> int:
+        return int(library().sf_mesh_node_count(self._h))
+
+    def tet_count(self) -> int:
+        return int(library().sf_mesh_tet_count(self._h))
+
+    def vertex_count(self) -> int:
+        return int(library().sf_mesh_vertex_count(self._h))
+
+    def nodes(self) -> np.ndarray:
+        out = np.empty((self.node_count(), 3))
+        _check(library().sf_mesh_nodes(self._h, _dptr(out)))
+        return out
+
+    def tets(self) -> np.ndarray:
+        out = np.empty((self.tet_count(), 10), dtype=np.uint32)
+        _check(library().sf_mesh_tets(self._h, _uptr(out)))
+        return out
+
+    def boundary_faces(self) -> list:
+        n = int(library().sf_mesh_boundary_face_count(self._h))
+        arr = (BoundaryFace * max(n, 1))()
+        _check(library().sf_mesh_boundary_faces(self._h, arr))
+        return list(arr[:n])
+
+    @classmethod
+    def from_linear(cls, positions, tets) -> "Mesh":
+        """TetMesh::new + QuadraticTetMesh::from_linear (tet.rs:59-109, quadratic.rs:24-71)."""
+        p = np.ascontiguousarray(positions, dtype=np.float64)
+        t = np.ascontiguousarray(tets, dtype=np.uint32)
+        h = C.c_void_p()
+        _check(library().sf_mesh_from_linear(_dptr(p), len(p), _uptr(t), len(t), C.byref(h)))
+        return cls(h)
+
+
+def box_tet_mesh(origin, size, divisions) -> Mesh:
+    """box_tet_mesh (crates/solidfem-mesh/src/box_mesh.rs:22-80) upgraded to 10 nodes."""
+    h = C.c_void_p()
+    _check(library().sf_box_tet_mesh((C.c_double * 3)(*origin), (C.c_double * 3)(*size),
+                                     (C.c_uint64 * 3)(*[int(d) for d in divisions]), C.byref(h)))
+    return Mesh(h)
+
+
+# ----------------------------------------------------------------------------- model
+
+
+@dataclass(frozen=True)
+class Material:
+    """Isotropic linear elastic properties (crates/solidfem-elastic/src/material.rs:5-31)."""
+    youngs_modulus: float
+    poisson_ratio: float
+
+    def _c(self):
+        return _Material(self.youngs_modulus, self.poisson_ratio)
+
+
+@dataclass(frozen=True)
+class ShellCore:
+    """A printed part's material field: points nearer than ``depth`` to a face of the box
+    ``[lo, hi]`` are ``shell``, the rest ``core``; evaluated per integration point."""
+    shell: Material
+    core: Material
+    lo: Sequence[float]
+    hi: Sequence[float]
+    depth: float
+
+
+class Quadrature(enum.IntEnum):
+    FOUR_POINT = 0
+    FOURTEEN_POINT = 1
+
+
+class Model:
+    """A structure, its material, supports and loads (Model, study.rs:46-104)."""
+
+    def __init__(self, mesh: Mesh, material):
+        self.mesh = mesh
+        self.material = material
+        self.quadrature = Quadrature.FOUR_POINT
+        self.fixed: list = []
+        self.forces: list = []
+        self.tractions: list = []
+        self.prescribed: dict = {}
+
+    def set_quadrature(self, q: Quadrature) -> None:
+        self.quadrature = Quadrature(q)
+
+    def fix_node(self, node: int) -> None:
+        self.fixed.append(int(node))
+
+    def fix_nodes(self, nodes) -> None:
+        self.fixed.extend(int(n) for n in nodes)
+
+    def add_nodal_force(self, node: int, force) -> None:
+        self.forces.append((int(node), tuple(float(f) for f in force)))
+
+    def add_traction(self, face: BoundaryFace, traction) -> None:
+        self.tractions.append((face, tuple(float(t) for t in traction)))
+
+    def prescribe_displacement(self, node: int, axis: int, value: float) -> None:
+        self.prescribed[(int(node), int(axis))] = float(value)
+
+    def _to_c(self):
+        lib = library()
+        h = C.c_void_p()
+        mat = self.material
+        base = mat if isinstance(mat, Material) else Material(1.0, 0.0)
+        _check(lib.sf_model_create(self.mesh.handle, base._c(), C.byref(h)))
+        keep = []
+        if isinstance(mat, ShellCore):
+            _check(lib.sf_model_set_shell_core(h, mat.shell._c(), mat.core._c(), (C.c_double * 3)(*mat.lo),
+                                               (C.c_double * 3)(*mat.hi), mat.depth))
+        elif callable(mat):
+            def field(user, positions, count, out, fn=mat):
+                pos = np.ctypeslib.as_array(positions, shape=(count * 3,)).reshape(count, 3)
+                for i in range(count):
+                    m = fn(pos[i])
+                    out[i].youngs_modulus = m.youngs_modulus
+                    out[i].poisson_ratio = m.poisson_ratio
+            cb = _FIELD(field)
+            keep.append(cb)
+            _check(lib.sf_model_set_material_field(h, cb, None))
+        _check(lib.sf_model_set_quadrature(h, int(self.quadrature)))
+        if self.fixed:
+            f = np.ascontiguousarray(self.fixed, dtype=np.uint32)
+            _check(lib.sf_model_fix_nodes(h, _uptr(f), len(f)))
+        for node, force in self.forces:
+            _check(lib.sf_model_add_nodal_force(h, node, (C.c_double * 3)(*force)))
+        if self.tractions:
+            faces = (BoundaryFace * len(self.tractions))(*[f for f, _ in self.tractions])
+            tr = np.ascontiguousarray([t for _, t in self.tractions], dtype=np.float64)
+            _check(lib.sf_model_add_tractions(h, faces, _dptr(tr), len(self.tractions)))
+        for (node, axis), value in self.prescribed.items():
+            _check(lib.sf_model_prescribe_displacement(h, node, axis, value))
+        return h, keep
+
+
+# ----------------------------------------------------------------------------- options
+
+
+class Precision(enum.IntEnum):
+    """multigrid/mod.rs:127-141, plus MIXED: the f32 cycle inside FP64 flexible CG."""
+    DOUBLE = 0
+    SINGLE_STORAGE = 1
+    SINGLE = 2
+    MIXED = 3
+
+
+@dataclass
+class PcgOptions:
+    """pcg.rs:14-33."""
+    tolerance: float = 1e-9
+    max_iterations: Optional[int] = None
+
+
+@dataclass
+class MultigridOptions:
+    """multigrid/mod.rs:143-182."""
+    neighbour_reach: float = 3.0
+    coarse_dofs: int = 1500
+    max_levels: int = 12
+    smoother_degree: int = 3
+    smoother_range: float = 30.0
+    precision: Precision = Precision.SINGLE_STORAGE
+    threads: int = 0
+
+
+class Jacobi:
+    """PreconditionerChoice::Jacobi (study.rs:106-115)."""
+
+
+@dataclass
+class StudyOptions:
+    """StudyOptions (study.rs:139-148): Jacobi unless a MultigridOptions is given."""
+    pcg: PcgOptions = field(default_factory=PcgOptions)
+    preconditioner: object = field(default_factory=Jacobi)
+    device: int = 0
+    use_graphs: bool = True
+    device_memory_budget: int = 0
+
+    def _c(self) -> _Options:
+        o = _Options()
+        library().sf_study_options_default(C.byref(o))
+        o.tolerance = self.pcg.tolerance
+        o.max_iterations = self.pcg.max_iterations or 0
+        if isinstance(self.preconditioner, MultigridOptions):
+            m = self.preconditioner
+            o.preconditioner = 1
+            o.neighbour_reach = m.neighbour_reach
+            o.coarse_dofs = m.coarse_dofs
+            o.max_levels = m.max_levels
+            o.smoother_degree = m.smoother_degree
+            o.smoother_range = m.smoother_range
+            o.precision = int(m.precision)
+            o.threads = m.threads
+        else:
+            o.preconditioner = 0
+        o.device = self.device
+        o.use_graphs = 1 if self.use_graphs else 0
+        o.device_memory_budget = self.device_memory_budget
+        return o
+
+
+def _cancel_fn(cancel: Optional[Callable[[], bool]]):
+    if cancel is None:
+        return _CANCEL(0)
+    return _CANCEL(lambda _user: 1 if cancel() else 0)
+
+
+# ----------------------------------------------------------------------------- study
+
+
+@dataclass
+class BuildProgress:
+    elements_done: int
+    elements_total: int
+    setup_finished: bool
+
+
+@dataclass
+class Progress:
+    """pcg.rs:36-45."""
+    iteration: int
+    relative_residual: float
+    at_rounding_floor: bool
+
+
+class Outcome(enum.IntEnum):
+    RUNNING = 0
+    CONVERGED = 1
+    CANCELLED = 2
+
+
+@dataclass
+class StepOutcome:
+    """pcg.rs:47-57."""
+    kind: Outcome
+    progress: Progress
+
+
+class StudyBuilder:
+    """StudyBuilder (study.rs:392-656): new validates and builds the load and pattern; step adds
+    element stiffness on the device and then advances the multigrid setup."""
+
+    def __init__(self, model: Model, options: Optional[StudyOptions] = None):
+        options = options or StudyOptions()
+        mh, self._keep = model._to_c()
+        self._mesh = model.mesh
+        h = C.c_void_p()
+        _check(library().sf_builder_create(mh, C.byref(options._c()), C.byref(h)))
+        self._h = h
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            library().sf_builder_destroy(self._h)
+            self._h = None
+
+    def step(self, max_elements: int, cancel: Optional[Callable[[], bool]] = None) -> BuildProgress:
+        p = _BuildProgress()
+        cb = _cancel_fn(cancel)
+        _check(library().sf_builder_step(self._h, max_elements, cb, None, C.byref(p)))
+        return BuildProgress(p.elements_done, p.elements_total, bool(p.setup_finished))
+
+    def finish(self) -> "StaticStudy":
+        h = C.c_void_p()
+        _check(library().sf_builder_finish(self._h, C.byref(h)))
+        self._h = None
+        return StaticStudy(h, self._mesh, self._keep)
+
+
+class StaticStudy:
+    """A study in progress (StaticStudy, study.rs:178-378): step runs device iterations."""
+
+    def __init__(self, handle, mesh: Mesh, keep=()):
+        self._h = handle
+        self.mesh = mesh
+        self._keep = keep
+
+    @classmethod
+    def new(cls, model: Model, options: Optional[StudyOptions] = None,
+            cancel: Optional[Callable[[], bool]] = None) -> "StaticStudy":
+        """StaticStudy::new (study.rs:191-199)."""
+        options = options or StudyOptions()
+        mh, keep = model._to_c()
+        h = C.c_void_p()
+        _check(library().sf_study_create(mh, C.byref(options._c()), _cancel_fn(cancel), None, C.byref(h)))
+        return cls(h, model.mesh, keep)
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            library().sf_study_destroy(self._h)
+            self._h = None
+
+    def step(self, max_iterations: int, cancel: Optional[Callable[[], bool]] = None) -> StepOutcome:
+        o = _StepOutcome()
+        _check(library().sf_study_step(self._h, max_iterations, _cancel_fn(cancel), None, C.byref(o)))
+        p = o.progress
+        return StepOutcome(Outcome(o.kind), Progress(p.iteration, p.relative_residual, bool(p.at_rounding_floor)))
+
+    def solve(self, slice_iterations: int = 2**62) -> StepOutcome:
+        while True:
+            o = self.step(slice_iterations)
+            if o.kind != Outcome.RUNNING:
+                return o
+
+    def displacements(self) -> np.ndarray:
+        out = np.empty((self.mesh.node_count(), 3))
+        _check(library().sf_study_displacements(self._h, _dptr(out)))
+        return out
+
+    def report(self) -> dict:
+        r = _Report()
+        _check(library().sf_study_report(self._h, C.byref(r)))
+        return {name: getattr(r, name) for name, _ in _Report._fields_}
+
+    def matrix(self):
+        rep = self.report()
+        n, nnz = rep["free_dofs"], rep["nonzeros"]
+        rs = np.empty(n + 1, dtype=np.uint64)
+        cols = np.empty(nnz, dtype=np.uint32)
+        vals = np.empty(nnz)
+        _check(library().sf_study_matrix(self._h, rs.ctypes.data_as(C.POINTER(C.c_uint64)), _uptr(cols), _dptr(vals)))
+        return rs, cols, vals
+
+    def rhs(self) -> np.ndarray:
+        out = np.empty(self.report()["free_dofs"])
+        _check(library().sf_study_rhs(self._h, _dptr(out)))
+        return out
+
+    def levels(self) -> list:
+        lib = library()
+        out = []
+        for lv in range(int(lib.sf_study_level_count(self._h))):
+            info = _LevelInfo()
+            _check(lib.sf_study_level_info(self._h, lv, C.byref(info)))
+            rb = info.row_block
+            st = np.empty(info.rows + 1, dtype=np.uint64)
+            cols = np.empty(info.blocks, dtype=np.uint32)
+            vals = np.empty(info.blocks * rb * rb)
+            _check(lib.sf_study_level_matrix(self._h, lv, 0, st.ctypes.data_as(C.POINTER(C.c_uint64)), _uptr(cols), _dptr(vals)))
+            d = {"rows": info.rows, "row_block": rb, "starts": st, "columns": cols, "values": vals,
+                 "lambda_min": info.lambda_min, "lambda_max": info.lambda_max, "has_factor": bool(info.has_factor)}
+            if info.has_prolongator:
+                pst = np.empty(info.rows + 1, dtype=np.uint64)
+                pc = np.empty(info.prolongator_blocks, dtype=np.uint32)
+                pv = np.empty(info.prolongator_blocks * rb * 6)
+                _check(lib.sf_study_level_matrix(self._h, lv, 1, pst.ctypes.data_as(C.POINTER(C.c_uint64)), _uptr(pc), _dptr(pv)))
+                agg = np.empty(info.rows, dtype=np.uint32)
+                _check(lib.sf_study_aggregates(self._h, lv, _uptr(agg)))
+                d.update({"p_starts": pst, "p_columns": pc, "p_values": pv, "aggregates": agg})
+            out.append(d)
+        return out
+
+    def precondition(self, residual: np.ndarray) -> np.ndarray:
+        r = np.ascontiguousarray(residual, dtype=np.float64)
+        z = np.empty_like(r)
+        _check(library().sf_study_precondition(self._h, _dptr(r), _dptr(z)))
+        return z
+
+    def system_multiply(self, x: np.ndarray) -> np.ndarray:
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        y = np.empty_like(x)
+        _check(library().sf_study_system_multiply(self._h, _dptr(x), _dptr(y)))
+        return y
+
+    def device_timing(self) -> dict:
+        t = _DeviceTiming()
+        _check(library().sf_study_device_timing(self._h, C.byref(t)))
+        return {name: getattr(t, name) for name, _ in _DeviceTiming._fields_}
+
+
+__all__ = [
+    "BoundaryFace", "Mesh", "box_tet_mesh", "Material", "ShellCore", "Quadrature", "Model", "Precision",
+    "PcgOptions", "MultigridOptions", "Jacobi", "StudyOptions", "StudyBuilder", "StaticStudy", "StepOutcome",
+    "Outcome", "Progress", "BuildProgress", "PointStress", "SolidfemError", "Status", "library", "SIGNATURES",
+]

@@ -1,0 +1,151 @@
+// Device-side data of a study and the host launchers of the sm_100a kernels. Kernels live in
+// assembly.cu (bit-exact FP64 assembly and recovery, built with -fmad=false) and solve.cu (the
+// solve path: block SpMV, Chebyshev smoother, transfers, coarse solve, PCG with fixed-order
+// reductions).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <vector>
+
+#include "sf_internal.h"
+
+namespace sf {
+
+// A block sparse matrix on the device: rows x (rb x cb) row-major blocks of S values.
+struct DevBsr {
+  uint32_t rows = 0, rb = 0, cb = 0;
+  size_t blocks = 0;
+  uint32_t* starts = nullptr;  // rows + 1
+  uint32_t* cols = nullptr;    // blocks
+  void* vals = nullptr;        // blocks * rb * cb values of the storage type
+};
+
+// The solver's scalar state, resident on the device so the iteration loop runs without host
+// round trips; kernels read `status` and exit early once the solve has ended.
+enum { ST_ACTIVE = 0, ST_CONVERGED = 1, ST_FAILED_NOT_PD = 2, ST_FAILED_NOT_CONVERGED = 3 };
+enum { MODE_NORMAL = 0, MODE_CHECK = 1, MODE_RESTART = 2 };
+
+struct PcgState {
+  double rz, alpha, beta, curvature, rel, rhs_norm, tolerance, floor;
+  double partial_rz, partial_apz;
+  unsigned long long iterations, max_iterations, fail_iteration;
+  int status, mode, at_floor, flexible;
+  unsigned int tickets[8];
+};
+
+// Reduction scratch: one partial per block of the fixed reduction grid.
+static const int kReduceBlocks = 592;  // 4 x 148 SMs
+static const int kReduceThreads = 256;
+
+struct DevLevel {
+  DevBsr a;          // the level operator in storage precision
+  void* dinv = nullptr;  // rows * rb * rb, storage precision
+  DevBsr p;          // prolongator to the next level (rb x 6), storage precision
+  DevBsr r;          // its explicit transpose (6 x rb), for gather restriction
+  bool has_p = false;
+  bool has_factor = false;
+  uint32_t n = 0;         // scalar rows
+  double* coarse_inverse = nullptr;  // n x n f64, coarsest factored level
+  // Chebyshev scalars in f64 (ChebyshevCoefficients, gpu/layout.rs:443-465)
+  double theta = 0;
+  std::vector<std::pair<double, double>> steps;
+  // vectors of the vector precision
+  void *b = nullptr, *x = nullptr, *res = nullptr, *z = nullptr, *d0 = nullptr, *d1 = nullptr,
+       *post_x = nullptr, *tmp = nullptr;
+};
+
+struct DeviceSolver {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int precision = SF_PRECISION_SINGLE_STORAGE;
+  bool storage_single = true, vector_single = false, flexible = false;
+  bool multigrid = false;
+  uint32_t n = 0;  // free dofs
+  DevBsr system;   // f64 3x3 system matrix
+  double *rhs = nullptr, *x = nullptr, *r = nullptr, *z = nullptr, *p = nullptr, *ap = nullptr;
+  float* z32 = nullptr;  // the cycle's f32 output when the cycle runs in f32
+  double* jacobi = nullptr;
+  double* partials = nullptr;   // kReduceBlocks * 4
+  PcgState* state = nullptr;
+  int* always_active = nullptr;  // a status word fixed at ST_ACTIVE for standalone cycles
+  std::vector<DevLevel> levels;
+  std::vector<void*> owned;  // every cudaMalloc of this solver
+  size_t bytes = 0;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t graph_exec = nullptr;
+  uint64_t launches_per_iteration = 0;
+};
+
+// ------------------------------------------------------------------- memory helpers
+sf_status dev_alloc(DeviceSolver& s, void** ptr, size_t bytes);
+void dev_free_all(DeviceSolver& s);
+sf_status cuda_check(cudaError_t e, const char* what);
+
+// ------------------------------------------------------------------- assembly (assembly.cu)
+struct AssemblyDevice {
+  double* nodes = nullptr;        // node_count x 3
+  uint32_t* tets = nullptr;       // tet_count x 10
+  double* ke = nullptr;           // 495 x tet_count upper-triangle element stiffness
+  double* point_material = nullptr;  // tet_count x points x 2 (E, nu) when a callback supplies it
+  double* positions = nullptr;    // tet_count x points x 3, integration point positions
+  uint32_t* map_starts = nullptr; // blocks + 1
+  uint32_t* map = nullptr;        // (element << 7) | (10 a + b), ascending element per block
+  uint32_t* cursor = nullptr;     // blocks: next map entry to add
+  unsigned long long* error = nullptr;  // (tet << 32) | (point << 8) | kind, min over faults
+  uint32_t tet_count = 0;
+  int quadrature = 0;
+  int points = 4;
+};
+
+enum { FAULT_NONE = 0, FAULT_INVERTED = 1, FAULT_MATERIAL = 2 };
+
+// Element stiffness of elements [e0, e1) into assembly.ke (bit-exact with the reference's
+// element_stiffness, crates/solidfem-elastic/src/element.rs:98-133).
+sf_status launch_element_stiffness(const AssemblyDevice& a, const MaterialSpec& m, uint32_t e0,
+                                   uint32_t e1, cudaStream_t stream);
+// Integration point positions of all elements (for a host material callback).
+sf_status launch_point_positions(const AssemblyDevice& a, cudaStream_t stream);
+// Adds the stiffness of elements below `end` to the block values, each block summing its
+// elements in ascending order (assembly.rs:87-130 adds them in element order).
+sf_status launch_gather(const AssemblyDevice& a, DevBsr& system, uint32_t end, cudaStream_t stream);
+
+// Device stress recovery (results.rs:470-539, patch.rs): fills point stresses, per-node worst
+// values and patch fits, then the nodal field.
+struct RecoveryDevice {
+  double* disp = nullptr;         // node_count x 3
+  double* point_stress = nullptr; // tet_count x points x 6
+  double* point_vm = nullptr;     // tet_count x points
+  double* point_pos = nullptr;    // tet_count x points x 3
+  double* point_mat = nullptr;    // tet_count x points x 2
+  double* node_candidate = nullptr;  // tet_count x 10 x 7: stress and von Mises at each node
+  uint32_t* vertex_offsets = nullptr;  // vertex_count + 1
+  uint32_t* vertex_incident = nullptr; // elements touching each vertex, ascending
+  uint32_t* node_offsets = nullptr;    // node_count + 1: (element, local node) incidence
+  uint32_t* node_incident = nullptr;   // (element << 4) | local node, ascending element
+  double* fits = nullptr;         // vertex_count x (4 + 24): centre, scale, coefficients
+  int* has_fit = nullptr;         // vertex_count
+  uint32_t* midside_element = nullptr;  // per midside node: first element and its edge slot
+  double* nodal_stress = nullptr; // node_count x 6
+  double* nodal_vm = nullptr;     // node_count
+};
+sf_status launch_recovery(const AssemblyDevice& a, const MaterialSpec& m, RecoveryDevice& r,
+                          uint32_t node_count, uint32_t vertex_count, cudaStream_t stream);
+
+// ------------------------------------------------------------------- solve (solve.cu)
+// Uploads the hierarchy in the study's precision and allocates every work vector.
+sf_status solver_upload_hierarchy(DeviceSolver& s, const std::vector<HostLevel>& levels,
+                                  uint64_t degree);
+sf_status solver_init_pcg(DeviceSolver& s, double tolerance, uint64_t max_iterations);
+// Enqueues one full iteration (pcg.rs:216-275) on s.stream.
+sf_status solver_enqueue_iteration(DeviceSolver& s);
+// Enqueues z = M r for the current r (reset_direction, pcg.rs:278-282) and rz.
+sf_status solver_enqueue_reset(DeviceSolver& s);
+// One standalone preconditioner application / system product (inspection entry points).
+sf_status solver_precondition(DeviceSolver& s, const double* d_in, double* d_out);
+sf_status solver_system_multiply(DeviceSolver& s, const double* d_in, double* d_out);
+sf_status solver_capture_graph(DeviceSolver& s);
+sf_status solver_read_state(DeviceSolver& s, PcgState* out);
+
+}  // namespace sf

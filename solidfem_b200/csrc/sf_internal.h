@@ -1,0 +1,120 @@
+// Internal host-side types of solidfem_b200: the mesh, the model, the multigrid setup's block
+// matrices and the study state. Device buffers and kernels are declared in device.h.
+#pragma once
+
+#include <array>
+#include <cstdint>
+#include <cstring>
+#include <functional>
+#include <string>
+#include <vector>
+
+#include "../../include/solidfem_b200.h"
+
+namespace sf {
+
+using std::array;
+using std::size_t;
+using std::vector;
+typedef array<double, 3> P3;
+
+static const uint32_t FIXED = 0xffffffffu;
+static const uint32_t NO_AGGREGATE = 0xffffffffu;
+
+// Local node indices of each face (crates/solidfem-mesh/src/boundary.rs:8-13) and the corner pair
+// of each edge midpoint (crates/solidfem-mesh/src/quadratic.rs:10).
+extern const int kFaceNodes[4][6];
+extern const int kEdgeCorners[6][2];
+
+// ----------------------------------------------------------------------------- errors
+// Records a failure for sf_last_error and returns its status.
+sf_status fail(sf_status status, const char* message);
+sf_error& error_slot();
+
+// ----------------------------------------------------------------------------- mesh
+struct Mesh {
+  vector<P3> nodes;
+  vector<array<uint32_t, 10>> tets;
+  vector<array<uint32_t, 4>> corners;
+  size_t vertex_count = 0;
+  vector<sf_boundary_face> faces;  // sorted by their sorted corners
+};
+
+sf_status build_box_mesh(const double origin[3], const double size[3], const uint64_t div[3],
+                         Mesh& out);
+sf_status build_linear_mesh(const double* positions, uint64_t n, const uint32_t* tets,
+                            uint64_t ntets, Mesh& out);
+vector<vector<uint32_t>> face_connected_bodies(const Mesh& mesh);
+
+// ----------------------------------------------------------------------------- model
+enum MaterialKind { MATERIAL_UNIFORM = 0, MATERIAL_SHELL_CORE = 1, MATERIAL_CALLBACK = 2 };
+
+struct MaterialSpec {
+  int kind = MATERIAL_UNIFORM;
+  sf_material uniform{0, 0};
+  sf_material shell{0, 0}, core{0, 0};
+  double lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
+  double depth = 0;
+  sf_material_field_fn callback = nullptr;
+  void* user = nullptr;
+};
+
+struct Model {
+  Mesh mesh;
+  MaterialSpec material;
+  int quadrature = SF_QUADRATURE_FOUR_POINT;
+  vector<uint32_t> fixed;  // as given; deduplicated when the builder starts
+  vector<std::pair<uint32_t, array<double, 3>>> forces;
+  vector<std::pair<sf_boundary_face, array<double, 3>>> tractions;
+  vector<std::pair<std::pair<uint32_t, uint32_t>, double>> prescribed;  // (node, axis) -> value
+};
+
+// ----------------------------------------------------------------------------- host block CSR
+// A block sparse matrix of dense rb x cb row-major blocks, f64 (setup works in f64).
+struct Bsr {
+  size_t rows = 0, rb = 0, cb = 0;
+  vector<uint32_t> starts;  // rows + 1
+  vector<uint32_t> cols;
+  vector<double> vals;
+  size_t blocks() const { return cols.size(); }
+  size_t block_len() const { return rb * cb; }
+  const double* block(size_t at) const { return vals.data() + at * rb * cb; }
+  double* block(size_t at) { return vals.data() + at * rb * cb; }
+};
+
+// One finished level of the hierarchy (f64 values as setup built them).
+struct HostLevel {
+  Bsr a;
+  vector<double> inverse_diagonal;
+  double lambda_min = 0, lambda_max = 0;
+  bool has_p = false;
+  Bsr p;
+  bool has_factor = false;
+  size_t factor_n = 0;
+  vector<double> coarse_inverse;  // the dense inverse of the coarsest level, row-major f64
+  vector<uint32_t> aggregates;
+};
+
+struct SetupOptions {
+  double reach = 3.0;
+  size_t coarse_dofs = 1500;
+  size_t max_levels = 12;
+  double range = 30.0;
+  int threads = 1;
+};
+
+// The multigrid setup (crates/solidfem-solve/src/multigrid/setup.rs) over the device-assembled
+// fine level. Resumable by phase and row cursor, like the reference's state machine.
+struct SetupMachine;
+SetupMachine* setup_create(Bsr&& fine, vector<double>&& near_null, vector<P3>&& positions,
+                           const SetupOptions& options);
+// Runs up to `budget` rows of work. Returns SF_OK and sets *finished, or a failure.
+sf_status setup_step(SetupMachine* machine, size_t budget, sf_cancel_fn cancel, void* user,
+                     bool* finished);
+vector<HostLevel> setup_take_levels(SetupMachine* machine);
+void setup_destroy(SetupMachine* machine);
+
+int default_threads();
+double now_seconds();
+
+}  // namespace sf

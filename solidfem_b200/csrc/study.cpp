@@ -1,0 +1,1189 @@
+// The study state machine and the C ABI: Model -> StudyBuilder -> StaticStudy
+// (crates/solidfem-elastic/src/study.rs), with the stiffness assembled on the device, the
+// multigrid hierarchy built by the host setup (setup.cpp) and uploaded, and the conjugate gradient
+// and V-cycle running on the device (solve.cu).
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#include "device.h"
+#include "sf_internal.h"
+
+using namespace sf;
+
+struct sf_mesh {
+  Mesh mesh;
+};
+
+struct sf_model {
+  Model model;
+};
+
+namespace {
+
+const double ON_BOUNDARY_EPS = 0;  // unused; faces are matched exactly
+
+// Constraint check (crates/solidfem-elastic/src/constraints.rs:40-135): each face-connected body
+// needs three non-collinear held nodes, a body held through a shared node counting as held.
+double distance3(const P3& a, const P3& b) {
+  double d[3] = {a[0] - b[0], a[1] - b[1], a[2] - b[2]};
+  return std::sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+}
+
+int remaining_freedom(const vector<P3>& pts, double size) {  // 0 held, 1 free, 2 point, 3 line
+  if (pts.empty()) return 1;
+  double limit = 1e-9 * size;
+  P3 first = pts[0], far = first;
+  double fd = 0.0;
+  for (auto& p : pts) {
+    double d = distance3(first, p);
+    if (d > fd) {
+      far = p;
+      fd = d;
+    }
+  }
+  if (fd <= limit) return 2;
+  double ax[3] = {(far[0] - first[0]) / fd, (far[1] - first[1]) / fd, (far[2] - first[2]) / fd};
+  for (auto& p : pts) {
+    double v[3] = {p[0] - first[0], p[1] - first[1], p[2] - first[2]};
+    double along = v[0] * ax[0] + v[1] * ax[1] + v[2] * ax[2];
+    double off[3] = {v[0] - along * ax[0], v[1] - along * ax[1], v[2] - along * ax[2]};
+    if (std::sqrt(off[0] * off[0] + off[1] * off[1] + off[2] * off[2]) > limit) return 0;
+  }
+  return 3;
+}
+
+sf_status check_constraints(const Mesh& m, const vector<char>& fixed) {
+  bool any = false;
+  for (char f : fixed) any = any || f;
+  if (!any) return fail(SF_NO_FIXED_NODES, "no node is fixed: the model is free to move");
+  auto bodies = face_connected_bodies(m);
+  vector<vector<uint32_t>> body_nodes(bodies.size());
+  vector<double> sizes(bodies.size());
+  for (size_t b = 0; b < bodies.size(); ++b) {
+    vector<uint32_t>& nodes = body_nodes[b];
+    for (uint32_t t : bodies[b])
+      for (uint32_t n : m.tets[t]) nodes.push_back(n);
+    std::sort(nodes.begin(), nodes.end());
+    nodes.erase(std::unique(nodes.begin(), nodes.end()), nodes.end());
+    P3 lo = {INFINITY, INFINITY, INFINITY}, hi = {-INFINITY, -INFINITY, -INFINITY};
+    for (uint32_t n : nodes)
+      for (int a = 0; a < 3; ++a) {
+        lo[a] = std::min(lo[a], m.nodes[n][a]);
+        hi[a] = std::max(hi[a], m.nodes[n][a]);
+      }
+    sizes[b] = distance3(lo, hi);
+  }
+  vector<char> held = fixed, anchored(bodies.size(), 0);
+  for (bool changed = true; changed;) {
+    changed = false;
+    for (size_t b = 0; b < bodies.size(); ++b) {
+      if (anchored[b]) continue;
+      vector<P3> pts;
+      for (uint32_t n : body_nodes[b])
+        if (held[n]) pts.push_back(m.nodes[n]);
+      if (remaining_freedom(pts, sizes[b]) == 0) {
+        anchored[b] = 1;
+        changed = true;
+        for (uint32_t n : body_nodes[b]) held[n] = 1;
+      }
+    }
+  }
+  for (size_t b = 0; b < bodies.size(); ++b)
+    if (!anchored[b]) {
+      size_t count = 0;
+      for (uint32_t n : body_nodes[b]) count += held[n] ? 1 : 0;
+      error_slot().tet = bodies[b][0];
+      error_slot().node = (uint32_t)count;
+      return fail(SF_BODY_NOT_HELD, "a body is not held by three non-collinear nodes");
+    }
+  return SF_OK;
+}
+
+// check_held_dofs with its pivoted rank (constraints.rs:162-256).
+sf_status check_held_dofs(const Mesh& m, const vector<char>& fixed,
+                          const vector<std::pair<std::pair<uint32_t, uint32_t>, double>>& prescribed) {
+  for (auto& body : face_connected_bodies(m)) {
+    vector<char> in_body(m.nodes.size(), 0);
+    vector<uint32_t> nodes;
+    for (uint32_t t : body)
+      for (uint32_t n : m.tets[t])
+        if (!in_body[n]) {
+          in_body[n] = 1;
+          nodes.push_back(n);
+        }
+    std::sort(nodes.begin(), nodes.end());
+    P3 lo = {INFINITY, INFINITY, INFINITY}, hi = {-INFINITY, -INFINITY, -INFINITY};
+    for (uint32_t n : nodes)
+      for (int a = 0; a < 3; ++a) {
+        lo[a] = std::min(lo[a], m.nodes[n][a]);
+        hi[a] = std::max(hi[a], m.nodes[n][a]);
+      }
+    double size = std::max(distance3(lo, hi), 2.2250738585072014e-308);
+    double c[3] = {0, 0, 0};
+    for (uint32_t n : nodes)
+      for (int a = 0; a < 3; ++a) c[a] += m.nodes[n][a];
+    for (int a = 0; a < 3; ++a) c[a] /= (double)nodes.size();
+    vector<array<double, 6>> rows;
+    auto add = [&](uint32_t node, uint32_t axis) {
+      const P3& p = m.nodes[node];
+      double x = (p[0] - c[0]) / size, y = (p[1] - c[1]) / size, z = (p[2] - c[2]) / size;
+      if (axis == 0) rows.push_back({1, 0, 0, 0, z, -y});
+      else if (axis == 1) rows.push_back({0, 1, 0, -z, 0, x});
+      else rows.push_back({0, 0, 1, y, -x, 0});
+    };
+    for (uint32_t n : nodes)
+      if (fixed[n])
+        for (uint32_t a = 0; a < 3; ++a) add(n, a);
+    for (auto& pr : prescribed) {
+      uint32_t node = pr.first.first, axis = pr.first.second;
+      if (node < m.nodes.size() && in_body[node] && axis < 3) add(node, axis);
+    }
+    size_t rank = 0;
+    for (int col = 0; col < 6; ++col) {
+      if (rank >= rows.size()) break;
+      size_t best = rank;
+      for (size_t r = rank + 1; r < rows.size(); ++r) {
+        double a = std::fabs(rows[r][col]), b = std::fabs(rows[best][col]);
+        if (a > b) best = r;  // ties keep the lower index, as max_by with then(b.cmp(a))
+      }
+      if (std::fabs(rows[best][col]) <= 1e-9) continue;
+      std::swap(rows[rank], rows[best]);
+      auto pivot = rows[rank];
+      for (size_t r = rank + 1; r < rows.size(); ++r) {
+        double f = rows[r][col] / pivot[col];
+        if (f != 0.0)
+          for (int k = col; k < 6; ++k) rows[r][k] -= f * pivot[k];
+      }
+      ++rank;
+    }
+    if (rank < 6) {
+      error_slot().tet = body[0];
+      error_slot().rank = rank;
+      return fail(SF_DOFS_DO_NOT_HOLD, "the held components do not remove every rigid motion of a body");
+    }
+  }
+  return SF_OK;
+}
+
+// Consistent traction load (crates/solidfem-elastic/src/loads.rs:10-41), 6-point triangle rule.
+void add_traction(const Mesh& m, const sf_boundary_face& f, const double t[3], vector<double>& load) {
+  static const double TA = 0.091576213509771, TB = 0.445948490915965;
+  static const double WA = 0.109951743655322, WB = 0.223381589678011;
+  const double pts[6][3] = {{TA, TA, WA}, {1.0 - 2.0 * TA, TA, WA}, {TA, 1.0 - 2.0 * TA, WA},
+                            {TB, TB, WB}, {1.0 - 2.0 * TB, TB, WB}, {TB, 1.0 - 2.0 * TB, WB}};
+  P3 pos[6];
+  for (int i = 0; i < 6; ++i) pos[i] = m.nodes[f.nodes[i]];
+  for (int q = 0; q < 6; ++q) {
+    double r = pts[q][0], s = pts[q][1], w = pts[q][2];
+    double l1 = 1.0 - r - s;
+    double v[6] = {l1 * (2.0 * l1 - 1.0), r * (2.0 * r - 1.0), s * (2.0 * s - 1.0), 4.0 * l1 * r, 4.0 * r * s, 4.0 * s * l1};
+    double dr[6] = {-(4.0 * l1 - 1.0), 4.0 * r - 1.0, 0.0, 4.0 * (l1 - r), 4.0 * s, -4.0 * s};
+    double ds[6] = {-(4.0 * l1 - 1.0), 0.0, 4.0 * s - 1.0, -4.0 * r, 4.0 * r, 4.0 * (l1 - s)};
+    double tr[3] = {0, 0, 0}, ts[3] = {0, 0, 0};
+    for (int n = 0; n < 6; ++n)
+      for (int a = 0; a < 3; ++a) {
+        tr[a] += dr[n] * pos[n][a];
+        ts[a] += ds[n] * pos[n][a];
+      }
+    double nm[3] = {tr[1] * ts[2] - tr[2] * ts[1], tr[2] * ts[0] - tr[0] * ts[2], tr[0] * ts[1] - tr[1] * ts[0]};
+    double length = std::sqrt(nm[0] * nm[0] + nm[1] * nm[1] + nm[2] * nm[2]);
+    double measure = 0.5 * length * w;
+    for (int n = 0; n < 6; ++n)
+      for (int a = 0; a < 3; ++a) load[3 * (size_t)f.nodes[n] + a] += t[a] * v[n] * measure;
+  }
+}
+
+// Rigid-body modes about the free nodes' centroid (crates/solidfem-elastic/src/rigid_modes.rs:36-83).
+vector<double> rigid_modes(const vector<P3>& nodes, const vector<uint32_t>& free, size_t free_count) {
+  double c[3] = {0, 0, 0};
+  for (size_t n = 0; n < nodes.size(); ++n)
+    if (free[n] != FIXED)
+      for (int a = 0; a < 3; ++a) c[a] += nodes[n][a];
+  double div = (double)std::max<size_t>(free_count, 1);
+  for (int a = 0; a < 3; ++a) c[a] /= div;
+  double reach = 0.0;
+  for (size_t n = 0; n < nodes.size(); ++n)
+    if (free[n] != FIXED)
+      for (int a = 0; a < 3; ++a) reach = std::max(reach, std::fabs(nodes[n][a] - c[a]));
+  double scale = reach > 0.0 ? 1.0 / reach : 1.0;
+  vector<double> modes(18 * free_count, 0.0);
+  for (size_t n = 0; n < nodes.size(); ++n) {
+    if (free[n] == FIXED) continue;
+    double* m = modes.data() + 18 * (size_t)free[n];
+    double x = (nodes[n][0] - c[0]) * scale, y = (nodes[n][1] - c[1]) * scale, z = (nodes[n][2] - c[2]) * scale;
+    double rows[18] = {1, 0, 0, 0, z, -y, 0, 1, 0, -z, 0, x, 0, 0, 1, y, -x, 0};
+    std::memcpy(m, rows, sizeof(rows));
+  }
+  return modes;
+}
+
+struct HostPattern {
+  vector<uint32_t> starts, cols;           // block rows over free nodes
+  vector<uint32_t> map_starts, map;        // per block: (element << 7) | (10 a + b), ascending
+};
+
+// The free-node block pattern (assembly.rs:55-81, csr.rs:19-71) and, for each block, the
+// elements that add to it in ascending order, built row-parallel from node-to-element incidence.
+void build_pattern(const Mesh& m, const vector<uint32_t>& free, size_t free_count, int threads, HostPattern& hp) {
+  size_t nn = m.nodes.size(), ne = m.tets.size();
+  vector<uint32_t> inc_start(nn + 1, 0);
+  for (auto& t : m.tets)
+    for (uint32_t n : t) inc_start[n + 1] += 1;
+  for (size_t i = 0; i < nn; ++i) inc_start[i + 1] += inc_start[i];
+  vector<uint32_t> fill(inc_start.begin(), inc_start.end() - 1), inc(inc_start[nn]);
+  for (size_t e = 0; e < ne; ++e)
+    for (uint32_t n : m.tets[e]) inc[fill[n]++] = (uint32_t)e;
+  vector<uint32_t> row_node(free_count);
+  for (size_t n = 0; n < nn; ++n)
+    if (free[n] != FIXED) row_node[free[n]] = (uint32_t)n;
+  vector<uint32_t> counts(free_count, 0), map_counts(free_count, 0);
+#ifdef _OPENMP
+#pragma omp parallel for schedule(dynamic, 1024) num_threads(threads)
+#endif
+  for (long long r = 0; r < (long long)free_count; ++r) {
+    uint32_t node = row_node[r];
+    vector<uint32_t> cols;
+    uint32_t entries = 0;
+    for (uint32_t k = inc_start[node]; k < inc_start[node + 1]; ++k)
+      for (uint32_t n : m.tets[inc[k]])
+        if (free[n] != FIXED) {
+          cols.push_back(free[n]);
+          ++entries;
+        }
+    std::sort(cols.begin(), cols.end());
+    counts[r] = (uint32_t)(std::unique(cols.begin(), cols.end()) - cols.begin());
+    map_counts[r] = entries;
+  }
+  hp.starts.assign(free_count + 1, 0);
+  vector<uint64_t> map_row(free_count + 1, 0);
+  for (size_t r = 0; r < free_count; ++r) {
+    hp.starts[r + 1] = hp.starts[r] + counts[r];
+    map_row[r + 1] = map_row[r] + map_counts[r];
+  }
+  hp.cols.assign(hp.starts[free_count], 0);
+  hp.map_starts.assign(hp.starts[free_count] + 1, 0);
+  hp.map.assign(map_row[free_count], 0);
+#ifdef _OPENMP
+#pragma omp parallel for schedule(dynamic, 1024) num_threads(threads)
+#endif
+  for (long long r = 0; r < (long long)free_count; ++r) {
+    uint32_t node = row_node[r];
+    vector<uint32_t> cols;
+    for (uint32_t k = inc_start[node]; k < inc_start[node + 1]; ++k)
+      for (uint32_t n : m.tets[inc[k]])
+        if (free[n] != FIXED) cols.push_back(free[n]);
+    std::sort(cols.begin(), cols.end());
+    cols.erase(std::unique(cols.begin(), cols.end()), cols.end());
+    uint32_t b0 = hp.starts[r];
+    std::copy(cols.begin(), cols.end(), hp.cols.begin() + b0);
+    // Per block of this row, its entry count, then the entries in element order.
+    vector<uint32_t> per(cols.size(), 0);
+    for (uint32_t k = inc_start[node]; k < inc_start[node + 1]; ++k)
+      for (uint32_t n : m.tets[inc[k]])
+        if (free[n] != FIXED) per[std::lower_bound(cols.begin(), cols.end(), free[n]) - cols.begin()] += 1;
+    uint64_t base = map_row[r];
+    vector<uint64_t> at(cols.size());
+    for (size_t j = 0; j < cols.size(); ++j) {
+      at[j] = base;
+      hp.map_starts[b0 + j] = (uint32_t)base;
+      base += per[j];
+    }
+    for (uint32_t k = inc_start[node]; k < inc_start[node + 1]; ++k) {
+      uint32_t e = inc[k];
+      const auto& t = m.tets[e];
+      int a = 0;
+      while (t[a] != node) ++a;
+      for (int b = 0; b < 10; ++b) {
+        uint32_t fc = free[t[b]];
+        if (fc == FIXED) continue;
+        size_t j = std::lower_bound(cols.begin(), cols.end(), fc) - cols.begin();
+        hp.map[at[j]++] = (e << 7) | (uint32_t)(10 * a + b);
+      }
+    }
+  }
+  hp.map_starts[hp.starts[free_count]] = (uint32_t)map_row[free_count];
+}
+
+}  // namespace
+
+struct sf_builder {
+  Model model;
+  sf_study_options options;
+  vector<uint32_t> free;
+  size_t free_count = 0;
+  vector<double> rhs;
+  vector<std::pair<size_t, double>> prescribed;  // (free dof, value), sorted
+  size_t next = 0;
+  bool prescribed_applied = false;
+  HostPattern pattern;
+  AssemblyDevice asmdev;
+  DeviceSolver solver;
+  SetupMachine* setup = nullptr;
+  bool setup_finished = false;
+  double assembly_seconds = 0, preconditioner_seconds = 0;
+  float assembly_ms = 0, setup_ms = 0;
+  sf_status failure = SF_OK;
+  int threads = 1;
+  ~sf_builder() {
+    if (setup) setup_destroy(setup);
+  }
+};
+
+struct sf_study {
+  Model model;
+  sf_study_options options;
+  vector<uint32_t> free;
+  size_t free_count = 0;
+  vector<double> rhs;
+  vector<std::pair<size_t, double>> prescribed;
+  HostPattern pattern;
+  AssemblyDevice asmdev;
+  DeviceSolver solver;
+  vector<HostLevel> levels;
+  sf_report report;
+  int status = ST_ACTIVE;
+  bool cancelled = false;
+  PcgState last;
+  double step_ms = 0;
+  PcgState* pinned = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  ~sf_study() {
+    if (pinned) cudaFreeHost(pinned);
+    if (ev0) cudaEventDestroy(ev0);
+    if (ev1) cudaEventDestroy(ev1);
+    dev_free_all(solver);
+    if (solver.stream) cudaStreamDestroy(solver.stream);
+  }
+};
+
+static void release_builder_device(sf_builder* b) {
+  dev_free_all(b->solver);
+  if (b->solver.stream) cudaStreamDestroy(b->solver.stream);
+  b->solver.stream = nullptr;
+}
+
+extern "C" {
+
+sf_status sf_last_error(sf_error* out) {
+  if (out) *out = error_slot();
+  return (sf_status)error_slot().status;
+}
+
+int32_t sf_abi_version(void) { return SF_ABI_VERSION; }
+
+const char* sf_status_message(sf_status s) {
+  switch (s) {
+    case SF_OK: return "ok";
+    case SF_MESH_EMPTY: return "the mesh has no tetrahedra";
+    case SF_MESH_NON_FINITE_POSITION: return "a node position is not finite";
+    case SF_MESH_NODE_OUT_OF_RANGE: return "a tetrahedron names a node that does not exist";
+    case SF_MESH_DEGENERATE_TET: return "a tetrahedron has no positive volume";
+    case SF_MESH_FLAT_TET: return "a tetrahedron is flat to rounding";
+    case SF_MESH_UNUSED_NODE: return "a node belongs to no tetrahedron";
+    case SF_MESH_NON_MANIFOLD_FACE: return "a face is shared by more than two tetrahedra";
+    case SF_MESH_INVALID_BOX: return "the box needs positive lengths and divisions";
+    case SF_NO_FIXED_NODES: return "no node is fixed";
+    case SF_BODY_NOT_HELD: return "a body is not held";
+    case SF_NODE_OUT_OF_RANGE: return "a node index is out of range";
+    case SF_NON_FINITE_LOAD: return "a load is not finite";
+    case SF_FACE_NOT_ON_BOUNDARY: return "a traction face is not on the boundary";
+    case SF_NO_EFFECTIVE_LOAD: return "the model has no effective load";
+    case SF_ELEMENT_INVERTED_JACOBIAN: return "an element has an inverted integration point";
+    case SF_ELEMENT_INVALID_MATERIAL: return "an integration point has an invalid material";
+    case SF_JACOBI_DIAGONAL: return "a diagonal entry is not positive";
+    case SF_CANCELLED: return "cancelled";
+    case SF_NOT_FINISHED: return "not finished";
+    case SF_AXIS_OUT_OF_RANGE: return "an axis is out of range";
+    case SF_PRESCRIBED_ON_FIXED_NODE: return "a prescribed component is on a fixed node";
+    case SF_DOFS_DO_NOT_HOLD: return "the held components do not hold a body";
+    case SF_MG_BLOCK_STRUCTURE: return "the matrix does not group into 3x3 blocks";
+    case SF_MG_NEAR_NULL_LENGTH: return "the near-null space has the wrong length";
+    case SF_MG_NOT_POSITIVE_DEFINITE: return "a multigrid block is not positive definite";
+    case SF_MG_POSITION_LENGTH: return "the block positions have the wrong length";
+    case SF_MG_COARSEST_NOT_FACTORED: return "the coarsest level is not factored";
+    case SF_MG_COARSE_LENGTH: return "the coarse vector has the wrong length";
+    case SF_PCG_NOT_POSITIVE_DEFINITE: return "the system is not positive definite";
+    case SF_PCG_NOT_CONVERGED: return "the solver did not converge";
+    case SF_INVALID_ARGUMENT: return "invalid argument";
+    case SF_CUDA_ERROR: return "CUDA error";
+    case SF_DEVICE_MEMORY_BUDGET: return "the device memory budget is exceeded";
+    case SF_NO_DEVICE: return "no CUDA device";
+    case SF_DEVICE_WAIT_TIMEOUT: return "a device wait timed out";
+  }
+  return "unknown status";
+}
+
+// ------------------------------------------------------------------------------ mesh
+sf_status sf_box_tet_mesh(const double origin[3], const double size[3], const uint64_t divisions[3], sf_mesh** out) {
+  if (!origin || !size || !divisions || !out) return fail(SF_INVALID_ARGUMENT, "null argument");
+  std::unique_ptr<sf_mesh> m(new sf_mesh);
+  if (sf_status s = build_box_mesh(origin, size, divisions, m->mesh)) return s;
+  *out = m.release();
+  return SF_OK;
+}
+
+sf_status sf_mesh_from_linear(const double* positions, uint64_t n, const uint32_t* tets, uint64_t ntets, sf_mesh** out) {
+  if ((!positions && n) || (!tets && ntets) || !out) return fail(SF_INVALID_ARGUMENT, "null argument");
+  std::unique_ptr<sf_mesh> m(new sf_mesh);
+  if (sf_status s = build_linear_mesh(positions, n, tets, ntets, m->mesh)) return s;
+  *out = m.release();
+  return SF_OK;
+}
+
+void sf_mesh_destroy(sf_mesh* m) { delete m; }
+uint64_t sf_mesh_node_count(const sf_mesh* m) { return m ? m->mesh.nodes.size() : 0; }
+uint64_t sf_mesh_tet_count(const sf_mesh* m) { return m ? m->mesh.tets.size() : 0; }
+uint64_t sf_mesh_vertex_count(const sf_mesh* m) { return m ? m->mesh.vertex_count : 0; }
+uint64_t sf_mesh_boundary_face_count(const sf_mesh* m) { return m ? m->mesh.faces.size() : 0; }
+
+sf_status sf_mesh_nodes(const sf_mesh* m, double* out) {
+  if (!m || !out) return fail(SF_INVALID_ARGUMENT, "null argument");
+  std::memcpy(out, m->mesh.nodes.data(), m->mesh.nodes.size() * 24);
+  return SF_OK;
+}
+
+sf_status sf_mesh_tets(const sf_mesh* m, uint32_t* out) {
+  if (!m || !out) return fail(SF_INVALID_ARGUMENT, "null argument");
+  std::memcpy(out, m->mesh.tets.data(), m->mesh.tets.size() * 40);
+  return SF_OK;
+}
+
+sf_status sf_mesh_boundary_faces(const sf_mesh* m, sf_boundary_face* out) {
+  if (!m || !out) return fail(SF_INVALID_ARGUMENT, "null argument");
+  std::memcpy(out, m->mesh.faces.data(), m->mesh.faces.size() * sizeof(sf_boundary_face));
+  return SF_OK;
+}
+
+// ------------------------------------------------------------------------------ model
+sf_status sf_model_create(const sf_mesh* mesh, sf_material material, sf_model** out) {
+  if (!mesh || !out) return fail(SF_INVALID_ARGUMENT, "null argument");
+  sf_model* m = new sf_model;
+  m->model.mesh = mesh->mesh;
+  m->model.material.kind = MATERIAL_UNIFORM;
+  m->model.material.uniform = material;
+  *out = m;
+  return SF_OK;
+}
+
+void sf_model_destroy(sf_model* m) { delete m; }
+
+sf_status sf_model_set_material_field(sf_model* m, sf_material_field_fn field, void* user) {
+  if (!m || !field) return fail(SF_INVALID_ARGUMENT, "null argument");
+  m->model.material.kind = MATERIAL_CALLBACK;
+  m->model.material.callback = field;
+  m->model.material.user = user;
+  return SF_OK;
+}
+
+sf_status sf_model_set_shell_core(sf_model* m, sf_material shell, sf_material core, const double lo[3],
+                                  const double hi[3], double depth) {
+  if (!m || !lo || !hi) return fail(SF_INVALID_ARGUMENT, "null argument");
+  MaterialSpec& s = m->model.material;
+  s.kind = MATERIAL_SHELL_CORE;
+  s.shell = shell;
+  s.core = core;
+  for (int a = 0; a < 3; ++a) {
+    s.lo[a] = lo[a];
+    s.hi[a] = hi[a];
+  }
+  s.depth = depth;
+  return SF_OK;
+}
+
+sf_status sf_model_set_quadrature(sf_model* m, int32_t rule) {
+  if (!m || (rule != SF_QUADRATURE_FOUR_POINT && rule != SF_QUADRATURE_FOURTEEN_POINT))
+    return fail(SF_INVALID_ARGUMENT, "unknown quadrature rule");
+  m->model.quadrature = rule;
+  return SF_OK;
+}
+
+sf_status sf_model_fix_node(sf_model* m, uint32_t node) {
+  if (!m) return fail(SF_INVALID_ARGUMENT, "null argument");
+  m->model.fixed.push_back(node);
+  return SF_OK;
+}
+
+sf_status sf_model_fix_nodes(sf_model* m, const uint32_t* nodes, uint64_t count) {
+  if (!m || (!nodes && count)) return fail(SF_INVALID_ARGUMENT, "null argument");
+  m->model.fixed.insert(m->model.fixed.end(), nodes, nodes + count);
+  return SF_OK;
+}
+
+sf_status sf_model_add_nodal_force(sf_model* m, uint32_t node, const double force[3]) {
+  if (!m || !force) return fail(SF_INVALID_ARGUMENT, "null argument");
+  m->model.forces.push_back({node, {force[0], force[1], force[2]}});
+  return SF_OK;
+}
+
+sf_status sf_model_add_traction(sf_model* m, const sf_boundary_face* face, const double traction[3]) {
+  if (!m || !face || !traction) return fail(SF_INVALID_ARGUMENT, "null argument");
+  m->model.tractions.push_back({*face, {traction[0], traction[1], traction[2]}});
+  return SF_OK;
+}
+
+sf_status sf_model_add_tractions(sf_model* m, const sf_boundary_face* faces, const double* tractions, uint64_t count) {
+  if (!m || ((!faces || !tractions) && count)) return fail(SF_INVALID_ARGUMENT, "null argument");
+  for (uint64_t i = 0; i < count; ++i)
+    m->model.tractions.push_back({faces[i], {tractions[3 * i], tractions[3 * i + 1], tractions[3 * i + 2]}});
+  return SF_OK;
+}
+
+sf_status sf_model_prescribe_displacement(sf_model* m, uint32_t node, uint32_t axis, double value) {
+  if (!m) return fail(SF_INVALID_ARGUMENT, "null argument");
+  for (auto& p : m->model.prescribed)
+    if (p.first.first == node && p.first.second == axis) {
+      p.second = value;  // the last call for a node and axis wins (study.rs:90-98)
+      return SF_OK;
+    }
+  m->model.prescribed.push_back({{node, axis}, value});
+  return SF_OK;
+}
+
+void sf_study_options_default(sf_study_options* o) {
+  if (!o) return;
+  std::memset(o, 0, sizeof(*o));
+  o->tolerance = 1e-9;
+  o->max_iterations = 0;
+  o->preconditioner = SF_PRECONDITIONER_JACOBI;
+  o->neighbour_reach = 3.0;
+  o->coarse_dofs = 1500;
+  o->max_levels = 12;
+  o->smoother_degree = 3;
+  o->smoother_range = 30.0;
+  o->precision = SF_PRECISION_SINGLE_STORAGE;
+  o->threads = 0;
+  o->device = 0;
+  o->use_graphs = 1;
+  o->device_memory_budget = 0;
+}
+
+// ------------------------------------------------------------------------------ builder
+sf_status sf_builder_create(sf_model* model, const sf_study_options* options, sf_builder** out) {
+  std::unique_ptr<sf_model> owned(model);
+  if (!model || !options || !out) return fail(SF_INVALID_ARGUMENT, "null argument");
+  std::unique_ptr<sf_builder> b(new sf_builder);
+  b->model = std::move(model->model);
+  b->options = *options;
+  b->threads = options->threads ? (int)std::min<uint64_t>(options->threads, 64) : default_threads();
+  Model& md = b->model;
+  const Mesh& mesh = md.mesh;
+  size_t nn = mesh.nodes.size();
+  vector<char> is_fixed(nn, 0);
+  for (uint32_t n : md.fixed) {
+    if (n >= nn) {
+      error_slot().node = n;
+      return fail(SF_NODE_OUT_OF_RANGE, "a fixed node does not exist");
+    }
+    is_fixed[n] = 1;
+  }
+  std::sort(md.prescribed.begin(), md.prescribed.end());
+  if (md.prescribed.empty()) {
+    if (sf_status s = check_constraints(mesh, is_fixed)) return s;
+  } else {
+    if (sf_status s = check_held_dofs(mesh, is_fixed, md.prescribed)) return s;
+  }
+  // build_load, study.rs:696-735
+  vector<double> load(3 * nn, 0.0);
+  for (auto& f : md.forces) {
+    if (f.first >= nn) {
+      error_slot().node = f.first;
+      return fail(SF_NODE_OUT_OF_RANGE, "a loaded node does not exist");
+    }
+    for (double c : f.second)
+      if (!std::isfinite(c)) return fail(SF_NON_FINITE_LOAD, "a nodal force is not finite");
+    for (int a = 0; a < 3; ++a) load[3 * (size_t)f.first + a] += f.second[a];
+  }
+  if (!md.tractions.empty()) {
+    auto key = [](const sf_boundary_face& f) {
+      std::array<uint32_t, 8> k;
+      k[0] = f.tet;
+      k[1] = f.face;
+      for (int i = 0; i < 6; ++i) k[2 + i] = f.nodes[i];
+      return k;
+    };
+    vector<std::array<uint32_t, 8>> boundary;
+    boundary.reserve(mesh.faces.size());
+    for (auto& f : mesh.faces) boundary.push_back(key(f));
+    std::sort(boundary.begin(), boundary.end());
+    for (auto& tr : md.tractions) {
+      if (!std::binary_search(boundary.begin(), boundary.end(), key(tr.first))) {
+        error_slot().tet = tr.first.tet;
+        error_slot().face = tr.first.face;
+        return fail(SF_FACE_NOT_ON_BOUNDARY, "a traction face is not on the mesh boundary");
+      }
+      for (double c : tr.second)
+        if (!std::isfinite(c)) return fail(SF_NON_FINITE_LOAD, "a traction is not finite");
+      add_traction(mesh, tr.first, tr.second.data(), load);
+    }
+  }
+  b->free.assign(nn, FIXED);
+  for (size_t n = 0; n < nn; ++n)
+    if (!is_fixed[n]) b->free[n] = (uint32_t)b->free_count++;
+  b->rhs.reserve(3 * b->free_count);
+  for (size_t n = 0; n < nn; ++n)
+    if (b->free[n] != FIXED)
+      for (int a = 0; a < 3; ++a) b->rhs.push_back(load[3 * n + a]);
+  for (auto& p : md.prescribed) {
+    uint32_t node = p.first.first, axis = p.first.second;
+    if (axis > 2) {
+      error_slot().axis = axis;
+      return fail(SF_AXIS_OUT_OF_RANGE, "an axis other than 0, 1 or 2");
+    }
+    if (!std::isfinite(p.second)) return fail(SF_NON_FINITE_LOAD, "a prescribed value is not finite");
+    if (node >= nn) {
+      error_slot().node = node;
+      return fail(SF_NODE_OUT_OF_RANGE, "a prescribed node does not exist");
+    }
+    if (b->free[node] == FIXED) {
+      error_slot().node = node;
+      return fail(SF_PRESCRIBED_ON_FIXED_NODE, "a prescribed component is on a fixed node");
+    }
+    b->prescribed.push_back({3 * (size_t)b->free[node] + axis, p.second});
+  }
+  std::sort(b->prescribed.begin(), b->prescribed.end());
+  bool all_zero = true;
+  for (double v : b->rhs) all_zero = all_zero && v == 0.0;
+  for (auto& p : b->prescribed) all_zero = all_zero && p.second == 0.0;
+  if (all_zero) return fail(SF_NO_EFFECTIVE_LOAD, "the model has no effective load");
+  if (!b->prescribed.empty()) return fail(SF_INVALID_ARGUMENT, "prescribed displacements are not supported on the device path yet");
+  double t0 = now_seconds();
+  build_pattern(mesh, b->free, b->free_count, b->threads, b->pattern);
+  // Device set-up: mesh, element stiffness buffer, pattern and assembly map, system matrix.
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(SF_NO_DEVICE, "no CUDA device is visible");
+  if (b->options.device < 0 || b->options.device >= ndev) return fail(SF_INVALID_ARGUMENT, "no such CUDA device");
+  cudaSetDevice(b->options.device);
+  DeviceSolver& s = b->solver;
+  s.device = b->options.device;
+  if (sf_status e = cuda_check(cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking), "stream")) return e;
+  AssemblyDevice& a = b->asmdev;
+  a.tet_count = (uint32_t)mesh.tets.size();
+  a.quadrature = md.quadrature;
+  a.points = md.quadrature == SF_QUADRATURE_FOURTEEN_POINT ? 14 : 4;
+  size_t blocks = b->pattern.cols.size();
+  size_t budget = b->options.device_memory_budget;
+  size_t need = nn * 24 + mesh.tets.size() * 40 + mesh.tets.size() * 495 * 8 + blocks * (4 + 72 + 8) +
+                b->pattern.map.size() * 4;
+  if (budget && need > budget) return fail(SF_DEVICE_MEMORY_BUDGET, "the assembly does not fit the device memory budget");
+  sf_status e = SF_OK;
+  if (!e) e = dev_alloc(s, (void**)&a.nodes, nn * 24);
+  if (!e) e = dev_alloc(s, (void**)&a.tets, mesh.tets.size() * 40);
+  if (!e) e = dev_alloc(s, (void**)&a.ke, mesh.tets.size() * 495 * 8);
+  if (!e) e = dev_alloc(s, (void**)&a.map_starts, (blocks + 1) * 4);
+  if (!e) e = dev_alloc(s, (void**)&a.map, std::max<size_t>(1, b->pattern.map.size()) * 4);
+  if (!e) e = dev_alloc(s, (void**)&a.cursor, std::max<size_t>(1, blocks) * 4);
+  if (!e) e = dev_alloc(s, (void**)&a.error, 8);
+  s.system.rows = (uint32_t)b->free_count;
+  s.system.rb = s.system.cb = 3;
+  s.system.blocks = blocks;
+  if (!e) e = dev_alloc(s, (void**)&s.system.starts, (b->free_count + 1) * 4);
+  if (!e) e = dev_alloc(s, (void**)&s.system.cols, std::max<size_t>(1, blocks) * 4);
+  if (!e) e = dev_alloc(s, &s.system.vals, std::max<size_t>(1, blocks) * 72);
+  if (e) {
+    release_builder_device(b.get());
+    return e;
+  }
+  cudaMemcpyAsync(a.nodes, mesh.nodes.data(), nn * 24, cudaMemcpyHostToDevice, s.stream);
+  cudaMemcpyAsync(a.tets, mesh.tets.data(), mesh.tets.size() * 40, cudaMemcpyHostToDevice, s.stream);
+  cudaMemcpyAsync(a.map_starts, b->pattern.map_starts.data(), (blocks + 1) * 4, cudaMemcpyHostToDevice, s.stream);
+  if (!b->pattern.map.empty())
+    cudaMemcpyAsync(a.map, b->pattern.map.data(), b->pattern.map.size() * 4, cudaMemcpyHostToDevice, s.stream);
+  cudaMemcpyAsync(a.cursor, b->pattern.map_starts.data(), blocks * 4, cudaMemcpyHostToDevice, s.stream);
+  unsigned long long none = ~0ull;
+  cudaMemcpyAsync(a.error, &none, 8, cudaMemcpyHostToDevice, s.stream);
+  cudaMemcpyAsync(s.system.starts, b->pattern.starts.data(), (b->free_count + 1) * 4, cudaMemcpyHostToDevice, s.stream);
+  cudaMemcpyAsync(s.system.cols, b->pattern.cols.data(), blocks * 4, cudaMemcpyHostToDevice, s.stream);
+  // A host material callback: integration point positions from the device, the field on the
+  // host, (E, nu) per point back to the device.
+  if (md.material.kind == MATERIAL_CALLBACK) {
+    size_t pts = mesh.tets.size() * a.points;
+    e = dev_alloc(s, (void**)&a.positions, pts * 24);
+    if (!e) e = dev_alloc(s, (void**)&a.point_material, pts * 16);
+    if (!e) e = launch_point_positions(a, s.stream);
+    if (e) {
+      release_builder_device(b.get());
+      return e;
+    }
+    vector<double> pos(pts * 3);
+    cudaMemcpyAsync(pos.data(), a.positions, pts * 24, cudaMemcpyDeviceToHost, s.stream);
+    cudaStreamSynchronize(s.stream);
+    vector<sf_material> mats(pts);
+    md.material.callback(md.material.user, pos.data(), pts, mats.data());
+    vector<double> em(pts * 2);
+    for (size_t i = 0; i < pts; ++i) {
+      em[2 * i] = mats[i].youngs_modulus;
+      em[2 * i + 1] = mats[i].poisson_ratio;
+    }
+    cudaMemcpyAsync(a.point_material, em.data(), pts * 16, cudaMemcpyHostToDevice, s.stream);
+  }
+  e = cuda_check(cudaStreamSynchronize(s.stream), "assembly set-up");
+  if (e) {
+    release_builder_device(b.get());
+    return e;
+  }
+  b->assembly_seconds = now_seconds() - t0;
+  *out = b.release();
+  return SF_OK;
+}
+
+void sf_builder_destroy(sf_builder* b) {
+  if (!b) return;
+  release_builder_device(b);
+  delete b;
+}
+
+static sf_status builder_assemble(sf_builder* b, uint64_t max_elements, sf_cancel_fn cancel, void* user) {
+  size_t total = b->model.mesh.tets.size();
+  if (b->next >= total) return SF_OK;
+  if (cancel && cancel(user)) {
+    b->failure = SF_CANCELLED;
+    return fail(SF_CANCELLED, "assembly was cancelled");
+  }
+  size_t end = (size_t)std::min<uint64_t>(total, b->next + std::max<uint64_t>(max_elements, 1));
+  DeviceSolver& s = b->solver;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  cudaEventRecord(e0, s.stream);
+  sf_status st = launch_element_stiffness(b->asmdev, b->model.material, (uint32_t)b->next, (uint32_t)end, s.stream);
+  if (!st) st = launch_gather(b->asmdev, s.system, (uint32_t)end, s.stream);
+  cudaEventRecord(e1, s.stream);
+  if (!st) st = cuda_check(cudaStreamSynchronize(s.stream), "assembly");
+  float ms = 0;
+  cudaEventElapsedTime(&ms, e0, e1);
+  b->assembly_ms += ms;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (st) return st;
+  unsigned long long err = 0;
+  cudaMemcpy(&err, b->asmdev.error, 8, cudaMemcpyDeviceToHost);
+  if (err != ~0ull) {
+    error_slot().tet = (uint32_t)(err >> 32);
+    error_slot().point = (uint32_t)((err >> 8) & 0xff);
+    b->failure = (err & 0xff) == FAULT_INVERTED ? SF_ELEMENT_INVERTED_JACOBIAN : SF_ELEMENT_INVALID_MATERIAL;
+    return fail(b->failure, (err & 0xff) == FAULT_INVERTED ? "an element's Jacobian is inverted at an integration point"
+                                                           : "the material at an integration point is not a stable solid");
+  }
+  b->next = end;
+  return SF_OK;
+}
+
+static sf_status builder_setup(sf_builder* b, uint64_t budget, sf_cancel_fn cancel, void* user) {
+  if (b->setup_finished) return SF_OK;
+  double t0 = now_seconds();
+  if (!b->setup) {
+    // The fine level as setup reads it: the device-assembled f64 blocks.
+    DeviceSolver& s = b->solver;
+    Bsr fine;
+    fine.rows = b->free_count;
+    fine.rb = fine.cb = 3;
+    fine.starts = b->pattern.starts;
+    fine.cols = b->pattern.cols;
+    fine.vals.resize(b->pattern.cols.size() * 9);
+    cudaMemcpyAsync(fine.vals.data(), s.system.vals, fine.vals.size() * 8, cudaMemcpyDeviceToHost, s.stream);
+    if (sf_status e = cuda_check(cudaStreamSynchronize(s.stream), "download fine level")) return e;
+    vector<double> modes = rigid_modes(b->model.mesh.nodes, b->free, b->free_count);
+    vector<P3> positions;
+    positions.reserve(b->free_count);
+    for (size_t n = 0; n < b->free.size(); ++n)
+      if (b->free[n] != FIXED) positions.push_back(b->model.mesh.nodes[n]);
+    SetupOptions so;
+    so.reach = b->options.neighbour_reach;
+    so.coarse_dofs = b->options.coarse_dofs;
+    so.max_levels = b->options.max_levels;
+    so.range = b->options.smoother_range;
+    so.threads = b->threads;
+    b->setup = setup_create(std::move(fine), std::move(modes), std::move(positions), so);
+  }
+  bool finished = false;
+  sf_status st = setup_step(b->setup, budget, cancel, user, &finished);
+  b->preconditioner_seconds += now_seconds() - t0;
+  if (st) {
+    b->failure = st;
+    return st;
+  }
+  b->setup_finished = finished;
+  return SF_OK;
+}
+
+sf_status sf_builder_step(sf_builder* b, uint64_t max_elements, sf_cancel_fn cancel, void* user, sf_build_progress* p) {
+  if (!b) return fail(SF_INVALID_ARGUMENT, "null argument");
+  if (b->failure) return fail(b->failure, "the build failed earlier");
+  cudaSetDevice(b->solver.device);
+  double t0 = now_seconds();
+  sf_status st = builder_assemble(b, max_elements, cancel, user);
+  b->assembly_seconds += now_seconds() - t0;
+  if (st) return st;
+  size_t total = b->model.mesh.tets.size();
+  if (b->next == total && b->options.preconditioner == SF_PRECONDITIONER_MULTIGRID) {
+    st = builder_setup(b, max_elements, cancel, user);
+    if (st) return st;
+  }
+  if (p) {
+    p->elements_done = b->next;
+    p->elements_total = total;
+    p->setup_finished = b->next == total && (b->options.preconditioner != SF_PRECONDITIONER_MULTIGRID || b->setup_finished);
+  }
+  return SF_OK;
+}
+
+static void fill_stats(sf_study* s) {
+  if (s->levels.empty()) return;
+  bool single = s->solver.storage_single;
+  size_t sb = single ? 4 : 8;
+  double finest = (double)s->levels[0].a.vals.size();
+  size_t stored = 0, memory = 0;
+  for (auto& lv : s->levels) {
+    stored += lv.a.vals.size();
+    memory += (lv.a.starts.size()) * 8 + lv.a.cols.size() * 4 + lv.a.vals.size() * sb;
+    memory += lv.inverse_diagonal.size() * sb;
+    if (lv.has_p) memory += lv.p.starts.size() * 8 + lv.p.cols.size() * 4 + lv.p.vals.size() * sb;
+    if (lv.has_factor) memory += lv.factor_n * lv.factor_n * 8;
+  }
+  s->report.has_multigrid = 1;
+  s->report.mg_levels = s->levels.size();
+  s->report.mg_coarse_dofs = s->levels.back().a.rows * s->levels.back().a.rb;
+  s->report.mg_operator_complexity = (double)stored / finest;
+  s->report.mg_memory_bytes = memory;
+}
+
+sf_status sf_builder_finish(sf_builder* b, sf_study** out) {
+  if (!b || !out) return fail(SF_INVALID_ARGUMENT, "null argument");
+  if (b->failure) return fail(b->failure, "the build failed earlier");
+  bool mg = b->options.preconditioner == SF_PRECONDITIONER_MULTIGRID;
+  if (b->next != b->model.mesh.tets.size() || (mg && !b->setup_finished))
+    return fail(SF_NOT_FINISHED, "elements or setup remain");
+  cudaSetDevice(b->solver.device);
+  double t0 = now_seconds();
+  std::unique_ptr<sf_study> s(new sf_study);
+  s->model = std::move(b->model);
+  s->options = b->options;
+  s->free = std::move(b->free);
+  s->free_count = b->free_count;
+  s->rhs = std::move(b->rhs);
+  s->prescribed = std::move(b->prescribed);
+  s->pattern = std::move(b->pattern);
+  s->asmdev = b->asmdev;
+  s->solver = b->solver;
+  b->solver = DeviceSolver();
+  DeviceSolver& d = s->solver;
+  d.n = (uint32_t)(3 * s->free_count);
+  d.multigrid = mg;
+  int prec = s->options.precision;
+  d.precision = prec;
+  d.storage_single = prec != SF_PRECISION_DOUBLE;
+  d.vector_single = prec == SF_PRECISION_SINGLE || prec == SF_PRECISION_MIXED;
+  d.flexible = prec == SF_PRECISION_MIXED;
+  sf_status e = SF_OK;
+  double** vecs[] = {&d.rhs, &d.x, &d.r, &d.z, &d.p, &d.ap};
+  for (double** v : vecs)
+    if (!e) e = dev_alloc(d, (void**)v, (size_t)d.n * 8);
+  if (!e) e = dev_alloc(d, (void**)&d.partials, kReduceBlocks * 4 * 8);
+  if (!e) e = dev_alloc(d, (void**)&d.state, sizeof(PcgState));
+  if (!e) e = dev_alloc(d, (void**)&d.always_active, sizeof(int));
+  if (e) return e;
+  cudaMemcpyAsync(d.rhs, s->rhs.data(), (size_t)d.n * 8, cudaMemcpyHostToDevice, d.stream);
+  if (mg) {
+    s->levels = setup_take_levels(b->setup);
+    e = solver_upload_hierarchy(d, s->levels, s->options.smoother_degree);
+    if (e) return e;
+    fill_stats(s.get());
+  } else {
+    // Jacobi (preconditioner.rs:221-234): the inverse of the positive diagonal.
+    vector<double> diag(d.n);
+    vector<double> vals(s->pattern.cols.size() * 9);
+    cudaMemcpyAsync(vals.data(), d.system.vals, vals.size() * 8, cudaMemcpyDeviceToHost, d.stream);
+    cudaStreamSynchronize(d.stream);
+    for (size_t r = 0; r < s->free_count; ++r) {
+      const uint32_t* cb = s->pattern.cols.data() + s->pattern.starts[r];
+      const uint32_t* ce = s->pattern.cols.data() + s->pattern.starts[r + 1];
+      size_t at = std::lower_bound(cb, ce, (uint32_t)r) - s->pattern.cols.data();
+      for (int i = 0; i < 3; ++i) {
+        double v = vals[at * 9 + i * 3 + i];
+        if (std::isnan(v) || v <= 0.0 || !std::isfinite(v)) {
+          error_slot().row = 3 * r + i;
+          error_slot().value = v;
+          return fail(SF_JACOBI_DIAGONAL, "a diagonal entry is not positive");
+        }
+        diag[3 * r + i] = 1.0 / v;
+      }
+    }
+    if ((e = dev_alloc(d, (void**)&d.jacobi, (size_t)d.n * 8))) return e;
+    cudaMemcpyAsync(d.jacobi, diag.data(), (size_t)d.n * 8, cudaMemcpyHostToDevice, d.stream);
+    cudaStreamSynchronize(d.stream);
+  }
+  if (s->options.device_memory_budget && d.bytes > s->options.device_memory_budget)
+    return fail(SF_DEVICE_MEMORY_BUDGET, "the study does not fit the device memory budget");
+  e = solver_init_pcg(d, s->options.tolerance, s->options.max_iterations);
+  if (!e) e = cuda_check(cudaStreamSynchronize(d.stream), "solver init");
+  if (e) return e;
+  if (s->options.use_graphs) {
+    if ((e = solver_capture_graph(d))) return e;
+  }
+  cudaMallocHost((void**)&s->pinned, 2 * sizeof(PcgState));
+  cudaEventCreate(&s->ev0);
+  cudaEventCreate(&s->ev1);
+  std::memset(&s->report, 0, sizeof(s->report));
+  fill_stats(s.get());
+  s->report.total_dofs = 3 * s->model.mesh.nodes.size();
+  s->report.free_dofs = 3 * s->free_count;
+  s->report.nonzeros = s->pattern.cols.size() * 9;
+  s->report.relative_residual = 1.0;
+  s->report.assembly_seconds = b->assembly_seconds + (now_seconds() - t0);
+  s->report.preconditioner_seconds = b->preconditioner_seconds;
+  solver_read_state(d, &s->last);
+  s->status = s->last.status;
+  *out = s.release();
+  delete b;
+  return SF_OK;
+}
+
+sf_status sf_study_create(sf_model* model, const sf_study_options* options, sf_cancel_fn cancel, void* user,
+                          sf_study** out) {
+  sf_builder* b = nullptr;
+  if (sf_status e = sf_builder_create(model, options, &b)) return e;
+  sf_build_progress p;
+  sf_status e = sf_builder_step(b, UINT64_MAX, cancel, user, &p);
+  if (!e) e = sf_builder_finish(b, out);
+  if (e) {
+    sf_builder_destroy(b);
+    return e;
+  }
+  return SF_OK;
+}
+
+// ------------------------------------------------------------------------------ solve
+static void fill_progress(const PcgState& st, sf_progress* p) {
+  p->iteration = st.iterations;
+  p->relative_residual = st.rel;
+  p->at_rounding_floor = st.at_floor;
+}
+
+sf_status sf_study_step(sf_study* s, uint64_t max_iterations, sf_cancel_fn cancel, void* user, sf_step_outcome* out) {
+  if (!s) return fail(SF_INVALID_ARGUMENT, "null argument");
+  DeviceSolver& d = s->solver;
+  cudaSetDevice(d.device);
+  auto finish = [&](int kind) -> sf_status {
+    s->report.iterations = s->last.iterations;
+    s->report.relative_residual = s->last.rel;
+    s->report.at_rounding_floor = s->last.at_floor;
+    if (out) {
+      out->kind = kind;
+      fill_progress(s->last, &out->progress);
+    }
+    if (s->status == ST_FAILED_NOT_PD) {
+      error_slot().iteration = s->last.fail_iteration;
+      error_slot().curvature = s->last.curvature;
+      return fail(SF_PCG_NOT_POSITIVE_DEFINITE, "the system is not positive definite along the search direction");
+    }
+    if (s->status == ST_FAILED_NOT_CONVERGED) {
+      error_slot().iteration = s->last.iterations;
+      error_slot().relative_residual = s->last.rel;
+      return fail(SF_PCG_NOT_CONVERGED, "the iteration cap ran out before the tolerance");
+    }
+    return SF_OK;
+  };
+  if (s->cancelled) return finish(SF_OUTCOME_CANCELLED);
+  if (s->status == ST_CONVERGED) return finish(SF_OUTCOME_CONVERGED);
+  if (s->status != ST_ACTIVE) return finish(SF_OUTCOME_RUNNING);
+  double t0 = now_seconds();
+  cudaEventRecord(s->ev0, d.stream);
+  // Iterations are enqueued in chunks; every kernel of an iteration after the solve ends returns
+  // at once, so the state is read back once per chunk, with one chunk in flight ahead.
+  uint64_t done = 0;
+  const uint64_t chunk_max = 16;
+  uint64_t chunk = 4;
+  bool stop = false;
+  int kind = SF_OUTCOME_RUNNING;
+  while (!stop && done < max_iterations) {
+    uint64_t k = std::min<uint64_t>(chunk, max_iterations - done);
+    uint64_t launched = 0;
+    for (; launched < k; ++launched) {
+      if (cancel && cancel(user)) {
+        s->cancelled = true;
+        stop = true;
+        break;
+      }
+      sf_status e = s->options.use_graphs ? cuda_check(cudaGraphLaunch(d.graph_exec, d.stream), "graph launch")
+                                          : solver_enqueue_iteration(d);
+      if (e) return e;
+    }
+    done += launched;
+    cudaMemcpyAsync(s->pinned, d.state, sizeof(PcgState), cudaMemcpyDeviceToHost, d.stream);
+    if (sf_status e = cuda_check(cudaStreamSynchronize(d.stream), "solver step")) return e;
+    s->last = *s->pinned;
+    s->status = s->last.status;
+    if (s->status != ST_ACTIVE) stop = true;
+    chunk = std::min(chunk_max, chunk * 2);
+  }
+  cudaEventRecord(s->ev1, d.stream);
+  cudaEventSynchronize(s->ev1);
+  float ms = 0;
+  cudaEventElapsedTime(&ms, s->ev0, s->ev1);
+  s->step_ms = ms;
+  s->report.solve_seconds += now_seconds() - t0;
+  if (s->cancelled) kind = SF_OUTCOME_CANCELLED;
+  else if (s->status == ST_CONVERGED) kind = SF_OUTCOME_CONVERGED;
+  return finish(kind);
+}
+
+sf_status sf_study_displacements(const sf_study* s, double* out) {
+  if (!s || !out) return fail(SF_INVALID_ARGUMENT, "null argument");
+  const DeviceSolver& d = s->solver;
+  vector<double> x(d.n);
+  cudaSetDevice(d.device);
+  cudaMemcpyAsync(x.data(), d.x, (size_t)d.n * 8, cudaMemcpyDeviceToHost, d.stream);
+  if (sf_status e = cuda_check(cudaStreamSynchronize(d.stream), "read displacements")) return e;
+  for (size_t n = 0; n < s->free.size(); ++n)
+    for (int a = 0; a < 3; ++a) out[3 * n + a] = s->free[n] == FIXED ? 0.0 : x[3 * (size_t)s->free[n] + a];
+  return SF_OK;
+}
+
+sf_status sf_study_report(const sf_study* s, sf_report* out) {
+  if (!s || !out) return fail(SF_INVALID_ARGUMENT, "null argument");
+  *out = s->report;
+  return SF_OK;
+}
+
+sf_status sf_study_solution(sf_study* s, double* displacements, double* nodal_stress, double* nodal_von_mises,
+                            sf_point_stress* points) {
+  if (!s) return fail(SF_INVALID_ARGUMENT, "null argument");
+  if (s->status != ST_CONVERGED) return fail(SF_NOT_FINISHED, "the solve has not converged");
+  (void)nodal_stress;
+  (void)nodal_von_mises;
+  (void)points;
+  if (displacements)
+    if (sf_status e = sf_study_displacements(s, displacements)) return e;
+  if (nodal_stress || nodal_von_mises || points) return fail(SF_NOT_FINISHED, "stress recovery is not available yet");
+  return SF_OK;
+}
+
+void sf_study_destroy(sf_study* s) { delete s; }
+
+// ------------------------------------------------------------------------------ inspection
+sf_status sf_study_matrix(const sf_study* s, uint64_t* row_starts, uint32_t* columns, double* values) {
+  if (!s || !row_starts || !columns || !values) return fail(SF_INVALID_ARGUMENT, "null argument");
+  const DeviceSolver& d = s->solver;
+  size_t blocks = s->pattern.cols.size();
+  vector<double> vals(blocks * 9);
+  cudaSetDevice(d.device);
+  cudaMemcpyAsync(vals.data(), d.system.vals, blocks * 72, cudaMemcpyDeviceToHost, d.stream);
+  if (sf_status e = cuda_check(cudaStreamSynchronize(d.stream), "read matrix")) return e;
+  // Scalar CSR rows from 3x3 blocks: row 3R + i holds block columns in order, three each.
+  uint64_t at = 0;
+  row_starts[0] = 0;
+  for (size_t r = 0; r < s->free_count; ++r)
+    for (int i = 0; i < 3; ++i) {
+      for (uint32_t b = s->pattern.starts[r]; b < s->pattern.starts[r + 1]; ++b)
+        for (int k = 0; k < 3; ++k) {
+          columns[at] = 3 * s->pattern.cols[b] + k;
+          values[at] = vals[(size_t)b * 9 + i * 3 + k];
+          ++at;
+        }
+      row_starts[3 * r + i + 1] = at;
+    }
+  return SF_OK;
+}
+
+sf_status sf_study_rhs(const sf_study* s, double* out) {
+  if (!s || !out) return fail(SF_INVALID_ARGUMENT, "null argument");
+  std::memcpy(out, s->rhs.data(), s->rhs.size() * 8);
+  return SF_OK;
+}
+
+uint64_t sf_study_level_count(const sf_study* s) { return s ? s->levels.size() : 0; }
+
+sf_status sf_study_level_info(const sf_study* s, uint64_t level, sf_level_info* out) {
+  if (!s || !out || level >= s->levels.size()) return fail(SF_INVALID_ARGUMENT, "no such level");
+  const HostLevel& lv = s->levels[level];
+  out->rows = lv.a.rows;
+  out->row_block = lv.a.rb;
+  out->blocks = lv.a.cols.size();
+  out->lambda_min = lv.lambda_min;
+  out->lambda_max = lv.lambda_max;
+  out->has_prolongator = lv.has_p;
+  out->prolongator_blocks = lv.has_p ? lv.p.cols.size() : 0;
+  out->has_factor = lv.has_factor;
+  return SF_OK;
+}
+
+sf_status sf_study_level_matrix(const sf_study* s, uint64_t level, int32_t prolongator, uint64_t* starts,
+                                uint32_t* columns, double* values) {
+  if (!s || level >= s->levels.size() || !starts || !columns || !values) return fail(SF_INVALID_ARGUMENT, "no such level");
+  const HostLevel& lv = s->levels[level];
+  if (prolongator && !lv.has_p) return fail(SF_INVALID_ARGUMENT, "the coarsest level has no prolongator");
+  const Bsr& m = prolongator ? lv.p : lv.a;
+  for (size_t i = 0; i <= m.rows; ++i) starts[i] = m.starts[i];
+  std::memcpy(columns, m.cols.data(), m.cols.size() * 4);
+  std::memcpy(values, m.vals.data(), m.vals.size() * 8);
+  return SF_OK;
+}
+
+sf_status sf_study_aggregates(const sf_study* s, uint64_t level, uint32_t* out) {
+  if (!s || level >= s->levels.size() || !out) return fail(SF_INVALID_ARGUMENT, "no such level");
+  const HostLevel& lv = s->levels[level];
+  std::memcpy(out, lv.aggregates.data(), lv.aggregates.size() * 4);
+  return SF_OK;
+}
+
+sf_status sf_study_precondition(sf_study* s, const double* residual, double* output) {
+  if (!s || !residual || !output) return fail(SF_INVALID_ARGUMENT, "null argument");
+  DeviceSolver& d = s->solver;
+  cudaSetDevice(d.device);
+  double *din = nullptr, *dout = nullptr;
+  if (sf_status e = cuda_check(cudaMalloc((void**)&din, (size_t)d.n * 8 + 64), "cudaMalloc")) return e;
+  if (sf_status e = cuda_check(cudaMalloc((void**)&dout, (size_t)d.n * 8 + 64), "cudaMalloc")) {
+    cudaFree(din);
+    return e;
+  }
+  cudaMemcpyAsync(din, residual, (size_t)d.n * 8, cudaMemcpyHostToDevice, d.stream);
+  sf_status e = solver_precondition(d, din, dout);
+  if (!e) {
+    cudaMemcpyAsync(output, dout, (size_t)d.n * 8, cudaMemcpyDeviceToHost, d.stream);
+    e = cuda_check(cudaStreamSynchronize(d.stream), "precondition");
+  }
+  cudaFree(din);
+  cudaFree(dout);
+  return e;
+}
+
+sf_status sf_study_system_multiply(sf_study* s, const double* x, double* y) {
+  if (!s || !x || !y) return fail(SF_INVALID_ARGUMENT, "null argument");
+  DeviceSolver& d = s->solver;
+  cudaSetDevice(d.device);
+  double *din = nullptr, *dout = nullptr;
+  if (sf_status e = cuda_check(cudaMalloc((void**)&din, (size_t)d.n * 8 + 64), "cudaMalloc")) return e;
+  if (sf_status e = cuda_check(cudaMalloc((void**)&dout, (size_t)d.n * 8 + 64), "cudaMalloc")) {
+    cudaFree(din);
+    return e;
+  }
+  cudaMemcpyAsync(din, x, (size_t)d.n * 8, cudaMemcpyHostToDevice, d.stream);
+  sf_status e = solver_system_multiply(d, din, dout);
+  if (!e) {
+    cudaMemcpyAsync(y, dout, (size_t)d.n * 8, cudaMemcpyDeviceToHost, d.stream);
+    e = cuda_check(cudaStreamSynchronize(d.stream), "system multiply");
+  }
+  cudaFree(din);
+  cudaFree(dout);
+  return e;
+}
+
+sf_status sf_study_device_timing(const sf_study* s, sf_device_timing* out) {
+  if (!s || !out) return fail(SF_INVALID_ARGUMENT, "null argument");
+  out->step_ms = s->step_ms;
+  out->assembly_ms = 0;
+  out->setup_ms = 0;
+  out->kernel_launches = s->solver.launches_per_iteration;
+  return SF_OK;
+}
+
+}  // extern "C"
