@@ -1,0 +1,354 @@
+"""Benchmark: the 606k-DOF gate plate solve on B200.
+
+Workload (the gate-size plate): 100 x 100 x 0.8 mm on a 100 x 100 x 2 hex grid, six Tet10 per hex
+(120,000 elements, 202,005 nodes, 603,000 free DOFs), E = 2.0 GPa, nu = 0.35, edge x = 0 clamped,
+0.01 MPa pressure on the top face, solved to a relative residual of 1e-8 with the block
+smoothed-aggregation V-cycle (f32 hierarchy and vectors) inside FP64 flexible CG. Every input is
+generated here (synthetic, seeded by construction: the structured box builder).
+
+A step is one complete conjugate gradient solve of the plate on the device-resident matrix and
+hierarchy (restart from a zero estimate, iterate to convergence). `value` is solves per second
+over all ranks; `e2e` is the same metric through the public API with host buffers: model from the
+host mesh, device assembly, setup, solve, displacements back to the host. Under torchrun every
+rank runs its own replica (the solve does not shard): scaling is weak.
+
+--impl reference times the reference's CPU path (the bit-exact restatement in oracle/) on a
+bounded sample of the same workload on the host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+SIZE = (100.0, 100.0, 0.8)
+DIVISIONS = (100, 100, 2)
+YOUNGS, POISSON = 2000.0, 0.35
+PRESSURE = 0.01
+TOLERANCE = 1e-8
+METRIC = "606k-DOF plate solve throughput (mixed-precision V-cycle PCG)"
+UNIT = "solves/s"
+# The oracle's conjugate gradient iteration count for this workload in the reference's default
+# precision (SingleStorage), measured by running the committed oracle to convergence (it stops at
+# its f64 rounding floor, relative residual 5.2e-6); the CPU baseline extrapolates its per-iteration
+# time over these iterations.
+ORACLE_ITERATIONS = 358
+CPU_SAMPLE_ITERATIONS = 10
+
+
+def workload_config():
+    return {"workload": "gate plate 100x100x0.8 mm, 100x100x2 hex x 6 Tet10, 603,000 free DOFs, "
+                        "E 2.0 GPa nu 0.35, x=0 clamped, 0.01 MPa top pressure, rel. residual 1e-8",
+            "elements": 120000, "free_dofs": 603000, "precision": "f32 V-cycle in FP64 flexible CG",
+            "l2": "inputs larger than L2 (f32 fine operator 207.6 MB, f64 system 394 MB)",
+            "parallelism": "replicas"}
+
+
+def build_model(sf):
+    mesh = sf.box_tet_mesh((0.0, 0.0, 0.0), SIZE, DIVISIONS)
+    nodes = mesh.nodes()
+    model = sf.Model(mesh, sf.Material(YOUNGS, POISSON))
+    model.fix_nodes(np.nonzero(np.abs(nodes[:, 0]) < 1e-9)[0])
+    for f in mesh.boundary_faces():
+        if all(abs(nodes[n][2] - SIZE[2]) < 1e-9 for n in list(f.nodes)[:3]):
+            model.add_traction(f, (0.0, 0.0, -PRESSURE))
+    return mesh, model
+
+
+def options(sf, precision, device):
+    return sf.StudyOptions(pcg=sf.PcgOptions(tolerance=TOLERANCE),
+                           preconditioner=sf.MultigridOptions(precision=precision), device=device)
+
+
+class Clocks:
+    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                                          "-i", str(self.device), "-lms", "200"], stdout=self.file,
+                                         stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            self.proc.wait(timeout=10)
+
+    def summary(self):
+        self.file.flush()
+        rows = []
+        with open(self.file.name) as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.file.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+
+        def num(x):
+            try:
+                return float(x)
+            except ValueError:
+                return None
+        sm = [num(r[1]) for r in rows if num(r[1]) is not None]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": num(rows[0][2]),
+                "reasons": reasons, "samples": len(rows)}
+
+
+def measured_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def ncu_traffic():
+    """DRAM bytes per launch of the dominant kernel from the committed ncu summary, when present."""
+    path = os.path.join(ROOT, "profiles", "cheb_step_fine_gate_plate.txt")
+    if not os.path.exists(path):
+        return None
+    with open(path) as f:
+        for line in f:
+            if line.startswith("dram_bytes_per_launch:"):
+                return float(line.split(":", 1)[1].split()[0])
+    return None
+
+
+def cpu_baseline_sample(threads=None):
+    """The reference's CPU path (the oracle restatement) on a bounded sample of the workload:
+    assembly and multigrid setup in full, then CPU_SAMPLE_ITERATIONS conjugate gradient
+    iterations; a solve is the setup plus ORACLE_ITERATIONS iterations at the sampled rate."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    O.build()
+    threads = threads or O.default_threads()
+    O.set_threads(threads)
+    mesh = O.Mesh.box(SIZE, DIVISIONS)
+    nodes = mesh.nodes()
+    faces = O.faces_on_plane(mesh, 2, SIZE[2], nodes)
+    t0 = time.perf_counter()
+    study = O.Study(mesh, O.uniform(YOUNGS, POISSON), O.default_options(tolerance=TOLERANCE),
+                    O.nodes_on_plane(nodes, 0, 0.0), faces, [[0.0, 0.0, -PRESSURE]] * len(faces))
+    t1 = time.perf_counter()
+    study.step(CPU_SAMPLE_ITERATIONS)
+    t2 = time.perf_counter()
+    per_iteration = (t2 - t1) / CPU_SAMPLE_ITERATIONS
+    seconds = (t1 - t0) + ORACLE_ITERATIONS * per_iteration
+    return {"value": 1.0 / seconds, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"oracle (C++ restatement, SingleStorage): full assembly+setup ({t1 - t0:.2f} s) and "
+                      f"{CPU_SAMPLE_ITERATIONS} of {ORACLE_ITERATIONS} CG iterations ({per_iteration:.3f} s each), "
+                      f"extrapolated to one solve ({seconds:.1f} s)",
+            "seconds_per_solve": seconds}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return 0
+    samples = []
+    for i in range(args.warmup + args.steps):
+        s = cpu_baseline_sample()
+        if i >= args.warmup:
+            samples.append(s)
+    secs = statistics.mean(s["seconds_per_solve"] for s in samples)
+    value = 1.0 / secs
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": secs * 1000.0, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": workload_config(),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": samples[0]["cores"], "kind": "port",
+                             "sample": samples[0]["sample"]},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def timed_solves(torch, study, stream, steps):
+    """Solves `steps` times on the resident system; CUDA events on the study's stream."""
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    its = []
+    start.record(stream)
+    for _ in range(steps):
+        study.resolve()
+        out = study.solve()
+        its.append(out.progress.iteration)
+    end.record(stream)
+    end.synchronize()
+    return start.elapsed_time(end), its, out
+
+
+def run_mine(args, rank, world):
+    import torch
+
+    import solidfem_b200 as sf
+
+    device = int(os.environ.get("LOCAL_RANK", 0))
+    torch.cuda.set_device(device)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=torch.device("cuda", device))
+
+    def barrier():
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x):
+        if not dist:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    mesh, model = build_model(sf)
+    # --- e2e through the public API with host buffers (model -> study -> solve -> displacements).
+    def e2e_step():
+        _, m = build_model(sf)
+        t0 = time.perf_counter()
+        st = sf.StaticStudy.new(m, options(sf, sf.Precision.MIXED, device))
+        out = st.solve()
+        d = st.displacements()
+        t1 = time.perf_counter()
+        timing = st.device_timing()
+        return t1 - t0, timing, out, d, st
+
+    e2e_step()  # warm-up: CUDA context, module load, allocator
+    e2e_steps = max(1, min(args.steps, 3))
+    barrier()
+    e2e_times, h2d, d2h = [], 0, 0
+    for _ in range(e2e_steps):
+        dt, timing, out_e2e, disp_e2e, study = e2e_step()
+        e2e_times.append(dt)
+        h2d, d2h = timing["h2d_bytes"], timing["d2h_bytes"] + disp_e2e.nbytes
+    barrier()
+    e2e_sec = max_over_ranks(statistics.mean(e2e_times))
+    rep = study.report()
+
+    # --- value: device-resident solves of the mixed path.
+    stream = torch.cuda.ExternalStream(study.stream(), device=torch.device("cuda", device))
+    for _ in range(args.warmup):
+        study.resolve()
+        study.solve()
+    launches0 = study.device_timing()["kernel_launches"]
+    barrier()
+    with Clocks(device) as clocks:
+        ms, its, out = timed_solves(torch, study, stream, args.steps)
+    barrier()
+    launches = study.device_timing()["kernel_launches"] - launches0
+    ms = max_over_ranks(ms)
+    clock = clocks.summary()
+    ms_per_step = ms / args.steps
+    value = world * args.steps / (ms / 1000.0)
+    x_mixed = study.displacements()
+
+    # --- the plain FP64 path (Precision::Double semantics) for the mixed-vs-FP64 comparison.
+    double = sf.StaticStudy.new(model, options(sf, sf.Precision.DOUBLE, device))
+    double.solve()
+    dstream = torch.cuda.ExternalStream(double.stream(), device=torch.device("cuda", device))
+    barrier()
+    dms, dits, dout = timed_solves(torch, double, dstream, max(1, min(args.steps, 3)))
+    barrier()
+    dms = max_over_ranks(dms) / max(1, min(args.steps, 3))
+    x_double = double.displacements()
+    diff = float(np.linalg.norm(x_mixed - x_double) / np.linalg.norm(x_double))
+
+    # --- roofline of the dominant kernel: the finest level's fused Chebyshev step, timed live.
+    kt = study.time_kernel(sf.Kernel.CHEBYSHEV_STEP, 50)
+    st = study.time_kernel(sf.Kernel.SYSTEM_PRODUCT, 50)
+    peak, peak_kind = measured_peak()
+    achieved = kt["bytes_per_launch"] / (kt["ms_per_launch"] * 1e-3) / 1e9
+    traffic = ncu_traffic()
+
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 cycle / f64 outer", "data": "synthetic (structured box mesh)",
+            "config": workload_config(),
+            "iterations": its[-1], "relative_residual": out.progress.relative_residual,
+            "at_rounding_floor": out.progress.at_rounding_floor,
+            "fp64_path": {"ms_per_step": dms, "iterations": dout.progress.iteration,
+                          "relative_residual": dout.progress.relative_residual,
+                          "mixed_speedup": dms / ms_per_step, "mixed_vs_fp64_rel_l2": diff},
+            "setup": {"assembly_seconds": rep["assembly_seconds"], "preconditioner_seconds": rep["preconditioner_seconds"],
+                      "levels": rep["mg_levels"], "operator_complexity": rep["mg_operator_complexity"]},
+            "roofline": {"bound": "hbm", "kernel": "cheb_step_kernel<float,float,3> (finest level)",
+                         "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "peak_kind": peak_kind, "traffic": traffic,
+                         "bytes_per_launch": kt["bytes_per_launch"], "ms_per_launch": kt["ms_per_launch"],
+                         "system_product_gbs": st["bytes_per_launch"] / (st["ms_per_launch"] * 1e-3) / 1e9},
+            "e2e": {"value": world / e2e_sec, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "seconds_per_step": e2e_sec},
+            "gpu_launches": launches, "clocks": clock}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = {k: v for k, v in cpu_baseline_sample().items() if k != "seconds_per_solve"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    del study, double
+    if dist:
+        dist.destroy_process_group()
+    return 0
+
+
+def run_profile(args):
+    """One warm and one further resident solve of the mixed path, for profilers (no JSON line)."""
+    import solidfem_b200 as sf
+
+    precision = sf.Precision.DOUBLE if args.profile == "double" else sf.Precision.MIXED
+    _, model = build_model(sf)
+    study = sf.StaticStudy.new(model, options(sf, precision, 0))
+    for _ in range(2):
+        study.resolve()
+        out = study.solve()
+    print(f"profile {precision.name}: {out.progress.iteration} iterations, residual {out.progress.relative_residual:.3e}, "
+          f"{study.device_timing()['step_ms']:.1f} ms")
+    return 0
+
+
+def main():
+    p = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=["mine", "reference"], default="mine")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--profile", choices=["mixed", "double"], default=None,
+                   help="run one resident solve for a profiler and exit")
+    args = p.parse_args()
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    if args.profile:
+        return run_profile(args)
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+    return run_mine(args, rank, world)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

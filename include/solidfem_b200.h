@@ -303,16 +303,44 @@ sf_status sf_study_precondition(sf_study* study, const double* residual, double*
 /* CsrMatrix::multiply (csr.rs:112-120) on the device, FP64, host buffers. */
 sf_status sf_study_system_multiply(sf_study* study, const double* x, double* y);
 
-/* ------------------------------------------------------------- timing ---------------------- */
-/* Device time of the last sf_study_step call's kernels, measured with CUDA events on the
- * study's stream; and the summed device time of the solver's SpMV-class kernels. */
+/* ------------------------------------------------------------- re-solve and timing -------- */
+/* Restarts the solve from a zero estimate (Pcg::new, pcg.rs:135-164) on the resident matrix and
+ * preconditioner, with a new right-hand side over the free DOFs (host buffer), or the resident
+ * one when `rhs` is NULL. The reference builds a new Pcg for a new load; this keeps the assembled
+ * system and hierarchy on the device. */
+sf_status sf_study_resolve(sf_study* study, const double* rhs);
+
+/* The CUDA stream (cudaStream_t as an integer) every kernel of the study is launched on, so a
+ * caller can bracket work with its own CUDA events. */
+uint64_t sf_study_stream(const sf_study* study);
+
+/* Device time of the last sf_study_step call (CUDA events on the study's stream), the device time
+ * of the assembly, the kernels launched so far and the bytes copied each way. */
 typedef struct sf_device_timing {
   double step_ms;
   double assembly_ms;
   double setup_ms;
   uint64_t kernel_launches;
+  uint64_t h2d_bytes;
+  uint64_t d2h_bytes;
 } sf_device_timing;
 sf_status sf_study_device_timing(const sf_study* study, sf_device_timing* out);
+
+/* Times one solver kernel in isolation: `repeats` launches between CUDA events on the study's
+ * stream. kernel: SF_KERNEL_*. Returns the mean milliseconds per launch and the kernel's
+ * algorithmic bytes per launch (every value, index and vector entry it must move once). */
+enum {
+  SF_KERNEL_CHEBYSHEV_STEP = 0, /* finest level: A d, r -= A d, z = D^-1 r, d, x updates */
+  SF_KERNEL_LEVEL_RESIDUAL = 1, /* finest level: r = b - A x in the cycle's precision */
+  SF_KERNEL_SYSTEM_PRODUCT = 2, /* the FP64 system product of the conjugate gradient */
+  SF_KERNEL_RESTRICTION = 3     /* finest level: P^T r through the stored transpose */
+};
+typedef struct sf_kernel_timing {
+  double ms_per_launch;
+  double bytes_per_launch;
+  uint64_t launches;
+} sf_kernel_timing;
+sf_status sf_study_time_kernel(sf_study* study, int32_t kernel, uint64_t repeats, sf_kernel_timing* out);
 
 #ifdef __cplusplus
 }

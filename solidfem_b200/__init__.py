@@ -89,7 +89,19 @@ class _LevelInfo(C.Structure):
 
 class _DeviceTiming(C.Structure):
     _fields_ = [("step_ms", C.c_double), ("assembly_ms", C.c_double), ("setup_ms", C.c_double),
-                ("kernel_launches", C.c_uint64)]
+                ("kernel_launches", C.c_uint64), ("h2d_bytes", C.c_uint64), ("d2h_bytes", C.c_uint64)]
+
+
+class _KernelTiming(C.Structure):
+    _fields_ = [("ms_per_launch", C.c_double), ("bytes_per_launch", C.c_double), ("launches", C.c_uint64)]
+
+
+class Kernel(enum.IntEnum):
+    """Solver kernels that can be timed in isolation (SF_KERNEL_*)."""
+    CHEBYSHEV_STEP = 0
+    LEVEL_RESIDUAL = 1
+    SYSTEM_PRODUCT = 2
+    RESTRICTION = 3
 
 
 _CANCEL = C.CFUNCTYPE(C.c_int32, C.c_void_p)
@@ -143,6 +155,9 @@ SIGNATURES = {
     "sf_study_precondition": (C.c_int, [_V, _P(C.c_double), _P(C.c_double)]),
     "sf_study_system_multiply": (C.c_int, [_V, _P(C.c_double), _P(C.c_double)]),
     "sf_study_device_timing": (C.c_int, [_V, _P(_DeviceTiming)]),
+    "sf_study_resolve": (C.c_int, [_V, _P(C.c_double)]),
+    "sf_study_stream": (C.c_uint64, [_V]),
+    "sf_study_time_kernel": (C.c_int, [_V, C.c_int32, C.c_uint64, _P(_KernelTiming)]),
 }
 
 _lib = None
@@ -618,9 +633,26 @@ class StaticStudy:
         _check(library().sf_study_device_timing(self._h, C.byref(t)))
         return {name: getattr(t, name) for name, _ in _DeviceTiming._fields_}
 
+    def resolve(self, rhs: Optional[np.ndarray] = None) -> None:
+        """Restarts the solve from zero with a new right-hand side (free DOFs) or the resident one."""
+        if rhs is None:
+            _check(library().sf_study_resolve(self._h, None))
+        else:
+            r = np.ascontiguousarray(rhs, dtype=np.float64)
+            _check(library().sf_study_resolve(self._h, _dptr(r)))
+
+    def stream(self) -> int:
+        """The CUDA stream every kernel of this study runs on (cudaStream_t as an integer)."""
+        return int(library().sf_study_stream(self._h))
+
+    def time_kernel(self, kernel: "Kernel", repeats: int) -> dict:
+        t = _KernelTiming()
+        _check(library().sf_study_time_kernel(self._h, int(kernel), repeats, C.byref(t)))
+        return {"ms_per_launch": t.ms_per_launch, "bytes_per_launch": t.bytes_per_launch, "launches": t.launches}
+
 
 __all__ = [
     "BoundaryFace", "Mesh", "box_tet_mesh", "Material", "ShellCore", "Quadrature", "Model", "Precision",
     "PcgOptions", "MultigridOptions", "Jacobi", "StudyOptions", "StudyBuilder", "StaticStudy", "StepOutcome",
-    "Outcome", "Progress", "BuildProgress", "PointStress", "SolidfemError", "Status", "library", "SIGNATURES",
+    "Outcome", "Progress", "BuildProgress", "PointStress", "SolidfemError", "Status", "library", "SIGNATURES", "Kernel",
 ]

@@ -76,9 +76,21 @@ struct DeviceSolver {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t graph_exec = nullptr;
   uint64_t launches_per_iteration = 0;
+  uint64_t graph_kernels = 0;     // kernel nodes in the captured iteration graph
+  uint64_t launches = 0;          // kernels launched so far (graph replays count their kernels)
+  mutable uint64_t h2d_bytes = 0, d2h_bytes = 0;
 };
 
 // ------------------------------------------------------------------- memory helpers
+// Stream-ordered copies that count the bytes crossing the host-device link.
+inline void copy_h2d(const DeviceSolver& s, void* dst, const void* src, size_t bytes) {
+  cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s.stream);
+  s.h2d_bytes += bytes;
+}
+inline void copy_d2h(const DeviceSolver& s, void* dst, const void* src, size_t bytes) {
+  cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, s.stream);
+  s.d2h_bytes += bytes;
+}
 sf_status dev_alloc(DeviceSolver& s, void** ptr, size_t bytes);
 void dev_free_all(DeviceSolver& s);
 sf_status cuda_check(cudaError_t e, const char* what);
@@ -147,5 +159,9 @@ sf_status solver_precondition(DeviceSolver& s, const double* d_in, double* d_out
 sf_status solver_system_multiply(DeviceSolver& s, const double* d_in, double* d_out);
 sf_status solver_capture_graph(DeviceSolver& s);
 sf_status solver_read_state(DeviceSolver& s, PcgState* out);
+// Restarts the solve from x = 0 with the resident right-hand side (Pcg::new).
+sf_status solver_restart(DeviceSolver& s, double tolerance, uint64_t max_iterations);
+// Mean device milliseconds per launch of one solver kernel and its algorithmic bytes per launch.
+sf_status solver_time_kernel(DeviceSolver& s, int kernel, uint64_t repeats, double* ms, double* bytes);
 
 }  // namespace sf

@@ -629,15 +629,15 @@ sf_status upload_bsr(DeviceSolver& s, const Bsr& h, DevBsr& d) {
   if (sf_status e = dev_alloc(s, (void**)&d.starts, (h.rows + 1) * 4)) return e;
   if (sf_status e = dev_alloc(s, (void**)&d.cols, std::max<size_t>(1, h.cols.size()) * 4)) return e;
   if (sf_status e = dev_alloc(s, &d.vals, std::max<size_t>(1, h.vals.size()) * sizeof(S))) return e;
-  cudaMemcpyAsync(d.starts, h.starts.data(), (h.rows + 1) * 4, cudaMemcpyHostToDevice, s.stream);
-  if (!h.cols.empty()) cudaMemcpyAsync(d.cols, h.cols.data(), h.cols.size() * 4, cudaMemcpyHostToDevice, s.stream);
+  copy_h2d(s, d.starts, h.starts.data(), (h.rows + 1) * 4);
+  if (!h.cols.empty()) copy_h2d(s, d.cols, h.cols.data(), h.cols.size() * 4);
   if (!h.vals.empty()) {
     if (sizeof(S) == 8) {
-      cudaMemcpyAsync(d.vals, h.vals.data(), h.vals.size() * 8, cudaMemcpyHostToDevice, s.stream);
+      copy_h2d(s, d.vals, h.vals.data(), h.vals.size() * 8);
     } else {
       std::vector<float> f(h.vals.size());
       for (size_t i = 0; i < f.size(); ++i) f[i] = (float)h.vals[i];
-      cudaMemcpyAsync(d.vals, f.data(), f.size() * 4, cudaMemcpyHostToDevice, s.stream);
+      copy_h2d(s, d.vals, f.data(), f.size() * 4);
       cudaStreamSynchronize(s.stream);
     }
   }
@@ -686,10 +686,10 @@ sf_status solver_upload_hierarchy(DeviceSolver& s, const std::vector<HostLevel>&
     }
     if (sf_status e = dev_alloc(s, &L.dinv, h.inverse_diagonal.size() * S)) return e;
     if (S == 8) {
-      cudaMemcpyAsync(L.dinv, h.inverse_diagonal.data(), h.inverse_diagonal.size() * 8, cudaMemcpyHostToDevice, s.stream);
+      copy_h2d(s, L.dinv, h.inverse_diagonal.data(), h.inverse_diagonal.size() * 8);
     } else {
       std::vector<float> f(h.inverse_diagonal.begin(), h.inverse_diagonal.end());
-      cudaMemcpyAsync(L.dinv, f.data(), f.size() * 4, cudaMemcpyHostToDevice, s.stream);
+      copy_h2d(s, L.dinv, f.data(), f.size() * 4);
       cudaStreamSynchronize(s.stream);
     }
     L.has_p = h.has_p;
@@ -703,8 +703,7 @@ sf_status solver_upload_hierarchy(DeviceSolver& s, const std::vector<HostLevel>&
     L.has_factor = h.has_factor;
     if (h.has_factor) {
       if (sf_status e = dev_alloc(s, (void**)&L.coarse_inverse, h.coarse_inverse.size() * 8)) return e;
-      cudaMemcpyAsync(L.coarse_inverse, h.coarse_inverse.data(), h.coarse_inverse.size() * 8, cudaMemcpyHostToDevice,
-                      s.stream);
+      copy_h2d(s, L.coarse_inverse, h.coarse_inverse.data(), h.coarse_inverse.size() * 8);
     }
     // ChebyshevCoefficients (gpu/layout.rs:443-465), the recurrence of cycle.rs:578-626.
     double theta = 0.5 * (h.lambda_max + h.lambda_min);
@@ -734,9 +733,9 @@ sf_status solver_init_pcg(DeviceSolver& s, double tolerance, uint64_t max_iterat
   h.max_iterations = max_iterations ? max_iterations : 10ull * s.n + 1000ull;
   h.flexible = s.flexible ? 1 : 0;
   h.status = ST_ACTIVE;
-  cudaMemcpyAsync(s.state, &h, sizeof(h), cudaMemcpyHostToDevice, s.stream);
+  copy_h2d(s, s.state, &h, sizeof(h));
   int one_active = ST_ACTIVE;
-  cudaMemcpyAsync(s.always_active, &one_active, sizeof(int), cudaMemcpyHostToDevice, s.stream);
+  copy_h2d(s, s.always_active, &one_active, sizeof(int));
   pcg_init_kernel<<<kReduceBlocks, kReduceThreads, 0, s.stream>>>(s.n, s.rhs, s.x, s.r, s.partials, s.state);
   return solver_enqueue_reset(s);
 }
@@ -789,8 +788,89 @@ sf_status solver_capture_graph(DeviceSolver& s) {
   if (st) return st;
   if (e != cudaSuccess) return cuda_check(e, "end capture");
   s.graph = g;
+  size_t nodes = 0;
+  cudaGraphGetNodes(g, nullptr, &nodes);
+  s.graph_kernels = nodes;
   e = cudaGraphInstantiate(&s.graph_exec, g, 0);
   return cuda_check(e, "graph instantiate");
+}
+
+sf_status solver_restart(DeviceSolver& s, double tolerance, uint64_t max_iterations) {
+  s.launches_per_iteration = 0;
+  sf_status e = solver_init_pcg(s, tolerance, max_iterations);
+  s.launches += s.launches_per_iteration + 1;
+  return e;
+}
+
+namespace {
+
+template <typename S, typename V>
+sf_status time_level0(DeviceSolver& s, int kernel, uint64_t repeats, double* ms, double* bytes) {
+  DevLevel& L = s.levels[0];
+  const int* on = s.always_active;
+  double rows = L.a.rows, blocks = (double)L.a.blocks, rb = L.a.rb, sv = sizeof(V), ss = sizeof(S);
+  cudaEvent_t a, b;
+  cudaEventCreate(&a);
+  cudaEventCreate(&b);
+  cudaEventRecord(a, s.stream);
+  for (uint64_t i = 0; i < repeats; ++i) {
+    if (kernel == SF_KERNEL_CHEBYSHEV_STEP) {
+      V* d[2] = {(V*)L.d0, (V*)L.d1};
+      launch_cheb_step<S, V, 3>(L, d[i & 1], d[(i + 1) & 1], (V*)L.res, (V*)L.x, nullptr, 0.5, 0.25, on, s.stream);
+    } else if (kernel == SF_KERNEL_LEVEL_RESIDUAL) {
+      launch_bsr<S, V, 3, 3, OP_RESIDUAL>(L.a, (const V*)L.x, (V*)L.tmp, (const V*)L.b, on, s.stream);
+    } else {
+      bsr_dispatch<S, V, OP_SET>(L.r, (const V*)L.res, (V*)s.levels[1].b, nullptr, on, s.stream);
+    }
+  }
+  cudaEventRecord(b, s.stream);
+  cudaError_t e = cudaEventSynchronize(b);
+  float t = 0;
+  cudaEventElapsedTime(&t, a, b);
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  *ms = t / (double)repeats;
+  double matrix = rows * 4 + blocks * (rb * rb * ss + 4);
+  double vec = rows * rb * sv;
+  if (kernel == SF_KERNEL_CHEBYSHEV_STEP)
+    *bytes = matrix + vec /* d_old */ + 2 * vec /* r */ + rows * rb * rb * ss /* D^-1 */ + vec /* d_new */ + 2 * vec /* x */;
+  else if (kernel == SF_KERNEL_LEVEL_RESIDUAL)
+    *bytes = matrix + 3 * vec;
+  else
+    *bytes = (double)L.r.rows * 4 + (double)L.r.blocks * (L.r.rb * L.r.cb * ss + 4) + vec +
+             (double)L.r.rows * L.r.rb * sv;
+  s.launches += repeats;
+  return cuda_check(e, "time kernel");
+}
+
+}  // namespace
+
+sf_status solver_time_kernel(DeviceSolver& s, int kernel, uint64_t repeats, double* ms, double* bytes) {
+  if (repeats == 0) return fail(SF_INVALID_ARGUMENT, "repeats must be positive");
+  if (kernel == SF_KERNEL_SYSTEM_PRODUCT) {
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    cudaEventRecord(a, s.stream);
+    for (uint64_t i = 0; i < repeats; ++i)
+      launch_bsr<double, double, 3, 3, OP_SET>(s.system, s.p, s.ap, nullptr, s.always_active, s.stream);
+    cudaEventRecord(b, s.stream);
+    cudaError_t e = cudaEventSynchronize(b);
+    float t = 0;
+    cudaEventElapsedTime(&t, a, b);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    *ms = t / (double)repeats;
+    *bytes = (double)s.system.rows * 4 + (double)s.system.blocks * 76 + (double)s.n * 16;
+    s.launches += repeats;
+    return cuda_check(e, "time kernel");
+  }
+  if (!s.multigrid || s.levels.empty()) return fail(SF_INVALID_ARGUMENT, "the study has no multigrid hierarchy");
+  if (kernel == SF_KERNEL_RESTRICTION && !s.levels[0].has_p) return fail(SF_INVALID_ARGUMENT, "one-level hierarchy");
+  if (kernel < 0 || kernel > SF_KERNEL_RESTRICTION) return fail(SF_INVALID_ARGUMENT, "unknown kernel");
+  if (!s.storage_single) return time_level0<double, double>(s, kernel, repeats, ms, bytes);
+  if (!s.vector_single) return time_level0<float, double>(s, kernel, repeats, ms, bytes);
+  return time_level0<float, float>(s, kernel, repeats, ms, bytes);
 }
 
 sf_status solver_precondition(DeviceSolver& s, const double* d_in, double* d_out) {
@@ -798,10 +878,10 @@ sf_status solver_precondition(DeviceSolver& s, const double* d_in, double* d_out
   if (s.vector_single && s.multigrid) {
     // widen the f32 correction
     std::vector<float> h(s.n);
-    cudaMemcpyAsync(h.data(), s.z32, (size_t)s.n * 4, cudaMemcpyDeviceToHost, s.stream);
+    copy_d2h(s, h.data(), s.z32, (size_t)s.n * 4);
     cudaStreamSynchronize(s.stream);
     std::vector<double> w(h.begin(), h.end());
-    cudaMemcpyAsync(d_out, w.data(), (size_t)s.n * 8, cudaMemcpyHostToDevice, s.stream);
+    copy_h2d(s, d_out, w.data(), (size_t)s.n * 8);
   }
   return cuda_check(cudaStreamSynchronize(s.stream), "precondition");
 }
@@ -812,7 +892,7 @@ sf_status solver_system_multiply(DeviceSolver& s, const double* d_in, double* d_
 }
 
 sf_status solver_read_state(DeviceSolver& s, PcgState* out) {
-  cudaMemcpyAsync(out, s.state, sizeof(PcgState), cudaMemcpyDeviceToHost, s.stream);
+  copy_d2h(s, out, s.state, sizeof(PcgState));
   return cuda_check(cudaStreamSynchronize(s.stream), "read state");
 }
 

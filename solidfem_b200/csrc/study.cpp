@@ -354,6 +354,7 @@ struct sf_study {
   bool cancelled = false;
   PcgState last;
   double step_ms = 0;
+  double assembly_ms = 0;
   PcgState* pinned = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   ~sf_study() {
@@ -692,16 +693,16 @@ sf_status sf_builder_create(sf_model* model, const sf_study_options* options, sf
     release_builder_device(b.get());
     return e;
   }
-  cudaMemcpyAsync(a.nodes, mesh.nodes.data(), nn * 24, cudaMemcpyHostToDevice, s.stream);
-  cudaMemcpyAsync(a.tets, mesh.tets.data(), mesh.tets.size() * 40, cudaMemcpyHostToDevice, s.stream);
-  cudaMemcpyAsync(a.map_starts, b->pattern.map_starts.data(), (blocks + 1) * 4, cudaMemcpyHostToDevice, s.stream);
+  copy_h2d(s, a.nodes, mesh.nodes.data(), nn * 24);
+  copy_h2d(s, a.tets, mesh.tets.data(), mesh.tets.size() * 40);
+  copy_h2d(s, a.map_starts, b->pattern.map_starts.data(), (blocks + 1) * 4);
   if (!b->pattern.map.empty())
-    cudaMemcpyAsync(a.map, b->pattern.map.data(), b->pattern.map.size() * 4, cudaMemcpyHostToDevice, s.stream);
-  cudaMemcpyAsync(a.cursor, b->pattern.map_starts.data(), blocks * 4, cudaMemcpyHostToDevice, s.stream);
+    copy_h2d(s, a.map, b->pattern.map.data(), b->pattern.map.size() * 4);
+  copy_h2d(s, a.cursor, b->pattern.map_starts.data(), blocks * 4);
   unsigned long long none = ~0ull;
-  cudaMemcpyAsync(a.error, &none, 8, cudaMemcpyHostToDevice, s.stream);
-  cudaMemcpyAsync(s.system.starts, b->pattern.starts.data(), (b->free_count + 1) * 4, cudaMemcpyHostToDevice, s.stream);
-  cudaMemcpyAsync(s.system.cols, b->pattern.cols.data(), blocks * 4, cudaMemcpyHostToDevice, s.stream);
+  copy_h2d(s, a.error, &none, 8);
+  copy_h2d(s, s.system.starts, b->pattern.starts.data(), (b->free_count + 1) * 4);
+  copy_h2d(s, s.system.cols, b->pattern.cols.data(), blocks * 4);
   // A host material callback: integration point positions from the device, the field on the
   // host, (E, nu) per point back to the device.
   if (md.material.kind == MATERIAL_CALLBACK) {
@@ -714,7 +715,7 @@ sf_status sf_builder_create(sf_model* model, const sf_study_options* options, sf
       return e;
     }
     vector<double> pos(pts * 3);
-    cudaMemcpyAsync(pos.data(), a.positions, pts * 24, cudaMemcpyDeviceToHost, s.stream);
+    copy_d2h(s, pos.data(), a.positions, pts * 24);
     cudaStreamSynchronize(s.stream);
     vector<sf_material> mats(pts);
     md.material.callback(md.material.user, pos.data(), pts, mats.data());
@@ -723,7 +724,7 @@ sf_status sf_builder_create(sf_model* model, const sf_study_options* options, sf
       em[2 * i] = mats[i].youngs_modulus;
       em[2 * i + 1] = mats[i].poisson_ratio;
     }
-    cudaMemcpyAsync(a.point_material, em.data(), pts * 16, cudaMemcpyHostToDevice, s.stream);
+    copy_h2d(s, a.point_material, em.data(), pts * 16);
   }
   e = cuda_check(cudaStreamSynchronize(s.stream), "assembly set-up");
   if (e) {
@@ -756,6 +757,7 @@ static sf_status builder_assemble(sf_builder* b, uint64_t max_elements, sf_cance
   cudaEventRecord(e0, s.stream);
   sf_status st = launch_element_stiffness(b->asmdev, b->model.material, (uint32_t)b->next, (uint32_t)end, s.stream);
   if (!st) st = launch_gather(b->asmdev, s.system, (uint32_t)end, s.stream);
+  s.launches += 2;
   cudaEventRecord(e1, s.stream);
   if (!st) st = cuda_check(cudaStreamSynchronize(s.stream), "assembly");
   float ms = 0;
@@ -789,7 +791,7 @@ static sf_status builder_setup(sf_builder* b, uint64_t budget, sf_cancel_fn canc
     fine.starts = b->pattern.starts;
     fine.cols = b->pattern.cols;
     fine.vals.resize(b->pattern.cols.size() * 9);
-    cudaMemcpyAsync(fine.vals.data(), s.system.vals, fine.vals.size() * 8, cudaMemcpyDeviceToHost, s.stream);
+    copy_d2h(s, fine.vals.data(), s.system.vals, fine.vals.size() * 8);
     if (sf_status e = cuda_check(cudaStreamSynchronize(s.stream), "download fine level")) return e;
     vector<double> modes = rigid_modes(b->model.mesh.nodes, b->free, b->free_count);
     vector<P3> positions;
@@ -891,7 +893,7 @@ sf_status sf_builder_finish(sf_builder* b, sf_study** out) {
   if (!e) e = dev_alloc(d, (void**)&d.state, sizeof(PcgState));
   if (!e) e = dev_alloc(d, (void**)&d.always_active, sizeof(int));
   if (e) return e;
-  cudaMemcpyAsync(d.rhs, s->rhs.data(), (size_t)d.n * 8, cudaMemcpyHostToDevice, d.stream);
+  copy_h2d(d, d.rhs, s->rhs.data(), (size_t)d.n * 8);
   if (mg) {
     s->levels = setup_take_levels(b->setup);
     e = solver_upload_hierarchy(d, s->levels, s->options.smoother_degree);
@@ -901,7 +903,7 @@ sf_status sf_builder_finish(sf_builder* b, sf_study** out) {
     // Jacobi (preconditioner.rs:221-234): the inverse of the positive diagonal.
     vector<double> diag(d.n);
     vector<double> vals(s->pattern.cols.size() * 9);
-    cudaMemcpyAsync(vals.data(), d.system.vals, vals.size() * 8, cudaMemcpyDeviceToHost, d.stream);
+    copy_d2h(d, vals.data(), d.system.vals, vals.size() * 8);
     cudaStreamSynchronize(d.stream);
     for (size_t r = 0; r < s->free_count; ++r) {
       const uint32_t* cb = s->pattern.cols.data() + s->pattern.starts[r];
@@ -918,7 +920,7 @@ sf_status sf_builder_finish(sf_builder* b, sf_study** out) {
       }
     }
     if ((e = dev_alloc(d, (void**)&d.jacobi, (size_t)d.n * 8))) return e;
-    cudaMemcpyAsync(d.jacobi, diag.data(), (size_t)d.n * 8, cudaMemcpyHostToDevice, d.stream);
+    copy_h2d(d, d.jacobi, diag.data(), (size_t)d.n * 8);
     cudaStreamSynchronize(d.stream);
   }
   if (s->options.device_memory_budget && d.bytes > s->options.device_memory_budget)
@@ -940,6 +942,7 @@ sf_status sf_builder_finish(sf_builder* b, sf_study** out) {
   s->report.relative_residual = 1.0;
   s->report.assembly_seconds = b->assembly_seconds + (now_seconds() - t0);
   s->report.preconditioner_seconds = b->preconditioner_seconds;
+  s->assembly_ms = b->assembly_ms;
   solver_read_state(d, &s->last);
   s->status = s->last.status;
   *out = s.release();
@@ -1013,12 +1016,18 @@ sf_status sf_study_step(sf_study* s, uint64_t max_iterations, sf_cancel_fn cance
         stop = true;
         break;
       }
-      sf_status e = s->options.use_graphs ? cuda_check(cudaGraphLaunch(d.graph_exec, d.stream), "graph launch")
-                                          : solver_enqueue_iteration(d);
+      sf_status e = SF_OK;
+      if (s->options.use_graphs) {
+        e = cuda_check(cudaGraphLaunch(d.graph_exec, d.stream), "graph launch");
+        d.launches += d.graph_kernels;
+      } else {
+        e = solver_enqueue_iteration(d);
+        d.launches += d.launches_per_iteration;
+      }
       if (e) return e;
     }
     done += launched;
-    cudaMemcpyAsync(s->pinned, d.state, sizeof(PcgState), cudaMemcpyDeviceToHost, d.stream);
+    copy_d2h(d, s->pinned, d.state, sizeof(PcgState));
     if (sf_status e = cuda_check(cudaStreamSynchronize(d.stream), "solver step")) return e;
     s->last = *s->pinned;
     s->status = s->last.status;
@@ -1041,7 +1050,7 @@ sf_status sf_study_displacements(const sf_study* s, double* out) {
   const DeviceSolver& d = s->solver;
   vector<double> x(d.n);
   cudaSetDevice(d.device);
-  cudaMemcpyAsync(x.data(), d.x, (size_t)d.n * 8, cudaMemcpyDeviceToHost, d.stream);
+  copy_d2h(d, x.data(), d.x, (size_t)d.n * 8);
   if (sf_status e = cuda_check(cudaStreamSynchronize(d.stream), "read displacements")) return e;
   for (size_t n = 0; n < s->free.size(); ++n)
     for (int a = 0; a < 3; ++a) out[3 * n + a] = s->free[n] == FIXED ? 0.0 : x[3 * (size_t)s->free[n] + a];
@@ -1076,7 +1085,7 @@ sf_status sf_study_matrix(const sf_study* s, uint64_t* row_starts, uint32_t* col
   size_t blocks = s->pattern.cols.size();
   vector<double> vals(blocks * 9);
   cudaSetDevice(d.device);
-  cudaMemcpyAsync(vals.data(), d.system.vals, blocks * 72, cudaMemcpyDeviceToHost, d.stream);
+  copy_d2h(d, vals.data(), d.system.vals, blocks * 72);
   if (sf_status e = cuda_check(cudaStreamSynchronize(d.stream), "read matrix")) return e;
   // Scalar CSR rows from 3x3 blocks: row 3R + i holds block columns in order, three each.
   uint64_t at = 0;
@@ -1145,10 +1154,10 @@ sf_status sf_study_precondition(sf_study* s, const double* residual, double* out
     cudaFree(din);
     return e;
   }
-  cudaMemcpyAsync(din, residual, (size_t)d.n * 8, cudaMemcpyHostToDevice, d.stream);
+  copy_h2d(d, din, residual, (size_t)d.n * 8);
   sf_status e = solver_precondition(d, din, dout);
   if (!e) {
-    cudaMemcpyAsync(output, dout, (size_t)d.n * 8, cudaMemcpyDeviceToHost, d.stream);
+    copy_d2h(d, output, dout, (size_t)d.n * 8);
     e = cuda_check(cudaStreamSynchronize(d.stream), "precondition");
   }
   cudaFree(din);
@@ -1166,10 +1175,10 @@ sf_status sf_study_system_multiply(sf_study* s, const double* x, double* y) {
     cudaFree(din);
     return e;
   }
-  cudaMemcpyAsync(din, x, (size_t)d.n * 8, cudaMemcpyHostToDevice, d.stream);
+  copy_h2d(d, din, x, (size_t)d.n * 8);
   sf_status e = solver_system_multiply(d, din, dout);
   if (!e) {
-    cudaMemcpyAsync(y, dout, (size_t)d.n * 8, cudaMemcpyDeviceToHost, d.stream);
+    copy_d2h(d, y, dout, (size_t)d.n * 8);
     e = cuda_check(cudaStreamSynchronize(d.stream), "system multiply");
   }
   cudaFree(din);
@@ -1180,9 +1189,42 @@ sf_status sf_study_system_multiply(sf_study* s, const double* x, double* y) {
 sf_status sf_study_device_timing(const sf_study* s, sf_device_timing* out) {
   if (!s || !out) return fail(SF_INVALID_ARGUMENT, "null argument");
   out->step_ms = s->step_ms;
-  out->assembly_ms = 0;
+  out->assembly_ms = s->assembly_ms;
   out->setup_ms = 0;
-  out->kernel_launches = s->solver.launches_per_iteration;
+  out->kernel_launches = s->solver.launches;
+  out->h2d_bytes = s->solver.h2d_bytes;
+  out->d2h_bytes = s->solver.d2h_bytes;
+  return SF_OK;
+}
+
+sf_status sf_study_resolve(sf_study* s, const double* rhs) {
+  if (!s) return fail(SF_INVALID_ARGUMENT, "null argument");
+  DeviceSolver& d = s->solver;
+  cudaSetDevice(d.device);
+  if (rhs) {
+    std::memcpy(s->rhs.data(), rhs, (size_t)d.n * 8);
+    copy_h2d(d, d.rhs, rhs, (size_t)d.n * 8);
+  }
+  if (sf_status e = solver_restart(d, s->options.tolerance, s->options.max_iterations)) return e;
+  s->cancelled = false;
+  std::memset(&s->last, 0, sizeof(s->last));
+  s->status = ST_ACTIVE;
+  s->report.iterations = 0;
+  s->report.relative_residual = 1.0;
+  s->report.at_rounding_floor = 0;
+  return SF_OK;
+}
+
+uint64_t sf_study_stream(const sf_study* s) { return s ? (uint64_t)(uintptr_t)s->solver.stream : 0; }
+
+sf_status sf_study_time_kernel(sf_study* s, int32_t kernel, uint64_t repeats, sf_kernel_timing* out) {
+  if (!s || !out) return fail(SF_INVALID_ARGUMENT, "null argument");
+  cudaSetDevice(s->solver.device);
+  double ms = 0, bytes = 0;
+  if (sf_status e = solver_time_kernel(s->solver, kernel, repeats, &ms, &bytes)) return e;
+  out->ms_per_launch = ms;
+  out->bytes_per_launch = bytes;
+  out->launches = repeats;
   return SF_OK;
 }
 
