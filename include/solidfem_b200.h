@@ -180,6 +180,8 @@ typedef struct sf_study_options {
   int32_t device;          /* CUDA device ordinal */
   int32_t use_graphs;      /* capture each solver iteration in a CUDA graph (default 1) */
   uint64_t device_memory_budget; /* bytes a study may hold on the device; 0: no limit */
+  uint64_t sell_min_rows;  /* operators with at least this many block rows use the SELL-32 layout;
+                              0: 32768 */
 } sf_study_options;
 
 /* StudyOptions::default with the reference's defaults (Jacobi preconditioner). */

@@ -43,7 +43,7 @@ class _Options(C.Structure):
                 ("neighbour_reach", C.c_double), ("coarse_dofs", C.c_uint64), ("max_levels", C.c_uint64),
                 ("smoother_degree", C.c_uint64), ("smoother_range", C.c_double), ("precision", C.c_int32),
                 ("threads", C.c_uint64), ("device", C.c_int32), ("use_graphs", C.c_int32),
-                ("device_memory_budget", C.c_uint64)]
+                ("device_memory_budget", C.c_uint64), ("sell_min_rows", C.c_uint64)]
 
 
 class _BuildProgress(C.Structure):
@@ -442,6 +442,7 @@ class StudyOptions:
     device: int = 0
     use_graphs: bool = True
     device_memory_budget: int = 0
+    sell_min_rows: int = 0
 
     def _c(self) -> _Options:
         o = _Options()
@@ -463,6 +464,7 @@ class StudyOptions:
         o.device = self.device
         o.use_graphs = 1 if self.use_graphs else 0
         o.device_memory_budget = self.device_memory_budget
+        o.sell_min_rows = self.sell_min_rows
         return o
 
 

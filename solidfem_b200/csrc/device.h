@@ -20,7 +20,39 @@ struct DevBsr {
   uint32_t* starts = nullptr;  // rows + 1
   uint32_t* cols = nullptr;    // blocks
   void* vals = nullptr;        // blocks * rb * cb values of the storage type
+  // Row groups: runs of consecutive rows whose value slab fits a warp's staging buffer. A warp
+  // streams one group into shared memory while it multiplies the previous one.
+  uint4* groups = nullptr;     // per group {first row, end row, first block, end block}
+  uint32_t ngroups = 0;
+  uint32_t group_bytes = 0;    // the largest group's value bytes
+  uint32_t group_blocks = 0;   // the largest group's block count
+  uint32_t group_rows = 0;     // the largest group's row count
+  int lanes_per_row = 32;      // lanes sharing one row: 32, 16, 8 or 4
+  // SELL-32 copy for operators with many rows: slices of 32 rows (rows sorted by block count
+  // inside windows of kSellWindow rows), one thread per row. Block k of the row in lane t of
+  // slice s is block index slice_start[s] + 32 k + t; its element e is stored at
+  // value[(slice_start[s] + 32 k) * rb * cb + 32 e + t], so each (k, e) is one coalesced line.
+  bool sell = false;
+  uint32_t nslices = 0;
+  uint32_t* sell_rows = nullptr;   // nslices * 32: the row of each lane (rows when padding)
+  uint32_t* sell_len = nullptr;    // nslices * 32: its block count
+  uint32_t* sell_start = nullptr;  // nslices + 1, in blocks
+  uint32_t* sell_cols = nullptr;
+  void* sell_vals = nullptr;
 };
+
+static const uint32_t kSellWindow = 2048;    // rows are sorted by length inside windows this long
+
+// Builds the SELL-32 copy of a block matrix from host starts, columns and values (S values).
+template <typename S>
+sf_status make_sell(struct DeviceSolver& s, DevBsr& m, const uint32_t* starts, const uint32_t* cols, const S* vals);
+// The SELL copy of a matrix whose values live only on the device (the assembled f64 system):
+// the layout from host starts/columns, the values permuted on the device.
+sf_status make_sell_from_device(struct DeviceSolver& s, DevBsr& m, const uint32_t* starts, const uint32_t* cols);
+
+// Splits the rows of a block matrix into groups of at most `target` value bytes (a longer row is
+// a group of its own) and chooses the lanes per row from the mean blocks per row.
+sf_status make_row_groups(struct DeviceSolver& s, DevBsr& m, const uint32_t* host_starts, size_t value_bytes);
 
 // The solver's scalar state, resident on the device so the iteration loop runs without host
 // round trips; kernels read `status` and exit early once the solve has ended.
@@ -79,6 +111,7 @@ struct DeviceSolver {
   uint64_t graph_kernels = 0;     // kernel nodes in the captured iteration graph
   uint64_t launches = 0;          // kernels launched so far (graph replays count their kernels)
   mutable uint64_t h2d_bytes = 0, d2h_bytes = 0;
+  uint64_t sell_min_rows = 32768;  // operators with at least this many rows use SELL-32
 };
 
 // ------------------------------------------------------------------- memory helpers

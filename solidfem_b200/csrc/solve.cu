@@ -2,13 +2,16 @@
 // the fused Chebyshev smoother, restriction through the stored transpose, prolongation, the
 // coarsest level's dense solve and the FP64 conjugate gradient with fixed-order reductions.
 //
-// Layout: a block row's values are one contiguous slab of row-major blocks. A warp owns a block
-// row; it stages the slab into shared memory with 16-byte coalesced streaming loads and then each
-// lane multiplies one block, so the value stream is read once, fully coalesced, and x (held in
-// L2) is gathered per block. Sums are reduced across the warp with a fixed butterfly, so every run
-// gives the same bits. Each kernel reads the solver's status word first and returns at once when
-// the solve has ended, so a batch of iterations can be enqueued (or replayed as a CUDA graph)
-// without a host round trip per iteration.
+// The block products are HBM-bound streams over each operator's value slab. A matrix's rows are
+// cut on the host into row groups (consecutive rows, about 4 KB of values each). A warp walks its
+// groups in a grid-stride loop and stages each one into its own shared-memory buffer with 16-byte
+// cp.async copies (L2 only), double-buffered: while it multiplies group k out of shared memory,
+// group k+1 is already streaming in, so every warp keeps kilobytes in flight without register
+// cost. A row is shared by `LPR` lanes (32 for the stiffness and transpose operators, fewer for
+// the thin prolongators), each multiplying one block at a time with its x gathered through L2;
+// the lanes' sums meet in a fixed xor butterfly, so every run gives the same bits. Each kernel
+// reads the solver's status word first and returns at once when the solve has ended, so a batch
+// of iterations can be enqueued (or replayed as a CUDA graph) without a host round trip each.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -24,139 +27,301 @@ namespace {
 const unsigned kFull = 0xffffffffu;
 const int kThreads = 256;
 const int kWarps = kThreads / 32;
-const int kBlocksPerPass = 32;
+const uint32_t kGroupTarget = 4096;     // value bytes a row group aims at
+const int kSmemPerBlockTarget = 72 * 1024;
 
-template <typename S, int RB, int CB>
-struct Slab {
-  static constexpr int kLen = RB * CB;
-  static constexpr int kBytes = kBlocksPerPass * kLen * (int)sizeof(S) + 32;
-  static constexpr int kInt4 = (kBytes + 15) / 16;
-};
+// ------------------------------------------------------------ asynchronous staging
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_one() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
-__device__ __forceinline__ int stage_slab(const void* src, int bytes, int4* dst, int lane) {
+// Issues the copies of [src, src + bytes) into dst as whole aligned 16-byte chunks; returns the
+// byte offset of src inside dst. The chunks may reach 15 bytes past either end of the range:
+// every device array is allocated 256-byte aligned with 64 bytes of slack at its end.
+__device__ __forceinline__ int stage_async(const void* src, uint32_t bytes, char* dst, int lane) {
   uintptr_t a = reinterpret_cast<uintptr_t>(src);
   uintptr_t a0 = a & ~uintptr_t(15);
   int off = (int)(a - a0);
-  int chunks = (off + bytes + 15) >> 4;
-  const int4* g = reinterpret_cast<const int4*>(a0);
-  for (int c = lane; c < chunks; c += 32) dst[c] = __ldcs(g + c);
+  int chunks = (int)((off + bytes + 15) >> 4);
+  const char* g = reinterpret_cast<const char*>(a0);
+  for (int c = lane; c < chunks; c += 32) cp_async16(dst + 16 * c, g + 16 * c);
   return off;
 }
 
-template <typename V>
-__device__ __forceinline__ V ld_vec(const V* p) {
-  return __ldg(p);
+// A block matrix as the kernels read it. Each row group is described by {first row, end row,
+// first block, end block}, so a warp needs one 16-byte load to start staging a group.
+template <typename S>
+struct Op {
+  const uint32_t* __restrict__ starts;
+  const uint32_t* __restrict__ cols;
+  const S* __restrict__ vals;
+  const uint4* __restrict__ groups;
+  uint32_t ngroups;
+  uint32_t vbuf, cbuf, sbuf;  // bytes of one value / column / row-start staging buffer
+};
+
+template <typename S>
+Op<S> op_of(const DevBsr& m) {
+  Op<S> o;
+  o.starts = m.starts;
+  o.cols = m.cols;
+  o.vals = (const S*)m.vals;
+  o.groups = m.groups;
+  o.ngroups = m.ngroups;
+  o.vbuf = (m.group_bytes + 31) & ~15u;
+  o.cbuf = (m.group_blocks * 4 + 31) & ~15u;
+  o.sbuf = ((m.group_rows + 1) * 4 + 31) & ~15u;
+  return o;
 }
 
-// The RB sums of one block row of A x, in every lane of the warp.
-template <typename S, typename V, int RB, int CB>
-__device__ __forceinline__ void warp_row_product(const uint32_t* __restrict__ starts,
-                                                 const uint32_t* __restrict__ cols,
-                                                 const S* __restrict__ vals,
-                                                 const V* __restrict__ x, uint32_t row, int lane,
-                                                 int4* sbuf, V acc[RB]) {
+template <typename S>
+__host__ __device__ __forceinline__ uint32_t slot_bytes(const Op<S>& A) {
+  return A.vbuf + A.cbuf + A.sbuf;
+}
+
+// Walks this warp's row groups. Per row (one team of LPR lanes each) it calls epi.pre(row, live,
+// lane) before the row's blocks are read, so the epilogue's own loads overlap the gathers, and
+// epi.post(row, live, sums[RB], mag[RB], lane) after the team's fixed butterfly, in every lane.
+// With MAG it also sums |a_ij x_j| per row (the rounding floor of pcg.rs:246-248). A group is
+// staged one grid-stride step ahead (double buffer), its descriptor two steps ahead.
+template <typename S, typename V, int RB, int CB, int LPR, bool MAG, class Epi>
+__device__ __forceinline__ void run_groups(const Op<S>& A, const V* __restrict__ x, char* wbase, Epi& epi) {
   constexpr int LEN = RB * CB;
-#pragma unroll
-  for (int p = 0; p < RB; ++p) acc[p] = V(0);
-  uint32_t s = starts[row], e = starts[row + 1];
-  for (uint32_t base = s; base < e; base += kBlocksPerPass) {
-    int count = (int)min((uint32_t)kBlocksPerPass, e - base);
-    int off = stage_slab(vals + (size_t)base * LEN, count * LEN * (int)sizeof(S), sbuf, lane);
-    uint32_t c = lane < count ? __ldcs(cols + base + lane) : 0u;
+  constexpr int TEAMS = 32 / LPR;
+  const int lane = threadIdx.x & 31;
+  const int team = lane / LPR, tl = lane % LPR;
+  const uint32_t nw = gridDim.x * (blockDim.x >> 5);
+  uint32_t g = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const uint32_t sb = slot_bytes(A);
+  int vo0 = 0, vo1 = 0, co0 = 0, co1 = 0, so0 = 0, so1 = 0;
+  auto issue = [&](const uint4& d, int slot) {
+    char* base = wbase + slot * sb;
+    int vo = stage_async(A.vals + (size_t)d.z * LEN, (d.w - d.z) * LEN * (uint32_t)sizeof(S), base, lane);
+    int co = stage_async(A.cols + d.z, (d.w - d.z) * 4u, base + A.vbuf, lane);
+    int so = stage_async(A.starts + d.x, (d.y - d.x + 1) * 4u, base + A.vbuf + A.cbuf, lane);
+    if (slot) {
+      vo1 = vo;
+      co1 = co;
+      so1 = so;
+    } else {
+      vo0 = vo;
+      co0 = co;
+      so0 = so;
+    }
+  };
+  const uint4 none = make_uint4(0, 0, 0, 0);
+  uint4 cur = g < A.ngroups ? A.groups[g] : none;
+  uint4 nxt = g + nw < A.ngroups ? A.groups[g + nw] : none;
+  if (g < A.ngroups) issue(cur, 0);
+  cp_async_commit();
+  for (int k = 0; g < A.ngroups; ++k, g += nw) {
+    const int slot = k & 1;
+    const bool has_next = g + nw < A.ngroups;
+    if (has_next) issue(nxt, slot ^ 1);
+    uint4 after = g + 2 * nw < A.ngroups ? A.groups[g + 2 * nw] : none;
+    cp_async_commit();
+    cp_async_wait_one();
     __syncwarp();
-    if (lane < count) {
-      const S* blk = reinterpret_cast<const S*>(reinterpret_cast<const char*>(sbuf) + off) + lane * LEN;
-      V xv[CB];
+    char* base = wbase + slot * sb;
+    const S* vals = reinterpret_cast<const S*>(base + (slot ? vo1 : vo0));
+    const uint32_t* cols = reinterpret_cast<const uint32_t*>(base + A.vbuf + (slot ? co1 : co0));
+    const uint32_t* rst = reinterpret_cast<const uint32_t*>(base + A.vbuf + A.cbuf + (slot ? so1 : so0));
+    const uint32_t nrows = cur.y - cur.x;
+    for (uint32_t rb = 0; rb < nrows; rb += TEAMS) {
+      const uint32_t lr = rb + team;
+      const bool live = lr < nrows;
+      const uint32_t row = cur.x + (live ? lr : 0);
+      epi.pre(row, live, tl);
+      V acc[RB], mag[RB];
 #pragma unroll
-      for (int q = 0; q < CB; ++q) xv[q] = ld_vec(x + (size_t)c * CB + q);
+      for (int p = 0; p < RB; ++p) acc[p] = mag[p] = V(0);
+      if (live) {
+        const uint32_t b0 = rst[lr] - cur.z, b1 = rst[lr + 1] - cur.z;
+        for (uint32_t j = b0 + tl; j < b1; j += 2 * LPR) {
+          const uint32_t j2 = j + LPR;
+          const bool two = j2 < b1;
+          const uint32_t c0 = cols[j], c1 = two ? cols[j2] : c0;
+          V xa[CB], xb[CB];
+#pragma unroll
+          for (int q = 0; q < CB; ++q) {
+            xa[q] = __ldg(x + (size_t)c0 * CB + q);
+            xb[q] = __ldg(x + (size_t)c1 * CB + q);
+          }
+          const S* ba = vals + (size_t)j * LEN;
+          const S* bb = vals + (size_t)(two ? j2 : j) * LEN;
+#pragma unroll
+          for (int p = 0; p < RB; ++p)
+#pragma unroll
+            for (int q = 0; q < CB; ++q) {
+              V t = V(ba[p * CB + q]) * xa[q];
+              acc[p] += t;
+              if (MAG) mag[p] += fabs(t);
+            }
+          if (two) {
+#pragma unroll
+            for (int p = 0; p < RB; ++p)
+#pragma unroll
+              for (int q = 0; q < CB; ++q) {
+                V t = V(bb[p * CB + q]) * xb[q];
+                acc[p] += t;
+                if (MAG) mag[p] += fabs(t);
+              }
+          }
+        }
+      }
+      __syncwarp();
 #pragma unroll
       for (int p = 0; p < RB; ++p)
 #pragma unroll
-        for (int q = 0; q < CB; ++q) acc[p] += V(blk[p * CB + q]) * xv[q];
+        for (int o = LPR / 2; o > 0; o >>= 1) {
+          acc[p] += __shfl_xor_sync(kFull, acc[p], o);
+          if (MAG) mag[p] += __shfl_xor_sync(kFull, mag[p], o);
+        }
+      epi.post(row, live, acc, mag, tl);
     }
     __syncwarp();
+    cur = nxt;
+    nxt = after;
   }
-#pragma unroll
-  for (int p = 0; p < RB; ++p)
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) acc[p] += __shfl_xor_sync(kFull, acc[p], o);
+  cp_async_wait_all();
 }
 
 template <typename V, int RB>
-__device__ __forceinline__ V select_lane(const V acc[RB], int lane) {
-  V v = acc[0];
+__device__ __forceinline__ V pick(const V (&v)[RB], int p) {
+  V out = v[0];
 #pragma unroll
-  for (int p = 1; p < RB; ++p)
-    if (lane == p) v = acc[p];
-  return v;
+  for (int q = 1; q < RB; ++q)
+    if (p == q) out = v[q];
+  return out;
 }
+
+// The components p = lane, lane + LPR, ... < RB of a row this lane finishes.
+template <int RB, int LPR>
+struct Parts {
+  static constexpr int N = (RB + LPR - 1) / LPR;
+};
 
 enum { OP_SET = 0, OP_RESIDUAL = 1, OP_ADD = 2 };
 
-// y = A x (OP_SET), y = b - A x (OP_RESIDUAL), y = y + A x (OP_ADD).
-template <typename S, typename V, int RB, int CB, int OP>
-__global__ void __launch_bounds__(kThreads) bsr_kernel(uint32_t rows, const uint32_t* __restrict__ starts,
-                                                       const uint32_t* __restrict__ cols,
-                                                       const S* __restrict__ vals, const V* __restrict__ x,
-                                                       V* __restrict__ y, const V* __restrict__ b,
-                                                       const int* __restrict__ status) {
-  if (*status != ST_ACTIVE) return;
-  extern __shared__ int4 smem[];
-  int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  int4* sbuf = smem + warp * Slab<S, RB, CB>::kInt4;
-  uint32_t nw = gridDim.x * kWarps;
-  for (uint32_t row = blockIdx.x * kWarps + warp; row < rows; row += nw) {
-    V acc[RB];
-    warp_row_product<S, V, RB, CB>(starts, cols, vals, x, row, lane, sbuf, acc);
-    if (lane < RB) {
-      V sum = select_lane<V, RB>(acc, lane);
-      size_t i = (size_t)row * RB + lane;
-      if (OP == OP_SET) y[i] = sum;
-      if (OP == OP_RESIDUAL) y[i] = b[i] - sum;
-      if (OP == OP_ADD) y[i] = y[i] + sum;
+// y = A x, y = b - A x, or y = y + A x.
+template <typename V, int RB, int LPR, int OP>
+struct EpiAxpy {
+  V* __restrict__ y;
+  const V* __restrict__ b;
+  V in[Parts<RB, LPR>::N];
+  __device__ __forceinline__ void pre(uint32_t row, bool live, int tl) {
+    if (OP == OP_SET || !live) return;
+#pragma unroll
+    for (int k = 0; k < Parts<RB, LPR>::N; ++k) {
+      int p = tl + k * LPR;
+      if (p < RB) in[k] = OP == OP_RESIDUAL ? b[(size_t)row * RB + p] : y[(size_t)row * RB + p];
     }
   }
+  __device__ __forceinline__ void post(uint32_t row, bool live, const V (&acc)[RB], const V (&)[RB], int tl) {
+    if (!live) return;
+#pragma unroll
+    for (int k = 0; k < Parts<RB, LPR>::N; ++k) {
+      int p = tl + k * LPR;
+      if (p >= RB) continue;
+      size_t i = (size_t)row * RB + p;
+      V sum = pick<V, RB>(acc, p);
+      if (OP == OP_SET) y[i] = sum;
+      if (OP == OP_RESIDUAL) y[i] = in[k] - sum;
+      if (OP == OP_ADD) y[i] = in[k] + sum;
+    }
+  }
+};
+
+template <typename S, typename V, int RB, int CB, int LPR, int OP>
+__global__ void __launch_bounds__(kThreads) bsr_kernel(Op<S> A, const V* __restrict__ x, V* __restrict__ y,
+                                                       const V* __restrict__ b, const int* __restrict__ status) {
+  if (*status != ST_ACTIVE) return;
+  extern __shared__ __align__(16) char smem[];
+  char* wbase = smem + (threadIdx.x >> 5) * 2 * slot_bytes(A);
+  EpiAxpy<V, RB, LPR, OP> epi{y, b, {}};
+  run_groups<S, V, RB, CB, LPR, false>(A, x, wbase, epi);
 }
 
 // One Chebyshev step fused with its product (cycle.rs:611-650): ad = A d_old; r -= ad;
 // z = D^-1 r; d_new = keep d_old + step z; x += d_new. With `outer` set (the last step of the
-// post-smoother) the smoothed correction is added straight into the level's x:
-// outer += (x + d_new), the reference's post_x += d then x += post_x (cycle.rs:533-536).
-template <typename S, typename V, int RB>
-__global__ void __launch_bounds__(kThreads) cheb_step_kernel(
-    uint32_t rows, const uint32_t* __restrict__ starts, const uint32_t* __restrict__ cols,
-    const S* __restrict__ vals, const S* __restrict__ dinv, const V* __restrict__ d_old,
-    V* __restrict__ d_new, V* __restrict__ r, V* __restrict__ x, V* __restrict__ outer, V keep, V step,
-    const int* __restrict__ status) {
-  if (*status != ST_ACTIVE) return;
-  extern __shared__ int4 smem[];
-  int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  int4* sbuf = smem + warp * Slab<S, RB, RB>::kInt4;
-  uint32_t nw = gridDim.x * kWarps;
-  for (uint32_t row = blockIdx.x * kWarps + warp; row < rows; row += nw) {
-    V acc[RB];
-    warp_row_product<S, V, RB, RB>(starts, cols, vals, d_old, row, lane, sbuf, acc);
-    size_t base = (size_t)row * RB;
+// post-smoother) the smoothed correction goes straight into the level's x: outer += (x + d_new),
+// the reference's post_x += d and then x += post_x (cycle.rs:533-536).
+template <typename S, typename V, int RB, int LPR>
+struct EpiCheb {
+  static constexpr int N = Parts<RB, LPR>::N;
+  const S* __restrict__ dinv;
+  const V* __restrict__ d_old;
+  V* __restrict__ d_new;
+  V* __restrict__ r;
+  V* __restrict__ x;
+  V* __restrict__ outer;
+  V keep, step;
+  V rv[RB];
+  V dv[N], xv[N], ov[N];
+  S di[N][RB];
+  __device__ __forceinline__ void pre(uint32_t row, bool live, int tl) {
+    if (!live) return;
+    const size_t base = (size_t)row * RB;
+#pragma unroll
+    for (int q = 0; q < RB; ++q) rv[q] = r[base + q];
+#pragma unroll
+    for (int k = 0; k < N; ++k) {
+      int p = tl + k * LPR;
+      if (p >= RB) continue;
+#pragma unroll
+      for (int q = 0; q < RB; ++q) di[k][q] = dinv[base * RB + p * RB + q];
+      dv[k] = d_old[base + p];
+      xv[k] = x[base + p];
+      if (outer) ov[k] = outer[base + p];
+    }
+  }
+  __device__ __forceinline__ void post(uint32_t row, bool live, const V (&acc)[RB], const V (&)[RB], int tl) {
+    if (!live) return;
+    const size_t base = (size_t)row * RB;
     V rn[RB];
 #pragma unroll
-    for (int q = 0; q < RB; ++q) rn[q] = r[base + q] - acc[q];
-    int p = lane < RB ? lane : 0;
-    V z = V(0);
+    for (int q = 0; q < RB; ++q) rn[q] = rv[q] - acc[q];
 #pragma unroll
-    for (int q = 0; q < RB; ++q) z += V(dinv[base * RB + p * RB + q]) * rn[q];
-    V dn = keep * d_old[base + p] + step * z;
-    V mine = select_lane<V, RB>(rn, p);
-    __syncwarp();
-    if (lane < RB) {
-      r[base + p] = mine;
+    for (int k = 0; k < N; ++k) {
+      int p = tl + k * LPR;
+      if (p >= RB) continue;
+      V z = V(0);
+#pragma unroll
+      for (int q = 0; q < RB; ++q) z += V(di[k][q]) * rn[q];
+      V dn = keep * dv[k] + step * z;
+      r[base + p] = pick<V, RB>(rn, p);
       d_new[base + p] = dn;
-      V xn = x[base + p] + dn;
+      V xn = xv[k] + dn;
       if (outer)
-        outer[base + p] = outer[base + p] + xn;
+        outer[base + p] = ov[k] + xn;
       else
         x[base + p] = xn;
     }
   }
+};
+
+template <typename S, typename V, int RB, int LPR>
+__global__ void __launch_bounds__(kThreads) cheb_step_kernel(Op<S> A, const S* __restrict__ dinv, const V* __restrict__ d_old,
+                                                             V* __restrict__ d_new, V* __restrict__ r, V* __restrict__ x,
+                                                             V* __restrict__ outer, V keep, V step,
+                                                             const int* __restrict__ status) {
+  if (*status != ST_ACTIVE) return;
+  extern __shared__ __align__(16) char smem[];
+  char* wbase = smem + (threadIdx.x >> 5) * 2 * slot_bytes(A);
+  EpiCheb<S, V, RB, LPR> epi;
+  epi.dinv = dinv;
+  epi.d_old = d_old;
+  epi.d_new = d_new;
+  epi.r = r;
+  epi.x = x;
+  epi.outer = outer;
+  epi.keep = keep;
+  epi.step = step;
+  run_groups<S, V, RB, RB, LPR, false>(A, d_old, wbase, epi);
 }
 
 // The smoother's start from a zero guess (cycle.rs:591-610): r = b; d = (D^-1 b) / theta; x = d.
@@ -195,6 +360,13 @@ __global__ void add_kernel(size_t n, V* __restrict__ x, const V* __restrict__ y,
   if (*status != ST_ACTIVE) return;
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
     x[i] = x[i] + y[i];
+}
+
+template <typename B, typename V>
+__global__ void convert_kernel(size_t n, const B* __restrict__ in, V* __restrict__ out, const int* __restrict__ status) {
+  if (*status != ST_ACTIVE) return;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    out[i] = V(in[i]);
 }
 
 // The coarsest level's direct solve as x = V(A^-1 widen(b)), one warp per row of the f64 inverse
@@ -256,29 +428,316 @@ __device__ __forceinline__ bool finish_partials(double (&v)[K], double* partials
   return true;
 }
 
-// ap = A p on the f64 system with the curvature p.ap; then alpha = rz / curvature
-// (pcg.rs:217-228).
-__global__ void __launch_bounds__(kThreads) pcg_spmv_dot_kernel(uint32_t rows, const uint32_t* __restrict__ starts,
-                                                                 const uint32_t* __restrict__ cols,
-                                                                 const double* __restrict__ vals,
-                                                                 const double* __restrict__ p, double* __restrict__ ap,
-                                                                 double* partials, PcgState* st) {
-  if (st->status != ST_ACTIVE) return;
-  extern __shared__ int4 smem[];
-  int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  int4* sbuf = smem + warp * Slab<double, 3, 3>::kInt4;
-  double local = 0.0;
-  for (uint32_t row = blockIdx.x * kWarps + warp; row < rows; row += gridDim.x * kWarps) {
-    double acc[3];
-    warp_row_product<double, double, 3, 3>(starts, cols, vals, p, row, lane, sbuf, acc);
-    if (lane < 3) {
-      double sum = select_lane<double, 3>(acc, lane);
-      size_t i = (size_t)row * 3 + lane;
-      ap[i] = sum;
-      local += p[i] * sum;
+// ------------------------------------------------------------ SELL-32: one thread per row
+// For operators with many rows (the finest level and the f64 system): a warp holds a slice of 32
+// rows of similar length, each thread sums its own row's blocks in column order, and every load
+// of a value plane or a column index is one coalesced 128-byte line. No shared memory, no
+// shuffles: the instruction stream is the blocks' FMAs plus their loads.
+template <typename S>
+struct SellOp {
+  const uint32_t* __restrict__ rows;
+  const uint32_t* __restrict__ len;
+  const uint32_t* __restrict__ start;
+  const uint32_t* __restrict__ cols;
+  const S* __restrict__ vals;
+  uint32_t nslices, nrows;
+};
+
+template <typename S>
+SellOp<S> sell_of(const DevBsr& m) {
+  SellOp<S> o;
+  o.rows = m.sell_rows;
+  o.len = m.sell_len;
+  o.start = m.sell_start;
+  o.cols = m.sell_cols;
+  o.vals = (const S*)m.sell_vals;
+  o.nslices = m.nslices;
+  o.nrows = m.rows;
+  return o;
+}
+
+template <typename S, typename V, int RB, int CB, bool MAG, class Epi>
+__device__ __forceinline__ void sell_rows(const SellOp<S>& A, const V* __restrict__ x, Epi& epi) {
+  constexpr int LEN = RB * CB;
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t warps = blockDim.x >> 5;
+  for (uint32_t s = blockIdx.x * warps + (threadIdx.x >> 5); s < A.nslices; s += gridDim.x * warps) {
+    const uint32_t slot = s * 32 + lane;
+    const uint32_t row = A.rows[slot];
+    const uint32_t n = A.len[slot];
+    const bool live = row < A.nrows;
+    epi.pre(row, live);
+    V acc[RB], mag[RB];
+#pragma unroll
+    for (int p = 0; p < RB; ++p) acc[p] = mag[p] = V(0);
+    const uint32_t base = A.start[s];
+    // U blocks per step: their column indices and values are loaded together (U * (LEN + 1)
+    // independent coalesced loads in flight per thread), then their x gathers, then the FMAs,
+    // still in column order, so the row's sum keeps its sequential order.
+    constexpr int U = (LEN <= 9 && sizeof(S) == 4) ? 4 : 2;
+    for (uint32_t k0 = 0; k0 < n; k0 += U) {
+      uint32_t c[U];
+      S v[U][LEN];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const bool in = k0 + u < n;
+        const uint32_t q0 = base + 32 * (k0 + (in ? u : 0));
+        c[u] = in ? __ldcs(A.cols + q0 + lane) : 0u;
+        const S* vp = A.vals + (size_t)q0 * LEN + lane;
+#pragma unroll
+        for (int e = 0; e < LEN; ++e) v[u][e] = in ? __ldcs(vp + 32 * e) : S(0);
+      }
+      V xv[U][CB];
+#pragma unroll
+      for (int u = 0; u < U; ++u)
+#pragma unroll
+        for (int q = 0; q < CB; ++q) xv[u][q] = k0 + u < n ? __ldg(x + (size_t)c[u] * CB + q) : V(0);
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        if (k0 + u >= n) break;
+#pragma unroll
+        for (int p = 0; p < RB; ++p)
+#pragma unroll
+          for (int q = 0; q < CB; ++q) {
+            V t = V(v[u][p * CB + q]) * xv[u][q];
+            acc[p] += t;
+            if (MAG) mag[p] += fabs(t);
+          }
+      }
+    }
+    epi.post(row, live, n, acc, mag);
+  }
+}
+
+template <typename V, int RB, int OP>
+struct SellAxpy {
+  V* __restrict__ y;
+  const V* __restrict__ b;
+  V in[RB];
+  __device__ __forceinline__ void pre(uint32_t row, bool live) {
+    if (OP == OP_SET || !live) return;
+#pragma unroll
+    for (int p = 0; p < RB; ++p) in[p] = OP == OP_RESIDUAL ? b[(size_t)row * RB + p] : y[(size_t)row * RB + p];
+  }
+  __device__ __forceinline__ void post(uint32_t row, bool live, uint32_t, const V (&acc)[RB], const V (&)[RB]) {
+    if (!live) return;
+#pragma unroll
+    for (int p = 0; p < RB; ++p) {
+      size_t i = (size_t)row * RB + p;
+      if (OP == OP_SET) y[i] = acc[p];
+      if (OP == OP_RESIDUAL) y[i] = in[p] - acc[p];
+      if (OP == OP_ADD) y[i] = in[p] + acc[p];
     }
   }
-  double v[1] = {local}, total[1];
+};
+
+template <typename S, typename V, int RB, int CB, int OP>
+__global__ void __launch_bounds__(kThreads) sell_kernel(SellOp<S> A, const V* __restrict__ x, V* __restrict__ y,
+                                                        const V* __restrict__ b, const int* __restrict__ status) {
+  if (*status != ST_ACTIVE) return;
+  SellAxpy<V, RB, OP> epi{y, b, {}};
+  sell_rows<S, V, RB, CB, false>(A, x, epi);
+}
+
+// The fused Chebyshev step of cheb_step_kernel, one thread per row.
+template <typename S, typename V, int RB>
+struct SellCheb {
+  const S* __restrict__ dinv;
+  const V* __restrict__ d_old;
+  V* __restrict__ d_new;
+  V* __restrict__ r;
+  V* __restrict__ x;
+  V* __restrict__ outer;
+  V keep, step;
+  // The row's own operands are loaded after its blocks: every thread already keeps several
+  // blocks' loads in flight, and holding these 21 values across the block loop would cost the
+  // registers of a resident block.
+  __device__ __forceinline__ void pre(uint32_t, bool) {}
+  __device__ __forceinline__ void post(uint32_t row, bool live, uint32_t, const V (&acc)[RB], const V (&)[RB]) {
+    if (!live) return;
+    const size_t base = (size_t)row * RB;
+    V rn[RB];
+#pragma unroll
+    for (int q = 0; q < RB; ++q) rn[q] = r[base + q] - acc[q];
+#pragma unroll
+    for (int p = 0; p < RB; ++p) {
+      V z = V(0);
+#pragma unroll
+      for (int q = 0; q < RB; ++q) z += V(dinv[base * RB + p * RB + q]) * rn[q];
+      V dn = keep * d_old[base + p] + step * z;
+      r[base + p] = rn[p];
+      d_new[base + p] = dn;
+      V xn = x[base + p] + dn;
+      if (outer)
+        outer[base + p] = outer[base + p] + xn;
+      else
+        x[base + p] = xn;
+    }
+  }
+};
+
+template <typename S, typename V, int RB>
+__global__ void __launch_bounds__(kThreads) sell_cheb_kernel(SellOp<S> A, const S* __restrict__ dinv,
+                                                             const V* __restrict__ d_old, V* __restrict__ d_new,
+                                                             V* __restrict__ r, V* __restrict__ x, V* __restrict__ outer,
+                                                             V keep, V step, const int* __restrict__ status) {
+  if (*status != ST_ACTIVE) return;
+  SellCheb<S, V, RB> epi;
+  epi.dinv = dinv;
+  epi.d_old = d_old;
+  epi.d_new = d_new;
+  epi.r = r;
+  epi.x = x;
+  epi.outer = outer;
+  epi.keep = keep;
+  epi.step = step;
+  sell_rows<S, V, RB, RB, false>(A, d_old, epi);
+}
+
+struct SellDot {
+  const double* __restrict__ p;
+  double* __restrict__ ap;
+  double local;
+  double pv[3];
+  __device__ __forceinline__ void pre(uint32_t row, bool live) {
+    if (!live) return;
+#pragma unroll
+    for (int q = 0; q < 3; ++q) pv[q] = p[(size_t)row * 3 + q];
+  }
+  __device__ __forceinline__ void post(uint32_t row, bool live, uint32_t, const double (&acc)[3], const double (&)[3]) {
+    if (!live) return;
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+      ap[(size_t)row * 3 + q] = acc[q];
+      local += pv[q] * acc[q];
+    }
+  }
+};
+
+__global__ void __launch_bounds__(kThreads) sell_pcg_spmv_dot_kernel(SellOp<double> A, const double* __restrict__ p,
+                                                                      double* __restrict__ ap, double* partials,
+                                                                      PcgState* st) {
+  if (st->status != ST_ACTIVE) return;
+  SellDot epi;
+  epi.p = p;
+  epi.ap = ap;
+  epi.local = 0.0;
+  sell_rows<double, double, 3, 3, false>(A, p, epi);
+  double v[1] = {epi.local}, total[1];
+  if (finish_partials<1>(v, partials, &st->tickets[0], total) && threadIdx.x == 0) {
+    double curvature = total[0];
+    st->curvature = curvature;
+    if (isnan(curvature) || curvature <= 0.0 || !isfinite(st->rz)) {
+      st->status = ST_FAILED_NOT_PD;
+      st->fail_iteration = st->iterations;
+    } else {
+      st->alpha = st->rz / curvature;
+    }
+  }
+}
+
+struct SellCheck {
+  const double* __restrict__ b;
+  double* __restrict__ r;
+  double res2, bound2;
+  double bv[3];
+  __device__ __forceinline__ void pre(uint32_t row, bool live) {
+    if (!live) return;
+#pragma unroll
+    for (int q = 0; q < 3; ++q) bv[q] = b[(size_t)row * 3 + q];
+  }
+  __device__ __forceinline__ void post(uint32_t row, bool live, uint32_t n, const double (&acc)[3], const double (&mag)[3]) {
+    if (!live) return;
+    const double eps = 2.220446049250313e-16;
+    double terms = (double)(n * 3);
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+      double res = bv[q] - acc[q];
+      r[(size_t)row * 3 + q] = res;
+      res2 += res * res;
+      double bound = terms * eps * mag[q];
+      bound2 += bound * bound;
+    }
+  }
+};
+
+__global__ void __launch_bounds__(kThreads) sell_pcg_check_kernel(SellOp<double> A, const double* __restrict__ x,
+                                                                   const double* __restrict__ b, double* __restrict__ r,
+                                                                   double* partials, PcgState* st) {
+  if (st->status != ST_ACTIVE || st->mode != MODE_CHECK) return;
+  SellCheck epi;
+  epi.b = b;
+  epi.r = r;
+  epi.res2 = 0.0;
+  epi.bound2 = 0.0;
+  sell_rows<double, double, 3, 3, true>(A, x, epi);
+  double v[2] = {epi.res2, epi.bound2}, total[2];
+  if (finish_partials<2>(v, partials, &st->tickets[2], total) && threadIdx.x == 0) {
+    double rel = sqrt(total[0]) / st->rhs_norm;
+    double floor = sqrt(total[1]) / st->rhs_norm;
+    st->rel = rel;
+    st->floor = floor;
+    st->at_floor = (rel > st->tolerance && rel <= floor) ? 1 : 0;
+    if (rel <= st->tolerance || st->at_floor)
+      st->status = ST_CONVERGED;
+    else
+      st->mode = MODE_RESTART;
+  }
+}
+
+// Places each block of a device-resident BSR matrix at its SELL position.
+template <typename S, int LEN>
+__global__ void sell_permute_kernel(size_t blocks, const uint32_t* __restrict__ pos, const S* __restrict__ in,
+                                    S* __restrict__ out) {
+  for (size_t b = blockIdx.x * (size_t)blockDim.x + threadIdx.x; b < blocks; b += (size_t)gridDim.x * blockDim.x) {
+    uint32_t q = pos[b], t = q & 31u;
+    size_t base = (size_t)(q - t) * LEN + t;
+#pragma unroll
+    for (int e = 0; e < LEN; ++e) out[base + 32 * e] = in[b * LEN + e];
+  }
+}
+
+// ap = A p with the curvature p.ap.
+template <int LPR>
+struct EpiDot {
+  static constexpr int N = Parts<3, LPR>::N;
+  const double* __restrict__ p;
+  double* __restrict__ ap;
+  double local;
+  double pv[N];
+  __device__ __forceinline__ void pre(uint32_t row, bool live, int tl) {
+    if (!live) return;
+#pragma unroll
+    for (int k = 0; k < N; ++k)
+      if (tl + k * LPR < 3) pv[k] = p[(size_t)row * 3 + tl + k * LPR];
+  }
+  __device__ __forceinline__ void post(uint32_t row, bool live, const double (&acc)[3], const double (&)[3], int tl) {
+    if (!live) return;
+#pragma unroll
+    for (int k = 0; k < N; ++k) {
+      int q = tl + k * LPR;
+      if (q >= 3) continue;
+      double sum = pick<double, 3>(acc, q);
+      ap[(size_t)row * 3 + q] = sum;
+      local += pv[k] * sum;
+    }
+  }
+};
+
+// ap = A p on the f64 system with the curvature p.ap; then alpha = rz / curvature
+// (pcg.rs:217-228).
+template <int LPR>
+__global__ void __launch_bounds__(kThreads) pcg_spmv_dot_kernel(Op<double> A, const double* __restrict__ p,
+                                                                 double* __restrict__ ap, double* partials, PcgState* st) {
+  if (st->status != ST_ACTIVE) return;
+  extern __shared__ __align__(16) char smem[];
+  char* wbase = smem + (threadIdx.x >> 5) * 2 * slot_bytes(A);
+  EpiDot<LPR> epi;
+  epi.p = p;
+  epi.ap = ap;
+  epi.local = 0.0;
+  run_groups<double, double, 3, 3, LPR, false>(A, p, wbase, epi);
+  double v[1] = {epi.local}, total[1];
   if (finish_partials<1>(v, partials, &st->tickets[0], total) && threadIdx.x == 0) {
     double curvature = total[0];
     st->curvature = curvature;
@@ -313,46 +772,56 @@ __global__ void __launch_bounds__(kThreads) pcg_update_kernel(uint32_t n, const 
   }
 }
 
-// The true residual when the recursive one reports convergence, with the rounding floor of the
-// product (pcg.rs:234-255, csr.rs:142-154): r = b - A x; converge, or restart from it.
-__global__ void __launch_bounds__(kThreads) pcg_check_kernel(uint32_t rows, const uint32_t* __restrict__ starts,
-                                                              const uint32_t* __restrict__ cols,
-                                                              const double* __restrict__ vals,
-                                                              const double* __restrict__ x, const double* __restrict__ b,
-                                                              double* __restrict__ r, double* partials, PcgState* st) {
-  if (st->status != ST_ACTIVE || st->mode != MODE_CHECK) return;
-  extern __shared__ int4 smem[];
-  int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  int4* sbuf = smem + warp * Slab<double, 3, 3>::kInt4;
-  double res2 = 0.0, bound2 = 0.0;
-  const double eps = 2.220446049250313e-16;
-  for (uint32_t row = blockIdx.x * kWarps + warp; row < rows; row += gridDim.x * kWarps) {
-    double acc[3];
-    warp_row_product<double, double, 3, 3>(starts, cols, vals, x, row, lane, sbuf, acc);
-    // |a_ij x_j| row sums for the floor: a second pass over the staged row.
-    double mag[3] = {0.0, 0.0, 0.0};
-    uint32_t s = starts[row], e = starts[row + 1];
-    for (uint32_t at = s + lane; at < e; at += 32) {
-      uint32_t c = cols[at];
-      const double* blk = vals + (size_t)at * 9;
+// r = b - A x with the rounding-floor row bounds (csr.rs:142-154).
+template <int LPR>
+struct EpiCheck {
+  static constexpr int N = Parts<3, LPR>::N;
+  const double* __restrict__ b;
+  double* __restrict__ r;
+  const uint32_t* __restrict__ starts;
+  double res2, bound2;
+  double bv[N];
+  __device__ __forceinline__ void pre(uint32_t row, bool live, int tl) {
+    if (!live) return;
 #pragma unroll
-      for (int pp = 0; pp < 3; ++pp)
+    for (int k = 0; k < N; ++k)
+      if (tl + k * LPR < 3) bv[k] = b[(size_t)row * 3 + tl + k * LPR];
+  }
+  __device__ __forceinline__ void post(uint32_t row, bool live, const double (&acc)[3], const double (&mag)[3], int tl) {
+    if (!live) return;
+    const double eps = 2.220446049250313e-16;
+    double terms = (double)((starts[row + 1] - starts[row]) * 3);
 #pragma unroll
-        for (int q = 0; q < 3; ++q) mag[pp] += fabs(blk[pp * 3 + q] * x[(size_t)c * 3 + q]);
-    }
-#pragma unroll
-    for (int pp = 0; pp < 3; ++pp)
-      for (int o = 16; o > 0; o >>= 1) mag[pp] += __shfl_xor_sync(kFull, mag[pp], o);
-    if (lane < 3) {
-      size_t i = (size_t)row * 3 + lane;
-      double res = b[i] - select_lane<double, 3>(acc, lane);
+    for (int k = 0; k < N; ++k) {
+      int q = tl + k * LPR;
+      if (q >= 3) continue;
+      size_t i = (size_t)row * 3 + q;
+      double res = bv[k] - pick<double, 3>(acc, q);
       r[i] = res;
       res2 += res * res;
-      double bound = (double)((e - s) * 3) * eps * select_lane<double, 3>(mag, lane);
+      double bound = terms * eps * pick<double, 3>(mag, q);
       bound2 += bound * bound;
     }
   }
-  double v[2] = {res2, bound2}, total[2];
+};
+
+// The true residual when the recursive one reports convergence, with the rounding floor of the
+// product (pcg.rs:234-255): r = b - A x; converge, or restart from it.
+template <int LPR>
+__global__ void __launch_bounds__(kThreads) pcg_check_kernel(Op<double> A, const double* __restrict__ x,
+                                                              const double* __restrict__ b, double* __restrict__ r,
+                                                              double* partials, PcgState* st) {
+  if (st->status != ST_ACTIVE || st->mode != MODE_CHECK) return;
+  extern __shared__ __align__(16) char smem[];
+  char* wbase = smem + (threadIdx.x >> 5) * 2 * slot_bytes(A);
+  EpiCheck<LPR> epi;
+  epi.b = b;
+  epi.r = r;
+  epi.starts = A.starts;
+  epi.res2 = 0.0;
+  epi.bound2 = 0.0;
+  run_groups<double, double, 3, 3, LPR, true>(A, x, wbase, epi);
+  double v[2] = {epi.res2, epi.bound2}, total[2];
   if (finish_partials<2>(v, partials, &st->tickets[2], total) && threadIdx.x == 0) {
     double rel = sqrt(total[0]) / st->rhs_norm;
     double floor = sqrt(total[1]) / st->rhs_norm;
@@ -437,39 +906,88 @@ __global__ void jacobi_kernel(uint32_t n, const double* __restrict__ inv, const 
 // ------------------------------------------------------------ launch helpers
 int g_sm_count = 0;
 
-int grid_for_rows(size_t rows_per_unit_work) {
+int sm_count() {
   if (g_sm_count == 0) {
     int dev = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&g_sm_count, cudaDevAttrMultiProcessorCount, dev);
     if (g_sm_count <= 0) g_sm_count = 148;
   }
-  size_t blocks = (rows_per_unit_work + kWarps - 1) / kWarps;
-  size_t cap = (size_t)g_sm_count * 8;
-  return (int)std::max<size_t>(1, std::min(blocks, cap));
+  return g_sm_count;
 }
 
 int grid_for_elems(size_t n) {
   size_t blocks = (n + kThreads - 1) / kThreads;
-  size_t cap = (size_t)(g_sm_count ? g_sm_count : 148) * 8;
+  size_t cap = (size_t)sm_count() * 8;
   return (int)std::max<size_t>(1, std::min(blocks, cap));
 }
 
+int grid_for_rows(size_t rows) {
+  size_t blocks = (rows + kWarps - 1) / kWarps;
+  return (int)std::max<size_t>(1, std::min(blocks, (size_t)sm_count() * 8));
+}
+
+// Launch shape of a grouped product: warps per block so a block stages at most about 72 KB, and
+// a grid of whole waves (resident blocks per SM times SMs), never more warps than groups.
+struct Shape {
+  int threads, grid;
+  size_t smem;
+};
+
+template <typename S>
+Shape shape_of(const Op<S>& A, bool reduction) {
+  size_t per_warp = 2 * (size_t)slot_bytes(A);
+  int warps = (int)std::max<size_t>(1, std::min<size_t>(kWarps, kSmemPerBlockTarget / per_warp));
+  size_t smem = per_warp * warps;
+  // 228 KB of shared memory per SM, 1 KB of it reserved per resident block.
+  int per_sm = (int)std::max<size_t>(1, std::min<size_t>(2048 / (32 * warps), (228 * 1024) / (smem + 1024)));
+  size_t want = (A.ngroups + warps - 1) / warps;
+  size_t grid = std::min<size_t>(want, (size_t)sm_count() * per_sm);
+  if (reduction) grid = std::min<size_t>((size_t)sm_count() * per_sm, (size_t)kReduceBlocks * 2);
+  return {32 * warps, (int)std::max<size_t>(1, grid), smem};
+}
+
+// Lets a kernel use up to 200 KB of dynamic shared memory; called once per kernel, before any
+// capture (the first launches happen in the solver's initial reset).
 template <typename K>
-void smem_opt_in(K kernel, int bytes) {
-  if (bytes > 48 * 1024) cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+void smem_opt_in(K kernel, bool& done) {
+  if (done) return;
+  cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  done = true;
+}
+
+template <typename S, typename V, int RB, int CB, int LPR, int OP>
+void launch_bsr_lpr(const DevBsr& m, const V* x, V* y, const V* b, const int* status, cudaStream_t st) {
+  Op<S> A = op_of<S>(m);
+  Shape sh = shape_of(A, false);
+  auto k = bsr_kernel<S, V, RB, CB, LPR, OP>;
+  static bool opted = false;
+  smem_opt_in(k, opted);
+  k<<<sh.grid, sh.threads, sh.smem, st>>>(A, x, y, b, status);
+}
+
+int grid_for_slices(uint32_t nslices) {
+  size_t blocks = (nslices + kWarps - 1) / kWarps;
+  return (int)std::max<size_t>(1, std::min<size_t>(blocks, (size_t)sm_count() * 8));
+}
+
+template <typename S, typename V, int RB, int CB, int OP>
+void launch_sell(const DevBsr& m, const V* x, V* y, const V* b, const int* status, cudaStream_t st) {
+  sell_kernel<S, V, RB, CB, OP><<<grid_for_slices(m.nslices), kThreads, 0, st>>>(sell_of<S>(m), x, y, b, status);
 }
 
 template <typename S, typename V, int RB, int CB, int OP>
 void launch_bsr(const DevBsr& m, const V* x, V* y, const V* b, const int* status, cudaStream_t st) {
-  int smem = kWarps * Slab<S, RB, CB>::kInt4 * 16;
-  auto k = bsr_kernel<S, V, RB, CB, OP>;
-  static bool opted = false;
-  if (!opted) {
-    smem_opt_in(k, smem);
-    opted = true;
+  if (m.sell) {
+    launch_sell<S, V, RB, CB, OP>(m, x, y, b, status, st);
+    return;
   }
-  k<<<grid_for_rows(m.rows), kThreads, smem, st>>>(m.rows, m.starts, m.cols, (const S*)m.vals, x, y, b, status);
+  switch (m.lanes_per_row) {
+    case 4: launch_bsr_lpr<S, V, RB, CB, 4, OP>(m, x, y, b, status, st); break;
+    case 8: launch_bsr_lpr<S, V, RB, CB, 8, OP>(m, x, y, b, status, st); break;
+    case 16: launch_bsr_lpr<S, V, RB, CB, 16, OP>(m, x, y, b, status, st); break;
+    default: launch_bsr_lpr<S, V, RB, CB, 32, OP>(m, x, y, b, status, st); break;
+  }
 }
 
 template <typename S, typename V, int RB, int OP>
@@ -488,19 +1006,31 @@ void bsr_dispatch(const DevBsr& m, const V* x, V* y, const V* b, const int* stat
     bsr_dispatch_cb<S, V, 6, OP>(m, x, y, b, status, st);
 }
 
+template <typename S, typename V, int RB, int LPR>
+void launch_cheb_step_lpr(const DevLevel& L, const V* d_old, V* d_new, V* r, V* x, V* outer, double keep, double step,
+                          const int* status, cudaStream_t st) {
+  Op<S> A = op_of<S>(L.a);
+  Shape sh = shape_of(A, false);
+  auto k = cheb_step_kernel<S, V, RB, LPR>;
+  static bool opted = false;
+  smem_opt_in(k, opted);
+  k<<<sh.grid, sh.threads, sh.smem, st>>>(A, (const S*)L.dinv, d_old, d_new, r, x, outer, (V)keep, (V)step, status);
+}
+
 template <typename S, typename V, int RB>
 void launch_cheb_step(const DevLevel& L, const V* d_old, V* d_new, V* r, V* x, V* outer, double keep, double step,
                       const int* status, cudaStream_t st) {
-  int smem = kWarps * Slab<S, RB, RB>::kInt4 * 16;
-  auto k = cheb_step_kernel<S, V, RB>;
-  static bool opted = false;
-  if (!opted) {
-    smem_opt_in(k, smem);
-    opted = true;
+  if (L.a.sell) {
+    sell_cheb_kernel<S, V, RB><<<grid_for_slices(L.a.nslices), kThreads, 0, st>>>(
+        sell_of<S>(L.a), (const S*)L.dinv, d_old, d_new, r, x, outer, (V)keep, (V)step, status);
+    return;
   }
-  k<<<grid_for_rows(L.a.rows), kThreads, smem, st>>>(L.a.rows, L.a.starts, L.a.cols, (const S*)L.a.vals,
-                                                     (const S*)L.dinv, d_old, d_new, r, x, outer, (V)keep, (V)step,
-                                                     status);
+  switch (L.a.lanes_per_row) {
+    case 4: launch_cheb_step_lpr<S, V, RB, 4>(L, d_old, d_new, r, x, outer, keep, step, status, st); break;
+    case 8: launch_cheb_step_lpr<S, V, RB, 8>(L, d_old, d_new, r, x, outer, keep, step, status, st); break;
+    case 16: launch_cheb_step_lpr<S, V, RB, 16>(L, d_old, d_new, r, x, outer, keep, step, status, st); break;
+    default: launch_cheb_step_lpr<S, V, RB, 32>(L, d_old, d_new, r, x, outer, keep, step, status, st); break;
+  }
 }
 
 template <typename S, typename V, typename B, int RB>
@@ -537,18 +1067,18 @@ void enqueue_smooth(DeviceSolver& s, DevLevel& L, const B* b_in, V* b_out, V* x,
   }
 }
 
-// One V-cycle from level `li` (cycle.rs:461-539). B is the type of the right-hand side.
+// One V-cycle from level `li` (cycle.rs:461-539). B is the type of the right-hand side; an f64
+// right-hand side reaching an f32 level is rounded into b_store first.
 template <typename S, typename V, typename B>
 void enqueue_cycle(DeviceSolver& s, size_t li, const B* rhs, V* b_store, V* x, const int* status) {
   DevLevel& L = s.levels[li];
   cudaStream_t st = s.stream;
-  // The level's right-hand side in V: rounded into b_store when it arrives as another type.
   if (!L.has_p) {
     if (L.has_factor) {
       const V* bv = (const V*)rhs;
       if (b_store) {
-        // An f64 right-hand side reaching an f32 coarsest level directly (a one-level hierarchy).
-        enqueue_smooth<S, V, B>(s, L, rhs, b_store, (V*)L.tmp, nullptr, status);
+        convert_kernel<B, V><<<grid_for_elems(L.n), kThreads, 0, st>>>(L.n, rhs, b_store, status);
+        s.launches_per_iteration++;
         bv = b_store;
       }
       coarse_solve_kernel<V><<<grid_for_rows(L.n), kThreads, 0, st>>>(L.n, L.coarse_inverse, bv, x, status);
@@ -587,6 +1117,20 @@ void enqueue_precondition(DeviceSolver& s, const double* r, double* z, float* z3
     enqueue_cycle<float, float, double>(s, 0, r, (float*)L0.b, z32, status);
 }
 
+template <int LPR>
+void launch_pcg_spmv_lpr(DeviceSolver& s) {
+  Op<double> A = op_of<double>(s.system);
+  Shape sh = shape_of(A, true);
+  auto k = pcg_spmv_dot_kernel<LPR>;
+  static bool opted = false, opted_check = false;
+  smem_opt_in(k, opted);
+  k<<<sh.grid, sh.threads, sh.smem, s.stream>>>(A, s.p, s.ap, s.partials, s.state);
+  auto c = pcg_check_kernel<LPR>;
+  smem_opt_in(c, opted_check);
+  pcg_update_kernel<<<kReduceBlocks, kReduceThreads, 0, s.stream>>>(s.n, s.p, s.ap, s.x, s.r, s.partials, s.state);
+  c<<<sh.grid, sh.threads, sh.smem, s.stream>>>(A, s.x, s.rhs, s.r, s.partials, s.state);
+}
+
 }  // namespace
 
 sf_status cuda_check(cudaError_t e, const char* what) {
@@ -618,6 +1162,136 @@ void dev_free_all(DeviceSolver& s) {
   s.bytes = 0;
 }
 
+sf_status make_row_groups(DeviceSolver& s, DevBsr& m, const uint32_t* starts, size_t value_bytes) {
+  // Rows per group: as many mean rows as fit kGroupTarget bytes (1 to 8, a power of two). The
+  // warp splits into that many teams of 32 / teams lanes, one row each, so a warp works on several
+  // light rows at once (their x gathers and epilogue loads overlap) and on a heavy row whole.
+  double mean = m.rows ? (double)starts[m.rows] / m.rows : 0.0;
+  double row_bytes = std::max(1.0, mean * (double)value_bytes);
+  int teams = 1;
+  while (teams < 8 && (teams * 2) * row_bytes <= kGroupTarget) teams *= 2;
+  m.lanes_per_row = 32 / teams;
+  size_t target = std::min<size_t>(kGroupTarget, (size_t)(teams * row_bytes * 1.15));
+  std::vector<uint4> g;
+  g.reserve(m.rows / 2 + 2);
+  uint32_t max_bytes = 0, max_blocks = 0, max_rows = 0;
+  uint32_t r = 0;
+  while (r < m.rows) {
+    uint32_t e = r + 1;
+    size_t bytes = (size_t)(starts[e] - starts[r]) * value_bytes;
+    while (e < m.rows && bytes + (size_t)(starts[e + 1] - starts[e]) * value_bytes <= target) {
+      bytes += (size_t)(starts[e + 1] - starts[e]) * value_bytes;
+      ++e;
+    }
+    max_bytes = std::max<uint32_t>(max_bytes, (uint32_t)bytes);
+    max_blocks = std::max<uint32_t>(max_blocks, starts[e] - starts[r]);
+    max_rows = std::max<uint32_t>(max_rows, e - r);
+    g.push_back(make_uint4(r, e, starts[r], starts[e]));
+    r = e;
+  }
+  m.ngroups = (uint32_t)g.size();
+  m.group_bytes = max_bytes;
+  m.group_blocks = max_blocks;
+  m.group_rows = max_rows;
+  if (sf_status e = dev_alloc(s, (void**)&m.groups, std::max<size_t>(1, g.size()) * sizeof(uint4))) return e;
+  if (!g.empty()) copy_h2d(s, m.groups, g.data(), g.size() * sizeof(uint4));
+  return cuda_check(cudaStreamSynchronize(s.stream), "row groups");
+}
+
+namespace {
+
+struct SellLayout {
+  uint32_t nslices = 0;
+  std::vector<uint32_t> rows, len, start, pos, cols;
+};
+
+// Rows sorted by descending block count inside windows of kSellWindow rows (stable, so equal
+// lengths keep row order), cut into slices of 32; pos[b] is the SELL block index of BSR block b.
+SellLayout sell_layout(uint32_t nrows, const uint32_t* starts, const uint32_t* cols) {
+  SellLayout L;
+  L.nslices = (nrows + 31) / 32;
+  std::vector<uint32_t> order(nrows);
+  for (uint32_t i = 0; i < nrows; ++i) order[i] = i;
+  auto rlen = [&](uint32_t r) { return starts[r + 1] - starts[r]; };
+  for (uint32_t w0 = 0; w0 < nrows; w0 += kSellWindow) {
+    uint32_t w1 = std::min(nrows, w0 + kSellWindow);
+    std::stable_sort(order.begin() + w0, order.begin() + w1, [&](uint32_t a, uint32_t b) { return rlen(a) > rlen(b); });
+  }
+  L.rows.assign((size_t)L.nslices * 32, nrows);
+  L.len.assign((size_t)L.nslices * 32, 0);
+  L.start.assign(L.nslices + 1, 0);
+  for (uint32_t i = 0; i < nrows; ++i) {
+    L.rows[i] = order[i];
+    L.len[i] = rlen(order[i]);
+  }
+  for (uint32_t sl = 0; sl < L.nslices; ++sl) {
+    uint32_t width = 0;
+    for (uint32_t t = 0; t < 32; ++t) width = std::max(width, L.len[sl * 32 + t]);
+    L.start[sl + 1] = L.start[sl] + 32 * width;
+  }
+  L.pos.assign(starts[nrows], 0);
+  L.cols.assign(L.start[L.nslices], 0);
+  for (uint32_t i = 0; i < nrows; ++i) {
+    uint32_t r = order[i], sl = i / 32, t = i % 32;
+    for (uint32_t k = 0; k < rlen(r); ++k) {
+      uint32_t q = L.start[sl] + 32 * k + t;
+      L.pos[starts[r] + k] = q;
+      L.cols[q] = cols[starts[r] + k];
+    }
+  }
+  return L;
+}
+
+sf_status upload_sell_layout(DeviceSolver& s, DevBsr& m, const SellLayout& L, size_t value_bytes) {
+  m.nslices = L.nslices;
+  sf_status e = SF_OK;
+  if (!e) e = dev_alloc(s, (void**)&m.sell_rows, L.rows.size() * 4);
+  if (!e) e = dev_alloc(s, (void**)&m.sell_len, L.len.size() * 4);
+  if (!e) e = dev_alloc(s, (void**)&m.sell_start, L.start.size() * 4);
+  if (!e) e = dev_alloc(s, (void**)&m.sell_cols, std::max<size_t>(1, L.cols.size()) * 4);
+  if (!e) e = dev_alloc(s, &m.sell_vals, std::max<size_t>(1, L.cols.size()) * value_bytes);
+  if (e) return e;
+  copy_h2d(s, m.sell_rows, L.rows.data(), L.rows.size() * 4);
+  copy_h2d(s, m.sell_len, L.len.data(), L.len.size() * 4);
+  copy_h2d(s, m.sell_start, L.start.data(), L.start.size() * 4);
+  if (!L.cols.empty()) copy_h2d(s, m.sell_cols, L.cols.data(), L.cols.size() * 4);
+  return SF_OK;
+}
+
+}  // namespace
+
+template <typename S>
+sf_status make_sell(DeviceSolver& s, DevBsr& m, const uint32_t* starts, const uint32_t* cols, const S* vals) {
+  SellLayout L = sell_layout(m.rows, starts, cols);
+  const size_t len = (size_t)m.rb * m.cb;
+  if (sf_status e = upload_sell_layout(s, m, L, len * sizeof(S))) return e;
+  std::vector<S> v(L.cols.size() * len, S(0));
+  for (size_t b = 0; b < L.pos.size(); ++b) {
+    uint32_t q = L.pos[b], t = q & 31u;
+    size_t base = (size_t)(q - t) * len + t;
+    for (size_t el = 0; el < len; ++el) v[base + 32 * el] = vals[b * len + el];
+  }
+  if (!v.empty()) copy_h2d(s, m.sell_vals, v.data(), v.size() * sizeof(S));
+  m.sell = true;
+  return cuda_check(cudaStreamSynchronize(s.stream), "SELL upload");
+}
+
+template sf_status make_sell<float>(DeviceSolver&, DevBsr&, const uint32_t*, const uint32_t*, const float*);
+template sf_status make_sell<double>(DeviceSolver&, DevBsr&, const uint32_t*, const uint32_t*, const double*);
+
+sf_status make_sell_from_device(DeviceSolver& s, DevBsr& m, const uint32_t* starts, const uint32_t* cols) {
+  SellLayout L = sell_layout(m.rows, starts, cols);
+  if (sf_status e = upload_sell_layout(s, m, L, 72)) return e;
+  uint32_t* pos = nullptr;
+  if (sf_status e = dev_alloc(s, (void**)&pos, std::max<size_t>(1, L.pos.size()) * 4)) return e;
+  if (!L.pos.empty()) copy_h2d(s, pos, L.pos.data(), L.pos.size() * 4);
+  sell_permute_kernel<double, 9><<<grid_for_elems(L.pos.size()), kThreads, 0, s.stream>>>(L.pos.size(), pos,
+                                                                                         (const double*)m.vals,
+                                                                                         (double*)m.sell_vals);
+  m.sell = true;
+  return cuda_check(cudaStreamSynchronize(s.stream), "SELL permute");
+}
+
 namespace {
 
 template <typename S>
@@ -640,6 +1314,11 @@ sf_status upload_bsr(DeviceSolver& s, const Bsr& h, DevBsr& d) {
       copy_h2d(s, d.vals, f.data(), f.size() * 4);
       cudaStreamSynchronize(s.stream);
     }
+  }
+  if (sf_status e = make_row_groups(s, d, h.starts.data(), h.rb * h.cb * sizeof(S))) return e;
+  if (h.rows >= s.sell_min_rows) {
+    std::vector<S> v(h.vals.begin(), h.vals.end());
+    if (sf_status e = make_sell<S>(s, d, h.starts.data(), h.cols.data(), v.data())) return e;
   }
   return cuda_check(cudaGetLastError(), "upload");
 }
@@ -750,6 +1429,7 @@ sf_status solver_enqueue_reset(DeviceSolver& s) {
     pcg_dot_rz_kernel<double><<<kReduceBlocks, kReduceThreads, 0, s.stream>>>(s.n, s.r, s.z, s.ap, s.partials, s.state);
     pcg_update_p_kernel<double><<<grid_for_elems(s.n), kThreads, 0, s.stream>>>(s.n, s.z, s.p, s.state);
   }
+  s.launches_per_iteration += 2;
   return cuda_check(cudaGetLastError(), "reset direction");
 }
 
@@ -757,14 +1437,17 @@ sf_status solver_enqueue_iteration(DeviceSolver& s) {
   cudaStream_t st = s.stream;
   const int* status = &s.state->status;
   s.launches_per_iteration = 0;
-  int smem = kWarps * Slab<double, 3, 3>::kInt4 * 16;
-  pcg_spmv_dot_kernel<<<kReduceBlocks, kThreads, smem, st>>>(s.system.rows, s.system.starts, s.system.cols,
-                                                             (const double*)s.system.vals, s.p, s.ap, s.partials,
-                                                             s.state);
-  pcg_update_kernel<<<kReduceBlocks, kReduceThreads, 0, st>>>(s.n, s.p, s.ap, s.x, s.r, s.partials, s.state);
-  pcg_check_kernel<<<kReduceBlocks, kThreads, smem, st>>>(s.system.rows, s.system.starts, s.system.cols,
-                                                          (const double*)s.system.vals, s.x, s.rhs, s.r, s.partials,
-                                                          s.state);
+  if (s.system.sell) {
+    SellOp<double> A = sell_of<double>(s.system);
+    int grid = std::min(grid_for_slices(s.system.nslices), kReduceBlocks * 2);
+    sell_pcg_spmv_dot_kernel<<<grid, kThreads, 0, st>>>(A, s.p, s.ap, s.partials, s.state);
+    pcg_update_kernel<<<kReduceBlocks, kReduceThreads, 0, st>>>(s.n, s.p, s.ap, s.x, s.r, s.partials, s.state);
+    sell_pcg_check_kernel<<<grid, kThreads, 0, st>>>(A, s.x, s.rhs, s.r, s.partials, s.state);
+  } else switch (s.system.lanes_per_row) {
+    case 8: launch_pcg_spmv_lpr<8>(s); break;
+    case 16: launch_pcg_spmv_lpr<16>(s); break;
+    default: launch_pcg_spmv_lpr<32>(s); break;
+  }
   s.launches_per_iteration += 3;
   enqueue_precondition(s, s.r, s.z, s.z32, status);
   if (s.vector_single && s.multigrid) {
@@ -875,14 +1558,8 @@ sf_status solver_time_kernel(DeviceSolver& s, int kernel, uint64_t repeats, doub
 
 sf_status solver_precondition(DeviceSolver& s, const double* d_in, double* d_out) {
   enqueue_precondition(s, d_in, d_out, s.z32, s.always_active);
-  if (s.vector_single && s.multigrid) {
-    // widen the f32 correction
-    std::vector<float> h(s.n);
-    copy_d2h(s, h.data(), s.z32, (size_t)s.n * 4);
-    cudaStreamSynchronize(s.stream);
-    std::vector<double> w(h.begin(), h.end());
-    copy_h2d(s, d_out, w.data(), (size_t)s.n * 8);
-  }
+  if (s.vector_single && s.multigrid)
+    convert_kernel<float, double><<<grid_for_elems(s.n), kThreads, 0, s.stream>>>(s.n, s.z32, d_out, s.always_active);
   return cuda_check(cudaStreamSynchronize(s.stream), "precondition");
 }
 

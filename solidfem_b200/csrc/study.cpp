@@ -565,6 +565,7 @@ void sf_study_options_default(sf_study_options* o) {
   o->device = 0;
   o->use_graphs = 1;
   o->device_memory_budget = 0;
+  o->sell_min_rows = 0;
 }
 
 // ------------------------------------------------------------------------------ builder
@@ -665,6 +666,7 @@ sf_status sf_builder_create(sf_model* model, const sf_study_options* options, sf
   cudaSetDevice(b->options.device);
   DeviceSolver& s = b->solver;
   s.device = b->options.device;
+  s.sell_min_rows = b->options.sell_min_rows ? b->options.sell_min_rows : 32768;
   if (sf_status e = cuda_check(cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking), "stream")) return e;
   AssemblyDevice& a = b->asmdev;
   a.tet_count = (uint32_t)mesh.tets.size();
@@ -703,6 +705,10 @@ sf_status sf_builder_create(sf_model* model, const sf_study_options* options, sf
   copy_h2d(s, a.error, &none, 8);
   copy_h2d(s, s.system.starts, b->pattern.starts.data(), (b->free_count + 1) * 4);
   copy_h2d(s, s.system.cols, b->pattern.cols.data(), blocks * 4);
+  if ((e = make_row_groups(s, s.system, b->pattern.starts.data(), 72))) {
+    release_builder_device(b.get());
+    return e;
+  }
   // A host material callback: integration point positions from the device, the field on the
   // host, (E, nu) per point back to the device.
   if (md.material.kind == MATERIAL_CALLBACK) {
@@ -894,6 +900,9 @@ sf_status sf_builder_finish(sf_builder* b, sf_study** out) {
   if (!e) e = dev_alloc(d, (void**)&d.always_active, sizeof(int));
   if (e) return e;
   copy_h2d(d, d.rhs, s->rhs.data(), (size_t)d.n * 8);
+  // The conjugate gradient's f64 product runs on a SELL copy when the system has many rows.
+  if (d.system.rows >= d.sell_min_rows)
+    if ((e = make_sell_from_device(d, d.system, s->pattern.starts.data(), s->pattern.cols.data()))) return e;
   if (mg) {
     s->levels = setup_take_levels(b->setup);
     e = solver_upload_hierarchy(d, s->levels, s->options.smoother_degree);

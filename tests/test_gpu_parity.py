@@ -19,10 +19,12 @@ CASES = {
 }
 
 
-def build(name, precision, tolerance=1e-9):
+def build(name, precision, tolerance=1e-9, sell=False):
+    """The case on the device; `sell` puts every operator in the SELL-32 layout (by default only
+    operators of at least 32768 block rows use it, which these small cases never reach)."""
     size, div, E, nu = CASES[name]
     mesh, model = product_model(size, div, E, nu)
-    study = sf.StaticStudy.new(model, mg_options(precision, tolerance))
+    study = sf.StaticStudy.new(model, mg_options(precision, tolerance, sell_min_rows=1 if sell else 0))
     return mesh, study
 
 
@@ -60,13 +62,14 @@ def test_hierarchy_is_bit_exact(oracle, name):
             assert np.array_equal(a["p_values"].view(np.uint64), b["p_values"].view(np.uint64)), lv
 
 
+@pytest.mark.parametrize("sell", [False, True])
 @pytest.mark.parametrize("precision,tol", [(sf.Precision.DOUBLE, 1e-11), (sf.Precision.SINGLE_STORAGE, 1e-5),
                                            (sf.Precision.SINGLE, 1e-4)])
-def test_device_cycle_matches_oracle_cycle(oracle, precision, tol):
+def test_device_cycle_matches_oracle_cycle(oracle, precision, tol, sell):
     """One V-cycle on the device against the oracle's cycle in the same precision."""
     opr = {sf.Precision.DOUBLE: oracle.DOUBLE, sf.Precision.SINGLE_STORAGE: oracle.SINGLE_STORAGE,
            sf.Precision.SINGLE: oracle.SINGLE}[precision]
-    _, study = build("plate", precision)
+    _, study = build("plate", precision, sell=sell)
     ref = oracle_for(oracle, "plate", opr)
     r = np.random.default_rng(7).standard_normal(ref.n)
     z, zr = study.precondition(r), ref.precondition(r)
@@ -75,19 +78,21 @@ def test_device_cycle_matches_oracle_cycle(oracle, precision, tol):
     assert rel <= tol
 
 
-def test_system_multiply_matches_oracle(oracle):
-    _, study = build("cantilever", sf.Precision.DOUBLE)
+@pytest.mark.parametrize("sell", [False, True])
+def test_system_multiply_matches_oracle(oracle, sell):
+    _, study = build("cantilever", sf.Precision.DOUBLE, sell=sell)
     ref = oracle_for(oracle, "cantilever", oracle.DOUBLE)
     x = np.random.default_rng(3).standard_normal(ref.n)
     y, yr = study.system_multiply(x), ref.system_multiply(x)
     assert np.linalg.norm(y - yr) <= 1e-13 * np.linalg.norm(yr)
 
 
+@pytest.mark.parametrize("sell", [False, True])
 @pytest.mark.parametrize("name", list(CASES))
 @pytest.mark.parametrize("precision", [sf.Precision.DOUBLE, sf.Precision.SINGLE_STORAGE, sf.Precision.SINGLE,
                                        sf.Precision.MIXED])
-def test_solve_matches_oracle(oracle, name, precision):
-    mesh, study = build(name, precision)
+def test_solve_matches_oracle(oracle, name, precision, sell):
+    mesh, study = build(name, precision, sell=sell)
     out = study.solve()
     assert out.kind == sf.Outcome.CONVERGED
     ref = oracle_for(oracle, name, oracle.DOUBLE)
@@ -122,10 +127,11 @@ def test_tight_double_solve_agrees_to_1e8(oracle):
     assert rel <= 1e-8
 
 
-def test_sliced_solve_gives_identical_bits():
-    _, one = build("plate", sf.Precision.MIXED)
+@pytest.mark.parametrize("sell", [False, True])
+def test_sliced_solve_gives_identical_bits(sell):
+    _, one = build("plate", sf.Precision.MIXED, sell=sell)
     one.solve()
-    _, sliced = build("plate", sf.Precision.MIXED)
+    _, sliced = build("plate", sf.Precision.MIXED, sell=sell)
     while sliced.step(3).kind == sf.Outcome.RUNNING:
         pass
     a, b = one.displacements(), sliced.displacements()
