@@ -298,7 +298,7 @@ def run_mine(args, rank, world):
                           "mixed_speedup": dms / ms_per_step, "mixed_vs_fp64_rel_l2": diff},
             "setup": {"assembly_seconds": rep["assembly_seconds"], "preconditioner_seconds": rep["preconditioner_seconds"],
                       "levels": rep["mg_levels"], "operator_complexity": rep["mg_operator_complexity"]},
-            "roofline": {"bound": "hbm", "kernel": "cheb_step_kernel<float,float,3> (finest level)",
+            "roofline": {"bound": "hbm", "kernel": "sell_cheb_kernel<float,float,3> (finest level, fused Chebyshev step)",
                          "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "peak_kind": peak_kind, "traffic": traffic,
                          "bytes_per_launch": kt["bytes_per_launch"], "ms_per_launch": kt["ms_per_launch"],

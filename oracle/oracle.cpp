@@ -2388,6 +2388,15 @@ int orc_study_recover(orc_study* s) {
   s->recovered_done = c == 0;
   return c;
 }
+// Recovery of caller-given displacements (every mesh node, x 3), for comparing recovery alone.
+int orc_study_recover_with(orc_study* s, const double* flat) {
+  vector<P3> disp(s->free.size());
+  for (size_t n = 0; n < disp.size(); ++n) disp[n] = {flat[3 * n], flat[3 * n + 1], flat[3 * n + 2]};
+  int c = recover(s->mesh->q, s->field, s->quadrature, disp, s->recovered);
+  s->recovered_done = c == 0;
+  return c;
+}
+
 void orc_study_nodal_stress(const orc_study* s, double* stress6, double* von_mises_out) {
   for (size_t n = 0; n < s->recovered.nodal_stress.size(); ++n) {
     for (int k = 0; k < 6; ++k) stress6[6 * n + k] = s->recovered.nodal_stress[n][k];

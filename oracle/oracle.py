@@ -120,6 +120,7 @@ def lib():
         L.orc_multiply_rounding_bound.argtypes = [C.c_void_p, p(C.c_double)]
         L.orc_multiply_rounding_bound.restype = C.c_double
         L.orc_study_recover.argtypes = [C.c_void_p]
+        L.orc_study_recover_with.argtypes = [C.c_void_p, p(C.c_double)]
         L.orc_study_nodal_stress.argtypes = [C.c_void_p, p(C.c_double), p(C.c_double)]
         L.orc_study_point_count.argtypes = [C.c_void_p]
         L.orc_study_point_count.restype = C.c_uint64
@@ -326,6 +327,18 @@ class Study:
 
     def recover(self):
         code = lib().orc_study_recover(self.h)
+        if code:
+            raise ValueError(f"recovery refused: code {code}")
+        n = self.mesh.node_count
+        s6 = np.empty((n, 6))
+        vm = np.empty(n)
+        lib().orc_study_nodal_stress(self.h, _ptr(s6, C.c_double), _ptr(vm, C.c_double))
+        return s6, vm
+
+    def recover_with(self, displacements):
+        """Recovery (results.rs) of the given displacements of every mesh node."""
+        d = np.ascontiguousarray(displacements, dtype=np.float64)
+        code = lib().orc_study_recover_with(self.h, _ptr(d, C.c_double))
         if code:
             raise ValueError(f"recovery refused: code {code}")
         n = self.mesh.node_count

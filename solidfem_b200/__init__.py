@@ -505,6 +505,20 @@ class StepOutcome:
     progress: Progress
 
 
+@dataclass
+class Solution:
+    """A solved study's results (Solution, crates/solidfem-elastic/src/results.rs:81-95)."""
+    displacements: np.ndarray      # node_count x 3
+    point_stresses: np.ndarray     # structured: tet, point, position[3], stress[6], von_mises
+    nodal_stress: np.ndarray       # node_count x 6: [xx, yy, zz, xy, yz, zx]
+    nodal_von_mises: np.ndarray    # node_count
+    report: dict
+
+
+POINT_STRESS_DTYPE = np.dtype([("tet", "<u4"), ("point", "<u4"), ("position", "<f8", 3), ("stress", "<f8", 6),
+                               ("von_mises", "<f8")])
+
+
 class StudyBuilder:
     """StudyBuilder (study.rs:392-656): new validates and builds the load and pattern; step adds
     element stiffness on the device and then advances the multigrid setup."""
@@ -513,6 +527,7 @@ class StudyBuilder:
         options = options or StudyOptions()
         mh, self._keep = model._to_c()
         self._mesh = model.mesh
+        self._quadrature = model.quadrature
         h = C.c_void_p()
         _check(library().sf_builder_create(mh, C.byref(options._c()), C.byref(h)))
         self._h = h
@@ -532,16 +547,17 @@ class StudyBuilder:
         h = C.c_void_p()
         _check(library().sf_builder_finish(self._h, C.byref(h)))
         self._h = None
-        return StaticStudy(h, self._mesh, self._keep)
+        return StaticStudy(h, self._mesh, self._keep, self._quadrature)
 
 
 class StaticStudy:
     """A study in progress (StaticStudy, study.rs:178-378): step runs device iterations."""
 
-    def __init__(self, handle, mesh: Mesh, keep=()):
+    def __init__(self, handle, mesh: Mesh, keep=(), quadrature=None):
         self._h = handle
         self.mesh = mesh
         self._keep = keep
+        self._quadrature = Quadrature.FOUR_POINT if quadrature is None else quadrature
 
     @classmethod
     def new(cls, model: Model, options: Optional[StudyOptions] = None,
@@ -551,7 +567,7 @@ class StaticStudy:
         mh, keep = model._to_c()
         h = C.c_void_p()
         _check(library().sf_study_create(mh, C.byref(options._c()), _cancel_fn(cancel), None, C.byref(h)))
-        return cls(h, model.mesh, keep)
+        return cls(h, model.mesh, keep, model.quadrature)
 
     def __del__(self):
         if getattr(self, "_h", None):
@@ -574,6 +590,19 @@ class StaticStudy:
         out = np.empty((self.mesh.node_count(), 3))
         _check(library().sf_study_displacements(self._h, _dptr(out)))
         return out
+
+    def solution(self) -> Solution:
+        """StaticStudy::solution (study.rs:246-260): displacements and the stress field recovered on
+        the device; refuses (NOT_FINISHED) until the solve has converged."""
+        n = self.mesh.node_count()
+        q = 14 if self._quadrature == Quadrature.FOURTEEN_POINT else 4
+        d = np.empty((n, 3))
+        s6 = np.empty((n, 6))
+        vm = np.empty(n)
+        pts = np.empty(self.mesh.tet_count() * q, dtype=POINT_STRESS_DTYPE)
+        _check(library().sf_study_solution(self._h, _dptr(d), _dptr(s6), _dptr(vm),
+                                           pts.ctypes.data_as(C.POINTER(PointStress))))
+        return Solution(d, pts, s6, vm, self.report())
 
     def report(self) -> dict:
         r = _Report()
@@ -656,5 +685,5 @@ class StaticStudy:
 __all__ = [
     "BoundaryFace", "Mesh", "box_tet_mesh", "Material", "ShellCore", "Quadrature", "Model", "Precision",
     "PcgOptions", "MultigridOptions", "Jacobi", "StudyOptions", "StudyBuilder", "StaticStudy", "StepOutcome",
-    "Outcome", "Progress", "BuildProgress", "PointStress", "SolidfemError", "Status", "library", "SIGNATURES", "Kernel",
+    "Outcome", "Progress", "BuildProgress", "PointStress", "SolidfemError", "Status", "library", "SIGNATURES", "Kernel", "Solution",
 ]

@@ -160,6 +160,7 @@ sf_status launch_gather(const AssemblyDevice& a, DevBsr& system, uint32_t end, c
 // values and patch fits, then the nodal field.
 struct RecoveryDevice {
   double* disp = nullptr;         // node_count x 3
+  uint32_t* free = nullptr;       // node_count: free index or FIXED
   double* point_stress = nullptr; // tet_count x points x 6
   double* point_vm = nullptr;     // tet_count x points
   double* point_pos = nullptr;    // tet_count x points x 3
@@ -169,14 +170,19 @@ struct RecoveryDevice {
   uint32_t* vertex_incident = nullptr; // elements touching each vertex, ascending
   uint32_t* node_offsets = nullptr;    // node_count + 1: (element, local node) incidence
   uint32_t* node_incident = nullptr;   // (element << 4) | local node, ascending element
-  double* fits = nullptr;         // vertex_count x (4 + 24): centre, scale, coefficients
+  double* fits = nullptr;         // vertex_count x 28: centre (3), scale, coefficients (4 x 6)
   int* has_fit = nullptr;         // vertex_count
-  uint32_t* midside_element = nullptr;  // per midside node: first element and its edge slot
+  uint32_t* midside_first = nullptr;  // per midside node: (first element << 3) | edge slot
   double* nodal_stress = nullptr; // node_count x 6
   double* nodal_vm = nullptr;     // node_count
+  bool ready = false;             // incidence uploaded
 };
+// Device stress recovery of the displacements in r.disp (crates/solidfem-elastic/src/results.rs:
+// 470-539 and 376-410, patch.rs:37-120), bit-identical to the reference's serial recovery.
 sf_status launch_recovery(const AssemblyDevice& a, const MaterialSpec& m, RecoveryDevice& r,
                           uint32_t node_count, uint32_t vertex_count, cudaStream_t stream);
+// The displacement of every mesh node from the free-DOF solution (zero at fixed nodes).
+sf_status launch_scatter_displacements(const double* x, RecoveryDevice& r, uint32_t node_count, cudaStream_t stream);
 
 // ------------------------------------------------------------------- solve (solve.cu)
 // Uploads the hierarchy in the study's precision and allocates every work vector.

@@ -357,6 +357,8 @@ struct sf_study {
   double assembly_ms = 0;
   PcgState* pinned = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  RecoveryDevice rec;
+  bool recovered = false;  // rec holds the field of the converged displacements
   ~sf_study() {
     if (pinned) cudaFreeHost(pinned);
     if (ev0) cudaEventDestroy(ev0);
@@ -1072,16 +1074,115 @@ sf_status sf_study_report(const sf_study* s, sf_report* out) {
   return SF_OK;
 }
 
+// Device stress recovery of the current displacements (Recovery, results.rs:97-124): the
+// incidence lists are built once on the host, the three recovery kernels run on the study stream.
+static sf_status study_recover(sf_study* s) {
+  if (s->recovered) return SF_OK;
+  DeviceSolver& d = s->solver;
+  RecoveryDevice& r = s->rec;
+  const Mesh& m = s->model.mesh;
+  const size_t nn = m.nodes.size(), ne = m.tets.size(), nv = m.vertex_count;
+  const size_t pts = (size_t)s->asmdev.points * ne;
+  double t0 = now_seconds();
+  if (!r.ready) {
+    // Elements touching each vertex through a corner, and (element, local node) per node, both in
+    // element order (results.rs:414-435); the first element reaching each midside node.
+    vector<uint32_t> voff(nv + 1, 0), noff(nn + 1, 0);
+    for (auto& t : m.tets) {
+      for (int c = 0; c < 4; ++c) voff[t[c] + 1] += 1;
+      for (int a = 0; a < 10; ++a) noff[t[a] + 1] += 1;
+    }
+    for (size_t i = 0; i < nv; ++i) voff[i + 1] += voff[i];
+    for (size_t i = 0; i < nn; ++i) noff[i + 1] += noff[i];
+    vector<uint32_t> vinc(voff[nv]), ninc(noff[nn]);
+    vector<uint32_t> vf(voff.begin(), voff.end() - 1), nf(noff.begin(), noff.end() - 1);
+    vector<uint32_t> mid(nn - nv, 0xffffffffu);
+    for (size_t e = 0; e < ne; ++e) {
+      const auto& t = m.tets[e];
+      for (int c = 0; c < 4; ++c) vinc[vf[t[c]]++] = (uint32_t)e;
+      for (int a = 0; a < 10; ++a) ninc[nf[t[a]]++] = ((uint32_t)e << 4) | (uint32_t)a;
+      for (int k = 0; k < 6; ++k)
+        if (mid[t[4 + k] - nv] == 0xffffffffu) mid[t[4 + k] - nv] = ((uint32_t)e << 3) | (uint32_t)k;
+    }
+    sf_status e = SF_OK;
+    if (!e) e = dev_alloc(d, (void**)&r.disp, nn * 24);
+    if (!e) e = dev_alloc(d, (void**)&r.free, nn * 4);
+    if (!e) e = dev_alloc(d, (void**)&r.point_stress, pts * 48);
+    if (!e) e = dev_alloc(d, (void**)&r.point_vm, pts * 8);
+    if (!e) e = dev_alloc(d, (void**)&r.point_pos, pts * 24);
+    if (!e) e = dev_alloc(d, (void**)&r.point_mat, pts * 16);
+    if (!e) e = dev_alloc(d, (void**)&r.node_candidate, ne * 10 * 56);
+    if (!e) e = dev_alloc(d, (void**)&r.vertex_offsets, (nv + 1) * 4);
+    if (!e) e = dev_alloc(d, (void**)&r.vertex_incident, std::max<size_t>(1, vinc.size()) * 4);
+    if (!e) e = dev_alloc(d, (void**)&r.node_offsets, (nn + 1) * 4);
+    if (!e) e = dev_alloc(d, (void**)&r.node_incident, std::max<size_t>(1, ninc.size()) * 4);
+    if (!e) e = dev_alloc(d, (void**)&r.fits, nv * 28 * 8);
+    if (!e) e = dev_alloc(d, (void**)&r.has_fit, nv * 4);
+    if (!e) e = dev_alloc(d, (void**)&r.midside_first, std::max<size_t>(1, mid.size()) * 4);
+    if (!e) e = dev_alloc(d, (void**)&r.nodal_stress, nn * 48);
+    if (!e) e = dev_alloc(d, (void**)&r.nodal_vm, nn * 8);
+    if (e) return e;
+    copy_h2d(d, r.free, s->free.data(), nn * 4);
+    copy_h2d(d, r.vertex_offsets, voff.data(), voff.size() * 4);
+    if (!vinc.empty()) copy_h2d(d, r.vertex_incident, vinc.data(), vinc.size() * 4);
+    copy_h2d(d, r.node_offsets, noff.data(), noff.size() * 4);
+    if (!ninc.empty()) copy_h2d(d, r.node_incident, ninc.data(), ninc.size() * 4);
+    if (!mid.empty()) copy_h2d(d, r.midside_first, mid.data(), mid.size() * 4);
+    if ((e = cuda_check(cudaStreamSynchronize(d.stream), "recovery set-up"))) return e;
+    r.ready = true;
+  }
+  unsigned long long none = ~0ull;
+  copy_h2d(d, s->asmdev.error, &none, 8);
+  sf_status e = launch_scatter_displacements(d.x, r, (uint32_t)nn, d.stream);
+  if (!e) e = launch_recovery(s->asmdev, s->model.material, r, (uint32_t)nn, (uint32_t)nv, d.stream);
+  d.launches += 4;
+  unsigned long long err = 0;
+  if (!e) copy_d2h(d, &err, s->asmdev.error, 8);
+  if (!e) e = cuda_check(cudaStreamSynchronize(d.stream), "recovery");
+  if (e) return e;
+  if (err != ~0ull) {
+    error_slot().tet = (uint32_t)(err >> 32);
+    error_slot().point = (uint32_t)((err >> 8) & 0xff);
+    return fail((err & 0xff) == FAULT_INVERTED ? SF_ELEMENT_INVERTED_JACOBIAN : SF_ELEMENT_INVALID_MATERIAL,
+                "recovery met an inverted element or an invalid material");
+  }
+  s->report.recovery_seconds += now_seconds() - t0;
+  s->recovered = true;
+  return SF_OK;
+}
+
 sf_status sf_study_solution(sf_study* s, double* displacements, double* nodal_stress, double* nodal_von_mises,
                             sf_point_stress* points) {
   if (!s) return fail(SF_INVALID_ARGUMENT, "null argument");
   if (s->status != ST_CONVERGED) return fail(SF_NOT_FINISHED, "the solve has not converged");
-  (void)nodal_stress;
-  (void)nodal_von_mises;
-  (void)points;
+  DeviceSolver& d = s->solver;
+  cudaSetDevice(d.device);
   if (displacements)
     if (sf_status e = sf_study_displacements(s, displacements)) return e;
-  if (nodal_stress || nodal_von_mises || points) return fail(SF_NOT_FINISHED, "stress recovery is not available yet");
+  if (!nodal_stress && !nodal_von_mises && !points) return SF_OK;
+  if (sf_status e = study_recover(s)) return e;
+  const size_t nn = s->model.mesh.nodes.size(), ne = s->model.mesh.tets.size();
+  const size_t q = (size_t)s->asmdev.points, pts = q * ne;
+  if (nodal_stress) copy_d2h(d, nodal_stress, s->rec.nodal_stress, nn * 48);
+  if (nodal_von_mises) copy_d2h(d, nodal_von_mises, s->rec.nodal_vm, nn * 8);
+  vector<double> ps, pv, pp;
+  if (points) {
+    ps.resize(pts * 6);
+    pv.resize(pts);
+    pp.resize(pts * 3);
+    copy_d2h(d, ps.data(), s->rec.point_stress, pts * 48);
+    copy_d2h(d, pv.data(), s->rec.point_vm, pts * 8);
+    copy_d2h(d, pp.data(), s->rec.point_pos, pts * 24);
+  }
+  if (sf_status e = cuda_check(cudaStreamSynchronize(d.stream), "read recovery")) return e;
+  if (points)
+    for (size_t i = 0; i < pts; ++i) {
+      points[i].tet = (uint32_t)(i / q);
+      points[i].point = (uint32_t)(i % q);
+      for (int k = 0; k < 3; ++k) points[i].position[k] = pp[i * 3 + k];
+      for (int k = 0; k < 6; ++k) points[i].stress[k] = ps[i * 6 + k];
+      points[i].von_mises = pv[i];
+    }
   return SF_OK;
 }
 
@@ -1215,6 +1316,7 @@ sf_status sf_study_resolve(sf_study* s, const double* rhs) {
     copy_h2d(d, d.rhs, rhs, (size_t)d.n * 8);
   }
   if (sf_status e = solver_restart(d, s->options.tolerance, s->options.max_iterations)) return e;
+  s->recovered = false;
   s->cancelled = false;
   std::memset(&s->last, 0, sizeof(s->last));
   s->status = ST_ACTIVE;
