@@ -305,6 +305,33 @@ sf_status sf_study_precondition(sf_study* study, const double* residual, double*
 /* CsrMatrix::multiply (csr.rs:112-120) on the device, FP64, host buffers. */
 sf_status sf_study_system_multiply(sf_study* study, const double* x, double* y);
 
+/* No counterpart in the reference. System products with their energies, on device memory the
+ * caller owns, allocating nothing: for k < count, y_k = A x_k and energy[k] = x_k . y_k in FP64,
+ * where x_k and y_k are the free-DOF vectors at x + k * free_dofs and y + k * free_dofs.
+ *
+ * For callers that must not allocate device memory on this path: a serving loop that has given
+ * its whole device budget to resident studies, or one that keeps other streams busy, where
+ * cudaMalloc can fail and cudaFree waits for the whole device. (sf_study_system_multiply
+ * allocates two device buffers per call and copies through the host.) The reduction's scratch is
+ * a static 65,792-byte device array in this library, one per device.
+ *
+ * - count at most 8; a larger count is refused with SF_INVALID_ARGUMENT before any work. count 0
+ *   does nothing. x, y and energy: 8-byte-aligned device (or managed) memory of the study's
+ *   device, not overlapping; x and y hold count * free_dofs doubles, energy count doubles.
+ * - Asynchronous: the kernel is enqueued on the study's stream (sf_study_stream); read y and
+ *   energy after that stream has reached it.
+ * - The first call on a device looks up the scratch's address with that device current, which can
+ *   load this library's device code on it. Make that first call before any stream capture begins
+ *   on the device.
+ * - The scratch holds arrival tickets that must be zero when a call starts: they are zero when the
+ *   library loads, and each call leaves them at zero when its kernel completes. Nothing else in
+ *   it needs an initial value.
+ * - Every study on a device shares the one scratch array: two calls whose kernels can run at the
+ *   same time (different streams, studies or host threads) race and give wrong results. Order
+ *   them, for example on one stream. */
+sf_status sf_study_energy_products(sf_study* study, const double* x, double* y, double* energy,
+                                   uint64_t count);
+
 /* ------------------------------------------------------------- re-solve and timing -------- */
 /* Restarts the solve from a zero estimate (Pcg::new, pcg.rs:135-164) on the resident matrix and
  * preconditioner, with a new right-hand side over the free DOFs (host buffer), or the resident

@@ -154,6 +154,7 @@ SIGNATURES = {
     "sf_study_aggregates": (C.c_int, [_V, C.c_uint64, _P(C.c_uint32)]),
     "sf_study_precondition": (C.c_int, [_V, _P(C.c_double), _P(C.c_double)]),
     "sf_study_system_multiply": (C.c_int, [_V, _P(C.c_double), _P(C.c_double)]),
+    "sf_study_energy_products": (C.c_int, [_V, _V, _V, _V, C.c_uint64]),
     "sf_study_device_timing": (C.c_int, [_V, _P(_DeviceTiming)]),
     "sf_study_resolve": (C.c_int, [_V, _P(C.c_double)]),
     "sf_study_stream": (C.c_uint64, [_V]),
@@ -658,6 +659,11 @@ class StaticStudy:
         y = np.empty_like(x)
         _check(library().sf_study_system_multiply(self._h, _dptr(x), _dptr(y)))
         return y
+
+    def energy_products(self, x: int, y: int, energy: int, count: int) -> None:
+        """y_k = A x_k and energy[k] = x_k . y_k for count (<= 8) vectors of the caller's device memory
+        (raw device addresses), enqueued on stream() without allocating device memory."""
+        _check(library().sf_study_energy_products(self._h, x, y, energy, count))
 
     def device_timing(self) -> dict:
         t = _DeviceTiming()

@@ -202,5 +202,10 @@ sf_status solver_read_state(DeviceSolver& s, PcgState* out);
 sf_status solver_restart(DeviceSolver& s, double tolerance, uint64_t max_iterations);
 // Mean device milliseconds per launch of one solver kernel and its algorithmic bytes per launch.
 sf_status solver_time_kernel(DeviceSolver& s, int kernel, uint64_t repeats, double* ms, double* bytes);
+// y_k = A x_k and energy[k] = x_k . y_k for count vectors of device memory (count x n each),
+// enqueued on s.stream; the reduction scratch is a static device array, so nothing is allocated.
+sf_status solver_energy_products(DeviceSolver& s, const double* x, double* y, double* energy, uint64_t count);
+// The most vectors one solver_energy_products call takes.
+uint64_t solver_energy_max_vectors();
 
 }  // namespace sf

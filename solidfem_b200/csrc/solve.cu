@@ -17,6 +17,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <mutex>
 
 #include "device.h"
 
@@ -1571,6 +1572,136 @@ sf_status solver_system_multiply(DeviceSolver& s, const double* d_in, double* d_
 sf_status solver_read_state(DeviceSolver& s, PcgState* out) {
   copy_d2h(s, out, s.state, sizeof(PcgState));
   return cuda_check(cudaStreamSynchronize(s.stream), "read state");
+}
+
+// ------------------------------------------------------------ energy products, allocating nothing
+// A variant of the conjugate gradient's system product (pcg_spmv_dot_kernel and
+// sell_pcg_spmv_dot_kernel): for each of `count` vectors x_k of caller-owned device memory it
+// writes y_k = A x_k and the energy e_k = x_k . y_k. Rows are summed exactly as the system product
+// sums them; vector k runs in blockIdx.y = k. The reduction's scratch is not the solver's: it is
+// the file-scope array below, whose address is looked up once per device, so a call allocates no
+// memory at all.
+//
+// Scratch layout (g_energy_scratch, 65,792 bytes per device):
+//   bytes [0, 256):   one arrival ticket (unsigned) per vector. Each ticket must be zero when a
+//                     launch starts. Static device storage is zero when the module loads, and the
+//                     last block of each vector puts its ticket back to zero before it exits, so
+//                     the tickets are zero again after every completed call.
+//   bytes [256, ...): kEnergyMaxBlocks partial sums per vector. No initial value is needed: every
+//                     block writes its slot before it takes its ticket.
+// One array serves every study on a device, so two calls whose kernels can run at the same time
+// (different streams, different studies, different host threads) race on it.
+constexpr int kEnergyMaxVectors = 8;
+constexpr int kEnergyMaxBlocks = 1024;  // blocks per vector of one launch
+constexpr size_t kEnergyTicketBytes = 256;
+constexpr size_t kEnergyScratchBytes = kEnergyTicketBytes + (size_t)kEnergyMaxVectors * kEnergyMaxBlocks * sizeof(double);
+constexpr int kEnergyMaxDevices = 64;
+static_assert(kEnergyMaxVectors * sizeof(unsigned) <= kEnergyTicketBytes, "tickets fit their header");
+
+static __device__ __align__(256) unsigned char g_energy_scratch[kEnergyScratchBytes];
+
+namespace {
+
+__device__ __forceinline__ void energy_finish(double local, unsigned char* scratch, double* energy) {
+  const uint32_t k = blockIdx.y;
+  unsigned* tickets = reinterpret_cast<unsigned*>(scratch);
+  double* partials = reinterpret_cast<double*>(scratch + kEnergyTicketBytes) + (size_t)k * kEnergyMaxBlocks;
+  double v[1] = {local}, total[1];
+  if (finish_partials<1>(v, partials, tickets + k, total) && threadIdx.x == 0) energy[k] = total[0];
+}
+
+// SELL-32 system: one thread per row, rows summed as sell_kernel sums them.
+__global__ void __launch_bounds__(kThreads) sell_energy_kernel(SellOp<double> A, const double* __restrict__ x,
+                                                                double* __restrict__ y, uint32_t n,
+                                                                double* __restrict__ energy, unsigned char* scratch) {
+  const size_t off = (size_t)blockIdx.y * n;
+  SellDot epi;
+  epi.p = x + off;
+  epi.ap = y + off;
+  epi.local = 0.0;
+  sell_rows<double, double, 3, 3, false>(A, x + off, epi);
+  energy_finish(epi.local, scratch, energy);
+}
+
+// Row-group system: LPR lanes per row, rows summed as bsr_kernel sums them.
+template <int LPR>
+__global__ void __launch_bounds__(kThreads) energy_kernel(Op<double> A, const double* __restrict__ x,
+                                                           double* __restrict__ y, uint32_t n,
+                                                           double* __restrict__ energy, unsigned char* scratch) {
+  extern __shared__ __align__(16) char smem[];
+  char* wbase = smem + (threadIdx.x >> 5) * 2 * slot_bytes(A);
+  const size_t off = (size_t)blockIdx.y * n;
+  EpiDot<LPR> epi;
+  epi.p = x + off;
+  epi.ap = y + off;
+  epi.local = 0.0;
+  run_groups<double, double, 3, 3, LPR, false>(A, x + off, wbase, epi);
+  energy_finish(epi.local, scratch, energy);
+}
+
+std::mutex g_energy_mutex;
+unsigned char* g_energy_address[kEnergyMaxDevices] = {};
+
+// Once per device, with that device current: the scratch's device address and the row-group
+// variants' shared-memory opt-in. Neither allocates memory; the first lookup on a device can load
+// this library's device code there.
+sf_status energy_setup(int device, unsigned char** out) {
+  std::lock_guard<std::mutex> lock(g_energy_mutex);
+  if (device < 0 || device >= kEnergyMaxDevices) return fail(SF_INVALID_ARGUMENT, "device ordinal out of range");
+  if (!g_energy_address[device]) {
+    unsigned char* ptr = nullptr;
+    if (sf_status e = cuda_check(cudaGetSymbolAddress((void**)&ptr, g_energy_scratch), "cudaGetSymbolAddress"))
+      return e;
+    const int smem = 200 * 1024;
+    cudaError_t e = cudaFuncSetAttribute(energy_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(energy_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(energy_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(energy_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (sf_status st = cuda_check(e, "cudaFuncSetAttribute")) return st;
+    g_energy_address[device] = ptr;
+  }
+  *out = g_energy_address[device];
+  return SF_OK;
+}
+
+template <int LPR>
+void launch_energy_lpr(const DevBsr& m, const double* x, double* y, uint32_t n, double* energy, uint64_t count,
+                       unsigned char* scratch, cudaStream_t st) {
+  Op<double> A = op_of<double>(m);
+  Shape sh = shape_of(A, true);
+  dim3 grid((unsigned)std::min(sh.grid, kEnergyMaxBlocks), (unsigned)count);
+  energy_kernel<LPR><<<grid, sh.threads, sh.smem, st>>>(A, x, y, n, energy, scratch);
+}
+
+}  // namespace
+
+uint64_t solver_energy_max_vectors() { return kEnergyMaxVectors; }
+
+sf_status solver_energy_products(DeviceSolver& s, const double* x, double* y, double* energy, uint64_t count) {
+  if (count > (uint64_t)kEnergyMaxVectors) {
+    char msg[160];
+    std::snprintf(msg, sizeof msg, "count %llu exceeds the %d vectors the energy scratch holds",
+                  (unsigned long long)count, kEnergyMaxVectors);
+    return fail(SF_INVALID_ARGUMENT, msg);
+  }
+  if (count == 0) return SF_OK;
+  unsigned char* scratch = nullptr;
+  if (sf_status e = energy_setup(s.device, &scratch)) return e;
+  const DevBsr& m = s.system;
+  if (m.sell) {
+    SellOp<double> A = sell_of<double>(m);
+    dim3 grid((unsigned)std::min(grid_for_slices(m.nslices), kEnergyMaxBlocks), (unsigned)count);
+    sell_energy_kernel<<<grid, kThreads, 0, s.stream>>>(A, x, y, s.n, energy, scratch);
+  } else {
+    switch (m.lanes_per_row) {
+      case 4: launch_energy_lpr<4>(m, x, y, s.n, energy, count, scratch, s.stream); break;
+      case 8: launch_energy_lpr<8>(m, x, y, s.n, energy, count, scratch, s.stream); break;
+      case 16: launch_energy_lpr<16>(m, x, y, s.n, energy, count, scratch, s.stream); break;
+      default: launch_energy_lpr<32>(m, x, y, s.n, energy, count, scratch, s.stream); break;
+    }
+  }
+  s.launches += 1;
+  return cuda_check(cudaGetLastError(), "energy products");
 }
 
 }  // namespace sf

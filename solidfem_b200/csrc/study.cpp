@@ -1296,6 +1296,39 @@ sf_status sf_study_system_multiply(sf_study* s, const double* x, double* y) {
   return e;
 }
 
+namespace {
+// A device (or managed) pointer of the study's device, aligned for doubles.
+bool on_study_device(const void* p, int device) {
+  if ((uintptr_t)p % alignof(double) != 0) return false;
+  cudaPointerAttributes attr{};
+  if (cudaPointerGetAttributes(&attr, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  if (attr.type == cudaMemoryTypeManaged) return true;
+  return attr.type == cudaMemoryTypeDevice && attr.device == device;
+}
+bool overlaps(const void* a, size_t abytes, const void* b, size_t bbytes) {
+  uintptr_t a0 = (uintptr_t)a, b0 = (uintptr_t)b;
+  return a0 < b0 + bbytes && b0 < a0 + abytes;
+}
+}  // namespace
+
+sf_status sf_study_energy_products(sf_study* s, const double* x, double* y, double* energy, uint64_t count) {
+  if (!s) return fail(SF_INVALID_ARGUMENT, "null study");
+  DeviceSolver& d = s->solver;
+  if (count > solver_energy_max_vectors()) return solver_energy_products(d, x, y, energy, count);
+  if (count == 0) return SF_OK;
+  if (!x || !y || !energy) return fail(SF_INVALID_ARGUMENT, "null argument");
+  if (sf_status e = cuda_check(cudaSetDevice(d.device), "cudaSetDevice")) return e;
+  if (!on_study_device(x, d.device) || !on_study_device(y, d.device) || !on_study_device(energy, d.device))
+    return fail(SF_INVALID_ARGUMENT, "x, y and energy must be 8-byte aligned device memory of the study's device");
+  const size_t vbytes = (size_t)count * d.n * sizeof(double), ebytes = (size_t)count * sizeof(double);
+  if (overlaps(x, vbytes, y, vbytes) || overlaps(x, vbytes, energy, ebytes) || overlaps(y, vbytes, energy, ebytes))
+    return fail(SF_INVALID_ARGUMENT, "x, y and energy must not overlap");
+  return solver_energy_products(d, x, y, energy, count);
+}
+
 sf_status sf_study_device_timing(const sf_study* s, sf_device_timing* out) {
   if (!s || !out) return fail(SF_INVALID_ARGUMENT, "null argument");
   out->step_ms = s->step_ms;
