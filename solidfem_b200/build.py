@@ -1,7 +1,8 @@
 """Builds libsolidfem_b200.so in-tree for sm_100a (B200).
 
-The CUDA sources are compiled with nvcc for compute_100a/sm_100a; assembly.cu additionally with
--fmad=false so the FP64 stiffness is bit-identical to the reference's serial assembly. The host
+The CUDA sources are compiled with nvcc for compute_100a/sm_100a; assembly.cu and setup_device.cu
+additionally with -fmad=false so the FP64 stiffness and multigrid hierarchy are bit-identical to the
+reference's serial loops. The host
 C++ is compiled without multiply-add contraction for the same reason (setup must reproduce the
 reference's aggregates and coarse matrices to the bit). Objects go to solidfem_b200/_build/.
 """
@@ -26,6 +27,7 @@ NVCC_COMMON = ["-O3", "-std=c++17", "-lineinfo", "-ccbin", CXX, "-Xcompiler", "-
 CU_SOURCES = {
     "solve.cu": [],
     "assembly.cu": ["-fmad=false", "-prec-div=true", "-prec-sqrt=true"],
+    "setup_device.cu": ["-fmad=false", "-prec-div=true", "-prec-sqrt=true"],
 }
 CPP_SOURCES = ["mesh.cpp", "setup.cpp", "study.cpp"]
 CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-fopenmp", "-ffp-contract=off", "-fno-fast-math", "-Wall",

@@ -43,9 +43,6 @@ struct DevBsr {
 
 static const uint32_t kSellWindow = 2048;    // rows are sorted by length inside windows this long
 
-// Builds the SELL-32 copy of a block matrix from host starts, columns and values (S values).
-template <typename S>
-sf_status make_sell(struct DeviceSolver& s, DevBsr& m, const uint32_t* starts, const uint32_t* cols, const S* vals);
 // The SELL copy of a matrix whose values live only on the device (the assembled f64 system):
 // the layout from host starts/columns, the values permuted on the device.
 sf_status make_sell_from_device(struct DeviceSolver& s, DevBsr& m, const uint32_t* starts, const uint32_t* cols);
@@ -103,7 +100,7 @@ struct DeviceSolver {
   PcgState* state = nullptr;
   int* always_active = nullptr;  // a status word fixed at ST_ACTIVE for standalone cycles
   std::vector<DevLevel> levels;
-  std::vector<void*> owned;  // every cudaMalloc of this solver
+  std::vector<std::pair<void*, size_t>> owned;  // every cudaMalloc of this solver, with its size
   size_t bytes = 0;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t graph_exec = nullptr;
@@ -125,8 +122,39 @@ inline void copy_d2h(const DeviceSolver& s, void* dst, const void* src, size_t b
   s.d2h_bytes += bytes;
 }
 sf_status dev_alloc(DeviceSolver& s, void** ptr, size_t bytes);
+// Frees one allocation of dev_alloc before the solver ends (setup temporaries).
+void dev_free(DeviceSolver& s, void* ptr);
 void dev_free_all(DeviceSolver& s);
 sf_status cuda_check(cudaError_t e, const char* what);
+
+// ------------------------------------------------------------------- setup (setup_device.cu)
+// FP64 numeric phases of the multigrid setup, bit-identical to the reference's serial loops.
+// Patterns (starts, cols) are device copies of the host-built patterns; values are f64.
+sf_status setup_inverse_diagonal(cudaStream_t st, uint32_t rows, int rb, const uint32_t* starts, const uint32_t* cols,
+                                 const double* vals, double* inv, unsigned long long* bad, double* pivots);
+sf_status setup_block_norms(cudaStream_t st, size_t blocks, int len, const double* vals, double* out);
+// 20 (`iterations`) power steps of D^-1 A from start_value; norms[1] ends as the last norm.
+sf_status setup_power_iteration(cudaStream_t st, uint32_t rows, int rb, const uint32_t* starts, const uint32_t* cols,
+                                const double* vals, const double* inv, double* v, double* s2, double* norms,
+                                int iterations);
+sf_status setup_entry_rows(cudaStream_t st, uint32_t rows, const uint32_t* starts, uint32_t* out);
+sf_status setup_smooth(cudaStream_t st, int rb, size_t entries, const uint32_t* entry_row, const uint32_t* p_cols,
+                       const uint32_t* a_starts, const uint32_t* a_cols, const double* a_vals, const uint32_t* n_starts,
+                       const uint32_t* n_cols, const uint32_t* aggregate, const double* t_vals, const double* inv,
+                       double omega, double* p_vals);
+sf_status setup_product(cudaStream_t st, int rb, size_t entries, const uint32_t* entry_row, const uint32_t* ap_cols,
+                        const uint32_t* a_starts, const uint32_t* a_cols, const double* a_vals, const uint32_t* p_starts,
+                        const uint32_t* p_cols, const double* p_vals, double* ap_vals);
+sf_status setup_galerkin(cudaStream_t st, int rb, size_t entries, const uint32_t* entry_row, const uint32_t* c_cols,
+                         const uint32_t* pt_starts, const uint32_t* pt_rows, const uint32_t* pt_at, const double* p_vals,
+                         const uint32_t* ap_starts, const uint32_t* ap_cols, const double* ap_vals, double* c_vals);
+template <typename S>
+sf_status setup_convert(cudaStream_t st, size_t n, const double* in, S* out);
+template <typename S>
+sf_status setup_transpose_blocks(cudaStream_t st, size_t blocks, int rb, int cb, const uint32_t* src, const double* in,
+                                 S* out);
+template <typename S>
+sf_status setup_sell_place(cudaStream_t st, size_t blocks, int len, const uint32_t* pos, const double* in, S* out);
 
 // ------------------------------------------------------------------- assembly (assembly.cu)
 struct AssemblyDevice {

@@ -1,11 +1,16 @@
-// The block smoothed-aggregation multigrid setup, host side. It follows the phase sequence of
+// The block smoothed-aggregation multigrid setup. It follows the phase sequence of
 // crates/solidfem-solve/src/multigrid/setup.rs:242-263 (diagonal, strength, seed, join, sweep,
-// group, tentative, spectral, filter, smooth, product, Galerkin, factor) with every floating-point
-// operation in the reference's order, so the aggregates and every coarse matrix are the
-// reference's to the bit. The aggregation passes are order-dependent graph work and run serially;
-// every row-local phase runs on `threads` host threads in contiguous row chunks that are stitched
-// back in row order, so the thread count never changes a bit. Setup advances in whole phases; the
-// budget counts block rows like the reference's (setup.rs:191-222).
+// group, tentative, spectral, filter, smooth, product, Galerkin, factor) and reproduces the
+// reference's aggregates and coarse matrices to the bit.
+//
+// The split: order-dependent graph work (strong neighbours, the greedy aggregation passes, the
+// per-aggregate Gram-Schmidt of the near-null modes, the smoothing filter) and every sparsity
+// pattern (P, A P, the coarse matrix, P's transpose) are built here on the host; every value of
+// every level (inverse diagonal, block norms, lambda_max, P, A P, P^T A P) is computed on the
+// device in FP64 (setup_device.cu) and stays there. Row-local host work runs on `threads` threads
+// in contiguous row chunks stitched back in row order, so the thread count never changes a bit.
+// Setup advances in whole phases; the budget counts block rows like the reference's
+// (setup.rs:191-222).
 #include <algorithm>
 #include <atomic>
 #include <cmath>
@@ -16,6 +21,7 @@
 #include <omp.h>
 #endif
 
+#include "device.h"
 #include "sf_internal.h"
 
 namespace sf {
@@ -27,7 +33,7 @@ const size_t DENSE_LIMIT = 3000;        // setup.rs:28
 const double MAX_COARSE_FRACTION = 0.7; // setup.rs:32
 const double RETRY_WIDENING = 1.5;      // setup.rs:36
 const size_t MAX_RETRIES = 3;           // setup.rs:37
-const size_t POWER_ITERATIONS = 20;     // setup.rs:41
+const int POWER_ITERATIONS = 20;        // setup.rs:41
 const double SPECTRAL_MARGIN = 1.15;    // setup.rs:45
 const double RANK_TOLERANCE = 1e-10;    // transfer.rs:12
 
@@ -51,99 +57,39 @@ void rows_parallel(size_t rows, int threads, F&& f) {
   });
 }
 
-// C += A B for row-major dense blocks (block.rs:229-245), same loop order.
-inline void add_product(double* out, const double* a, size_t a_rows, size_t middle, const double* b, size_t b_cols) {
-  for (size_t r = 0; r < a_rows; ++r)
-    for (size_t m = 0; m < middle; ++m) {
-      double s = a[r * middle + m];
-      for (size_t c = 0; c < b_cols; ++c) out[r * b_cols + c] += s * b[m * b_cols + c];
-    }
-}
-
-// Cholesky-based SPD block inverse (block.rs:186-224).
-bool invert_spd_block(const double* in, size_t n, double* out, double* pivot) {
-  double lower[36] = {0};
-  for (size_t i = 0; i < n; ++i)
-    for (size_t j = 0; j <= i; ++j) {
-      double sum = in[i * n + j];
-      for (size_t k = 0; k < j; ++k) sum -= lower[i * n + k] * lower[j * n + k];
-      if (i == j) {
-        if (!std::isfinite(sum) || sum <= 0.0) {
-          *pivot = sum;
-          return false;
+// A pattern: per row the sorted distinct columns that `candidates(row, emit)` emits. Columns are
+// below `width`; each thread dedupes with its own marker array.
+template <class F>
+void symbolic_rows(size_t rows, size_t width, int threads, F&& candidates, vector<uint32_t>& starts,
+                   vector<uint32_t>& cols) {
+  int chunks = (rows < 4096 || threads <= 1) ? 1 : threads;
+  vector<vector<uint32_t>> lengths(chunks), parts(chunks);
+  chunked(rows, threads, [&](int ci, size_t b, size_t e) {
+    vector<uint32_t> mark(width, 0xffffffffu), list;
+    vector<uint32_t>& len = lengths[ci];
+    vector<uint32_t>& out = parts[ci];
+    for (size_t row = b; row < e; ++row) {
+      list.clear();
+      candidates(row, [&](uint32_t c) {
+        if (mark[c] != (uint32_t)row) {
+          mark[c] = (uint32_t)row;
+          list.push_back(c);
         }
-        lower[i * n + j] = std::sqrt(sum);
-      } else {
-        lower[i * n + j] = sum / lower[j * n + j];
-      }
+      });
+      std::sort(list.begin(), list.end());
+      len.push_back((uint32_t)list.size());
+      out.insert(out.end(), list.begin(), list.end());
     }
-  double inv[36] = {0};
-  for (size_t c = 0; c < n; ++c)
-    for (size_t i = c; i < n; ++i) {
-      double sum = i == c ? 1.0 : 0.0;
-      for (size_t k = c; k < i; ++k) sum -= lower[i * n + k] * inv[k * n + c];
-      inv[i * n + c] = sum / lower[i * n + i];
-    }
-  for (size_t i = 0; i < n; ++i)
-    for (size_t j = 0; j < n; ++j) {
-      double sum = 0.0;
-      for (size_t k = std::max(i, j); k < n; ++k) sum += inv[k * n + i] * inv[k * n + j];
-      out[i * n + j] = sum;
-    }
-  return true;
-}
-
-// A sparse row whose block columns arrive in any order, read back sorted (block.rs:249-302).
-struct RowAccumulator {
-  vector<uint32_t> slot, touched;
-  vector<double> data;
-  size_t len;
-  RowAccumulator(size_t columns, size_t block_len) : slot(columns, 0xffffffffu), len(block_len) {}
-  void begin() {
-    for (uint32_t c : touched) slot[c] = 0xffffffffu;
-    touched.clear();
-    data.clear();
-  }
-  double* entry(uint32_t c) {
-    uint32_t at = slot[c];
-    if (at == 0xffffffffu) {
-      at = (uint32_t)touched.size();
-      slot[c] = at;
-      touched.push_back(c);
-      data.resize(data.size() + len, 0.0);
-    }
-    return data.data() + (size_t)at * len;
-  }
-  template <class F>
-  void drain(F&& emit) {
-    std::sort(touched.begin(), touched.end());
-    for (uint32_t c : touched) emit(c, data.data() + (size_t)slot[c] * len);
-  }
-};
-
-// A chunk of consecutive output rows built by one thread.
-struct RowChunk {
-  vector<uint32_t> lengths, cols;
-  vector<double> vals;
-};
-
-void stitch(vector<RowChunk>& chunks, size_t rows, size_t rb, size_t cb, Bsr& out) {
-  out.rows = rows;
-  out.rb = rb;
-  out.cb = cb;
+  });
+  starts.assign(1, 0);
+  starts.reserve(rows + 1);
   size_t total = 0;
-  for (auto& c : chunks) total += c.cols.size();
-  out.starts.assign(1, 0);
-  out.starts.reserve(rows + 1);
-  out.cols.clear();
-  out.cols.reserve(total);
-  out.vals.clear();
-  out.vals.reserve(total * rb * cb);
-  for (auto& c : chunks) {
-    for (uint32_t l : c.lengths) out.starts.push_back(out.starts.back() + l);
-    out.cols.insert(out.cols.end(), c.cols.begin(), c.cols.end());
-    out.vals.insert(out.vals.end(), c.vals.begin(), c.vals.end());
-    c = RowChunk();
+  for (auto& p : parts) total += p.size();
+  cols.clear();
+  cols.reserve(total);
+  for (int c = 0; c < chunks; ++c) {
+    for (uint32_t l : lengths[c]) starts.push_back(starts.back() + l);
+    cols.insert(cols.end(), parts[c].begin(), parts[c].end());
   }
 }
 
@@ -152,36 +98,21 @@ double squared_distance(const vector<P3>& p, size_t a, size_t b) {
   return dx * dx + dy * dy + dz * dz;
 }
 
-double block_norm(const double* b, size_t len) {
-  double s = 0.0;
-  for (size_t i = 0; i < len; ++i) s += b[i] * b[i];
-  return std::sqrt(s);
-}
-
-double start_value(size_t index) {  // block.rs:379-382
-  uint64_t mixed = ((uint64_t)index + 1) * 0x9E3779B97F4A7C15ull;
-  return 0.5 + (double)(mixed >> 11) / (double)(1ull << 53);
-}
-
-double norm2(const vector<double>& x) {  // block.rs:398-404, serial in index order
-  double s = 0.0;
-  for (double v : x) s += v * v;
-  return std::sqrt(s);
-}
-
 enum Phase { DIAGONAL, STRENGTH, AGGREGATE, TENTATIVE, SPECTRAL, FILTER, SMOOTH, PRODUCT, GALERKIN, FACTOR, DONE };
 
 }  // namespace
 
 struct SetupMachine {
+  DeviceSolver& dev;
   SetupOptions opt;
   Phase phase = DIAGONAL;
-  Bsr current;
+  Bsr current;  // host pattern, device values
   vector<double> near_null;
   vector<P3> positions;
   vector<HostLevel> levels;
   // per-level state
-  vector<double> inv;
+  double* inv = nullptr;  // device inverse diagonal
+  vector<double> norms;   // host copy of the block norms (join pass)
   bool is_coarsest = false;
   double reach = 3.0;
   size_t retries = 0;
@@ -191,13 +122,15 @@ struct SetupMachine {
   size_t aggregates = 0;
   vector<uint32_t> member_starts, members;
   vector<P3> coarse_positions;
-  Bsr tentative;
+  vector<double> tentative;  // rows x rb x 6, host (uploaded for smoothing)
   vector<double> coarse_null;
   double lambda_max = 0;
   vector<uint32_t> filter_starts, filter_cols;
   Bsr prolongator, ap, coarse;
   sf_status failure = SF_OK;
   bool cancelled = false;
+
+  explicit SetupMachine(DeviceSolver& d) : dev(d) {}
 
   size_t level_index() const { return levels.size(); }
 
@@ -208,34 +141,67 @@ struct SetupMachine {
     return fail(SF_MG_NOT_POSITIVE_DEFINITE, "a multigrid block is not positive definite");
   }
 
-  // setup.rs:269-321
+  template <class T>
+  sf_status upload(const vector<T>& h, T** d) {
+    if (sf_status e = dev_alloc(dev, (void**)d, std::max<size_t>(1, h.size()) * sizeof(T))) return e;
+    if (!h.empty()) copy_h2d(dev, *d, h.data(), h.size() * sizeof(T));
+    return SF_OK;
+  }
+  sf_status upload_pattern(Bsr& m) {
+    if (sf_status e = upload(m.starts, &m.dev_starts)) return e;
+    return upload(m.cols, &m.dev_cols);
+  }
+  void release(Bsr& m) {
+    dev_free(dev, m.dev);
+    dev_free(dev, m.dev_starts);
+    dev_free(dev, m.dev_cols);
+    m = Bsr();
+  }
+  sf_status sync(const char* what) { return cuda_check(cudaStreamSynchronize(dev.stream), what); }
+
+  // setup.rs:269-321 on the device; the block norms for the join pass come back to the host.
   sf_status run_diagonal() {
-    size_t rb = current.rb;
-    inv.assign(current.rows * rb * rb, 0.0);
-    std::atomic_size_t bad(SIZE_MAX);
-    vector<double> pivots(current.rows, 0.0);
-    rows_parallel(current.rows, opt.threads, [&](size_t row) {
-      const uint32_t* b = current.cols.data() + current.starts[row];
-      const uint32_t* e = current.cols.data() + current.starts[row + 1];
-      const uint32_t* it = std::lower_bound(b, e, (uint32_t)row);
-      double pivot = 0.0;
-      bool ok = it != e && *it == row &&
-                invert_spd_block(current.block(it - current.cols.data()), rb, inv.data() + row * rb * rb, &pivot);
-      if (!ok) {
-        pivots[row] = pivot;
-        size_t prev = bad.load();
-        while (row < prev && !bad.compare_exchange_weak(prev, row)) {
-        }
-      }
-    });
-    if (bad.load() != SIZE_MAX) return fail_pd(bad.load(), pivots[bad.load()]);
-    size_t dofs = current.rows * rb;
+    const size_t rb = current.rb, rows = current.rows;
+    unsigned long long* bad = nullptr;
+    double* pivots = nullptr;
+    sf_status e = dev_alloc(dev, (void**)&inv, rows * rb * rb * 8);
+    if (!e) e = dev_alloc(dev, (void**)&bad, 8);
+    if (!e) e = dev_alloc(dev, (void**)&pivots, std::max<size_t>(1, rows) * 8);
+    if (e) return e;
+    unsigned long long none = ~0ull;
+    copy_h2d(dev, bad, &none, 8);
+    e = setup_inverse_diagonal(dev.stream, (uint32_t)rows, (int)rb, current.dev_starts, current.dev_cols, current.dev,
+                               inv, bad, pivots);
+    unsigned long long first = ~0ull;
+    double pivot = 0.0;
+    if (!e) {
+      copy_d2h(dev, &first, bad, 8);
+      e = sync("inverse diagonal");
+    }
+    if (!e && first != ~0ull) {
+      copy_d2h(dev, &pivot, pivots + first, 8);
+      e = sync("inverse diagonal");
+      if (!e) e = fail_pd((size_t)first, pivot);
+    }
+    dev_free(dev, bad);
+    dev_free(dev, pivots);
+    if (e) return e;
+    size_t dofs = rows * rb;
     if (dofs <= opt.coarse_dofs || level_index() + 1 >= opt.max_levels) {
       is_coarsest = true;
       phase = SPECTRAL;
-    } else {
-      phase = STRENGTH;
+      return SF_OK;
     }
+    double* d_norms = nullptr;
+    size_t blocks = current.cols.size();
+    if ((e = dev_alloc(dev, (void**)&d_norms, std::max<size_t>(1, blocks) * 8))) return e;
+    e = setup_block_norms(dev.stream, blocks, (int)(rb * current.cb), current.dev, d_norms);
+    norms.assign(blocks, 0.0);
+    if (!e && blocks) copy_d2h(dev, norms.data(), d_norms, blocks * 8);
+    if (!e) e = sync("block norms");
+    dev_free(dev, d_norms);
+    if (e) return e;
+    phase = STRENGTH;
     return SF_OK;
   }
 
@@ -294,7 +260,6 @@ struct SetupMachine {
         seeded[strong_cols[k]] = 1;
       }
     }
-    size_t bl = current.rb * current.cb;
     for (size_t row = 0; row < rows; ++row) {
       if (aggregate[row] != NO_AGGREGATE) continue;
       const uint32_t* nb = strong_cols.data() + strong_starts[row];
@@ -304,7 +269,7 @@ struct SetupMachine {
       for (uint32_t at = current.starts[row]; at < current.starts[row + 1]; ++at) {
         uint32_t col = current.cols[at];
         if (!std::binary_search(nb, ne, col) || !seeded[col]) continue;
-        double n = block_norm(current.block(at), bl);
+        double n = norms[at];
         if (n > best) {
           best = n;
           chosen = aggregate[col];
@@ -353,13 +318,7 @@ struct SetupMachine {
   // Tentative prolongator by two-pass Gram-Schmidt per aggregate (transfer.rs:19-68).
   void run_tentative() {
     size_t rb = current.rb, rows = current.rows, block = rb * MODES;
-    tentative.rows = rows;
-    tentative.rb = rb;
-    tentative.cb = MODES;
-    tentative.starts.resize(rows + 1);
-    for (size_t r = 0; r <= rows; ++r) tentative.starts[r] = (uint32_t)r;
-    tentative.cols = aggregate;
-    tentative.vals.assign(rows * block, 0.0);
+    tentative.assign(rows * block, 0.0);
     coarse_null.assign(aggregates * 36, 0.0);
     rows_parallel(aggregates, opt.threads, [&](size_t a) {
       size_t count = member_starts[a + 1] - member_starts[a];
@@ -395,50 +354,38 @@ struct SetupMachine {
         }
       }
       for (size_t m = 0; m < count; ++m)
-        std::copy(local.begin() + m * block, local.begin() + (m + 1) * block,
-                  tentative.vals.begin() + (size_t)mem[m] * block);
+        std::copy(local.begin() + m * block, local.begin() + (m + 1) * block, tentative.begin() + (size_t)mem[m] * block);
     });
     phase = SPECTRAL;
   }
 
-  // Power iteration for lambda_max(D^-1 A) (setup.rs:390-449): row-parallel products, serial norm.
-  void run_spectral() {
+  // Power iteration for lambda_max(D^-1 A) (setup.rs:390-449), on the device.
+  sf_status run_spectral() {
     size_t rb = current.rb, rows = current.rows, dofs = rows * rb;
-    vector<double> v(dofs), s2(dofs);
-    for (size_t i = 0; i < dofs; ++i) v[i] = start_value(i);
-    double n0 = norm2(v);
-    for (double& x : v) x /= n0;
-    double lm = 0.0;
-    for (size_t it = 0; it < POWER_ITERATIONS; ++it) {
-      rows_parallel(rows, opt.threads, [&](size_t row) {
-        double y[6] = {0, 0, 0, 0, 0, 0};
-        for (uint32_t at = current.starts[row]; at < current.starts[row + 1]; ++at) {
-          const double* b = current.block(at);
-          size_t col = (size_t)current.cols[at] * current.cb;
-          for (size_t p = 0; p < rb; ++p) {
-            double sum = y[p];
-            for (size_t q = 0; q < current.cb; ++q) sum += b[p * current.cb + q] * v[col + q];
-            y[p] = sum;
-          }
-        }
-        const double* d = inv.data() + row * rb * rb;
-        for (size_t p = 0; p < rb; ++p) {
-          double sum = 0.0;
-          for (size_t q = 0; q < rb; ++q) sum += d[p * rb + q] * y[q];
-          s2[row * rb + p] = sum;
-        }
-      });
-      double n = norm2(s2);
-      lm = n;
-      rows_parallel(dofs, opt.threads, [&](size_t i) { v[i] = s2[i] / n; });
+    double *v = nullptr, *s2 = nullptr, *d_norms = nullptr;
+    sf_status e = dev_alloc(dev, (void**)&v, std::max<size_t>(1, dofs) * 8);
+    if (!e) e = dev_alloc(dev, (void**)&s2, std::max<size_t>(1, dofs) * 8);
+    if (!e) e = dev_alloc(dev, (void**)&d_norms, 16);
+    if (!e)
+      e = setup_power_iteration(dev.stream, (uint32_t)rows, (int)rb, current.dev_starts, current.dev_cols, current.dev,
+                                inv, v, s2, d_norms, POWER_ITERATIONS);
+    double lm[2] = {0.0, 0.0};
+    if (!e) {
+      copy_d2h(dev, lm, d_norms, 16);
+      e = sync("power iteration");
     }
-    lambda_max = lm * SPECTRAL_MARGIN;
+    dev_free(dev, v);
+    dev_free(dev, s2);
+    dev_free(dev, d_norms);
+    if (e) return e;
+    lambda_max = lm[1] * SPECTRAL_MARGIN;
     if (is_coarsest) {
       phase = (rows * rb <= DENSE_LIMIT) ? FACTOR : DONE;
       if (phase == DONE) push_final(false);
-      return;
+      return SF_OK;
     }
     phase = FILTER;
+    return SF_OK;
   }
 
   // Smoothing neighbours of a coarse level (aggregate.rs:80-96); the finest keeps its strong ones.
@@ -479,128 +426,129 @@ struct SetupMachine {
     phase = SMOOTH;
   }
 
-  // P = T - omega D^-1 A_f T, row by row (transfer.rs:108-152).
-  void run_smooth() {
-    double omega = 4.0 / (3.0 * lambda_max);
-    size_t rb = current.rb, cb = MODES, rows = current.rows;
-    int chunks = (rows < 4096 || opt.threads <= 1) ? 1 : opt.threads;
-    vector<RowChunk> out(chunks);
-    const vector<uint32_t>& ns = filter_starts.empty() ? strong_starts : filter_starts;
-    const vector<uint32_t>& nc = filter_starts.empty() ? strong_cols : filter_cols;
-    chunked(rows, opt.threads, [&](int ci, size_t b, size_t e) {
-      RowAccumulator acc(aggregates, rb * cb);
-      RowChunk& o = out[ci];
-      vector<double> scaled(rb * cb);
-      for (size_t row = b; row < e; ++row) {
-        acc.begin();
-        uint32_t t_col = tentative.cols[row];
-        acc.entry(t_col);
-        const uint32_t* nb = nc.data() + ns[row];
-        const uint32_t* ne = nc.data() + ns[row + 1];
-        for (uint32_t at = current.starts[row]; at < current.starts[row + 1]; ++at) {
-          uint32_t col = current.cols[at];
-          size_t src = (col == row || std::binary_search(nb, ne, col)) ? col : row;
-          double* acc_block = acc.entry(tentative.cols[src]);
-          add_product(acc_block, current.block(at), rb, current.cb, tentative.block(src), cb);
-        }
-        const double* dinv = inv.data() + row * rb * rb;
-        const double* t_block = tentative.block(row);
-        uint32_t n = 0;
-        acc.drain([&](uint32_t col, const double* blk) {
-          std::fill(scaled.begin(), scaled.end(), 0.0);
-          add_product(scaled.data(), dinv, rb, rb, blk, cb);
-          o.cols.push_back(col);
-          for (size_t i = 0; i < rb * cb; ++i) {
-            double t = col == t_col ? t_block[i] : 0.0;
-            o.vals.push_back(t - omega * scaled[i]);
-          }
-          ++n;
-        });
-        o.lengths.push_back(n);
-      }
-    });
-    stitch(out, rows, rb, cb, prolongator);
-    tentative = Bsr();
-    phase = PRODUCT;
+  // The row of every entry of a pattern, on the device.
+  sf_status entry_rows(const Bsr& m, uint32_t** out) {
+    if (sf_status e = dev_alloc(dev, (void**)out, std::max<size_t>(1, m.cols.size()) * 4)) return e;
+    return setup_entry_rows(dev.stream, (uint32_t)m.rows, m.dev_starts, *out);
   }
 
-  // A P row by row (transfer.rs:155-169).
-  void run_product() {
-    size_t rb = current.rb, cb = MODES, rows = current.rows;
-    int chunks = (rows < 4096 || opt.threads <= 1) ? 1 : opt.threads;
-    vector<RowChunk> out(chunks);
-    chunked(rows, opt.threads, [&](int ci, size_t b, size_t e) {
-      RowAccumulator acc(aggregates, rb * cb);
-      RowChunk& o = out[ci];
-      for (size_t row = b; row < e; ++row) {
-        acc.begin();
-        for (uint32_t at = current.starts[row]; at < current.starts[row + 1]; ++at) {
-          uint32_t col = current.cols[at];
-          for (uint32_t in = prolongator.starts[col]; in < prolongator.starts[col + 1]; ++in)
-            add_product(acc.entry(prolongator.cols[in]), current.block(at), rb, current.cb, prolongator.block(in), cb);
-        }
-        uint32_t n = 0;
-        acc.drain([&](uint32_t col, const double* blk) {
-          o.cols.push_back(col);
-          o.vals.insert(o.vals.end(), blk, blk + rb * cb);
-          ++n;
-        });
-        o.lengths.push_back(n);
-      }
-    });
-    stitch(out, rows, rb, cb, ap);
+  // P = T - omega D^-1 A_f T (transfer.rs:108-152). P's pattern: the row's own aggregate and the
+  // aggregates of its smoothing neighbours; its values on the device.
+  sf_status run_smooth() {
+    double omega = 4.0 / (3.0 * lambda_max);
+    size_t rb = current.rb, rows = current.rows;
+    const vector<uint32_t>& ns = filter_starts.empty() ? strong_starts : filter_starts;
+    const vector<uint32_t>& nc = filter_starts.empty() ? strong_cols : filter_cols;
+    prolongator = Bsr();
+    prolongator.rows = rows;
+    prolongator.rb = rb;
+    prolongator.cb = MODES;
+    symbolic_rows(
+        rows, aggregates, opt.threads,
+        [&](size_t row, auto&& emit) {
+          emit(aggregate[row]);
+          for (uint32_t k = ns[row]; k < ns[row + 1]; ++k) emit(aggregate[nc[k]]);
+        },
+        prolongator.starts, prolongator.cols);
+    uint32_t *n_starts = nullptr, *n_cols = nullptr, *agg = nullptr, *rows_of = nullptr;
+    double* t = nullptr;
+    size_t entries = prolongator.cols.size();
+    sf_status e = upload_pattern(prolongator);
+    if (!e) e = upload(ns, &n_starts);
+    if (!e) e = upload(nc, &n_cols);
+    if (!e) e = upload(aggregate, &agg);
+    if (!e) e = upload(tentative, &t);
+    if (!e) e = dev_alloc(dev, (void**)&prolongator.dev, std::max<size_t>(1, entries) * rb * MODES * 8);
+    if (!e) e = entry_rows(prolongator, &rows_of);
+    if (!e)
+      e = setup_smooth(dev.stream, (int)rb, entries, rows_of, prolongator.dev_cols, current.dev_starts,
+                       current.dev_cols, current.dev, n_starts, n_cols, agg, t, inv, omega, prolongator.dev);
+    if (!e) e = sync("smooth");
+    for (void* p : {(void*)n_starts, (void*)n_cols, (void*)agg, (void*)rows_of, (void*)t}) dev_free(dev, p);
+    if (e) return e;
+    tentative.clear();
+    tentative.shrink_to_fit();
+    phase = PRODUCT;
+    return SF_OK;
+  }
+
+  // A P (transfer.rs:155-169): pattern the union of P's rows at A's columns.
+  sf_status run_product() {
+    size_t rb = current.rb, rows = current.rows;
+    ap = Bsr();
+    ap.rows = rows;
+    ap.rb = rb;
+    ap.cb = MODES;
+    symbolic_rows(
+        rows, aggregates, opt.threads,
+        [&](size_t row, auto&& emit) {
+          for (uint32_t at = current.starts[row]; at < current.starts[row + 1]; ++at) {
+            uint32_t col = current.cols[at];
+            for (uint32_t in = prolongator.starts[col]; in < prolongator.starts[col + 1]; ++in)
+              emit(prolongator.cols[in]);
+          }
+        },
+        ap.starts, ap.cols);
+    uint32_t* rows_of = nullptr;
+    size_t entries = ap.cols.size();
+    sf_status e = upload_pattern(ap);
+    if (!e) e = dev_alloc(dev, (void**)&ap.dev, std::max<size_t>(1, entries) * rb * MODES * 8);
+    if (!e) e = entry_rows(ap, &rows_of);
+    if (!e)
+      e = setup_product(dev.stream, (int)rb, entries, rows_of, ap.dev_cols, current.dev_starts, current.dev_cols,
+                        current.dev, prolongator.dev_starts, prolongator.dev_cols, prolongator.dev, ap.dev);
+    if (!e) e = sync("product");
+    dev_free(dev, rows_of);
+    if (e) return e;
     phase = GALERKIN;
+    return SF_OK;
   }
 
   // P^T (A P) by coarse row, P read by columns with fine rows ascending (transfer.rs:173-238).
-  void run_galerkin() {
-    size_t fine = prolongator.rb, cdim = MODES;
-    vector<uint32_t> cstarts(aggregates + 1, 0);
-    for (uint32_t c : prolongator.cols) cstarts[c + 1] += 1;
-    for (size_t i = 0; i < aggregates; ++i) cstarts[i + 1] += cstarts[i];
-    vector<uint32_t> filled(cstarts.begin(), cstarts.end() - 1);
-    vector<std::pair<uint32_t, uint32_t>> entries(prolongator.cols.size());
+  sf_status run_galerkin() {
+    const size_t cdim = MODES;
+    vector<uint32_t> pt_starts(aggregates + 1, 0);
+    for (uint32_t c : prolongator.cols) pt_starts[c + 1] += 1;
+    for (size_t i = 0; i < aggregates; ++i) pt_starts[i + 1] += pt_starts[i];
+    vector<uint32_t> filled(pt_starts.begin(), pt_starts.end() - 1);
+    vector<uint32_t> pt_rows(prolongator.cols.size()), pt_at(prolongator.cols.size());
     for (size_t row = 0; row < prolongator.rows; ++row)
-      for (uint32_t at = prolongator.starts[row]; at < prolongator.starts[row + 1]; ++at)
-        entries[filled[prolongator.cols[at]]++] = {(uint32_t)row, at};
-    int chunks = (aggregates < 4096 || opt.threads <= 1) ? 1 : opt.threads;
-    vector<RowChunk> out(chunks);
-    chunked(aggregates, opt.threads, [&](int ci, size_t b, size_t e) {
-      RowAccumulator acc(aggregates, cdim * cdim);
-      RowChunk& o = out[ci];
-      vector<double> tr(fine * cdim);
-      for (size_t c = b; c < e; ++c) {
-        acc.begin();
-        for (uint32_t k = cstarts[c]; k < cstarts[c + 1]; ++k) {
-          uint32_t fine_row = entries[k].first;
-          const double* blk = prolongator.block(entries[k].second);
-          for (size_t p = 0; p < fine; ++p)
-            for (size_t q = 0; q < cdim; ++q) tr[q * fine + p] = blk[p * cdim + q];
-          for (uint32_t in = ap.starts[fine_row]; in < ap.starts[fine_row + 1]; ++in)
-            add_product(acc.entry(ap.cols[in]), tr.data(), cdim, fine, ap.block(in), cdim);
-        }
-        uint32_t n = 0;
-        acc.drain([&](uint32_t col, const double* blk) {
-          o.cols.push_back(col);
-          o.vals.insert(o.vals.end(), blk, blk + cdim * cdim);
-          ++n;
-        });
-        o.lengths.push_back(n);
+      for (uint32_t at = prolongator.starts[row]; at < prolongator.starts[row + 1]; ++at) {
+        uint32_t o = filled[prolongator.cols[at]]++;
+        pt_rows[o] = (uint32_t)row;
+        pt_at[o] = at;
       }
-    });
-    stitch(out, aggregates, cdim, cdim, coarse);
-    // finish_level, setup.rs:650-695: a zero coarse diagonal becomes one.
-    for (size_t row = 0; row < coarse.rows; ++row)
-      for (uint32_t at = coarse.starts[row]; at < coarse.starts[row + 1]; ++at) {
-        if (coarse.cols[at] != row) continue;
-        for (size_t d = 0; d < cdim; ++d) {
-          double& v = coarse.vals[(size_t)at * 36 + d * cdim + d];
-          if (v == 0.0) v = 1.0;
-        }
-      }
+    coarse = Bsr();
+    coarse.rows = aggregates;
+    coarse.rb = coarse.cb = cdim;
+    symbolic_rows(
+        aggregates, aggregates, opt.threads,
+        [&](size_t c, auto&& emit) {
+          for (uint32_t k = pt_starts[c]; k < pt_starts[c + 1]; ++k) {
+            uint32_t fine_row = pt_rows[k];
+            for (uint32_t in = ap.starts[fine_row]; in < ap.starts[fine_row + 1]; ++in) emit(ap.cols[in]);
+          }
+        },
+        coarse.starts, coarse.cols);
+    uint32_t *d_pt_starts = nullptr, *d_pt_rows = nullptr, *d_pt_at = nullptr, *rows_of = nullptr;
+    size_t entries = coarse.cols.size();
+    sf_status e = upload_pattern(coarse);
+    if (!e) e = upload(pt_starts, &d_pt_starts);
+    if (!e) e = upload(pt_rows, &d_pt_rows);
+    if (!e) e = upload(pt_at, &d_pt_at);
+    if (!e) e = dev_alloc(dev, (void**)&coarse.dev, std::max<size_t>(1, entries) * cdim * cdim * 8);
+    if (!e) e = entry_rows(coarse, &rows_of);
+    if (!e)
+      e = setup_galerkin(dev.stream, (int)prolongator.rb, entries, rows_of, coarse.dev_cols, d_pt_starts, d_pt_rows,
+                         d_pt_at, prolongator.dev, ap.dev_starts, ap.dev_cols, ap.dev, coarse.dev);
+    if (!e) e = sync("galerkin");
+    for (void* p : {(void*)d_pt_starts, (void*)d_pt_rows, (void*)d_pt_at, (void*)rows_of}) dev_free(dev, p);
+    release(ap);
+    if (e) return e;
     HostLevel lv;
     lv.a = std::move(current);
-    lv.inverse_diagonal = std::move(inv);
+    lv.inverse_diagonal = inv;
+    inv = nullptr;
     lv.lambda_max = lambda_max;
     lv.lambda_min = lambda_max / opt.range;
     lv.has_p = true;
@@ -609,20 +557,23 @@ struct SetupMachine {
     levels.push_back(std::move(lv));
     current = std::move(coarse);
     coarse = Bsr();
-    ap = Bsr();
+    prolongator = Bsr();
     near_null = std::move(coarse_null);
     positions = std::move(coarse_positions);
+    norms.clear();
     reach = opt.reach;
     retries = 0;
     is_coarsest = false;
     aggregates = 0;
     phase = DIAGONAL;
+    return SF_OK;
   }
 
   void push_final(bool factored) {
     HostLevel lv;
     lv.a = std::move(current);
-    lv.inverse_diagonal = std::move(inv);
+    lv.inverse_diagonal = inv;
+    inv = nullptr;
     lv.lambda_max = lambda_max;
     lv.lambda_min = lambda_max / opt.range;
     lv.has_factor = factored;
@@ -633,6 +584,9 @@ struct SetupMachine {
   // L^-T L^-1, which the device applies as one matrix-vector product per cycle.
   sf_status run_factor() {
     size_t n = current.rows * current.rb;
+    current.vals.assign(current.cols.size() * current.rb * current.cb, 0.0);
+    if (!current.vals.empty()) copy_d2h(dev, current.vals.data(), current.dev, current.vals.size() * 8);
+    if (sf_status e = sync("coarsest level")) return e;
     vector<double> f(n * n, 0.0);
     for (size_t row = 0; row < current.rows; ++row)
       for (uint32_t at = current.starts[row]; at < current.starts[row + 1]; ++at) {
@@ -674,7 +628,8 @@ struct SetupMachine {
     });
     lv.factor_n = n;
     lv.a = std::move(current);
-    lv.inverse_diagonal = std::move(inv);
+    lv.inverse_diagonal = inv;
+    inv = nullptr;
     lv.lambda_max = lambda_max;
     lv.lambda_min = lambda_max / opt.range;
     lv.has_factor = true;
@@ -684,9 +639,9 @@ struct SetupMachine {
   }
 };
 
-SetupMachine* setup_create(Bsr&& fine, vector<double>&& near_null, vector<P3>&& positions,
+SetupMachine* setup_create(DeviceSolver& solver, Bsr&& fine, vector<double>&& near_null, vector<P3>&& positions,
                            const SetupOptions& options) {
-  SetupMachine* m = new SetupMachine;
+  SetupMachine* m = new SetupMachine(solver);
   m->opt = options;
   m->current = std::move(fine);
   m->near_null = std::move(near_null);
@@ -712,11 +667,14 @@ sf_status setup_step(SetupMachine* m, size_t budget, sf_cancel_fn cancel, void* 
       case STRENGTH: m->run_strength(); break;
       case AGGREGATE: m->run_aggregate(); break;
       case TENTATIVE: m->run_tentative(); break;
-      case SPECTRAL: m->run_spectral(); rows *= 20; break;
+      case SPECTRAL:
+        s = m->run_spectral();
+        rows *= 20;
+        break;
       case FILTER: m->run_filter(); break;
-      case SMOOTH: m->run_smooth(); break;
-      case PRODUCT: m->run_product(); break;
-      case GALERKIN: m->run_galerkin(); break;
+      case SMOOTH: s = m->run_smooth(); break;
+      case PRODUCT: s = m->run_product(); break;
+      case GALERKIN: s = m->run_galerkin(); break;
       case FACTOR: s = m->run_factor(); break;
       case DONE: break;
     }

@@ -1,0 +1,489 @@
+// The FP64 numeric phases of the multigrid setup on the device: block-diagonal inversion, block
+// norms for the join pass, the power iteration for lambda_max(D^-1 A), prolongator smoothing,
+// A P and the Galerkin product P^T (A P) (crates/solidfem-solve/src/multigrid/setup.rs:269-321,
+// 390-449, 527-647; transfer.rs:108-238; block.rs:186-245, 379-404).
+//
+// Built with -fmad=false and IEEE division and square root. Every output value is one thread's
+// sequential sum over its contributions in the order the reference's serial loops visit them, so
+// the device hierarchy equals the reference's to the bit. Parallelism comes from independent
+// outputs: a thread owns one block row of the power iteration, one block of P, of A P or of the
+// coarse matrix. The order-dependent graph work (strength, aggregation, tentative prolongator)
+// and every sparsity pattern are built on the host (setup.cpp); only values live here.
+//
+// The one sequential reduction is the power iteration's norm (block.rs:398-404 sums the squares
+// in index order): a single block squares a chunk in parallel into shared memory while thread 0
+// adds the previous chunk in order.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+
+#include "device.h"
+
+namespace sf {
+
+namespace {
+
+const int kT = 256;
+
+int grid_for(size_t n) { return (int)std::max<size_t>(1, std::min<size_t>((n + kT - 1) / kT, 148 * 32)); }
+
+// C += A B for row-major dense blocks, the loop order of block.rs:229-245.
+template <int AR, int MID, int BC>
+__device__ __forceinline__ void add_product(double* out, const double* a, const double* b) {
+#pragma unroll
+  for (int r = 0; r < AR; ++r)
+#pragma unroll
+    for (int m = 0; m < MID; ++m) {
+      double s = a[r * MID + m];
+#pragma unroll
+      for (int c = 0; c < BC; ++c) out[r * BC + c] += s * b[m * BC + c];
+    }
+}
+
+__device__ __forceinline__ bool contains(const uint32_t* b, const uint32_t* e, uint32_t v) {
+  while (b < e) {
+    const uint32_t* mid = b + (e - b) / 2;
+    if (*mid < v)
+      b = mid + 1;
+    else if (*mid > v)
+      e = mid;
+    else
+      return true;
+  }
+  return false;
+}
+
+// Cholesky-based inverse of an SPD block (block.rs:186-224).
+template <int N>
+__device__ bool invert_spd(const double* in, double* out, double* pivot) {
+  double lower[N * N];
+  double inv[N * N];
+#pragma unroll
+  for (int i = 0; i < N * N; ++i) lower[i] = inv[i] = 0.0;
+  for (int i = 0; i < N; ++i)
+    for (int j = 0; j <= i; ++j) {
+      double sum = in[i * N + j];
+      for (int k = 0; k < j; ++k) sum -= lower[i * N + k] * lower[j * N + k];
+      if (i == j) {
+        if (!isfinite(sum) || sum <= 0.0) {
+          *pivot = sum;
+          return false;
+        }
+        lower[i * N + j] = sqrt(sum);
+      } else {
+        lower[i * N + j] = sum / lower[j * N + j];
+      }
+    }
+  for (int c = 0; c < N; ++c)
+    for (int i = c; i < N; ++i) {
+      double sum = i == c ? 1.0 : 0.0;
+      for (int k = c; k < i; ++k) sum -= lower[i * N + k] * inv[k * N + c];
+      inv[i * N + c] = sum / lower[i * N + i];
+    }
+  for (int i = 0; i < N; ++i)
+    for (int j = 0; j < N; ++j) {
+      double sum = 0.0;
+      for (int k = i > j ? i : j; k < N; ++k) sum += inv[k * N + i] * inv[k * N + j];
+      out[i * N + j] = sum;
+    }
+  return true;
+}
+
+template <int N>
+__global__ void inverse_diagonal_kernel(uint32_t rows, const uint32_t* __restrict__ starts,
+                                        const uint32_t* __restrict__ cols, const double* __restrict__ vals,
+                                        double* __restrict__ inv, unsigned long long* bad, double* __restrict__ pivots) {
+  for (uint32_t row = blockIdx.x * blockDim.x + threadIdx.x; row < rows; row += gridDim.x * blockDim.x) {
+    const uint32_t* b = cols + starts[row];
+    const uint32_t* e = cols + starts[row + 1];
+    const uint32_t* lo = b;
+    const uint32_t* hi = e;
+    while (lo < hi) {
+      const uint32_t* mid = lo + (hi - lo) / 2;
+      if (*mid < row)
+        lo = mid + 1;
+      else
+        hi = mid;
+    }
+    double pivot = 0.0;
+    bool ok = lo != e && *lo == row &&
+              invert_spd<N>(vals + (size_t)(lo - cols) * N * N, inv + (size_t)row * N * N, &pivot);
+    if (!ok) {
+      pivots[row] = pivot;
+      atomicMin(bad, (unsigned long long)row);
+    }
+  }
+}
+
+template <int LEN>
+__global__ void block_norms_kernel(size_t blocks, const double* __restrict__ vals, double* __restrict__ out) {
+  for (size_t b = blockIdx.x * (size_t)blockDim.x + threadIdx.x; b < blocks; b += (size_t)gridDim.x * blockDim.x) {
+    double s = 0.0;
+#pragma unroll
+    for (int i = 0; i < LEN; ++i) {
+      double v = vals[b * LEN + i];
+      s += v * v;
+    }
+    out[b] = sqrt(s);
+  }
+}
+
+// start_value (block.rs:379-382): a fixed pseudo-random vector in [0.5, 1.5).
+__global__ void start_vector_kernel(size_t n, double* __restrict__ v) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    unsigned long long mixed = (unsigned long long)(i + 1) * 0x9E3779B97F4A7C15ull;
+    v[i] = 0.5 + (double)(mixed >> 11) / 9007199254740992.0;
+  }
+}
+
+// norm2 (block.rs:398-404): the squares summed in index order, then the square root.
+const int kNormChunk = 2048;
+const int kNormThreads = 512;
+__global__ void __launch_bounds__(kNormThreads) serial_norm_kernel(size_t n, const double* __restrict__ v,
+                                                                    double* __restrict__ out) {
+  __shared__ double sq[2][kNormChunk];
+  const size_t chunks = (n + kNormChunk - 1) / kNormChunk;
+  for (int t = threadIdx.x; t < kNormChunk; t += blockDim.x) {
+    double x = (size_t)t < n ? v[t] : 0.0;
+    sq[0][t] = x * x;
+  }
+  __syncthreads();
+  double s = 0.0;
+  for (size_t c = 0; c < chunks; ++c) {
+    const int cur = (int)(c & 1);
+    if (threadIdx.x == 0) {
+      const int len = (int)min((size_t)kNormChunk, n - c * kNormChunk);
+      const double* q = sq[cur];
+#pragma unroll 16
+      for (int k = 0; k < len; ++k) s += q[k];
+    } else if (c + 1 < chunks) {
+      const size_t base = (c + 1) * kNormChunk;
+      for (int t = threadIdx.x - 1; t < kNormChunk; t += blockDim.x - 1) {
+        double x = base + t < n ? v[base + t] : 0.0;
+        sq[cur ^ 1][t] = x * x;
+      }
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *out = sqrt(s);
+}
+
+// v = src / norm, element by element.
+__global__ void scale_kernel(size_t n, const double* __restrict__ src, const double* __restrict__ norm,
+                             double* __restrict__ v) {
+  const double d = *norm;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    v[i] = src[i] / d;
+}
+
+// s2 = D^-1 (A v) for one block row per thread, in the order of setup.rs:404-432.
+template <int N>
+__global__ void power_step_kernel(uint32_t rows, const uint32_t* __restrict__ starts, const uint32_t* __restrict__ cols,
+                                  const double* __restrict__ vals, const double* __restrict__ inv,
+                                  const double* __restrict__ v, double* __restrict__ s2) {
+  for (uint32_t row = blockIdx.x * blockDim.x + threadIdx.x; row < rows; row += gridDim.x * blockDim.x) {
+    double y[N];
+#pragma unroll
+    for (int p = 0; p < N; ++p) y[p] = 0.0;
+    for (uint32_t at = starts[row]; at < starts[row + 1]; ++at) {
+      const double* b = vals + (size_t)at * N * N;
+      const double* x = v + (size_t)cols[at] * N;
+      double xv[N];
+#pragma unroll
+      for (int q = 0; q < N; ++q) xv[q] = x[q];
+#pragma unroll
+      for (int p = 0; p < N; ++p) {
+        double sum = y[p];
+#pragma unroll
+        for (int q = 0; q < N; ++q) sum += b[p * N + q] * xv[q];
+        y[p] = sum;
+      }
+    }
+    const double* d = inv + (size_t)row * N * N;
+#pragma unroll
+    for (int p = 0; p < N; ++p) {
+      double sum = 0.0;
+#pragma unroll
+      for (int q = 0; q < N; ++q) sum += d[p * N + q] * y[q];
+      s2[(size_t)row * N + p] = sum;
+    }
+  }
+}
+
+// The block row of each entry of a block pattern.
+__global__ void entry_rows_kernel(uint32_t rows, const uint32_t* __restrict__ starts, uint32_t* __restrict__ out) {
+  for (uint32_t row = blockIdx.x * blockDim.x + threadIdx.x; row < rows; row += gridDim.x * blockDim.x)
+    for (uint32_t j = starts[row]; j < starts[row + 1]; ++j) out[j] = row;
+}
+
+// One block of P = T - omega D^-1 A_f T (transfer.rs:108-152): A's blocks whose column is the row
+// or a smoothing neighbour act on that column's tentative block; the others are lumped onto the
+// row's own (src = row). Contributions to this block's coarse column add in A's column order.
+template <int N>
+__global__ void smooth_kernel(size_t entries, const uint32_t* __restrict__ entry_row, const uint32_t* __restrict__ p_cols,
+                              const uint32_t* __restrict__ a_starts, const uint32_t* __restrict__ a_cols,
+                              const double* __restrict__ a_vals, const uint32_t* __restrict__ n_starts,
+                              const uint32_t* __restrict__ n_cols, const uint32_t* __restrict__ aggregate,
+                              const double* __restrict__ t_vals, const double* __restrict__ inv, double omega,
+                              double* __restrict__ p_vals) {
+  constexpr int L = N * 6;
+  for (size_t j = blockIdx.x * (size_t)blockDim.x + threadIdx.x; j < entries; j += (size_t)gridDim.x * blockDim.x) {
+    const uint32_t row = entry_row[j], c = p_cols[j];
+    const uint32_t* nb = n_cols + n_starts[row];
+    const uint32_t* ne = n_cols + n_starts[row + 1];
+    double acc[L];
+#pragma unroll
+    for (int i = 0; i < L; ++i) acc[i] = 0.0;
+    for (uint32_t at = a_starts[row]; at < a_starts[row + 1]; ++at) {
+      const uint32_t col = a_cols[at];
+      const uint32_t src = (col == row || contains(nb, ne, col)) ? col : row;
+      if (aggregate[src] != c) continue;
+      add_product<N, N, 6>(acc, a_vals + (size_t)at * N * N, t_vals + (size_t)src * L);
+    }
+    const double* d = inv + (size_t)row * N * N;
+    const double* t = t_vals + (size_t)row * L;
+    const bool own = c == aggregate[row];
+    double* out = p_vals + j * L;
+#pragma unroll
+    for (int r = 0; r < N; ++r)
+#pragma unroll
+      for (int q = 0; q < 6; ++q) {
+        double s = 0.0;
+#pragma unroll
+        for (int m = 0; m < N; ++m) s += d[r * N + m] * acc[m * 6 + q];
+        double tv = own ? t[r * 6 + q] : 0.0;
+        out[r * 6 + q] = tv - omega * s;
+      }
+  }
+}
+
+// One block of A P (transfer.rs:155-169): A's blocks in column order, each times the blocks of
+// P's row at that column whose coarse column is this block's.
+template <int N>
+__global__ void product_kernel(size_t entries, const uint32_t* __restrict__ entry_row, const uint32_t* __restrict__ ap_cols,
+                               const uint32_t* __restrict__ a_starts, const uint32_t* __restrict__ a_cols,
+                               const double* __restrict__ a_vals, const uint32_t* __restrict__ p_starts,
+                               const uint32_t* __restrict__ p_cols, const double* __restrict__ p_vals,
+                               double* __restrict__ ap_vals) {
+  constexpr int L = N * 6;
+  for (size_t j = blockIdx.x * (size_t)blockDim.x + threadIdx.x; j < entries; j += (size_t)gridDim.x * blockDim.x) {
+    const uint32_t row = entry_row[j], c = ap_cols[j];
+    double acc[L];
+#pragma unroll
+    for (int i = 0; i < L; ++i) acc[i] = 0.0;
+    for (uint32_t at = a_starts[row]; at < a_starts[row + 1]; ++at) {
+      const uint32_t col = a_cols[at];
+      for (uint32_t in = p_starts[col]; in < p_starts[col + 1]; ++in) {
+        const uint32_t pc = p_cols[in];
+        if (pc < c) continue;
+        if (pc == c) add_product<N, N, 6>(acc, a_vals + (size_t)at * N * N, p_vals + (size_t)in * L);
+        break;
+      }
+    }
+    double* out = ap_vals + j * L;
+#pragma unroll
+    for (int i = 0; i < L; ++i) out[i] = acc[i];
+  }
+}
+
+// One block of P^T (A P) (transfer.rs:173-238): the fine rows of P's column in ascending order,
+// each P block transposed times the A P block of that fine row at this block's column; a zero on
+// the diagonal of a diagonal block becomes one (finish_level, setup.rs:650-695).
+template <int N>
+__global__ void galerkin_kernel(size_t entries, const uint32_t* __restrict__ entry_row, const uint32_t* __restrict__ c_cols,
+                                const uint32_t* __restrict__ pt_starts, const uint32_t* __restrict__ pt_rows,
+                                const uint32_t* __restrict__ pt_at, const double* __restrict__ p_vals,
+                                const uint32_t* __restrict__ ap_starts, const uint32_t* __restrict__ ap_cols,
+                                const double* __restrict__ ap_vals, double* __restrict__ c_vals) {
+  constexpr int L = N * 6;
+  for (size_t j = blockIdx.x * (size_t)blockDim.x + threadIdx.x; j < entries; j += (size_t)gridDim.x * blockDim.x) {
+    const uint32_t crow = entry_row[j], c = c_cols[j];
+    double acc[36];
+#pragma unroll
+    for (int i = 0; i < 36; ++i) acc[i] = 0.0;
+    for (uint32_t k = pt_starts[crow]; k < pt_starts[crow + 1]; ++k) {
+      const uint32_t fine_row = pt_rows[k];
+      const uint32_t* b = ap_cols + ap_starts[fine_row];
+      const uint32_t* e = ap_cols + ap_starts[fine_row + 1];
+      const uint32_t* lo = b;
+      const uint32_t* hi = e;
+      while (lo < hi) {
+        const uint32_t* mid = lo + (hi - lo) / 2;
+        if (*mid < c)
+          lo = mid + 1;
+        else
+          hi = mid;
+      }
+      if (lo == e || *lo != c) continue;
+      const double* pb = p_vals + (size_t)pt_at[k] * L;
+      const double* ab = ap_vals + (size_t)(lo - ap_cols) * L;
+#pragma unroll
+      for (int r = 0; r < 6; ++r)
+#pragma unroll
+        for (int m = 0; m < N; ++m) {
+          double s = pb[m * 6 + r];
+#pragma unroll
+          for (int q = 0; q < 6; ++q) acc[r * 6 + q] += s * ab[m * 6 + q];
+        }
+    }
+    if (crow == c)
+#pragma unroll
+      for (int d = 0; d < 6; ++d)
+        if (acc[d * 6 + d] == 0.0) acc[d * 6 + d] = 1.0;
+    double* out = c_vals + j * 36;
+#pragma unroll
+    for (int i = 0; i < 36; ++i) out[i] = acc[i];
+  }
+}
+
+template <typename S>
+__global__ void convert_kernel(size_t n, const double* __restrict__ in, S* __restrict__ out) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    out[i] = (S)in[i];
+}
+
+// R = P^T block by block: R block o is P block src[o] transposed (rb x cb into cb x rb).
+template <typename S>
+__global__ void transpose_blocks_kernel(size_t blocks, int rb, int cb, const uint32_t* __restrict__ src,
+                                        const double* __restrict__ in, S* __restrict__ out) {
+  const int len = rb * cb;
+  for (size_t o = blockIdx.x * (size_t)blockDim.x + threadIdx.x; o < blocks; o += (size_t)gridDim.x * blockDim.x) {
+    const double* p = in + (size_t)src[o] * len;
+    S* t = out + o * len;
+    for (int a = 0; a < rb; ++a)
+      for (int b = 0; b < cb; ++b) t[b * rb + a] = (S)p[a * cb + b];
+  }
+}
+
+// SELL placement with conversion from the f64 setup values.
+template <typename S, int LEN>
+__global__ void sell_place_kernel(size_t blocks, const uint32_t* __restrict__ pos, const double* __restrict__ in,
+                                  S* __restrict__ out) {
+  for (size_t b = blockIdx.x * (size_t)blockDim.x + threadIdx.x; b < blocks; b += (size_t)gridDim.x * blockDim.x) {
+    uint32_t q = pos[b], t = q & 31u;
+    size_t base = (size_t)(q - t) * LEN + t;
+#pragma unroll
+    for (int e = 0; e < LEN; ++e) out[base + 32 * e] = (S)in[b * LEN + e];
+  }
+}
+
+}  // namespace
+
+sf_status setup_inverse_diagonal(cudaStream_t st, uint32_t rows, int rb, const uint32_t* starts, const uint32_t* cols,
+                                 const double* vals, double* inv, unsigned long long* bad, double* pivots) {
+  if (rows == 0) return SF_OK;
+  if (rb == 3)
+    inverse_diagonal_kernel<3><<<grid_for(rows), kT, 0, st>>>(rows, starts, cols, vals, inv, bad, pivots);
+  else
+    inverse_diagonal_kernel<6><<<grid_for(rows), kT, 0, st>>>(rows, starts, cols, vals, inv, bad, pivots);
+  return cuda_check(cudaGetLastError(), "inverse diagonal");
+}
+
+sf_status setup_block_norms(cudaStream_t st, size_t blocks, int len, const double* vals, double* out) {
+  if (blocks == 0) return SF_OK;
+  if (len == 9)
+    block_norms_kernel<9><<<grid_for(blocks), kT, 0, st>>>(blocks, vals, out);
+  else
+    block_norms_kernel<36><<<grid_for(blocks), kT, 0, st>>>(blocks, vals, out);
+  return cuda_check(cudaGetLastError(), "block norms");
+}
+
+sf_status setup_power_iteration(cudaStream_t st, uint32_t rows, int rb, const uint32_t* starts, const uint32_t* cols,
+                                const double* vals, const double* inv, double* v, double* s2, double* norms,
+                                int iterations) {
+  const size_t n = (size_t)rows * rb;
+  if (n == 0) return SF_OK;
+  start_vector_kernel<<<grid_for(n), kT, 0, st>>>(n, v);
+  serial_norm_kernel<<<1, kNormThreads, 0, st>>>(n, v, norms);
+  scale_kernel<<<grid_for(n), kT, 0, st>>>(n, v, norms, v);
+  for (int it = 0; it < iterations; ++it) {
+    if (rb == 3)
+      power_step_kernel<3><<<grid_for(rows), kT, 0, st>>>(rows, starts, cols, vals, inv, v, s2);
+    else
+      power_step_kernel<6><<<grid_for(rows), kT, 0, st>>>(rows, starts, cols, vals, inv, v, s2);
+    serial_norm_kernel<<<1, kNormThreads, 0, st>>>(n, s2, norms + 1);
+    scale_kernel<<<grid_for(n), kT, 0, st>>>(n, s2, norms + 1, v);
+  }
+  return cuda_check(cudaGetLastError(), "power iteration");
+}
+
+sf_status setup_entry_rows(cudaStream_t st, uint32_t rows, const uint32_t* starts, uint32_t* out) {
+  if (rows == 0) return SF_OK;
+  entry_rows_kernel<<<grid_for(rows), kT, 0, st>>>(rows, starts, out);
+  return cuda_check(cudaGetLastError(), "entry rows");
+}
+
+sf_status setup_smooth(cudaStream_t st, int rb, size_t entries, const uint32_t* entry_row, const uint32_t* p_cols,
+                       const uint32_t* a_starts, const uint32_t* a_cols, const double* a_vals, const uint32_t* n_starts,
+                       const uint32_t* n_cols, const uint32_t* aggregate, const double* t_vals, const double* inv,
+                       double omega, double* p_vals) {
+  if (entries == 0) return SF_OK;
+  if (rb == 3)
+    smooth_kernel<3><<<grid_for(entries), kT, 0, st>>>(entries, entry_row, p_cols, a_starts, a_cols, a_vals, n_starts,
+                                                       n_cols, aggregate, t_vals, inv, omega, p_vals);
+  else
+    smooth_kernel<6><<<grid_for(entries), kT, 0, st>>>(entries, entry_row, p_cols, a_starts, a_cols, a_vals, n_starts,
+                                                       n_cols, aggregate, t_vals, inv, omega, p_vals);
+  return cuda_check(cudaGetLastError(), "smooth");
+}
+
+sf_status setup_product(cudaStream_t st, int rb, size_t entries, const uint32_t* entry_row, const uint32_t* ap_cols,
+                        const uint32_t* a_starts, const uint32_t* a_cols, const double* a_vals, const uint32_t* p_starts,
+                        const uint32_t* p_cols, const double* p_vals, double* ap_vals) {
+  if (entries == 0) return SF_OK;
+  if (rb == 3)
+    product_kernel<3><<<grid_for(entries), kT, 0, st>>>(entries, entry_row, ap_cols, a_starts, a_cols, a_vals,
+                                                        p_starts, p_cols, p_vals, ap_vals);
+  else
+    product_kernel<6><<<grid_for(entries), kT, 0, st>>>(entries, entry_row, ap_cols, a_starts, a_cols, a_vals,
+                                                        p_starts, p_cols, p_vals, ap_vals);
+  return cuda_check(cudaGetLastError(), "product");
+}
+
+sf_status setup_galerkin(cudaStream_t st, int rb, size_t entries, const uint32_t* entry_row, const uint32_t* c_cols,
+                         const uint32_t* pt_starts, const uint32_t* pt_rows, const uint32_t* pt_at, const double* p_vals,
+                         const uint32_t* ap_starts, const uint32_t* ap_cols, const double* ap_vals, double* c_vals) {
+  if (entries == 0) return SF_OK;
+  if (rb == 3)
+    galerkin_kernel<3><<<grid_for(entries), kT, 0, st>>>(entries, entry_row, c_cols, pt_starts, pt_rows, pt_at, p_vals,
+                                                         ap_starts, ap_cols, ap_vals, c_vals);
+  else
+    galerkin_kernel<6><<<grid_for(entries), kT, 0, st>>>(entries, entry_row, c_cols, pt_starts, pt_rows, pt_at, p_vals,
+                                                         ap_starts, ap_cols, ap_vals, c_vals);
+  return cuda_check(cudaGetLastError(), "galerkin");
+}
+
+template <typename S>
+sf_status setup_convert(cudaStream_t st, size_t n, const double* in, S* out) {
+  if (n == 0) return SF_OK;
+  convert_kernel<S><<<grid_for(n), kT, 0, st>>>(n, in, out);
+  return cuda_check(cudaGetLastError(), "convert");
+}
+template sf_status setup_convert<float>(cudaStream_t, size_t, const double*, float*);
+template sf_status setup_convert<double>(cudaStream_t, size_t, const double*, double*);
+
+template <typename S>
+sf_status setup_transpose_blocks(cudaStream_t st, size_t blocks, int rb, int cb, const uint32_t* src, const double* in,
+                                 S* out) {
+  if (blocks == 0) return SF_OK;
+  transpose_blocks_kernel<S><<<grid_for(blocks), kT, 0, st>>>(blocks, rb, cb, src, in, out);
+  return cuda_check(cudaGetLastError(), "transpose blocks");
+}
+template sf_status setup_transpose_blocks<float>(cudaStream_t, size_t, int, int, const uint32_t*, const double*, float*);
+template sf_status setup_transpose_blocks<double>(cudaStream_t, size_t, int, int, const uint32_t*, const double*, double*);
+
+template <typename S>
+sf_status setup_sell_place(cudaStream_t st, size_t blocks, int len, const uint32_t* pos, const double* in, S* out) {
+  if (blocks == 0) return SF_OK;
+  switch (len) {
+    case 9: sell_place_kernel<S, 9><<<grid_for(blocks), kT, 0, st>>>(blocks, pos, in, out); break;
+    case 18: sell_place_kernel<S, 18><<<grid_for(blocks), kT, 0, st>>>(blocks, pos, in, out); break;
+    case 36: sell_place_kernel<S, 36><<<grid_for(blocks), kT, 0, st>>>(blocks, pos, in, out); break;
+    default: return fail(SF_INVALID_ARGUMENT, "unsupported block size for the SELL layout");
+  }
+  return cuda_check(cudaGetLastError(), "SELL placement");
+}
+template sf_status setup_sell_place<float>(cudaStream_t, size_t, int, const uint32_t*, const double*, float*);
+template sf_status setup_sell_place<double>(cudaStream_t, size_t, int, const uint32_t*, const double*, double*);
+
+}  // namespace sf

@@ -69,23 +69,28 @@ struct Model {
   vector<std::pair<std::pair<uint32_t, uint32_t>, double>> prescribed;  // (node, axis) -> value
 };
 
-// ----------------------------------------------------------------------------- host block CSR
-// A block sparse matrix of dense rb x cb row-major blocks, f64 (setup works in f64).
+// ----------------------------------------------------------------------------- block CSR
+// A block sparse matrix of dense rb x cb row-major blocks, f64 (setup works in f64). The pattern
+// is on the host; the multigrid levels keep their values on the device (`dev`, with device
+// copies of the pattern), and `vals` is filled on the host only where host code reads values.
 struct Bsr {
   size_t rows = 0, rb = 0, cb = 0;
   vector<uint32_t> starts;  // rows + 1
   vector<uint32_t> cols;
   vector<double> vals;
+  double* dev = nullptr;            // blocks * rb * cb f64 values on the device
+  uint32_t* dev_starts = nullptr;   // device copies of starts and cols
+  uint32_t* dev_cols = nullptr;
   size_t blocks() const { return cols.size(); }
   size_t block_len() const { return rb * cb; }
   const double* block(size_t at) const { return vals.data() + at * rb * cb; }
   double* block(size_t at) { return vals.data() + at * rb * cb; }
 };
 
-// One finished level of the hierarchy (f64 values as setup built them).
+// One finished level of the hierarchy: host patterns, f64 values on the device as setup built them.
 struct HostLevel {
   Bsr a;
-  vector<double> inverse_diagonal;
+  double* inverse_diagonal = nullptr;  // device, rows * rb * rb f64
   double lambda_min = 0, lambda_max = 0;
   bool has_p = false;
   Bsr p;
@@ -104,9 +109,12 @@ struct SetupOptions {
 };
 
 // The multigrid setup (crates/solidfem-solve/src/multigrid/setup.rs) over the device-assembled
-// fine level. Resumable by phase and row cursor, like the reference's state machine.
+// fine level (`fine` carries the host pattern and the device values and pattern). Graph phases
+// run on the host, numeric phases on the solver's device and stream; every allocation belongs to
+// the solver. Resumable by phase, like the reference's state machine.
 struct SetupMachine;
-SetupMachine* setup_create(Bsr&& fine, vector<double>&& near_null, vector<P3>&& positions,
+struct DeviceSolver;
+SetupMachine* setup_create(DeviceSolver& solver, Bsr&& fine, vector<double>&& near_null, vector<P3>&& positions,
                            const SetupOptions& options);
 // Runs up to `budget` rows of work. Returns SF_OK and sets *finished, or a failure.
 sf_status setup_step(SetupMachine* machine, size_t budget, sf_cancel_fn cancel, void* user,

@@ -1148,9 +1148,21 @@ sf_status dev_alloc(DeviceSolver& s, void** ptr, size_t bytes) {
   cudaError_t e = cudaMalloc(ptr, padded);
   if (e != cudaSuccess) return cuda_check(e, "cudaMalloc");
   cudaMemsetAsync(*ptr, 0, padded, s.stream);
-  s.owned.push_back(*ptr);
+  s.owned.push_back({*ptr, padded});
   s.bytes += padded;
   return SF_OK;
+}
+
+void dev_free(DeviceSolver& s, void* ptr) {
+  if (!ptr) return;
+  for (size_t i = 0; i < s.owned.size(); ++i)
+    if (s.owned[i].first == ptr) {
+      cudaFree(ptr);
+      s.bytes -= s.owned[i].second;
+      s.owned[i] = s.owned.back();
+      s.owned.pop_back();
+      return;
+    }
 }
 
 void dev_free_all(DeviceSolver& s) {
@@ -1158,7 +1170,7 @@ void dev_free_all(DeviceSolver& s) {
   if (s.graph) cudaGraphDestroy(s.graph);
   s.graph_exec = nullptr;
   s.graph = nullptr;
-  for (void* p : s.owned) cudaFree(p);
+  for (auto& p : s.owned) cudaFree(p.first);
   s.owned.clear();
   s.bytes = 0;
 }
@@ -1261,24 +1273,22 @@ sf_status upload_sell_layout(DeviceSolver& s, DevBsr& m, const SellLayout& L, si
 
 }  // namespace
 
+// The SELL copy of a matrix from its f64 values on the device, converted to S.
 template <typename S>
-sf_status make_sell(DeviceSolver& s, DevBsr& m, const uint32_t* starts, const uint32_t* cols, const S* vals) {
+sf_status make_sell_converted(DeviceSolver& s, DevBsr& m, const uint32_t* starts, const uint32_t* cols,
+                              const double* vals) {
   SellLayout L = sell_layout(m.rows, starts, cols);
-  const size_t len = (size_t)m.rb * m.cb;
-  if (sf_status e = upload_sell_layout(s, m, L, len * sizeof(S))) return e;
-  std::vector<S> v(L.cols.size() * len, S(0));
-  for (size_t b = 0; b < L.pos.size(); ++b) {
-    uint32_t q = L.pos[b], t = q & 31u;
-    size_t base = (size_t)(q - t) * len + t;
-    for (size_t el = 0; el < len; ++el) v[base + 32 * el] = vals[b * len + el];
-  }
-  if (!v.empty()) copy_h2d(s, m.sell_vals, v.data(), v.size() * sizeof(S));
+  const int len = (int)(m.rb * m.cb);
+  if (sf_status e = upload_sell_layout(s, m, L, (size_t)len * sizeof(S))) return e;
+  uint32_t* pos = nullptr;
+  if (sf_status e = dev_alloc(s, (void**)&pos, std::max<size_t>(1, L.pos.size()) * 4)) return e;
+  if (!L.pos.empty()) copy_h2d(s, pos, L.pos.data(), L.pos.size() * 4);
+  sf_status e = setup_sell_place<S>(s.stream, L.pos.size(), len, pos, vals, (S*)m.sell_vals);
+  if (!e) e = cuda_check(cudaStreamSynchronize(s.stream), "SELL placement");
+  dev_free(s, pos);
   m.sell = true;
-  return cuda_check(cudaStreamSynchronize(s.stream), "SELL upload");
+  return e;
 }
-
-template sf_status make_sell<float>(DeviceSolver&, DevBsr&, const uint32_t*, const uint32_t*, const float*);
-template sf_status make_sell<double>(DeviceSolver&, DevBsr&, const uint32_t*, const uint32_t*, const double*);
 
 sf_status make_sell_from_device(DeviceSolver& s, DevBsr& m, const uint32_t* starts, const uint32_t* cols) {
   SellLayout L = sell_layout(m.rows, starts, cols);
@@ -1295,39 +1305,35 @@ sf_status make_sell_from_device(DeviceSolver& s, DevBsr& m, const uint32_t* star
 
 namespace {
 
+// A level operator on the device from the setup's f64 values: the setup's device pattern, the
+// values converted to S (or the f64 values themselves when S is double and `alias` holds), row
+// groups, and a SELL copy when the operator has many rows.
 template <typename S>
-sf_status upload_bsr(DeviceSolver& s, const Bsr& h, DevBsr& d) {
+sf_status device_bsr(DeviceSolver& s, const Bsr& h, DevBsr& d, bool alias) {
   d.rows = (uint32_t)h.rows;
   d.rb = (uint32_t)h.rb;
   d.cb = (uint32_t)h.cb;
   d.blocks = h.cols.size();
-  if (sf_status e = dev_alloc(s, (void**)&d.starts, (h.rows + 1) * 4)) return e;
-  if (sf_status e = dev_alloc(s, (void**)&d.cols, std::max<size_t>(1, h.cols.size()) * 4)) return e;
-  if (sf_status e = dev_alloc(s, &d.vals, std::max<size_t>(1, h.vals.size()) * sizeof(S))) return e;
-  copy_h2d(s, d.starts, h.starts.data(), (h.rows + 1) * 4);
-  if (!h.cols.empty()) copy_h2d(s, d.cols, h.cols.data(), h.cols.size() * 4);
-  if (!h.vals.empty()) {
-    if (sizeof(S) == 8) {
-      copy_h2d(s, d.vals, h.vals.data(), h.vals.size() * 8);
-    } else {
-      std::vector<float> f(h.vals.size());
-      for (size_t i = 0; i < f.size(); ++i) f[i] = (float)h.vals[i];
-      copy_h2d(s, d.vals, f.data(), f.size() * 4);
-      cudaStreamSynchronize(s.stream);
-    }
+  d.starts = h.dev_starts;
+  d.cols = h.dev_cols;
+  const size_t n = h.cols.size() * h.rb * h.cb;
+  if (alias && sizeof(S) == 8) {
+    d.vals = h.dev;
+  } else {
+    if (sf_status e = dev_alloc(s, &d.vals, std::max<size_t>(1, n) * sizeof(S))) return e;
+    if (sf_status e = setup_convert<S>(s.stream, n, h.dev, (S*)d.vals)) return e;
   }
   if (sf_status e = make_row_groups(s, d, h.starts.data(), h.rb * h.cb * sizeof(S))) return e;
-  if (h.rows >= s.sell_min_rows) {
-    std::vector<S> v(h.vals.begin(), h.vals.end());
-    if (sf_status e = make_sell<S>(s, d, h.starts.data(), h.cols.data(), v.data())) return e;
-  }
-  return cuda_check(cudaGetLastError(), "upload");
+  if (h.rows >= s.sell_min_rows)
+    if (sf_status e = make_sell_converted<S>(s, d, h.starts.data(), h.cols.data(), h.dev)) return e;
+  return cuda_check(cudaGetLastError(), "level operator");
 }
 
-// The explicit transpose of a prolongator: coarse rows, fine block columns ascending, blocks
-// transposed (gpu/layout.rs:254-291 stores the same for gather restriction).
-Bsr transpose(const Bsr& p, size_t coarse_rows) {
-  Bsr t;
+// The pattern of a prolongator's explicit transpose (coarse rows, fine block columns ascending)
+// and, per transposed block, the prolongator block it comes from (gpu/layout.rs:254-291 stores
+// the same transpose for gather restriction).
+void transpose_pattern(const Bsr& p, size_t coarse_rows, Bsr& t, std::vector<uint32_t>& src) {
+  t = Bsr();
   t.rows = coarse_rows;
   t.rb = p.cb;
   t.cb = p.rb;
@@ -1336,50 +1342,67 @@ Bsr transpose(const Bsr& p, size_t coarse_rows) {
   for (size_t i = 0; i < coarse_rows; ++i) t.starts[i + 1] += t.starts[i];
   std::vector<uint32_t> fill(t.starts.begin(), t.starts.end() - 1);
   t.cols.resize(p.cols.size());
-  t.vals.resize(p.vals.size());
-  size_t len = p.rb * p.cb;
+  src.resize(p.cols.size());
   for (size_t row = 0; row < p.rows; ++row)
     for (uint32_t at = p.starts[row]; at < p.starts[row + 1]; ++at) {
-      uint32_t c = p.cols[at];
-      uint32_t o = fill[c]++;
+      uint32_t o = fill[p.cols[at]]++;
       t.cols[o] = (uint32_t)row;
-      for (size_t a = 0; a < p.rb; ++a)
-        for (size_t b = 0; b < p.cb; ++b) t.vals[(size_t)o * len + b * p.rb + a] = p.vals[(size_t)at * len + a * p.cb + b];
+      src[o] = at;
     }
-  return t;
+}
+
+template <typename S>
+sf_status upload_level(DeviceSolver& s, const std::vector<HostLevel>& levels, size_t li, DevLevel& L) {
+  const HostLevel& h = levels[li];
+  const bool alias = true;
+  if (li == 0 && sizeof(S) == 8) {
+    L.a = s.system;  // the f64 system matrix is the finest operator
+  } else if (sf_status e = device_bsr<S>(s, h.a, L.a, alias)) {
+    return e;
+  }
+  const size_t nd = h.a.rows * h.a.rb * h.a.rb;
+  if (sizeof(S) == 8) {
+    L.dinv = h.inverse_diagonal;
+  } else {
+    if (sf_status e = dev_alloc(s, &L.dinv, nd * sizeof(S))) return e;
+    if (sf_status e = setup_convert<S>(s.stream, nd, h.inverse_diagonal, (S*)L.dinv)) return e;
+  }
+  L.has_p = h.has_p;
+  if (h.has_p) {
+    if (sf_status e = device_bsr<S>(s, h.p, L.p, alias)) return e;
+    Bsr t;
+    std::vector<uint32_t> src;
+    transpose_pattern(h.p, levels[li + 1].a.rows, t, src);
+    uint32_t* d_src = nullptr;
+    sf_status e = dev_alloc(s, (void**)&d_src, std::max<size_t>(1, src.size()) * 4);
+    if (!e) e = dev_alloc(s, (void**)&t.dev_starts, (t.rows + 1) * 4);
+    if (!e) e = dev_alloc(s, (void**)&t.dev_cols, std::max<size_t>(1, t.cols.size()) * 4);
+    if (!e) e = dev_alloc(s, (void**)&t.dev, std::max<size_t>(1, t.cols.size()) * t.rb * t.cb * 8);
+    if (e) return e;
+    if (!src.empty()) copy_h2d(s, d_src, src.data(), src.size() * 4);
+    copy_h2d(s, t.dev_starts, t.starts.data(), (t.rows + 1) * 4);
+    if (!t.cols.empty()) copy_h2d(s, t.dev_cols, t.cols.data(), t.cols.size() * 4);
+    e = setup_transpose_blocks<double>(s.stream, t.cols.size(), (int)h.p.rb, (int)h.p.cb, d_src, h.p.dev, t.dev);
+    if (!e) e = device_bsr<S>(s, t, L.r, alias);
+    if (!e) e = cuda_check(cudaStreamSynchronize(s.stream), "transpose");
+    dev_free(s, d_src);
+    if (sizeof(S) != 8) dev_free(s, t.dev);  // the converted copy is the one kept
+    if (e) return e;
+  }
+  return SF_OK;
 }
 
 }  // namespace
 
 sf_status solver_upload_hierarchy(DeviceSolver& s, const std::vector<HostLevel>& levels, uint64_t degree) {
-  size_t S = s.storage_single ? 4 : 8, V = s.vector_single ? 4 : 8;
+  size_t V = s.vector_single ? 4 : 8;
   s.levels.assign(levels.size(), DevLevel());
   for (size_t li = 0; li < levels.size(); ++li) {
     const HostLevel& h = levels[li];
     DevLevel& L = s.levels[li];
     L.n = (uint32_t)(h.a.rows * h.a.rb);
-    if (li == 0 && !s.storage_single) {
-      L.a = s.system;  // the f64 system matrix is the finest operator
-    } else {
-      sf_status e = s.storage_single ? upload_bsr<float>(s, h.a, L.a) : upload_bsr<double>(s, h.a, L.a);
-      if (e) return e;
-    }
-    if (sf_status e = dev_alloc(s, &L.dinv, h.inverse_diagonal.size() * S)) return e;
-    if (S == 8) {
-      copy_h2d(s, L.dinv, h.inverse_diagonal.data(), h.inverse_diagonal.size() * 8);
-    } else {
-      std::vector<float> f(h.inverse_diagonal.begin(), h.inverse_diagonal.end());
-      copy_h2d(s, L.dinv, f.data(), f.size() * 4);
-      cudaStreamSynchronize(s.stream);
-    }
-    L.has_p = h.has_p;
-    if (h.has_p) {
-      Bsr t = transpose(h.p, levels[li + 1].a.rows);
-      sf_status e = s.storage_single ? upload_bsr<float>(s, h.p, L.p) : upload_bsr<double>(s, h.p, L.p);
-      if (e) return e;
-      e = s.storage_single ? upload_bsr<float>(s, t, L.r) : upload_bsr<double>(s, t, L.r);
-      if (e) return e;
-    }
+    sf_status e = s.storage_single ? upload_level<float>(s, levels, li, L) : upload_level<double>(s, levels, li, L);
+    if (e) return e;
     L.has_factor = h.has_factor;
     if (h.has_factor) {
       if (sf_status e = dev_alloc(s, (void**)&L.coarse_inverse, h.coarse_inverse.size() * 8)) return e;

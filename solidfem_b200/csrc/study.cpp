@@ -798,9 +798,9 @@ static sf_status builder_setup(sf_builder* b, uint64_t budget, sf_cancel_fn canc
     fine.rb = fine.cb = 3;
     fine.starts = b->pattern.starts;
     fine.cols = b->pattern.cols;
-    fine.vals.resize(b->pattern.cols.size() * 9);
-    copy_d2h(s, fine.vals.data(), s.system.vals, fine.vals.size() * 8);
-    if (sf_status e = cuda_check(cudaStreamSynchronize(s.stream), "download fine level")) return e;
+    fine.dev = (double*)s.system.vals;
+    fine.dev_starts = s.system.starts;
+    fine.dev_cols = s.system.cols;
     vector<double> modes = rigid_modes(b->model.mesh.nodes, b->free, b->free_count);
     vector<P3> positions;
     positions.reserve(b->free_count);
@@ -812,7 +812,7 @@ static sf_status builder_setup(sf_builder* b, uint64_t budget, sf_cancel_fn canc
     so.max_levels = b->options.max_levels;
     so.range = b->options.smoother_range;
     so.threads = b->threads;
-    b->setup = setup_create(std::move(fine), std::move(modes), std::move(positions), so);
+    b->setup = setup_create(s, std::move(fine), std::move(modes), std::move(positions), so);
   }
   bool finished = false;
   sf_status st = setup_step(b->setup, budget, cancel, user, &finished);
@@ -850,13 +850,14 @@ static void fill_stats(sf_study* s) {
   if (s->levels.empty()) return;
   bool single = s->solver.storage_single;
   size_t sb = single ? 4 : 8;
-  double finest = (double)s->levels[0].a.vals.size();
+  auto values = [](const Bsr& m) { return m.cols.size() * m.rb * m.cb; };
+  double finest = (double)values(s->levels[0].a);
   size_t stored = 0, memory = 0;
   for (auto& lv : s->levels) {
-    stored += lv.a.vals.size();
-    memory += (lv.a.starts.size()) * 8 + lv.a.cols.size() * 4 + lv.a.vals.size() * sb;
-    memory += lv.inverse_diagonal.size() * sb;
-    if (lv.has_p) memory += lv.p.starts.size() * 8 + lv.p.cols.size() * 4 + lv.p.vals.size() * sb;
+    stored += values(lv.a);
+    memory += (lv.a.starts.size()) * 8 + lv.a.cols.size() * 4 + values(lv.a) * sb;
+    memory += lv.a.rows * lv.a.rb * lv.a.rb * sb;
+    if (lv.has_p) memory += lv.p.starts.size() * 8 + lv.p.cols.size() * 4 + values(lv.p) * sb;
     if (lv.has_factor) memory += lv.factor_n * lv.factor_n * 8;
   }
   s->report.has_multigrid = 1;
@@ -1243,8 +1244,11 @@ sf_status sf_study_level_matrix(const sf_study* s, uint64_t level, int32_t prolo
   const Bsr& m = prolongator ? lv.p : lv.a;
   for (size_t i = 0; i <= m.rows; ++i) starts[i] = m.starts[i];
   std::memcpy(columns, m.cols.data(), m.cols.size() * 4);
-  std::memcpy(values, m.vals.data(), m.vals.size() * 8);
-  return SF_OK;
+  size_t n = m.cols.size() * m.rb * m.cb;
+  if (n == 0) return SF_OK;
+  cudaSetDevice(s->solver.device);
+  copy_d2h(s->solver, values, m.dev, n * 8);
+  return cuda_check(cudaStreamSynchronize(s->solver.stream), "level values");
 }
 
 sf_status sf_study_aggregates(const sf_study* s, uint64_t level, uint32_t* out) {
