@@ -29,9 +29,12 @@ struct DevBsr {
   uint32_t group_rows = 0;     // the largest group's row count
   int lanes_per_row = 32;      // lanes sharing one row: 32, 16, 8 or 4
   // SELL-32 copy for operators with many rows: slices of 32 rows (rows sorted by block count
-  // inside windows of kSellWindow rows), one thread per row. Block k of the row in lane t of
-  // slice s is block index slice_start[s] + 32 k + t; its element e is stored at
-  // value[(slice_start[s] + 32 k) * rb * cb + 32 e + t], so each (k, e) is one coalesced line.
+  // inside windows of kSellWindow rows), one thread per row. Each lane reads its row in chunks of
+  // U = sell_chunk_blocks(rb * cb, value bytes) consecutive blocks, 144 bytes of values stored as
+  // nine 16-byte vectors: chunk c of slice s starts at block Q0 = slice_start[s] + 32 U c; lane t's
+  // columns are cols[Q0 + U t ..], and value i (= u * rb * cb + e of its u-th block) sits at
+  // vals[Q0 * rb * cb + (i / VEC) * 32 VEC + t VEC + i % VEC] with VEC values per 16 bytes, so each
+  // vector load of a warp is 512 contiguous bytes. Slice widths are padded to whole chunks.
   bool sell = false;
   uint32_t nslices = 0;
   uint32_t* sell_rows = nullptr;   // nslices * 32: the row of each lane (rows when padding)
@@ -42,6 +45,18 @@ struct DevBsr {
 };
 
 static const uint32_t kSellWindow = 2048;    // rows are sorted by length inside windows this long
+
+// Blocks per SELL lane chunk: 144 bytes of values, at least one block.
+constexpr int sell_chunk_blocks(int len, int value_bytes) {
+  return len * value_bytes >= 144 ? 1 : 144 / (len * value_bytes);
+}
+// Where value e of the block in SELL slot q (a column index position) lives.
+__host__ __device__ inline size_t sell_value_offset(size_t q, int len, int chunk, int vec, int e) {
+  const size_t r = q % (32u * (size_t)chunk);
+  const size_t t = r / (size_t)chunk, u = r % (size_t)chunk;
+  const size_t i = u * (size_t)len + (size_t)e;
+  return (q - r) * (size_t)len + (i / (size_t)vec) * 32u * (size_t)vec + t * (size_t)vec + i % (size_t)vec;
+}
 
 // The SELL copy of a matrix whose values live only on the device (the assembled f64 system):
 // the layout from host starts/columns, the values permuted on the device.

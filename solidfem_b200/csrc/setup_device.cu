@@ -359,11 +359,12 @@ __global__ void transpose_blocks_kernel(size_t blocks, int rb, int cb, const uin
 template <typename S, int LEN>
 __global__ void sell_place_kernel(size_t blocks, const uint32_t* __restrict__ pos, const double* __restrict__ in,
                                   S* __restrict__ out) {
+  constexpr int U = sell_chunk_blocks(LEN, (int)sizeof(S));
+  constexpr int VEC = 16 / (int)sizeof(S);
   for (size_t b = blockIdx.x * (size_t)blockDim.x + threadIdx.x; b < blocks; b += (size_t)gridDim.x * blockDim.x) {
-    uint32_t q = pos[b], t = q & 31u;
-    size_t base = (size_t)(q - t) * LEN + t;
+    const uint32_t q = pos[b];
 #pragma unroll
-    for (int e = 0; e < LEN; ++e) out[base + 32 * e] = (S)in[b * LEN + e];
+    for (int e = 0; e < LEN; ++e) out[sell_value_offset(q, LEN, U, VEC, e)] = (S)in[b * LEN + e];
   }
 }
 

@@ -18,6 +18,7 @@
 #include <cmath>
 #include <cstdio>
 #include <mutex>
+#include <utility>
 
 #include "device.h"
 
@@ -30,6 +31,32 @@ const int kThreads = 256;
 const int kWarps = kThreads / 32;
 const uint32_t kGroupTarget = 4096;     // value bytes a row group aims at
 const int kSmemPerBlockTarget = 72 * 1024;
+
+// ------------------------------------------------------------ programmatic dependent launch
+// Every solve kernel is launched with programmatic stream serialization: it may be scheduled
+// while its predecessor is still finishing, waits at entry until the predecessor grid has
+// completed and its writes are visible (griddepcontrol.wait), then at once lets its own successor
+// be scheduled (griddepcontrol.launch_dependents). Launch latency and the ramp of each grid
+// overlap the tail of the previous one; the data dependence is unchanged. Without a programmatic
+// predecessor the wait returns at once.
+__device__ __forceinline__ void pdl_enter() {
+  asm volatile("griddepcontrol.wait;\n" ::: "memory");
+}
+
+template <typename... KArgs, typename... Args>
+void launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st, Args&&... args) {
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+}
 
 // ------------------------------------------------------------ asynchronous staging
 __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
@@ -240,6 +267,7 @@ struct EpiAxpy {
 template <typename S, typename V, int RB, int CB, int LPR, int OP>
 __global__ void __launch_bounds__(kThreads) bsr_kernel(Op<S> A, const V* __restrict__ x, V* __restrict__ y,
                                                        const V* __restrict__ b, const int* __restrict__ status) {
+  pdl_enter();
   if (*status != ST_ACTIVE) return;
   extern __shared__ __align__(16) char smem[];
   char* wbase = smem + (threadIdx.x >> 5) * 2 * slot_bytes(A);
@@ -310,6 +338,7 @@ __global__ void __launch_bounds__(kThreads) cheb_step_kernel(Op<S> A, const S* _
                                                              V* __restrict__ d_new, V* __restrict__ r, V* __restrict__ x,
                                                              V* __restrict__ outer, V keep, V step,
                                                              const int* __restrict__ status) {
+  pdl_enter();
   if (*status != ST_ACTIVE) return;
   extern __shared__ __align__(16) char smem[];
   char* wbase = smem + (threadIdx.x >> 5) * 2 * slot_bytes(A);
@@ -334,6 +363,7 @@ __global__ void __launch_bounds__(kThreads) cheb_start_kernel(uint32_t rows, con
                                                                V* __restrict__ r, V* __restrict__ d,
                                                                V* __restrict__ x, V theta,
                                                                const int* __restrict__ status) {
+  pdl_enter();
   if (*status != ST_ACTIVE) return;
   for (uint32_t row = blockIdx.x * blockDim.x + threadIdx.x; row < rows; row += gridDim.x * blockDim.x) {
     size_t base = (size_t)row * RB;
@@ -358,6 +388,7 @@ __global__ void __launch_bounds__(kThreads) cheb_start_kernel(uint32_t rows, con
 
 template <typename V>
 __global__ void add_kernel(size_t n, V* __restrict__ x, const V* __restrict__ y, const int* __restrict__ status) {
+  pdl_enter();
   if (*status != ST_ACTIVE) return;
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
     x[i] = x[i] + y[i];
@@ -365,6 +396,7 @@ __global__ void add_kernel(size_t n, V* __restrict__ x, const V* __restrict__ y,
 
 template <typename B, typename V>
 __global__ void convert_kernel(size_t n, const B* __restrict__ in, V* __restrict__ out, const int* __restrict__ status) {
+  pdl_enter();
   if (*status != ST_ACTIVE) return;
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
     out[i] = V(in[i]);
@@ -376,6 +408,7 @@ template <typename V>
 __global__ void __launch_bounds__(kThreads) coarse_solve_kernel(uint32_t n, const double* __restrict__ inv,
                                                                  const V* __restrict__ b, V* __restrict__ x,
                                                                  const int* __restrict__ status) {
+  pdl_enter();
   if (*status != ST_ACTIVE) return;
   int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   for (uint32_t row = blockIdx.x * kWarps + warp; row < n; row += gridDim.x * kWarps) {
@@ -431,9 +464,10 @@ __device__ __forceinline__ bool finish_partials(double (&v)[K], double* partials
 
 // ------------------------------------------------------------ SELL-32: one thread per row
 // For operators with many rows (the finest level and the f64 system): a warp holds a slice of 32
-// rows of similar length, each thread sums its own row's blocks in column order, and every load
-// of a value plane or a column index is one coalesced 128-byte line. No shared memory, no
-// shuffles: the instruction stream is the blocks' FMAs plus their loads.
+// rows of similar length, each thread sums its own row's blocks in column order. A thread reads
+// its row in chunks of 144 bytes of values (nine 16-byte vector loads, each 512 contiguous bytes
+// across the warp) plus one vector load of the chunk's columns. No shared memory, no shuffles:
+// the instruction stream is the blocks' FMAs plus their loads.
 template <typename S>
 struct SellOp {
   const uint32_t* __restrict__ rows;
@@ -457,9 +491,53 @@ SellOp<S> sell_of(const DevBsr& m) {
   return o;
 }
 
+template <typename S>
+struct Vec16;
+template <>
+struct Vec16<float> {
+  typedef float4 type;
+  __device__ __forceinline__ static void split(const float4& w, float* out) {
+    out[0] = w.x;
+    out[1] = w.y;
+    out[2] = w.z;
+    out[3] = w.w;
+  }
+};
+template <>
+struct Vec16<double> {
+  typedef double2 type;
+  __device__ __forceinline__ static void split(const double2& w, double* out) {
+    out[0] = w.x;
+    out[1] = w.y;
+  }
+};
+
+template <int U>
+__device__ __forceinline__ void load_cols(const uint32_t* p, uint32_t (&c)[U]) {
+  if constexpr (U == 4) {
+    uint4 w = __ldcs(reinterpret_cast<const uint4*>(p));
+    c[0] = w.x;
+    c[1] = w.y;
+    c[2] = w.z;
+    c[3] = w.w;
+  } else if constexpr (U == 2) {
+    uint2 w = __ldcs(reinterpret_cast<const uint2*>(p));
+    c[0] = w.x;
+    c[1] = w.y;
+  } else {
+#pragma unroll
+    for (int u = 0; u < U; ++u) c[u] = __ldcs(p + u);
+  }
+}
+
 template <typename S, typename V, int RB, int CB, bool MAG, class Epi>
 __device__ __forceinline__ void sell_rows(const SellOp<S>& A, const V* __restrict__ x, Epi& epi) {
   constexpr int LEN = RB * CB;
+  constexpr int U = sell_chunk_blocks(LEN, (int)sizeof(S));
+  constexpr int VEC = 16 / (int)sizeof(S);
+  constexpr int NV = U * LEN / VEC;
+  static_assert((U * LEN) % VEC == 0, "a lane chunk is whole 16-byte vectors");
+  typedef typename Vec16<S>::type W;
   const uint32_t lane = threadIdx.x & 31;
   const uint32_t warps = blockDim.x >> 5;
   for (uint32_t s = blockIdx.x * warps + (threadIdx.x >> 5); s < A.nslices; s += gridDim.x * warps) {
@@ -472,21 +550,32 @@ __device__ __forceinline__ void sell_rows(const SellOp<S>& A, const V* __restric
 #pragma unroll
     for (int p = 0; p < RB; ++p) acc[p] = mag[p] = V(0);
     const uint32_t base = A.start[s];
-    // U blocks per step: their column indices and values are loaded together (U * (LEN + 1)
-    // independent coalesced loads in flight per thread), then their x gathers, then the FMAs,
-    // still in column order, so the row's sum keeps its sequential order.
-    constexpr int U = (LEN <= 9 && sizeof(S) == 4) ? 4 : 2;
+    // One chunk of U blocks per step: its columns in one vector load, its values in NV 16-byte
+    // vector loads (each a contiguous 512 bytes across the warp). The loads of chunk k+1 are
+    // issued before chunk k's x gathers and FMAs, so a chunk's stream latency hides behind the
+    // previous chunk's gathers. The FMAs run in column order, so the row's sum keeps its
+    // sequential order.
+    uint32_t cn[U];
+    S vn[U * LEN];
+    if (n > 0) {
+      load_cols<U>(A.cols + base + lane * U, cn);
+      const W* vp = reinterpret_cast<const W*>(A.vals + (size_t)base * LEN) + lane;
+#pragma unroll
+      for (int q = 0; q < NV; ++q) Vec16<S>::split(__ldcs(vp + 32 * q), vn + q * VEC);
+    }
     for (uint32_t k0 = 0; k0 < n; k0 += U) {
       uint32_t c[U];
-      S v[U][LEN];
+      S v[U * LEN];
 #pragma unroll
-      for (int u = 0; u < U; ++u) {
-        const bool in = k0 + u < n;
-        const uint32_t q0 = base + 32 * (k0 + (in ? u : 0));
-        c[u] = in ? __ldcs(A.cols + q0 + lane) : 0u;
-        const S* vp = A.vals + (size_t)q0 * LEN + lane;
+      for (int u = 0; u < U; ++u) c[u] = cn[u];
 #pragma unroll
-        for (int e = 0; e < LEN; ++e) v[u][e] = in ? __ldcs(vp + 32 * e) : S(0);
+      for (int i = 0; i < U * LEN; ++i) v[i] = vn[i];
+      if (k0 + U < n) {
+        const uint32_t q1 = base + 32 * (k0 + U);
+        load_cols<U>(A.cols + q1 + lane * U, cn);
+        const W* vp = reinterpret_cast<const W*>(A.vals + (size_t)q1 * LEN) + lane;
+#pragma unroll
+        for (int q = 0; q < NV; ++q) Vec16<S>::split(__ldcs(vp + 32 * q), vn + q * VEC);
       }
       V xv[U][CB];
 #pragma unroll
@@ -500,7 +589,7 @@ __device__ __forceinline__ void sell_rows(const SellOp<S>& A, const V* __restric
         for (int p = 0; p < RB; ++p)
 #pragma unroll
           for (int q = 0; q < CB; ++q) {
-            V t = V(v[u][p * CB + q]) * xv[u][q];
+            V t = V(v[u * LEN + p * CB + q]) * xv[u][q];
             acc[p] += t;
             if (MAG) mag[p] += fabs(t);
           }
@@ -535,6 +624,7 @@ struct SellAxpy {
 template <typename S, typename V, int RB, int CB, int OP>
 __global__ void __launch_bounds__(kThreads) sell_kernel(SellOp<S> A, const V* __restrict__ x, V* __restrict__ y,
                                                         const V* __restrict__ b, const int* __restrict__ status) {
+  pdl_enter();
   if (*status != ST_ACTIVE) return;
   SellAxpy<V, RB, OP> epi{y, b, {}};
   sell_rows<S, V, RB, CB, false>(A, x, epi);
@@ -582,6 +672,7 @@ __global__ void __launch_bounds__(kThreads) sell_cheb_kernel(SellOp<S> A, const 
                                                              const V* __restrict__ d_old, V* __restrict__ d_new,
                                                              V* __restrict__ r, V* __restrict__ x, V* __restrict__ outer,
                                                              V keep, V step, const int* __restrict__ status) {
+  pdl_enter();
   if (*status != ST_ACTIVE) return;
   SellCheb<S, V, RB> epi;
   epi.dinv = dinv;
@@ -618,6 +709,7 @@ struct SellDot {
 __global__ void __launch_bounds__(kThreads) sell_pcg_spmv_dot_kernel(SellOp<double> A, const double* __restrict__ p,
                                                                       double* __restrict__ ap, double* partials,
                                                                       PcgState* st) {
+  pdl_enter();
   if (st->status != ST_ACTIVE) return;
   SellDot epi;
   epi.p = p;
@@ -665,6 +757,7 @@ struct SellCheck {
 __global__ void __launch_bounds__(kThreads) sell_pcg_check_kernel(SellOp<double> A, const double* __restrict__ x,
                                                                    const double* __restrict__ b, double* __restrict__ r,
                                                                    double* partials, PcgState* st) {
+  pdl_enter();
   if (st->status != ST_ACTIVE || st->mode != MODE_CHECK) return;
   SellCheck epi;
   epi.b = b;
@@ -690,11 +783,12 @@ __global__ void __launch_bounds__(kThreads) sell_pcg_check_kernel(SellOp<double>
 template <typename S, int LEN>
 __global__ void sell_permute_kernel(size_t blocks, const uint32_t* __restrict__ pos, const S* __restrict__ in,
                                     S* __restrict__ out) {
+  constexpr int U = sell_chunk_blocks(LEN, (int)sizeof(S));
+  constexpr int VEC = 16 / (int)sizeof(S);
   for (size_t b = blockIdx.x * (size_t)blockDim.x + threadIdx.x; b < blocks; b += (size_t)gridDim.x * blockDim.x) {
-    uint32_t q = pos[b], t = q & 31u;
-    size_t base = (size_t)(q - t) * LEN + t;
+    const uint32_t q = pos[b];
 #pragma unroll
-    for (int e = 0; e < LEN; ++e) out[base + 32 * e] = in[b * LEN + e];
+    for (int e = 0; e < LEN; ++e) out[sell_value_offset(q, LEN, U, VEC, e)] = in[b * LEN + e];
   }
 }
 
@@ -730,6 +824,7 @@ struct EpiDot {
 template <int LPR>
 __global__ void __launch_bounds__(kThreads) pcg_spmv_dot_kernel(Op<double> A, const double* __restrict__ p,
                                                                  double* __restrict__ ap, double* partials, PcgState* st) {
+  pdl_enter();
   if (st->status != ST_ACTIVE) return;
   extern __shared__ __align__(16) char smem[];
   char* wbase = smem + (threadIdx.x >> 5) * 2 * slot_bytes(A);
@@ -755,6 +850,7 @@ __global__ void __launch_bounds__(kThreads) pcg_spmv_dot_kernel(Op<double> A, co
 __global__ void __launch_bounds__(kThreads) pcg_update_kernel(uint32_t n, const double* __restrict__ p,
                                                                const double* __restrict__ ap, double* __restrict__ x,
                                                                double* __restrict__ r, double* partials, PcgState* st) {
+  pdl_enter();
   if (st->status != ST_ACTIVE) return;
   double alpha = st->alpha, na = -alpha;
   double local = 0.0;
@@ -812,6 +908,7 @@ template <int LPR>
 __global__ void __launch_bounds__(kThreads) pcg_check_kernel(Op<double> A, const double* __restrict__ x,
                                                               const double* __restrict__ b, double* __restrict__ r,
                                                               double* partials, PcgState* st) {
+  pdl_enter();
   if (st->status != ST_ACTIVE || st->mode != MODE_CHECK) return;
   extern __shared__ __align__(16) char smem[];
   char* wbase = smem + (threadIdx.x >> 5) * 2 * slot_bytes(A);
@@ -843,6 +940,7 @@ template <typename Z>
 __global__ void __launch_bounds__(kThreads) pcg_dot_rz_kernel(uint32_t n, const double* __restrict__ r,
                                                                const Z* __restrict__ z, const double* __restrict__ ap,
                                                                double* partials, PcgState* st) {
+  pdl_enter();
   if (st->status != ST_ACTIVE) return;
   bool flex = st->flexible && st->mode == MODE_NORMAL;
   double rz = 0.0, apz = 0.0;
@@ -869,6 +967,7 @@ __global__ void __launch_bounds__(kThreads) pcg_dot_rz_kernel(uint32_t n, const 
 // p = z + beta p, or p = z after a restart.
 template <typename Z>
 __global__ void pcg_update_p_kernel(uint32_t n, const Z* __restrict__ z, double* __restrict__ p, PcgState* st) {
+  pdl_enter();
   if (st->status != ST_ACTIVE) return;
   bool restart = st->mode == MODE_RESTART;
   double beta = st->beta;
@@ -881,6 +980,7 @@ __global__ void pcg_update_p_kernel(uint32_t n, const Z* __restrict__ z, double*
 // Initial state (Pcg::new, pcg.rs:135-164): x = 0, r = b, rhs norm; then reset_direction.
 __global__ void __launch_bounds__(kThreads) pcg_init_kernel(uint32_t n, const double* __restrict__ b, double* __restrict__ x,
                                                              double* __restrict__ r, double* partials, PcgState* st) {
+  pdl_enter();
   double local = 0.0;
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     x[i] = 0.0;
@@ -900,6 +1000,7 @@ __global__ void __launch_bounds__(kThreads) pcg_init_kernel(uint32_t n, const do
 // Jacobi: z = r / diag (preconditioner.rs:237-247), stored as the inverse diagonal.
 __global__ void jacobi_kernel(uint32_t n, const double* __restrict__ inv, const double* __restrict__ r,
                               double* __restrict__ z, const int* __restrict__ status) {
+  pdl_enter();
   if (*status != ST_ACTIVE) return;
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) z[i] = r[i] * inv[i];
 }
@@ -964,7 +1065,7 @@ void launch_bsr_lpr(const DevBsr& m, const V* x, V* y, const V* b, const int* st
   auto k = bsr_kernel<S, V, RB, CB, LPR, OP>;
   static bool opted = false;
   smem_opt_in(k, opted);
-  k<<<sh.grid, sh.threads, sh.smem, st>>>(A, x, y, b, status);
+  launch_pdl(k, sh.grid, sh.threads, sh.smem, st, A, x, y, b, status);
 }
 
 int grid_for_slices(uint32_t nslices) {
@@ -974,7 +1075,7 @@ int grid_for_slices(uint32_t nslices) {
 
 template <typename S, typename V, int RB, int CB, int OP>
 void launch_sell(const DevBsr& m, const V* x, V* y, const V* b, const int* status, cudaStream_t st) {
-  sell_kernel<S, V, RB, CB, OP><<<grid_for_slices(m.nslices), kThreads, 0, st>>>(sell_of<S>(m), x, y, b, status);
+  launch_pdl(sell_kernel<S, V, RB, CB, OP>, grid_for_slices(m.nslices), kThreads, 0, st, sell_of<S>(m), x, y, b, status);
 }
 
 template <typename S, typename V, int RB, int CB, int OP>
@@ -1015,14 +1116,14 @@ void launch_cheb_step_lpr(const DevLevel& L, const V* d_old, V* d_new, V* r, V* 
   auto k = cheb_step_kernel<S, V, RB, LPR>;
   static bool opted = false;
   smem_opt_in(k, opted);
-  k<<<sh.grid, sh.threads, sh.smem, st>>>(A, (const S*)L.dinv, d_old, d_new, r, x, outer, (V)keep, (V)step, status);
+  launch_pdl(k, sh.grid, sh.threads, sh.smem, st, A, (const S*)L.dinv, d_old, d_new, r, x, outer, (V)keep, (V)step, status);
 }
 
 template <typename S, typename V, int RB>
 void launch_cheb_step(const DevLevel& L, const V* d_old, V* d_new, V* r, V* x, V* outer, double keep, double step,
                       const int* status, cudaStream_t st) {
   if (L.a.sell) {
-    sell_cheb_kernel<S, V, RB><<<grid_for_slices(L.a.nslices), kThreads, 0, st>>>(
+    launch_pdl(sell_cheb_kernel<S, V, RB>, grid_for_slices(L.a.nslices), kThreads, 0, st,
         sell_of<S>(L.a), (const S*)L.dinv, d_old, d_new, r, x, outer, (V)keep, (V)step, status);
     return;
   }
@@ -1037,7 +1138,7 @@ void launch_cheb_step(const DevLevel& L, const V* d_old, V* d_new, V* r, V* x, V
 template <typename S, typename V, typename B, int RB>
 void launch_cheb_start(const DevLevel& L, const B* b_in, V* b_out, V* r, V* d, V* x, double theta, const int* status,
                        cudaStream_t st) {
-  cheb_start_kernel<S, V, B, RB><<<grid_for_elems(L.a.rows), kThreads, 0, st>>>(
+  launch_pdl(cheb_start_kernel<S, V, B, RB>, grid_for_elems(L.a.rows), kThreads, 0, st,
       L.a.rows, (const S*)L.dinv, b_in, b_out, r, d, x, (V)theta, status);
 }
 
@@ -1063,7 +1164,7 @@ void enqueue_smooth(DeviceSolver& s, DevLevel& L, const B* b_in, V* b_out, V* x,
     s.launches_per_iteration++;
   }
   if (outer && L.steps.empty()) {
-    add_kernel<V><<<grid_for_elems(L.n), kThreads, 0, st>>>(L.n, outer, x, status);
+    launch_pdl(add_kernel<V>, grid_for_elems(L.n), kThreads, 0, st, L.n, outer, x, status);
     s.launches_per_iteration++;
   }
 }
@@ -1078,11 +1179,11 @@ void enqueue_cycle(DeviceSolver& s, size_t li, const B* rhs, V* b_store, V* x, c
     if (L.has_factor) {
       const V* bv = (const V*)rhs;
       if (b_store) {
-        convert_kernel<B, V><<<grid_for_elems(L.n), kThreads, 0, st>>>(L.n, rhs, b_store, status);
+        launch_pdl(convert_kernel<B, V>, grid_for_elems(L.n), kThreads, 0, st, L.n, rhs, b_store, status);
         s.launches_per_iteration++;
         bv = b_store;
       }
-      coarse_solve_kernel<V><<<grid_for_rows(L.n), kThreads, 0, st>>>(L.n, L.coarse_inverse, bv, x, status);
+      launch_pdl(coarse_solve_kernel<V>, grid_for_rows(L.n), kThreads, 0, st, L.n, L.coarse_inverse, bv, x, status);
       s.launches_per_iteration++;
     } else {
       enqueue_smooth<S, V, B>(s, L, rhs, b_store, x, nullptr, status);
@@ -1105,7 +1206,7 @@ void enqueue_cycle(DeviceSolver& s, size_t li, const B* rhs, V* b_store, V* x, c
 // z = M r for the solver's r (f64) into z (f64) or z32.
 void enqueue_precondition(DeviceSolver& s, const double* r, double* z, float* z32, const int* status) {
   if (!s.multigrid) {
-    jacobi_kernel<<<grid_for_elems(s.n), kThreads, 0, s.stream>>>(s.n, s.jacobi, r, z, status);
+    launch_pdl(jacobi_kernel, grid_for_elems(s.n), kThreads, 0, s.stream, s.n, s.jacobi, r, z, status);
     s.launches_per_iteration++;
     return;
   }
@@ -1125,11 +1226,11 @@ void launch_pcg_spmv_lpr(DeviceSolver& s) {
   auto k = pcg_spmv_dot_kernel<LPR>;
   static bool opted = false, opted_check = false;
   smem_opt_in(k, opted);
-  k<<<sh.grid, sh.threads, sh.smem, s.stream>>>(A, s.p, s.ap, s.partials, s.state);
+  launch_pdl(k, sh.grid, sh.threads, sh.smem, s.stream, A, s.p, s.ap, s.partials, s.state);
   auto c = pcg_check_kernel<LPR>;
   smem_opt_in(c, opted_check);
-  pcg_update_kernel<<<kReduceBlocks, kReduceThreads, 0, s.stream>>>(s.n, s.p, s.ap, s.x, s.r, s.partials, s.state);
-  c<<<sh.grid, sh.threads, sh.smem, s.stream>>>(A, s.x, s.rhs, s.r, s.partials, s.state);
+  launch_pdl(pcg_update_kernel, kReduceBlocks, kReduceThreads, 0, s.stream, s.n, s.p, s.ap, s.x, s.r, s.partials, s.state);
+  launch_pdl(c, sh.grid, sh.threads, sh.smem, s.stream, A, s.x, s.rhs, s.r, s.partials, s.state);
 }
 
 }  // namespace
@@ -1219,8 +1320,9 @@ struct SellLayout {
 };
 
 // Rows sorted by descending block count inside windows of kSellWindow rows (stable, so equal
-// lengths keep row order), cut into slices of 32; pos[b] is the SELL block index of BSR block b.
-SellLayout sell_layout(uint32_t nrows, const uint32_t* starts, const uint32_t* cols) {
+// lengths keep row order), cut into slices of 32, slice widths padded to chunks of `chunk`
+// blocks; pos[b] is the SELL slot (column index position) of BSR block b.
+SellLayout sell_layout(uint32_t nrows, const uint32_t* starts, const uint32_t* cols, uint32_t chunk) {
   SellLayout L;
   L.nslices = (nrows + 31) / 32;
   std::vector<uint32_t> order(nrows);
@@ -1240,6 +1342,7 @@ SellLayout sell_layout(uint32_t nrows, const uint32_t* starts, const uint32_t* c
   for (uint32_t sl = 0; sl < L.nslices; ++sl) {
     uint32_t width = 0;
     for (uint32_t t = 0; t < 32; ++t) width = std::max(width, L.len[sl * 32 + t]);
+    width = (width + chunk - 1) / chunk * chunk;
     L.start[sl + 1] = L.start[sl] + 32 * width;
   }
   L.pos.assign(starts[nrows], 0);
@@ -1247,7 +1350,7 @@ SellLayout sell_layout(uint32_t nrows, const uint32_t* starts, const uint32_t* c
   for (uint32_t i = 0; i < nrows; ++i) {
     uint32_t r = order[i], sl = i / 32, t = i % 32;
     for (uint32_t k = 0; k < rlen(r); ++k) {
-      uint32_t q = L.start[sl] + 32 * k + t;
+      uint32_t q = L.start[sl] + 32 * (k - k % chunk) + t * chunk + k % chunk;
       L.pos[starts[r] + k] = q;
       L.cols[q] = cols[starts[r] + k];
     }
@@ -1277,8 +1380,8 @@ sf_status upload_sell_layout(DeviceSolver& s, DevBsr& m, const SellLayout& L, si
 template <typename S>
 sf_status make_sell_converted(DeviceSolver& s, DevBsr& m, const uint32_t* starts, const uint32_t* cols,
                               const double* vals) {
-  SellLayout L = sell_layout(m.rows, starts, cols);
   const int len = (int)(m.rb * m.cb);
+  SellLayout L = sell_layout(m.rows, starts, cols, (uint32_t)sell_chunk_blocks(len, (int)sizeof(S)));
   if (sf_status e = upload_sell_layout(s, m, L, (size_t)len * sizeof(S))) return e;
   uint32_t* pos = nullptr;
   if (sf_status e = dev_alloc(s, (void**)&pos, std::max<size_t>(1, L.pos.size()) * 4)) return e;
@@ -1291,7 +1394,7 @@ sf_status make_sell_converted(DeviceSolver& s, DevBsr& m, const uint32_t* starts
 }
 
 sf_status make_sell_from_device(DeviceSolver& s, DevBsr& m, const uint32_t* starts, const uint32_t* cols) {
-  SellLayout L = sell_layout(m.rows, starts, cols);
+  SellLayout L = sell_layout(m.rows, starts, cols, (uint32_t)sell_chunk_blocks(9, 8));
   if (sf_status e = upload_sell_layout(s, m, L, 72)) return e;
   uint32_t* pos = nullptr;
   if (sf_status e = dev_alloc(s, (void**)&pos, std::max<size_t>(1, L.pos.size()) * 4)) return e;
@@ -1439,7 +1542,7 @@ sf_status solver_init_pcg(DeviceSolver& s, double tolerance, uint64_t max_iterat
   copy_h2d(s, s.state, &h, sizeof(h));
   int one_active = ST_ACTIVE;
   copy_h2d(s, s.always_active, &one_active, sizeof(int));
-  pcg_init_kernel<<<kReduceBlocks, kReduceThreads, 0, s.stream>>>(s.n, s.rhs, s.x, s.r, s.partials, s.state);
+  launch_pdl(pcg_init_kernel, kReduceBlocks, kReduceThreads, 0, s.stream, s.n, s.rhs, s.x, s.r, s.partials, s.state);
   return solver_enqueue_reset(s);
 }
 
@@ -1447,11 +1550,11 @@ sf_status solver_enqueue_reset(DeviceSolver& s) {
   const int* status = &s.state->status;
   enqueue_precondition(s, s.r, s.z, s.z32, status);
   if (s.vector_single && s.multigrid) {
-    pcg_dot_rz_kernel<float><<<kReduceBlocks, kReduceThreads, 0, s.stream>>>(s.n, s.r, s.z32, s.ap, s.partials, s.state);
-    pcg_update_p_kernel<float><<<grid_for_elems(s.n), kThreads, 0, s.stream>>>(s.n, s.z32, s.p, s.state);
+    launch_pdl(pcg_dot_rz_kernel<float>, kReduceBlocks, kReduceThreads, 0, s.stream, s.n, s.r, s.z32, s.ap, s.partials, s.state);
+    launch_pdl(pcg_update_p_kernel<float>, grid_for_elems(s.n), kThreads, 0, s.stream, s.n, s.z32, s.p, s.state);
   } else {
-    pcg_dot_rz_kernel<double><<<kReduceBlocks, kReduceThreads, 0, s.stream>>>(s.n, s.r, s.z, s.ap, s.partials, s.state);
-    pcg_update_p_kernel<double><<<grid_for_elems(s.n), kThreads, 0, s.stream>>>(s.n, s.z, s.p, s.state);
+    launch_pdl(pcg_dot_rz_kernel<double>, kReduceBlocks, kReduceThreads, 0, s.stream, s.n, s.r, s.z, s.ap, s.partials, s.state);
+    launch_pdl(pcg_update_p_kernel<double>, grid_for_elems(s.n), kThreads, 0, s.stream, s.n, s.z, s.p, s.state);
   }
   s.launches_per_iteration += 2;
   return cuda_check(cudaGetLastError(), "reset direction");
@@ -1464,9 +1567,9 @@ sf_status solver_enqueue_iteration(DeviceSolver& s) {
   if (s.system.sell) {
     SellOp<double> A = sell_of<double>(s.system);
     int grid = std::min(grid_for_slices(s.system.nslices), kReduceBlocks * 2);
-    sell_pcg_spmv_dot_kernel<<<grid, kThreads, 0, st>>>(A, s.p, s.ap, s.partials, s.state);
-    pcg_update_kernel<<<kReduceBlocks, kReduceThreads, 0, st>>>(s.n, s.p, s.ap, s.x, s.r, s.partials, s.state);
-    sell_pcg_check_kernel<<<grid, kThreads, 0, st>>>(A, s.x, s.rhs, s.r, s.partials, s.state);
+    launch_pdl(sell_pcg_spmv_dot_kernel, grid, kThreads, 0, st, A, s.p, s.ap, s.partials, s.state);
+    launch_pdl(pcg_update_kernel, kReduceBlocks, kReduceThreads, 0, st, s.n, s.p, s.ap, s.x, s.r, s.partials, s.state);
+    launch_pdl(sell_pcg_check_kernel, grid, kThreads, 0, st, A, s.x, s.rhs, s.r, s.partials, s.state);
   } else switch (s.system.lanes_per_row) {
     case 8: launch_pcg_spmv_lpr<8>(s); break;
     case 16: launch_pcg_spmv_lpr<16>(s); break;
@@ -1475,11 +1578,11 @@ sf_status solver_enqueue_iteration(DeviceSolver& s) {
   s.launches_per_iteration += 3;
   enqueue_precondition(s, s.r, s.z, s.z32, status);
   if (s.vector_single && s.multigrid) {
-    pcg_dot_rz_kernel<float><<<kReduceBlocks, kReduceThreads, 0, st>>>(s.n, s.r, s.z32, s.ap, s.partials, s.state);
-    pcg_update_p_kernel<float><<<grid_for_elems(s.n), kThreads, 0, st>>>(s.n, s.z32, s.p, s.state);
+    launch_pdl(pcg_dot_rz_kernel<float>, kReduceBlocks, kReduceThreads, 0, st, s.n, s.r, s.z32, s.ap, s.partials, s.state);
+    launch_pdl(pcg_update_p_kernel<float>, grid_for_elems(s.n), kThreads, 0, st, s.n, s.z32, s.p, s.state);
   } else {
-    pcg_dot_rz_kernel<double><<<kReduceBlocks, kReduceThreads, 0, st>>>(s.n, s.r, s.z, s.ap, s.partials, s.state);
-    pcg_update_p_kernel<double><<<grid_for_elems(s.n), kThreads, 0, st>>>(s.n, s.z, s.p, s.state);
+    launch_pdl(pcg_dot_rz_kernel<double>, kReduceBlocks, kReduceThreads, 0, st, s.n, s.r, s.z, s.ap, s.partials, s.state);
+    launch_pdl(pcg_update_p_kernel<double>, grid_for_elems(s.n), kThreads, 0, st, s.n, s.z, s.p, s.state);
   }
   s.launches_per_iteration += 2;
   return cuda_check(cudaGetLastError(), "iteration");
@@ -1583,7 +1686,7 @@ sf_status solver_time_kernel(DeviceSolver& s, int kernel, uint64_t repeats, doub
 sf_status solver_precondition(DeviceSolver& s, const double* d_in, double* d_out) {
   enqueue_precondition(s, d_in, d_out, s.z32, s.always_active);
   if (s.vector_single && s.multigrid)
-    convert_kernel<float, double><<<grid_for_elems(s.n), kThreads, 0, s.stream>>>(s.n, s.z32, d_out, s.always_active);
+    launch_pdl(convert_kernel<float, double>, grid_for_elems(s.n), kThreads, 0, s.stream, s.n, s.z32, d_out, s.always_active);
   return cuda_check(cudaStreamSynchronize(s.stream), "precondition");
 }
 
