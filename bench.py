@@ -18,6 +18,7 @@ bounded sample of the same workload on the host cores.
 from __future__ import annotations
 
 import argparse
+import gc
 import json
 import os
 import statistics
@@ -241,15 +242,22 @@ def run_mine(args, rank, world):
         return t1 - t0, timing, out, d, st
 
     e2e_step()  # warm-up: CUDA context, module load, allocator
-    e2e_steps = max(1, min(args.steps, 3))
+    e2e_steps = max(1, min(args.steps, 5))
     barrier()
     e2e_times, h2d, d2h = [], 0, 0
+    study = None
     for _ in range(e2e_steps):
+        # The previous step's study is released before the clock starts, so its device memory is
+        # not freed inside the next timed region.
+        study = None
+        gc.collect()
         dt, timing, out_e2e, disp_e2e, study = e2e_step()
         e2e_times.append(dt)
         h2d, d2h = timing["h2d_bytes"], timing["d2h_bytes"] + disp_e2e.nbytes
     barrier()
-    e2e_sec = max_over_ranks(statistics.mean(e2e_times))
+    # Median of the steps: host phases (pattern, aggregation, layouts) share the box's cores with
+    # other tenants, and a step that met contention is listed in `samples` rather than averaged in.
+    e2e_sec = max_over_ranks(statistics.median(e2e_times))
     rep = study.report()
 
     # --- value: device-resident solves of the mixed path.
@@ -304,7 +312,7 @@ def run_mine(args, rank, world):
                          "bytes_per_launch": kt["bytes_per_launch"], "ms_per_launch": kt["ms_per_launch"],
                          "system_product_gbs": st["bytes_per_launch"] / (st["ms_per_launch"] * 1e-3) / 1e9},
             "e2e": {"value": world / e2e_sec, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                    "seconds_per_step": e2e_sec},
+                    "seconds_per_step": e2e_sec, "samples": [round(t, 4) for t in e2e_times]},
             "gpu_launches": launches, "clocks": clock}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = {k: v for k, v in cpu_baseline_sample().items() if k != "seconds_per_solve"}

@@ -148,10 +148,10 @@ sf_status cuda_check(cudaError_t e, const char* what);
 sf_status setup_inverse_diagonal(cudaStream_t st, uint32_t rows, int rb, const uint32_t* starts, const uint32_t* cols,
                                  const double* vals, double* inv, unsigned long long* bad, double* pivots);
 sf_status setup_block_norms(cudaStream_t st, size_t blocks, int len, const double* vals, double* out);
-// 20 (`iterations`) power steps of D^-1 A from start_value; norms[1] ends as the last norm.
-sf_status setup_power_iteration(cudaStream_t st, uint32_t rows, int rb, const uint32_t* starts, const uint32_t* cols,
-                                const double* vals, const double* inv, double* v, double* s2, double* norms,
-                                int iterations);
+// One power step s2 = D^-1 (A v), and v = src / d.
+sf_status setup_power_step(cudaStream_t st, uint32_t rows, int rb, const uint32_t* starts, const uint32_t* cols,
+                           const double* vals, const double* inv, const double* v, double* s2);
+sf_status setup_scale(cudaStream_t st, size_t n, const double* src, double d, double* v);
 sf_status setup_entry_rows(cudaStream_t st, uint32_t rows, const uint32_t* starts, uint32_t* out);
 sf_status setup_smooth(cudaStream_t st, int rb, size_t entries, const uint32_t* entry_row, const uint32_t* p_cols,
                        const uint32_t* a_starts, const uint32_t* a_cols, const double* a_vals, const uint32_t* n_starts,

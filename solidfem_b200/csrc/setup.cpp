@@ -93,6 +93,17 @@ void symbolic_rows(size_t rows, size_t width, int threads, F&& candidates, vecto
   }
 }
 
+double start_value(size_t index) {  // block.rs:379-382
+  uint64_t mixed = ((uint64_t)index + 1) * 0x9E3779B97F4A7C15ull;
+  return 0.5 + (double)(mixed >> 11) / (double)(1ull << 53);
+}
+
+double norm2(const double* x, size_t n) {  // block.rs:398-404, serial in index order
+  double s = 0.0;
+  for (size_t i = 0; i < n; ++i) s += x[i] * x[i];
+  return std::sqrt(s);
+}
+
 double squared_distance(const vector<P3>& p, size_t a, size_t b) {
   double dx = p[b][0] - p[a][0], dy = p[b][1] - p[a][1], dz = p[b][2] - p[a][2];
   return dx * dx + dy * dy + dz * dz;
@@ -129,8 +140,13 @@ struct SetupMachine {
   Bsr prolongator, ap, coarse;
   sf_status failure = SF_OK;
   bool cancelled = false;
+  double* pinned = nullptr;  // host copy of a power iterate
+  size_t pinned_size = 0;
 
   explicit SetupMachine(DeviceSolver& d) : dev(d) {}
+  ~SetupMachine() {
+    if (pinned) cudaFreeHost(pinned);
+  }
 
   size_t level_index() const { return levels.size(); }
 
@@ -359,26 +375,45 @@ struct SetupMachine {
     phase = SPECTRAL;
   }
 
-  // Power iteration for lambda_max(D^-1 A) (setup.rs:390-449), on the device.
+  // Power iteration for lambda_max(D^-1 A) (setup.rs:390-449): the products on the device, the
+  // order-exact norms on the host from a pinned copy of each iterate.
   sf_status run_spectral() {
     size_t rb = current.rb, rows = current.rows, dofs = rows * rb;
-    double *v = nullptr, *s2 = nullptr, *d_norms = nullptr;
+    double *v = nullptr, *s2 = nullptr;
     sf_status e = dev_alloc(dev, (void**)&v, std::max<size_t>(1, dofs) * 8);
     if (!e) e = dev_alloc(dev, (void**)&s2, std::max<size_t>(1, dofs) * 8);
-    if (!e) e = dev_alloc(dev, (void**)&d_norms, 16);
-    if (!e)
-      e = setup_power_iteration(dev.stream, (uint32_t)rows, (int)rb, current.dev_starts, current.dev_cols, current.dev,
-                                inv, v, s2, d_norms, POWER_ITERATIONS);
-    double lm[2] = {0.0, 0.0};
-    if (!e) {
-      copy_d2h(dev, lm, d_norms, 16);
-      e = sync("power iteration");
+    if (!e && pinned_size < dofs) {
+      if (pinned) cudaFreeHost(pinned);
+      pinned = nullptr;
+      pinned_size = 0;
+      e = cuda_check(cudaMallocHost((void**)&pinned, std::max<size_t>(1, dofs) * 8), "cudaMallocHost");
+      if (!e) pinned_size = dofs;
+    }
+    double lm = 0.0;
+    if (!e && dofs) {
+      for (size_t i = 0; i < dofs; ++i) pinned[i] = start_value(i);
+      double n0 = norm2(pinned, dofs);
+      for (size_t i = 0; i < dofs; ++i) pinned[i] /= n0;
+      copy_h2d(dev, v, pinned, dofs * 8);
+      for (int it = 0; it < POWER_ITERATIONS && !e; ++it) {
+        e = setup_power_step(dev.stream, (uint32_t)rows, (int)rb, current.dev_starts, current.dev_cols, current.dev,
+                             inv, v, s2);
+        if (!e) {
+          copy_d2h(dev, pinned, s2, dofs * 8);
+          e = sync("power iteration");
+        }
+        if (!e) {
+          double n = norm2(pinned, dofs);
+          lm = n;
+          e = setup_scale(dev.stream, dofs, s2, n, v);
+        }
+      }
+      if (!e) e = sync("power iteration");
     }
     dev_free(dev, v);
     dev_free(dev, s2);
-    dev_free(dev, d_norms);
     if (e) return e;
-    lambda_max = lm[1] * SPECTRAL_MARGIN;
+    lambda_max = lm * SPECTRAL_MARGIN;
     if (is_coarsest) {
       phase = (rows * rb <= DENSE_LIMIT) ? FACTOR : DONE;
       if (phase == DONE) push_final(false);

@@ -10,9 +10,9 @@
 // coarse matrix. The order-dependent graph work (strength, aggregation, tentative prolongator)
 // and every sparsity pattern are built on the host (setup.cpp); only values live here.
 //
-// The one sequential reduction is the power iteration's norm (block.rs:398-404 sums the squares
-// in index order): a single block squares a chunk in parallel into shared memory while thread 0
-// adds the previous chunk in order.
+// The one sequential reduction, the power iteration's norm (block.rs:398-404 sums the squares in
+// index order), runs on the host (setup.cpp), where a single core adds a dependent chain of
+// doubles several times faster than one GPU thread; the products stay here.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -128,50 +128,8 @@ __global__ void block_norms_kernel(size_t blocks, const double* __restrict__ val
   }
 }
 
-// start_value (block.rs:379-382): a fixed pseudo-random vector in [0.5, 1.5).
-__global__ void start_vector_kernel(size_t n, double* __restrict__ v) {
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-    unsigned long long mixed = (unsigned long long)(i + 1) * 0x9E3779B97F4A7C15ull;
-    v[i] = 0.5 + (double)(mixed >> 11) / 9007199254740992.0;
-  }
-}
-
-// norm2 (block.rs:398-404): the squares summed in index order, then the square root.
-const int kNormChunk = 2048;
-const int kNormThreads = 512;
-__global__ void __launch_bounds__(kNormThreads) serial_norm_kernel(size_t n, const double* __restrict__ v,
-                                                                    double* __restrict__ out) {
-  __shared__ double sq[2][kNormChunk];
-  const size_t chunks = (n + kNormChunk - 1) / kNormChunk;
-  for (int t = threadIdx.x; t < kNormChunk; t += blockDim.x) {
-    double x = (size_t)t < n ? v[t] : 0.0;
-    sq[0][t] = x * x;
-  }
-  __syncthreads();
-  double s = 0.0;
-  for (size_t c = 0; c < chunks; ++c) {
-    const int cur = (int)(c & 1);
-    if (threadIdx.x == 0) {
-      const int len = (int)min((size_t)kNormChunk, n - c * kNormChunk);
-      const double* q = sq[cur];
-#pragma unroll 16
-      for (int k = 0; k < len; ++k) s += q[k];
-    } else if (c + 1 < chunks) {
-      const size_t base = (c + 1) * kNormChunk;
-      for (int t = threadIdx.x - 1; t < kNormChunk; t += blockDim.x - 1) {
-        double x = base + t < n ? v[base + t] : 0.0;
-        sq[cur ^ 1][t] = x * x;
-      }
-    }
-    __syncthreads();
-  }
-  if (threadIdx.x == 0) *out = sqrt(s);
-}
-
-// v = src / norm, element by element.
-__global__ void scale_kernel(size_t n, const double* __restrict__ src, const double* __restrict__ norm,
-                             double* __restrict__ v) {
-  const double d = *norm;
+// v = src / d, element by element.
+__global__ void scale_kernel(size_t n, const double* __restrict__ src, double d, double* __restrict__ v) {
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
     v[i] = src[i] / d;
 }
@@ -389,23 +347,20 @@ sf_status setup_block_norms(cudaStream_t st, size_t blocks, int len, const doubl
   return cuda_check(cudaGetLastError(), "block norms");
 }
 
-sf_status setup_power_iteration(cudaStream_t st, uint32_t rows, int rb, const uint32_t* starts, const uint32_t* cols,
-                                const double* vals, const double* inv, double* v, double* s2, double* norms,
-                                int iterations) {
-  const size_t n = (size_t)rows * rb;
+sf_status setup_power_step(cudaStream_t st, uint32_t rows, int rb, const uint32_t* starts, const uint32_t* cols,
+                           const double* vals, const double* inv, const double* v, double* s2) {
+  if (rows == 0) return SF_OK;
+  if (rb == 3)
+    power_step_kernel<3><<<grid_for(rows), kT, 0, st>>>(rows, starts, cols, vals, inv, v, s2);
+  else
+    power_step_kernel<6><<<grid_for(rows), kT, 0, st>>>(rows, starts, cols, vals, inv, v, s2);
+  return cuda_check(cudaGetLastError(), "power step");
+}
+
+sf_status setup_scale(cudaStream_t st, size_t n, const double* src, double d, double* v) {
   if (n == 0) return SF_OK;
-  start_vector_kernel<<<grid_for(n), kT, 0, st>>>(n, v);
-  serial_norm_kernel<<<1, kNormThreads, 0, st>>>(n, v, norms);
-  scale_kernel<<<grid_for(n), kT, 0, st>>>(n, v, norms, v);
-  for (int it = 0; it < iterations; ++it) {
-    if (rb == 3)
-      power_step_kernel<3><<<grid_for(rows), kT, 0, st>>>(rows, starts, cols, vals, inv, v, s2);
-    else
-      power_step_kernel<6><<<grid_for(rows), kT, 0, st>>>(rows, starts, cols, vals, inv, v, s2);
-    serial_norm_kernel<<<1, kNormThreads, 0, st>>>(n, s2, norms + 1);
-    scale_kernel<<<grid_for(n), kT, 0, st>>>(n, s2, norms + 1, v);
-  }
-  return cuda_check(cudaGetLastError(), "power iteration");
+  scale_kernel<<<grid_for(n), kT, 0, st>>>(n, src, d, v);
+  return cuda_check(cudaGetLastError(), "scale");
 }
 
 sf_status setup_entry_rows(cudaStream_t st, uint32_t rows, const uint32_t* starts, uint32_t* out) {
