@@ -182,6 +182,9 @@ typedef struct sf_study_options {
   uint64_t device_memory_budget; /* bytes a study may hold on the device; 0: no limit */
   uint64_t sell_min_rows;  /* operators with at least this many block rows use the SELL-32 layout;
                               0: 32768 */
+  int32_t batchable;       /* lay every operator out by its block shape alone (no SELL, fixed lanes
+                              per row), so studies of the same depth can share a batch
+                              (sf_study_solve_batch); default 0 */
 } sf_study_options;
 
 /* StudyOptions::default with the reference's defaults (Jacobi preconditioner). */
@@ -339,6 +342,19 @@ sf_status sf_study_energy_products(sf_study* study, const double* x, double* y, 
  * system and hierarchy on the device. */
 sf_status sf_study_resolve(sf_study* study, const double* rhs);
 
+/* No counterpart in the reference: batched solves. Restarts every listed study from a zero
+ * estimate on its resident right-hand side and solves them together: each kernel of a conjugate
+ * gradient step is ONE grid over all of them (blockIdx.y selects the study, whose operator,
+ * vectors and scalars come from a per-study argument table), and each study's own status word
+ * masks its blocks once it has converged or failed. Runs until every study has stopped; studies
+ * that stopped leave the batch between chunks of iterations. The studies must share their device
+ * and their launch structure (the same number of levels and the same operator layouts, as small
+ * studies of the same depth do); SF_INVALID_ARGUMENT otherwise. outcomes and statuses (either may
+ * be NULL) receive count entries: each study's outcome and its SF_OK / SF_PCG_NOT_CONVERGED /
+ * SF_PCG_NOT_POSITIVE_DEFINITE. */
+sf_status sf_study_solve_batch(sf_study** studies, uint64_t count, sf_step_outcome* outcomes,
+                               sf_status* statuses);
+
 /* The CUDA stream (cudaStream_t as an integer) every kernel of the study is launched on, so a
  * caller can bracket work with its own CUDA events. */
 uint64_t sf_study_stream(const sf_study* study);
@@ -370,6 +386,53 @@ typedef struct sf_kernel_timing {
   uint64_t launches;
 } sf_kernel_timing;
 sf_status sf_study_time_kernel(sf_study* study, int32_t kernel, uint64_t repeats, sf_kernel_timing* out);
+
+/* ------------------------------------------------------------- serving ------------------- */
+/* No counterpart in the reference: a request loop for many solves on one GPU. Requests are
+ * admitted in arrival order while their device memory fits `memory_budget`, built on host worker
+ * threads (each study on its own CUDA stream, hierarchy and vectors resident on the device) and
+ * solved. Studies with fewer than `batch_max_dofs` free DOFs are built batchable and solved in
+ * continuous batches: between chunks of iterations a batch drops the studies that stopped and
+ * takes in the ones that became ready, and each step is one grid per kernel over all its studies
+ * (sf_study_solve_batch). Larger studies solve on their own streams, overlapping on the device. */
+typedef struct sf_server sf_server;
+typedef struct sf_server_options {
+  int32_t device;
+  uint64_t memory_budget;  /* bytes of device memory for admitted requests; 0: 150 GiB */
+  uint64_t batch_max_dofs; /* requests with fewer free DOFs are batched; 100000 by default */
+  uint64_t max_batch;      /* studies per batch; 0: 64 */
+  uint64_t build_threads;  /* host threads building (and solving unbatched) requests; 0: 4 */
+  uint64_t setup_threads;  /* host threads inside one build when its options leave it 0; 0: 2 */
+} sf_server_options;
+void sf_server_options_default(sf_server_options* options);
+sf_status sf_server_create(const sf_server_options* options, sf_server** out);
+/* Submits a model (consumed) with its study options; `id` names the request. */
+sf_status sf_server_submit(sf_server* server, sf_model* model, const sf_study_options* options,
+                           uint64_t* id);
+
+typedef struct sf_request_result {
+  int32_t status;    /* the request's sf_status once finished */
+  int32_t finished;
+  int32_t batched;
+  uint64_t batch_size; /* the largest batch it ran in */
+  sf_step_outcome outcome;
+  uint64_t free_dofs, node_count, device_bytes;
+  double queue_seconds, build_seconds, solve_seconds, latency_seconds; /* latency from submission */
+} sf_request_result;
+/* Waits up to timeout_ms (UINT64_MAX: until done) for a request; SF_NOT_FINISHED while it runs. */
+sf_status sf_server_wait(sf_server* server, uint64_t id, uint64_t timeout_ms, sf_request_result* out);
+/* Copies a finished request's displacements (node_count x 3, may be NULL) and forgets the request;
+ * returns the request's own failure status if it failed. */
+sf_status sf_server_take(sf_server* server, uint64_t id, double* displacements);
+
+typedef struct sf_server_stats {
+  uint64_t completed, pending, reserved_bytes, peak_reserved_bytes, batches, batched_requests;
+  double mean_batch_size; /* studies per batched chunk */
+} sf_server_stats;
+sf_status sf_server_statistics(sf_server* server, sf_server_stats* out);
+/* Stops taking requests, finishes the builds and batches in flight, then frees everything;
+ * requests not yet admitted are dropped. */
+void sf_server_destroy(sf_server* server);
 
 #ifdef __cplusplus
 }

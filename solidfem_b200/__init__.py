@@ -23,6 +23,9 @@ LIBRARY_PATH = os.path.join(_HERE, "libsolidfem_b200.so")
 # ----------------------------------------------------------------------------- C structures
 
 
+FACE_DTYPE = np.dtype([("tet", "<u4"), ("face", "<u4"), ("nodes", "<u4", (6,))])
+
+
 class BoundaryFace(C.Structure):
     """A boundary face: BoundaryFace, crates/solidfem-mesh/src/boundary.rs:15-24."""
     _fields_ = [("tet", C.c_uint32), ("face", C.c_uint32), ("nodes", C.c_uint32 * 6)]
@@ -43,7 +46,7 @@ class _Options(C.Structure):
                 ("neighbour_reach", C.c_double), ("coarse_dofs", C.c_uint64), ("max_levels", C.c_uint64),
                 ("smoother_degree", C.c_uint64), ("smoother_range", C.c_double), ("precision", C.c_int32),
                 ("threads", C.c_uint64), ("device", C.c_int32), ("use_graphs", C.c_int32),
-                ("device_memory_budget", C.c_uint64), ("sell_min_rows", C.c_uint64)]
+                ("device_memory_budget", C.c_uint64), ("sell_min_rows", C.c_uint64), ("batchable", C.c_int32)]
 
 
 class _BuildProgress(C.Structure):
@@ -104,6 +107,24 @@ class Kernel(enum.IntEnum):
     RESTRICTION = 3
 
 
+class _ServerOptions(C.Structure):
+    _fields_ = [("device", C.c_int32), ("memory_budget", C.c_uint64), ("batch_max_dofs", C.c_uint64),
+                ("max_batch", C.c_uint64), ("build_threads", C.c_uint64), ("setup_threads", C.c_uint64)]
+
+
+class _RequestResult(C.Structure):
+    _fields_ = [("status", C.c_int32), ("finished", C.c_int32), ("batched", C.c_int32), ("batch_size", C.c_uint64),
+                ("outcome", _StepOutcome), ("free_dofs", C.c_uint64), ("node_count", C.c_uint64),
+                ("device_bytes", C.c_uint64), ("queue_seconds", C.c_double), ("build_seconds", C.c_double),
+                ("solve_seconds", C.c_double), ("latency_seconds", C.c_double)]
+
+
+class _ServerStats(C.Structure):
+    _fields_ = [("completed", C.c_uint64), ("pending", C.c_uint64), ("reserved_bytes", C.c_uint64),
+                ("peak_reserved_bytes", C.c_uint64), ("batches", C.c_uint64), ("batched_requests", C.c_uint64),
+                ("mean_batch_size", C.c_double)]
+
+
 _CANCEL = C.CFUNCTYPE(C.c_int32, C.c_void_p)
 _FIELD = C.CFUNCTYPE(None, C.c_void_p, C.POINTER(C.c_double), C.c_uint64, C.POINTER(_Material))
 
@@ -155,6 +176,14 @@ SIGNATURES = {
     "sf_study_precondition": (C.c_int, [_V, _P(C.c_double), _P(C.c_double)]),
     "sf_study_system_multiply": (C.c_int, [_V, _P(C.c_double), _P(C.c_double)]),
     "sf_study_energy_products": (C.c_int, [_V, _V, _V, _V, C.c_uint64]),
+    "sf_study_solve_batch": (C.c_int, [_P(_V), C.c_uint64, _P(_StepOutcome), _P(C.c_int)]),
+    "sf_server_options_default": (None, [_P(_ServerOptions)]),
+    "sf_server_create": (C.c_int, [_P(_ServerOptions), _P(_V)]),
+    "sf_server_submit": (C.c_int, [_V, _V, _P(_Options), _P(C.c_uint64)]),
+    "sf_server_wait": (C.c_int, [_V, C.c_uint64, C.c_uint64, _P(_RequestResult)]),
+    "sf_server_take": (C.c_int, [_V, C.c_uint64, _P(C.c_double)]),
+    "sf_server_statistics": (C.c_int, [_V, _P(_ServerStats)]),
+    "sf_server_destroy": (None, [_V]),
     "sf_study_device_timing": (C.c_int, [_V, _P(_DeviceTiming)]),
     "sf_study_resolve": (C.c_int, [_V, _P(C.c_double)]),
     "sf_study_stream": (C.c_uint64, [_V]),
@@ -289,6 +318,13 @@ class Mesh:
         _check(library().sf_mesh_boundary_faces(self._h, arr))
         return list(arr[:n])
 
+    def boundary_face_array(self) -> np.ndarray:
+        """The boundary faces as a structured array (tet, face, nodes[6]), in boundary_faces() order."""
+        n = int(library().sf_mesh_boundary_face_count(self._h))
+        arr = np.zeros(max(n, 1), dtype=FACE_DTYPE)
+        _check(library().sf_mesh_boundary_faces(self._h, arr.ctypes.data_as(C.POINTER(BoundaryFace))))
+        return arr[:n]
+
     @classmethod
     def from_linear(cls, positions, tets) -> "Mesh":
         """TetMesh::new + QuadraticTetMesh::from_linear (tet.rs:59-109, quadratic.rs:24-71)."""
@@ -346,6 +382,7 @@ class Model:
         self.fixed: list = []
         self.forces: list = []
         self.tractions: list = []
+        self.face_tractions: list = []
         self.prescribed: dict = {}
 
     def set_quadrature(self, q: Quadrature) -> None:
@@ -362,6 +399,11 @@ class Model:
 
     def add_traction(self, face: BoundaryFace, traction) -> None:
         self.tractions.append((face, tuple(float(t) for t in traction)))
+
+    def add_face_tractions(self, faces: np.ndarray, traction) -> None:
+        """Adds one traction to every face of a FACE_DTYPE array (the array form of add_traction)."""
+        faces = np.ascontiguousarray(faces, dtype=FACE_DTYPE)
+        self.face_tractions.append((faces, np.tile(np.asarray(traction, dtype=np.float64), (len(faces), 1))))
 
     def prescribe_displacement(self, node: int, axis: int, value: float) -> None:
         self.prescribed[(int(node), int(axis))] = float(value)
@@ -396,6 +438,11 @@ class Model:
             faces = (BoundaryFace * len(self.tractions))(*[f for f, _ in self.tractions])
             tr = np.ascontiguousarray([t for _, t in self.tractions], dtype=np.float64)
             _check(lib.sf_model_add_tractions(h, faces, _dptr(tr), len(self.tractions)))
+        for faces, tr in self.face_tractions:
+            if len(faces):
+                tr = np.ascontiguousarray(tr, dtype=np.float64)
+                _check(lib.sf_model_add_tractions(h, faces.ctypes.data_as(C.POINTER(BoundaryFace)), _dptr(tr),
+                                                  len(faces)))
         for (node, axis), value in self.prescribed.items():
             _check(lib.sf_model_prescribe_displacement(h, node, axis, value))
         return h, keep
@@ -444,6 +491,7 @@ class StudyOptions:
     use_graphs: bool = True
     device_memory_budget: int = 0
     sell_min_rows: int = 0
+    batchable: bool = False
 
     def _c(self) -> _Options:
         o = _Options()
@@ -466,6 +514,7 @@ class StudyOptions:
         o.use_graphs = 1 if self.use_graphs else 0
         o.device_memory_budget = self.device_memory_budget
         o.sell_min_rows = self.sell_min_rows
+        o.batchable = 1 if self.batchable else 0
         return o
 
 
@@ -688,8 +737,115 @@ class StaticStudy:
         return {"ms_per_launch": t.ms_per_launch, "bytes_per_launch": t.bytes_per_launch, "launches": t.launches}
 
 
+@dataclass
+class ServerOptions:
+    """sf_server_options: device, memory budget (bytes, 0: 150 GiB), the batching threshold in free DOFs,
+    studies per batch, build threads and setup threads per build."""
+    device: int = 0
+    memory_budget: int = 0
+    batch_max_dofs: int = 100000
+    max_batch: int = 64
+    build_threads: int = 4
+    setup_threads: int = 2
+
+    def _c(self) -> _ServerOptions:
+        o = _ServerOptions()
+        o.device = self.device
+        o.memory_budget = self.memory_budget
+        o.batch_max_dofs = self.batch_max_dofs
+        o.max_batch = self.max_batch
+        o.build_threads = self.build_threads
+        o.setup_threads = self.setup_threads
+        return o
+
+
+@dataclass
+class RequestResult:
+    status: "Status"
+    finished: bool
+    batched: bool
+    batch_size: int
+    outcome: StepOutcome
+    free_dofs: int
+    node_count: int
+    device_bytes: int
+    queue_seconds: float
+    build_seconds: float
+    solve_seconds: float
+    latency_seconds: float
+
+
+class Server:
+    """The serving loop (sf_server): requests admitted by device memory budget, built on worker threads,
+    small ones solved in continuous batches, large ones on their own streams."""
+
+    def __init__(self, options: Optional[ServerOptions] = None):
+        self._h = C.c_void_p()
+        _check(library().sf_server_create(C.byref((options or ServerOptions())._c()), C.byref(self._h)))
+        self._keep = {}
+
+    def submit(self, model: Model, options: Optional[StudyOptions] = None) -> int:
+        mh, keep = model._to_c()
+        rid = C.c_uint64()
+        _check(library().sf_server_submit(self._h, mh, C.byref((options or StudyOptions())._c()), C.byref(rid)))
+        self._keep[rid.value] = keep
+        return rid.value
+
+    def wait(self, rid: int, timeout: Optional[float] = None) -> RequestResult:
+        r = _RequestResult()
+        ms = 2**64 - 1 if timeout is None else int(timeout * 1000)
+        code = library().sf_server_wait(self._h, rid, ms, C.byref(r))
+        if code not in (0, int(Status.NOT_FINISHED)):
+            _check(code)
+        p = r.outcome.progress
+        return RequestResult(Status(r.status), bool(r.finished), bool(r.batched), r.batch_size,
+                             StepOutcome(Outcome(r.outcome.kind), Progress(p.iteration, p.relative_residual,
+                                                                           bool(p.at_rounding_floor))),
+                             r.free_dofs, r.node_count, r.device_bytes, r.queue_seconds, r.build_seconds,
+                             r.solve_seconds, r.latency_seconds)
+
+    def take(self, rid: int, node_count: int) -> np.ndarray:
+        out = np.empty((node_count, 3), dtype=np.float64)
+        try:
+            _check(library().sf_server_take(self._h, rid, _dptr(out)))
+        finally:
+            self._keep.pop(rid, None)
+        return out
+
+    def stats(self) -> dict:
+        st = _ServerStats()
+        _check(library().sf_server_statistics(self._h, C.byref(st)))
+        return {name: getattr(st, name) for name, _ in _ServerStats._fields_}
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            library().sf_server_destroy(self._h)
+            self._h = None
+            self._keep.clear()
+
+    def __del__(self):
+        self.close()
+
+
+def solve_batch(studies) -> list:
+    """Solves resident studies together, one grid per kernel over all of them (sf_study_solve_batch).
+    Returns (StepOutcome, Status) per study."""
+    n = len(studies)
+    handles = (_V * n)(*[st._h for st in studies])
+    outs = (_StepOutcome * n)()
+    stats = (C.c_int * n)()
+    _check(library().sf_study_solve_batch(handles, n, outs, stats))
+    res = []
+    for i in range(n):
+        p = outs[i].progress
+        res.append((StepOutcome(Outcome(outs[i].kind), Progress(p.iteration, p.relative_residual,
+                                                                 bool(p.at_rounding_floor))), Status(stats[i])))
+    return res
+
+
 __all__ = [
-    "BoundaryFace", "Mesh", "box_tet_mesh", "Material", "ShellCore", "Quadrature", "Model", "Precision",
+    "FACE_DTYPE", "BoundaryFace", "Mesh", "box_tet_mesh", "Material", "ShellCore", "Quadrature", "Model", "Precision",
     "PcgOptions", "MultigridOptions", "Jacobi", "StudyOptions", "StudyBuilder", "StaticStudy", "StepOutcome",
     "Outcome", "Progress", "BuildProgress", "PointStress", "SolidfemError", "Status", "library", "SIGNATURES", "Kernel", "Solution",
+    "solve_batch", "Server", "ServerOptions", "RequestResult",
 ]

@@ -124,7 +124,19 @@ struct DeviceSolver {
   uint64_t launches = 0;          // kernels launched so far (graph replays count their kernels)
   mutable uint64_t h2d_bytes = 0, d2h_bytes = 0;
   uint64_t sell_min_rows = 32768;  // operators with at least this many rows use SELL-32
+  bool uniform_lanes = false;      // lanes per row by block shape alone (batchable studies)
 };
+
+// One recorded kernel launch: the batched form of the kernel, its launch shape and the bytes of its
+// argument pack. While `g_recorder` is set on a thread, solve launches on that thread are recorded
+// instead of executed (batch construction).
+struct LaunchRecord {
+  const void* batched = nullptr;
+  dim3 grid, block;
+  size_t smem = 0;
+  std::vector<unsigned char> pack;
+};
+extern thread_local std::vector<LaunchRecord>* g_recorder;
 
 // ------------------------------------------------------------------- memory helpers
 // Stream-ordered copies that count the bytes crossing the host-device link.
@@ -245,6 +257,20 @@ sf_status solver_read_state(DeviceSolver& s, PcgState* out);
 sf_status solver_restart(DeviceSolver& s, double tolerance, uint64_t max_iterations);
 // Mean device milliseconds per launch of one solver kernel and its algorithmic bytes per launch.
 sf_status solver_time_kernel(DeviceSolver& s, int kernel, uint64_t repeats, double* ms, double* bytes);
+// Several solvers advanced together: one graph whose nodes are single grids over all of them
+// (blockIdx.y = instance), each instance's arguments from a device table per launch site.
+struct BatchIteration {
+  cudaStream_t stream = nullptr;
+  size_t count = 0, sites = 0;
+  std::vector<void*> tables;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+};
+// Fails with SF_INVALID_ARGUMENT when the solvers do not share their launch structure.
+sf_status batch_build(const std::vector<DeviceSolver*>& inst, cudaStream_t stream, BatchIteration& out);
+sf_status batch_replay(BatchIteration& b, uint64_t iterations);
+void batch_destroy(BatchIteration& b);
+
 // y_k = A x_k and energy[k] = x_k . y_k for count vectors of device memory (count x n each),
 // enqueued on s.stream; the reduction scratch is a static device array, so nothing is allocated.
 sf_status solver_energy_products(DeviceSolver& s, const double* x, double* y, double* energy, uint64_t count);

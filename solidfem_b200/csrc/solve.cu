@@ -18,6 +18,7 @@
 #include <cmath>
 #include <cstdio>
 #include <mutex>
+#include <cstring>
 #include <utility>
 
 #include "device.h"
@@ -33,18 +34,115 @@ const uint32_t kGroupTarget = 4096;     // value bytes a row group aims at
 const int kSmemPerBlockTarget = 72 * 1024;
 
 // ------------------------------------------------------------ programmatic dependent launch
-// Every solve kernel is launched with programmatic stream serialization: it may be scheduled
-// while its predecessor is still finishing, waits at entry until the predecessor grid has
-// completed and its writes are visible (griddepcontrol.wait), then at once lets its own successor
-// be scheduled (griddepcontrol.launch_dependents). Launch latency and the ramp of each grid
-// overlap the tail of the previous one; the data dependence is unchanged. Without a programmatic
-// predecessor the wait returns at once.
+// Every solve kernel is launched with programmatic stream serialization: its launch is prepared
+// while the predecessor runs, and at entry it waits until the predecessor grid has completed and
+// its writes are visible (griddepcontrol.wait). The data dependence is unchanged; without a
+// programmatic predecessor the wait returns at once.
 __device__ __forceinline__ void pdl_enter() {
   asm volatile("griddepcontrol.wait;\n" ::: "memory");
 }
 
-template <typename... KArgs, typename... Args>
-void launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st, Args&&... args) {
+
+// ------------------------------------------------------------ kernel bodies and batched launches
+// Every solve kernel is written as a __device__ body. A launch either runs it as a single-instance
+// grid (its arguments by value) or, while a recorder is active, records the arguments so that a
+// batch of instances with the same launch sequence can run each step as ONE grid: blockIdx.y
+// selects the instance, whose arguments (operator, vectors, Chebyshev scalars, status word) come
+// from a device table. The status word of each instance is its convergence mask: a finished
+// instance's blocks return at once.
+template <typename... P>
+struct Pack;
+template <>
+struct Pack<> {};
+template <typename H, typename... T>
+struct Pack<H, T...> {
+  H head;
+  Pack<T...> tail;
+};
+
+inline Pack<> make_pack() { return {}; }
+template <typename H, typename... T>
+Pack<H, T...> make_pack(H h, T... t) {
+  Pack<H, T...> p;
+  p.head = h;
+  p.tail = make_pack(t...);
+  return p;
+}
+
+template <auto Body, typename... Done>
+__device__ __forceinline__ void apply_pack(const Pack<>&, Done... done) {
+  Body(done...);
+}
+template <auto Body, typename H, typename... T, typename... Done>
+__device__ __forceinline__ void apply_pack(const Pack<H, T...>& p, Done... done) {
+  apply_pack<Body>(p.tail, done..., p.head);
+}
+
+template <auto Body, typename... P>
+__global__ void __launch_bounds__(kThreads) single_kernel(P... args) {
+  pdl_enter();
+  Body(args...);
+}
+template <auto Body, typename PackT>
+__global__ void __launch_bounds__(kThreads) batched_kernel(const PackT* __restrict__ table) {
+  pdl_enter();
+  const PackT a = table[blockIdx.y];
+  apply_pack<Body>(a);
+}
+
+template <typename F>
+struct BodyTraits;
+template <typename... P>
+struct BodyTraits<void (*)(P...)> {
+  typedef Pack<P...> PackT;
+  template <typename... A>
+  static PackT pack(A&&... a) {
+    return make_pack<P...>(static_cast<P>(a)...);
+  }
+  template <auto Body>
+  static const void* single() {
+    return (const void*)single_kernel<Body, P...>;
+  }
+  template <auto Body>
+  static const void* batched() {
+    return (const void*)batched_kernel<Body, PackT>;
+  }
+};
+
+}  // namespace
+
+thread_local std::vector<LaunchRecord>* g_recorder = nullptr;
+
+namespace {
+
+inline void fill_argv(void**, Pack<>&) {}
+template <typename H, typename... T>
+void fill_argv(void** out, Pack<H, T...>& p) {
+  out[0] = &p.head;
+  fill_argv(out + 1, p.tail);
+}
+
+template <auto Body, typename... A>
+void launch_body(dim3 grid, dim3 block, size_t smem, cudaStream_t st, A&&... args) {
+  typedef BodyTraits<decltype(Body)> T;
+  typename T::PackT pk = T::pack(std::forward<A>(args)...);
+  if (g_recorder) {
+    LaunchRecord r;
+    r.batched = T::template batched<Body>();
+    r.grid = grid;
+    r.block = block;
+    r.smem = smem;
+    r.pack.resize(sizeof(pk));
+    std::memcpy(r.pack.data(), &pk, sizeof(pk));
+    g_recorder->push_back(std::move(r));
+    return;
+  }
+  const void* k = T::template single<Body>();
+  static bool opted = false;
+  if (smem > 48 * 1024 && !opted) {
+    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    opted = true;
+  }
   cudaLaunchAttribute attr[1];
   attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
   attr[0].val.programmaticStreamSerializationAllowed = 1;
@@ -55,7 +153,9 @@ void launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cu
   cfg.stream = st;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+  void* argv[sizeof...(A) + 1];
+  fill_argv(argv, pk);
+  cudaLaunchKernelExC(&cfg, k, argv);
 }
 
 // ------------------------------------------------------------ asynchronous staging
@@ -265,9 +365,8 @@ struct EpiAxpy {
 };
 
 template <typename S, typename V, int RB, int CB, int LPR, int OP>
-__global__ void __launch_bounds__(kThreads) bsr_kernel(Op<S> A, const V* __restrict__ x, V* __restrict__ y,
+__device__ __forceinline__ void bsr_kernel(Op<S> A, const V* __restrict__ x, V* __restrict__ y,
                                                        const V* __restrict__ b, const int* __restrict__ status) {
-  pdl_enter();
   if (*status != ST_ACTIVE) return;
   extern __shared__ __align__(16) char smem[];
   char* wbase = smem + (threadIdx.x >> 5) * 2 * slot_bytes(A);
@@ -334,11 +433,10 @@ struct EpiCheb {
 };
 
 template <typename S, typename V, int RB, int LPR>
-__global__ void __launch_bounds__(kThreads) cheb_step_kernel(Op<S> A, const S* __restrict__ dinv, const V* __restrict__ d_old,
+__device__ __forceinline__ void cheb_step_kernel(Op<S> A, const S* __restrict__ dinv, const V* __restrict__ d_old,
                                                              V* __restrict__ d_new, V* __restrict__ r, V* __restrict__ x,
                                                              V* __restrict__ outer, V keep, V step,
                                                              const int* __restrict__ status) {
-  pdl_enter();
   if (*status != ST_ACTIVE) return;
   extern __shared__ __align__(16) char smem[];
   char* wbase = smem + (threadIdx.x >> 5) * 2 * slot_bytes(A);
@@ -358,12 +456,11 @@ __global__ void __launch_bounds__(kThreads) cheb_step_kernel(Op<S> A, const S* _
 // B is the type the right-hand side arrives in: f64 at the finest level of an f32 cycle, which
 // rounds it here (cycle.rs:236-238) into `b_out`.
 template <typename S, typename V, typename B, int RB>
-__global__ void __launch_bounds__(kThreads) cheb_start_kernel(uint32_t rows, const S* __restrict__ dinv,
+__device__ __forceinline__ void cheb_start_kernel(uint32_t rows, const S* __restrict__ dinv,
                                                                const B* __restrict__ b_in, V* __restrict__ b_out,
                                                                V* __restrict__ r, V* __restrict__ d,
                                                                V* __restrict__ x, V theta,
                                                                const int* __restrict__ status) {
-  pdl_enter();
   if (*status != ST_ACTIVE) return;
   for (uint32_t row = blockIdx.x * blockDim.x + threadIdx.x; row < rows; row += gridDim.x * blockDim.x) {
     size_t base = (size_t)row * RB;
@@ -387,16 +484,14 @@ __global__ void __launch_bounds__(kThreads) cheb_start_kernel(uint32_t rows, con
 }
 
 template <typename V>
-__global__ void add_kernel(size_t n, V* __restrict__ x, const V* __restrict__ y, const int* __restrict__ status) {
-  pdl_enter();
+__device__ __forceinline__ void add_kernel(size_t n, V* __restrict__ x, const V* __restrict__ y, const int* __restrict__ status) {
   if (*status != ST_ACTIVE) return;
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
     x[i] = x[i] + y[i];
 }
 
 template <typename B, typename V>
-__global__ void convert_kernel(size_t n, const B* __restrict__ in, V* __restrict__ out, const int* __restrict__ status) {
-  pdl_enter();
+__device__ __forceinline__ void convert_kernel(size_t n, const B* __restrict__ in, V* __restrict__ out, const int* __restrict__ status) {
   if (*status != ST_ACTIVE) return;
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
     out[i] = V(in[i]);
@@ -405,10 +500,9 @@ __global__ void convert_kernel(size_t n, const B* __restrict__ in, V* __restrict
 // The coarsest level's direct solve as x = V(A^-1 widen(b)), one warp per row of the f64 inverse
 // (cycle.rs:476-486 solves with the f64 factor; the inverse is that factor's L^-T L^-1).
 template <typename V>
-__global__ void __launch_bounds__(kThreads) coarse_solve_kernel(uint32_t n, const double* __restrict__ inv,
+__device__ __forceinline__ void coarse_solve_kernel(uint32_t n, const double* __restrict__ inv,
                                                                  const V* __restrict__ b, V* __restrict__ x,
                                                                  const int* __restrict__ status) {
-  pdl_enter();
   if (*status != ST_ACTIVE) return;
   int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   for (uint32_t row = blockIdx.x * kWarps + warp; row < n; row += gridDim.x * kWarps) {
@@ -622,9 +716,8 @@ struct SellAxpy {
 };
 
 template <typename S, typename V, int RB, int CB, int OP>
-__global__ void __launch_bounds__(kThreads) sell_kernel(SellOp<S> A, const V* __restrict__ x, V* __restrict__ y,
+__device__ __forceinline__ void sell_kernel(SellOp<S> A, const V* __restrict__ x, V* __restrict__ y,
                                                         const V* __restrict__ b, const int* __restrict__ status) {
-  pdl_enter();
   if (*status != ST_ACTIVE) return;
   SellAxpy<V, RB, OP> epi{y, b, {}};
   sell_rows<S, V, RB, CB, false>(A, x, epi);
@@ -668,11 +761,10 @@ struct SellCheb {
 };
 
 template <typename S, typename V, int RB>
-__global__ void __launch_bounds__(kThreads) sell_cheb_kernel(SellOp<S> A, const S* __restrict__ dinv,
+__device__ __forceinline__ void sell_cheb_kernel(SellOp<S> A, const S* __restrict__ dinv,
                                                              const V* __restrict__ d_old, V* __restrict__ d_new,
                                                              V* __restrict__ r, V* __restrict__ x, V* __restrict__ outer,
                                                              V keep, V step, const int* __restrict__ status) {
-  pdl_enter();
   if (*status != ST_ACTIVE) return;
   SellCheb<S, V, RB> epi;
   epi.dinv = dinv;
@@ -706,10 +798,9 @@ struct SellDot {
   }
 };
 
-__global__ void __launch_bounds__(kThreads) sell_pcg_spmv_dot_kernel(SellOp<double> A, const double* __restrict__ p,
+__device__ __forceinline__ void sell_pcg_spmv_dot_kernel(SellOp<double> A, const double* __restrict__ p,
                                                                       double* __restrict__ ap, double* partials,
                                                                       PcgState* st) {
-  pdl_enter();
   if (st->status != ST_ACTIVE) return;
   SellDot epi;
   epi.p = p;
@@ -754,10 +845,9 @@ struct SellCheck {
   }
 };
 
-__global__ void __launch_bounds__(kThreads) sell_pcg_check_kernel(SellOp<double> A, const double* __restrict__ x,
+__device__ __forceinline__ void sell_pcg_check_kernel(SellOp<double> A, const double* __restrict__ x,
                                                                    const double* __restrict__ b, double* __restrict__ r,
                                                                    double* partials, PcgState* st) {
-  pdl_enter();
   if (st->status != ST_ACTIVE || st->mode != MODE_CHECK) return;
   SellCheck epi;
   epi.b = b;
@@ -822,9 +912,8 @@ struct EpiDot {
 // ap = A p on the f64 system with the curvature p.ap; then alpha = rz / curvature
 // (pcg.rs:217-228).
 template <int LPR>
-__global__ void __launch_bounds__(kThreads) pcg_spmv_dot_kernel(Op<double> A, const double* __restrict__ p,
+__device__ __forceinline__ void pcg_spmv_dot_kernel(Op<double> A, const double* __restrict__ p,
                                                                  double* __restrict__ ap, double* partials, PcgState* st) {
-  pdl_enter();
   if (st->status != ST_ACTIVE) return;
   extern __shared__ __align__(16) char smem[];
   char* wbase = smem + (threadIdx.x >> 5) * 2 * slot_bytes(A);
@@ -847,10 +936,9 @@ __global__ void __launch_bounds__(kThreads) pcg_spmv_dot_kernel(Op<double> A, co
 }
 
 // x += alpha p; r -= alpha ap; relative residual from r.r (pcg.rs:228-234).
-__global__ void __launch_bounds__(kThreads) pcg_update_kernel(uint32_t n, const double* __restrict__ p,
+__device__ __forceinline__ void pcg_update_kernel(uint32_t n, const double* __restrict__ p,
                                                                const double* __restrict__ ap, double* __restrict__ x,
                                                                double* __restrict__ r, double* partials, PcgState* st) {
-  pdl_enter();
   if (st->status != ST_ACTIVE) return;
   double alpha = st->alpha, na = -alpha;
   double local = 0.0;
@@ -905,10 +993,9 @@ struct EpiCheck {
 // The true residual when the recursive one reports convergence, with the rounding floor of the
 // product (pcg.rs:234-255): r = b - A x; converge, or restart from it.
 template <int LPR>
-__global__ void __launch_bounds__(kThreads) pcg_check_kernel(Op<double> A, const double* __restrict__ x,
+__device__ __forceinline__ void pcg_check_kernel(Op<double> A, const double* __restrict__ x,
                                                               const double* __restrict__ b, double* __restrict__ r,
                                                               double* partials, PcgState* st) {
-  pdl_enter();
   if (st->status != ST_ACTIVE || st->mode != MODE_CHECK) return;
   extern __shared__ __align__(16) char smem[];
   char* wbase = smem + (threadIdx.x >> 5) * 2 * slot_bytes(A);
@@ -937,10 +1024,9 @@ __global__ void __launch_bounds__(kThreads) pcg_check_kernel(Op<double> A, const
 // (z'.(r' - r))/rz with r' - r = -alpha ap. A restart takes p = z (pcg.rs:278-282). Then the
 // iteration cap (pcg.rs:266-273).
 template <typename Z>
-__global__ void __launch_bounds__(kThreads) pcg_dot_rz_kernel(uint32_t n, const double* __restrict__ r,
+__device__ __forceinline__ void pcg_dot_rz_kernel(uint32_t n, const double* __restrict__ r,
                                                                const Z* __restrict__ z, const double* __restrict__ ap,
                                                                double* partials, PcgState* st) {
-  pdl_enter();
   if (st->status != ST_ACTIVE) return;
   bool flex = st->flexible && st->mode == MODE_NORMAL;
   double rz = 0.0, apz = 0.0;
@@ -966,8 +1052,7 @@ __global__ void __launch_bounds__(kThreads) pcg_dot_rz_kernel(uint32_t n, const 
 
 // p = z + beta p, or p = z after a restart.
 template <typename Z>
-__global__ void pcg_update_p_kernel(uint32_t n, const Z* __restrict__ z, double* __restrict__ p, PcgState* st) {
-  pdl_enter();
+__device__ __forceinline__ void pcg_update_p_kernel(uint32_t n, const Z* __restrict__ z, double* __restrict__ p, PcgState* st) {
   if (st->status != ST_ACTIVE) return;
   bool restart = st->mode == MODE_RESTART;
   double beta = st->beta;
@@ -978,9 +1063,8 @@ __global__ void pcg_update_p_kernel(uint32_t n, const Z* __restrict__ z, double*
 }
 
 // Initial state (Pcg::new, pcg.rs:135-164): x = 0, r = b, rhs norm; then reset_direction.
-__global__ void __launch_bounds__(kThreads) pcg_init_kernel(uint32_t n, const double* __restrict__ b, double* __restrict__ x,
+__device__ __forceinline__ void pcg_init_kernel(uint32_t n, const double* __restrict__ b, double* __restrict__ x,
                                                              double* __restrict__ r, double* partials, PcgState* st) {
-  pdl_enter();
   double local = 0.0;
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     x[i] = 0.0;
@@ -998,9 +1082,8 @@ __global__ void __launch_bounds__(kThreads) pcg_init_kernel(uint32_t n, const do
 }
 
 // Jacobi: z = r / diag (preconditioner.rs:237-247), stored as the inverse diagonal.
-__global__ void jacobi_kernel(uint32_t n, const double* __restrict__ inv, const double* __restrict__ r,
+__device__ __forceinline__ void jacobi_kernel(uint32_t n, const double* __restrict__ inv, const double* __restrict__ r,
                               double* __restrict__ z, const int* __restrict__ status) {
-  pdl_enter();
   if (*status != ST_ACTIVE) return;
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) z[i] = r[i] * inv[i];
 }
@@ -1049,23 +1132,12 @@ Shape shape_of(const Op<S>& A, bool reduction) {
   return {32 * warps, (int)std::max<size_t>(1, grid), smem};
 }
 
-// Lets a kernel use up to 200 KB of dynamic shared memory; called once per kernel, before any
-// capture (the first launches happen in the solver's initial reset).
-template <typename K>
-void smem_opt_in(K kernel, bool& done) {
-  if (done) return;
-  cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-  done = true;
-}
 
 template <typename S, typename V, int RB, int CB, int LPR, int OP>
 void launch_bsr_lpr(const DevBsr& m, const V* x, V* y, const V* b, const int* status, cudaStream_t st) {
   Op<S> A = op_of<S>(m);
   Shape sh = shape_of(A, false);
-  auto k = bsr_kernel<S, V, RB, CB, LPR, OP>;
-  static bool opted = false;
-  smem_opt_in(k, opted);
-  launch_pdl(k, sh.grid, sh.threads, sh.smem, st, A, x, y, b, status);
+  launch_body<bsr_kernel<S, V, RB, CB, LPR, OP>>(sh.grid, sh.threads, sh.smem, st, A, x, y, b, status);
 }
 
 int grid_for_slices(uint32_t nslices) {
@@ -1075,7 +1147,7 @@ int grid_for_slices(uint32_t nslices) {
 
 template <typename S, typename V, int RB, int CB, int OP>
 void launch_sell(const DevBsr& m, const V* x, V* y, const V* b, const int* status, cudaStream_t st) {
-  launch_pdl(sell_kernel<S, V, RB, CB, OP>, grid_for_slices(m.nslices), kThreads, 0, st, sell_of<S>(m), x, y, b, status);
+  launch_body<sell_kernel<S, V, RB, CB, OP>>(grid_for_slices(m.nslices), kThreads, 0, st, sell_of<S>(m), x, y, b, status);
 }
 
 template <typename S, typename V, int RB, int CB, int OP>
@@ -1113,17 +1185,15 @@ void launch_cheb_step_lpr(const DevLevel& L, const V* d_old, V* d_new, V* r, V* 
                           const int* status, cudaStream_t st) {
   Op<S> A = op_of<S>(L.a);
   Shape sh = shape_of(A, false);
-  auto k = cheb_step_kernel<S, V, RB, LPR>;
-  static bool opted = false;
-  smem_opt_in(k, opted);
-  launch_pdl(k, sh.grid, sh.threads, sh.smem, st, A, (const S*)L.dinv, d_old, d_new, r, x, outer, (V)keep, (V)step, status);
+  launch_body<cheb_step_kernel<S, V, RB, LPR>>(sh.grid, sh.threads, sh.smem, st, A, (const S*)L.dinv, d_old, d_new, r,
+                                                x, outer, (V)keep, (V)step, status);
 }
 
 template <typename S, typename V, int RB>
 void launch_cheb_step(const DevLevel& L, const V* d_old, V* d_new, V* r, V* x, V* outer, double keep, double step,
                       const int* status, cudaStream_t st) {
   if (L.a.sell) {
-    launch_pdl(sell_cheb_kernel<S, V, RB>, grid_for_slices(L.a.nslices), kThreads, 0, st,
+    launch_body<sell_cheb_kernel<S, V, RB>>(grid_for_slices(L.a.nslices), kThreads, 0, st,
         sell_of<S>(L.a), (const S*)L.dinv, d_old, d_new, r, x, outer, (V)keep, (V)step, status);
     return;
   }
@@ -1138,7 +1208,7 @@ void launch_cheb_step(const DevLevel& L, const V* d_old, V* d_new, V* r, V* x, V
 template <typename S, typename V, typename B, int RB>
 void launch_cheb_start(const DevLevel& L, const B* b_in, V* b_out, V* r, V* d, V* x, double theta, const int* status,
                        cudaStream_t st) {
-  launch_pdl(cheb_start_kernel<S, V, B, RB>, grid_for_elems(L.a.rows), kThreads, 0, st,
+  launch_body<cheb_start_kernel<S, V, B, RB>>(grid_for_elems(L.a.rows), kThreads, 0, st,
       L.a.rows, (const S*)L.dinv, b_in, b_out, r, d, x, (V)theta, status);
 }
 
@@ -1164,7 +1234,7 @@ void enqueue_smooth(DeviceSolver& s, DevLevel& L, const B* b_in, V* b_out, V* x,
     s.launches_per_iteration++;
   }
   if (outer && L.steps.empty()) {
-    launch_pdl(add_kernel<V>, grid_for_elems(L.n), kThreads, 0, st, L.n, outer, x, status);
+    launch_body<add_kernel<V>>(grid_for_elems(L.n), kThreads, 0, st, L.n, outer, x, status);
     s.launches_per_iteration++;
   }
 }
@@ -1179,11 +1249,11 @@ void enqueue_cycle(DeviceSolver& s, size_t li, const B* rhs, V* b_store, V* x, c
     if (L.has_factor) {
       const V* bv = (const V*)rhs;
       if (b_store) {
-        launch_pdl(convert_kernel<B, V>, grid_for_elems(L.n), kThreads, 0, st, L.n, rhs, b_store, status);
+        launch_body<convert_kernel<B, V>>(grid_for_elems(L.n), kThreads, 0, st, L.n, rhs, b_store, status);
         s.launches_per_iteration++;
         bv = b_store;
       }
-      launch_pdl(coarse_solve_kernel<V>, grid_for_rows(L.n), kThreads, 0, st, L.n, L.coarse_inverse, bv, x, status);
+      launch_body<coarse_solve_kernel<V>>(grid_for_rows(L.n), kThreads, 0, st, L.n, L.coarse_inverse, bv, x, status);
       s.launches_per_iteration++;
     } else {
       enqueue_smooth<S, V, B>(s, L, rhs, b_store, x, nullptr, status);
@@ -1206,7 +1276,7 @@ void enqueue_cycle(DeviceSolver& s, size_t li, const B* rhs, V* b_store, V* x, c
 // z = M r for the solver's r (f64) into z (f64) or z32.
 void enqueue_precondition(DeviceSolver& s, const double* r, double* z, float* z32, const int* status) {
   if (!s.multigrid) {
-    launch_pdl(jacobi_kernel, grid_for_elems(s.n), kThreads, 0, s.stream, s.n, s.jacobi, r, z, status);
+    launch_body<jacobi_kernel>(grid_for_elems(s.n), kThreads, 0, s.stream, s.n, s.jacobi, r, z, status);
     s.launches_per_iteration++;
     return;
   }
@@ -1223,14 +1293,9 @@ template <int LPR>
 void launch_pcg_spmv_lpr(DeviceSolver& s) {
   Op<double> A = op_of<double>(s.system);
   Shape sh = shape_of(A, true);
-  auto k = pcg_spmv_dot_kernel<LPR>;
-  static bool opted = false, opted_check = false;
-  smem_opt_in(k, opted);
-  launch_pdl(k, sh.grid, sh.threads, sh.smem, s.stream, A, s.p, s.ap, s.partials, s.state);
-  auto c = pcg_check_kernel<LPR>;
-  smem_opt_in(c, opted_check);
-  launch_pdl(pcg_update_kernel, kReduceBlocks, kReduceThreads, 0, s.stream, s.n, s.p, s.ap, s.x, s.r, s.partials, s.state);
-  launch_pdl(c, sh.grid, sh.threads, sh.smem, s.stream, A, s.x, s.rhs, s.r, s.partials, s.state);
+  launch_body<pcg_spmv_dot_kernel<LPR>>(sh.grid, sh.threads, sh.smem, s.stream, A, s.p, s.ap, s.partials, s.state);
+  launch_body<pcg_update_kernel>(kReduceBlocks, kReduceThreads, 0, s.stream, s.n, s.p, s.ap, s.x, s.r, s.partials, s.state);
+  launch_body<pcg_check_kernel<LPR>>(sh.grid, sh.threads, sh.smem, s.stream, A, s.x, s.rhs, s.r, s.partials, s.state);
 }
 
 }  // namespace
@@ -1281,6 +1346,10 @@ sf_status make_row_groups(DeviceSolver& s, DevBsr& m, const uint32_t* starts, si
   // warp splits into that many teams of 32 / teams lanes, one row each, so a warp works on several
   // light rows at once (their x gathers and epilogue loads overlap) and on a heavy row whole.
   double mean = m.rows ? (double)starts[m.rows] / m.rows : 0.0;
+  // Batchable studies take a nominal row length per block shape (about 25 blocks on a 3x3
+  // stiffness level, 4 on a prolongator, 30 on a coarse level or a transpose), so the choice, and
+  // with it the kernel, is the same for every study of that shape.
+  if (s.uniform_lanes) mean = (m.rb == 3 && m.cb == 3) ? 25.0 : (m.cb == 6 && m.rb == 3) ? 4.0 : 30.0;
   double row_bytes = std::max(1.0, mean * (double)value_bytes);
   int teams = 1;
   while (teams < 8 && (teams * 2) * row_bytes <= kGroupTarget) teams *= 2;
@@ -1542,7 +1611,7 @@ sf_status solver_init_pcg(DeviceSolver& s, double tolerance, uint64_t max_iterat
   copy_h2d(s, s.state, &h, sizeof(h));
   int one_active = ST_ACTIVE;
   copy_h2d(s, s.always_active, &one_active, sizeof(int));
-  launch_pdl(pcg_init_kernel, kReduceBlocks, kReduceThreads, 0, s.stream, s.n, s.rhs, s.x, s.r, s.partials, s.state);
+  launch_body<pcg_init_kernel>(kReduceBlocks, kReduceThreads, 0, s.stream, s.n, s.rhs, s.x, s.r, s.partials, s.state);
   return solver_enqueue_reset(s);
 }
 
@@ -1550,11 +1619,11 @@ sf_status solver_enqueue_reset(DeviceSolver& s) {
   const int* status = &s.state->status;
   enqueue_precondition(s, s.r, s.z, s.z32, status);
   if (s.vector_single && s.multigrid) {
-    launch_pdl(pcg_dot_rz_kernel<float>, kReduceBlocks, kReduceThreads, 0, s.stream, s.n, s.r, s.z32, s.ap, s.partials, s.state);
-    launch_pdl(pcg_update_p_kernel<float>, grid_for_elems(s.n), kThreads, 0, s.stream, s.n, s.z32, s.p, s.state);
+    launch_body<pcg_dot_rz_kernel<float>>(kReduceBlocks, kReduceThreads, 0, s.stream, s.n, s.r, s.z32, s.ap, s.partials, s.state);
+    launch_body<pcg_update_p_kernel<float>>(grid_for_elems(s.n), kThreads, 0, s.stream, s.n, s.z32, s.p, s.state);
   } else {
-    launch_pdl(pcg_dot_rz_kernel<double>, kReduceBlocks, kReduceThreads, 0, s.stream, s.n, s.r, s.z, s.ap, s.partials, s.state);
-    launch_pdl(pcg_update_p_kernel<double>, grid_for_elems(s.n), kThreads, 0, s.stream, s.n, s.z, s.p, s.state);
+    launch_body<pcg_dot_rz_kernel<double>>(kReduceBlocks, kReduceThreads, 0, s.stream, s.n, s.r, s.z, s.ap, s.partials, s.state);
+    launch_body<pcg_update_p_kernel<double>>(grid_for_elems(s.n), kThreads, 0, s.stream, s.n, s.z, s.p, s.state);
   }
   s.launches_per_iteration += 2;
   return cuda_check(cudaGetLastError(), "reset direction");
@@ -1567,9 +1636,9 @@ sf_status solver_enqueue_iteration(DeviceSolver& s) {
   if (s.system.sell) {
     SellOp<double> A = sell_of<double>(s.system);
     int grid = std::min(grid_for_slices(s.system.nslices), kReduceBlocks * 2);
-    launch_pdl(sell_pcg_spmv_dot_kernel, grid, kThreads, 0, st, A, s.p, s.ap, s.partials, s.state);
-    launch_pdl(pcg_update_kernel, kReduceBlocks, kReduceThreads, 0, st, s.n, s.p, s.ap, s.x, s.r, s.partials, s.state);
-    launch_pdl(sell_pcg_check_kernel, grid, kThreads, 0, st, A, s.x, s.rhs, s.r, s.partials, s.state);
+    launch_body<sell_pcg_spmv_dot_kernel>(grid, kThreads, 0, st, A, s.p, s.ap, s.partials, s.state);
+    launch_body<pcg_update_kernel>(kReduceBlocks, kReduceThreads, 0, st, s.n, s.p, s.ap, s.x, s.r, s.partials, s.state);
+    launch_body<sell_pcg_check_kernel>(grid, kThreads, 0, st, A, s.x, s.rhs, s.r, s.partials, s.state);
   } else switch (s.system.lanes_per_row) {
     case 8: launch_pcg_spmv_lpr<8>(s); break;
     case 16: launch_pcg_spmv_lpr<16>(s); break;
@@ -1578,11 +1647,11 @@ sf_status solver_enqueue_iteration(DeviceSolver& s) {
   s.launches_per_iteration += 3;
   enqueue_precondition(s, s.r, s.z, s.z32, status);
   if (s.vector_single && s.multigrid) {
-    launch_pdl(pcg_dot_rz_kernel<float>, kReduceBlocks, kReduceThreads, 0, st, s.n, s.r, s.z32, s.ap, s.partials, s.state);
-    launch_pdl(pcg_update_p_kernel<float>, grid_for_elems(s.n), kThreads, 0, st, s.n, s.z32, s.p, s.state);
+    launch_body<pcg_dot_rz_kernel<float>>(kReduceBlocks, kReduceThreads, 0, st, s.n, s.r, s.z32, s.ap, s.partials, s.state);
+    launch_body<pcg_update_p_kernel<float>>(grid_for_elems(s.n), kThreads, 0, st, s.n, s.z32, s.p, s.state);
   } else {
-    launch_pdl(pcg_dot_rz_kernel<double>, kReduceBlocks, kReduceThreads, 0, st, s.n, s.r, s.z, s.ap, s.partials, s.state);
-    launch_pdl(pcg_update_p_kernel<double>, grid_for_elems(s.n), kThreads, 0, st, s.n, s.z, s.p, s.state);
+    launch_body<pcg_dot_rz_kernel<double>>(kReduceBlocks, kReduceThreads, 0, st, s.n, s.r, s.z, s.ap, s.partials, s.state);
+    launch_body<pcg_update_p_kernel<double>>(grid_for_elems(s.n), kThreads, 0, st, s.n, s.z, s.p, s.state);
   }
   s.launches_per_iteration += 2;
   return cuda_check(cudaGetLastError(), "iteration");
@@ -1603,6 +1672,137 @@ sf_status solver_capture_graph(DeviceSolver& s) {
   s.graph_kernels = nodes;
   e = cudaGraphInstantiate(&s.graph_exec, g, 0);
   return cuda_check(e, "graph instantiate");
+}
+
+// ------------------------------------------------------------ batched iterations
+// Records one conjugate gradient iteration of every instance, checks that they launch the same
+// kernels in the same order with the same block shapes, and captures one graph whose every node
+// is a single grid over all instances: grid.x is the largest instance's, grid.y the instance
+// count, and each launch site's argument packs sit in one device table (the per-instance offset
+// table: each pack holds that instance's operator, vectors, scalars and status word).
+sf_status batch_build(const std::vector<DeviceSolver*>& inst, cudaStream_t stream, BatchIteration& out) {
+  out = BatchIteration();
+  out.stream = stream;
+  out.count = inst.size();
+  if (inst.empty()) return fail(SF_INVALID_ARGUMENT, "an empty batch");
+  std::vector<std::vector<LaunchRecord>> rec(inst.size());
+  for (size_t i = 0; i < inst.size(); ++i) {
+    g_recorder = &rec[i];
+    sf_status e = solver_enqueue_iteration(*inst[i]);
+    g_recorder = nullptr;
+    if (e) return e;
+  }
+  const size_t sites = rec[0].size();
+  for (size_t i = 1; i < inst.size(); ++i) {
+    const char* why = nullptr;
+    size_t at = 0;
+    if (rec[i].size() != sites) why = "a different number of kernels per iteration";
+    for (size_t j = 0; !why && j < sites; ++j) {
+      at = j;
+      if (rec[i][j].batched != rec[0][j].batched) why = "a different kernel";
+      else if (rec[i][j].pack.size() != rec[0][j].pack.size()) why = "different arguments";
+    }
+    if (why) {
+      char msg[200];
+      std::snprintf(msg, sizeof msg, "the studies of a batch must share their launch structure: study %zu has %s (launch %zu)",
+                    i, why, at);
+      return fail(SF_INVALID_ARGUMENT, msg);
+    }
+  }
+  struct Site {
+    const void* kernel;
+    dim3 grid, block;
+    size_t smem;
+    void* table;
+  };
+  std::vector<Site> list(sites);
+  for (size_t j = 0; j < sites; ++j) {
+    Site& t = list[j];
+    t.kernel = rec[0][j].batched;
+    t.block = rec[0][j].block;
+    t.grid = dim3(1, (unsigned)inst.size(), 1);
+    t.smem = 0;
+    const size_t bytes = rec[0][j].pack.size();
+    std::vector<unsigned char> host(bytes * inst.size());
+    // Block sizes may differ (a row-group kernel's warps per block follow its largest group); the
+    // bodies work with any block size and place each warp's staging slot by their own operator,
+    // so the batch takes the largest block and the largest per-warp slot.
+    size_t per_warp = 0;
+    for (size_t i = 0; i < inst.size(); ++i) {
+      t.grid.x = std::max(t.grid.x, rec[i][j].grid.x);
+      t.block.x = std::max(t.block.x, rec[i][j].block.x);
+      per_warp = std::max(per_warp, rec[i][j].smem / std::max(1u, rec[i][j].block.x / 32));
+      std::memcpy(host.data() + i * bytes, rec[i][j].pack.data(), bytes);
+    }
+    t.smem = per_warp * (t.block.x / 32);
+    if (t.smem > 200 * 1024) {
+      batch_destroy(out);
+      return fail(SF_INVALID_ARGUMENT, "the studies of a batch need more shared memory per block than one SM holds");
+    }
+    cudaError_t e = cudaMalloc(&t.table, std::max<size_t>(host.size(), 16));
+    if (e != cudaSuccess) {
+      batch_destroy(out);
+      return cuda_check(e, "batch table");
+    }
+    out.tables.push_back(t.table);
+    e = cudaMemcpy(t.table, host.data(), host.size(), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && t.smem > 48 * 1024)
+      e = cudaFuncSetAttribute(t.kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    if (e != cudaSuccess) {
+      batch_destroy(out);
+      return cuda_check(e, "batch table");
+    }
+  }
+  out.sites = sites;
+  cudaError_t e = cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal);
+  if (e != cudaSuccess) {
+    batch_destroy(out);
+    return cuda_check(e, "begin batch capture");
+  }
+  cudaError_t launch = cudaSuccess;
+  for (Site& t : list) {
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = t.grid;
+    cfg.blockDim = t.block;
+    cfg.dynamicSmemBytes = t.smem;
+    cfg.stream = stream;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    void* argv[1] = {&t.table};
+    cudaError_t le = cudaLaunchKernelExC(&cfg, t.kernel, argv);
+    if (le != cudaSuccess && launch == cudaSuccess) launch = le;
+  }
+  e = cudaStreamEndCapture(stream, &out.graph);
+  if (launch != cudaSuccess || e != cudaSuccess) {
+    batch_destroy(out);
+    return cuda_check(launch != cudaSuccess ? launch : e, "batch capture");
+  }
+  e = cudaGraphInstantiate(&out.exec, out.graph, 0);
+  if (e != cudaSuccess) {
+    batch_destroy(out);
+    return cuda_check(e, "batch instantiate");
+  }
+  return SF_OK;
+}
+
+sf_status batch_replay(BatchIteration& b, uint64_t iterations) {
+  for (uint64_t i = 0; i < iterations; ++i) {
+    cudaError_t e = cudaGraphLaunch(b.exec, b.stream);
+    if (e != cudaSuccess) return cuda_check(e, "batch replay");
+  }
+  return SF_OK;
+}
+
+void batch_destroy(BatchIteration& b) {
+  if (b.exec) cudaGraphExecDestroy(b.exec);
+  if (b.graph) cudaGraphDestroy(b.graph);
+  for (void* t : b.tables) cudaFree(t);
+  b.exec = nullptr;
+  b.graph = nullptr;
+  b.tables.clear();
 }
 
 sf_status solver_restart(DeviceSolver& s, double tolerance, uint64_t max_iterations) {
@@ -1686,7 +1886,7 @@ sf_status solver_time_kernel(DeviceSolver& s, int kernel, uint64_t repeats, doub
 sf_status solver_precondition(DeviceSolver& s, const double* d_in, double* d_out) {
   enqueue_precondition(s, d_in, d_out, s.z32, s.always_active);
   if (s.vector_single && s.multigrid)
-    launch_pdl(convert_kernel<float, double>, grid_for_elems(s.n), kThreads, 0, s.stream, s.n, s.z32, d_out, s.always_active);
+    launch_body<convert_kernel<float, double>>(grid_for_elems(s.n), kThreads, 0, s.stream, s.n, s.z32, d_out, s.always_active);
   return cuda_check(cudaStreamSynchronize(s.stream), "precondition");
 }
 

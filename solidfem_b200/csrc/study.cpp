@@ -16,6 +16,7 @@
 
 #include "device.h"
 #include "sf_internal.h"
+#include "batch.h"
 
 using namespace sf;
 
@@ -568,6 +569,7 @@ void sf_study_options_default(sf_study_options* o) {
   o->use_graphs = 1;
   o->device_memory_budget = 0;
   o->sell_min_rows = 0;
+  o->batchable = 0;
 }
 
 // ------------------------------------------------------------------------------ builder
@@ -669,6 +671,8 @@ sf_status sf_builder_create(sf_model* model, const sf_study_options* options, sf
   DeviceSolver& s = b->solver;
   s.device = b->options.device;
   s.sell_min_rows = b->options.sell_min_rows ? b->options.sell_min_rows : 32768;
+  s.uniform_lanes = b->options.batchable != 0;
+  if (s.uniform_lanes) s.sell_min_rows = UINT64_MAX;
   if (sf_status e = cuda_check(cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking), "stream")) return e;
   AssemblyDevice& a = b->asmdev;
   a.tet_count = (uint32_t)mesh.tets.size();
@@ -1055,6 +1059,153 @@ sf_status sf_study_step(sf_study* s, uint64_t max_iterations, sf_cancel_fn cance
   if (s->cancelled) kind = SF_OUTCOME_CANCELLED;
   else if (s->status == ST_CONVERGED) kind = SF_OUTCOME_CONVERGED;
   return finish(kind);
+}
+
+}  // extern "C"
+
+namespace sf {
+
+BatchRunner::~BatchRunner() {
+  batch_destroy(it);
+  if (pinned) cudaFreeHost(pinned);
+  if (stream) cudaStreamDestroy(stream);
+}
+
+sf_status BatchRunner::init(int dev) {
+  device = dev;
+  cudaSetDevice(dev);
+  return cuda_check(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "batch stream");
+}
+
+sf_status BatchRunner::rebuild() {
+  batch_destroy(it);
+  dirty = false;
+  if (members.empty()) return SF_OK;
+  std::vector<DeviceSolver*> inst;
+  for (sf_study* m : members) inst.push_back(&m->solver);
+  if (pinned_cap < members.size()) {
+    if (pinned) cudaFreeHost(pinned);
+    pinned = nullptr;
+    pinned_cap = 0;
+    if (sf_status e = cuda_check(cudaMallocHost((void**)&pinned, members.size() * sizeof(PcgState)), "batch state"))
+      return e;
+    pinned_cap = members.size();
+  }
+  return batch_build(inst, stream, it);
+}
+
+sf_status BatchRunner::run_chunk(uint64_t iterations, std::vector<sf_study*>& finished) {
+  cudaSetDevice(device);
+  if (dirty)
+    if (sf_status e = rebuild()) return e;
+  if (members.empty()) return SF_OK;
+  double t0 = now_seconds();
+  if (sf_status e = batch_replay(it, iterations)) return e;
+  for (size_t i = 0; i < members.size(); ++i) {
+    cudaMemcpyAsync(pinned + i, members[i]->solver.state, sizeof(PcgState), cudaMemcpyDeviceToHost, stream);
+    members[i]->solver.d2h_bytes += sizeof(PcgState);
+    members[i]->solver.launches += it.sites * iterations;
+  }
+  if (sf_status e = cuda_check(cudaStreamSynchronize(stream), "batch chunk")) return e;
+  double dt = now_seconds() - t0;
+  std::vector<sf_study*> keep;
+  for (size_t i = 0; i < members.size(); ++i) {
+    sf_study* m = members[i];
+    m->last = pinned[i];
+    m->status = m->last.status;
+    m->report.solve_seconds += dt;
+    m->report.iterations = m->last.iterations;
+    m->report.relative_residual = m->last.rel;
+    m->report.at_rounding_floor = m->last.at_floor;
+    if (m->status == ST_ACTIVE)
+      keep.push_back(m);
+    else
+      finished.push_back(m);
+  }
+  if (keep.size() != members.size()) {
+    members.swap(keep);
+    dirty = true;
+  }
+  return SF_OK;
+}
+
+uint64_t study_signature(sf_study* s) {
+  std::vector<LaunchRecord> rec;
+  g_recorder = &rec;
+  sf_status e = solver_enqueue_iteration(s->solver);
+  g_recorder = nullptr;
+  if (e) return 0;
+  uint64_t h = 1469598103934665603ull;
+  auto mix = [&](uint64_t v) {
+    for (int i = 0; i < 8; ++i) {
+      h ^= (v >> (8 * i)) & 0xff;
+      h *= 1099511628211ull;
+    }
+  };
+  for (auto& r : rec) {
+    mix((uint64_t)(uintptr_t)r.batched);
+    mix(r.pack.size());
+  }
+  mix(s->solver.device);
+  return h;
+}
+
+uint64_t study_device_bytes(const sf_study* s) { return s->solver.bytes; }
+
+uint64_t model_free_dofs(const sf_model* m) {
+  std::vector<uint32_t> fixed = m->model.fixed;
+  std::sort(fixed.begin(), fixed.end());
+  fixed.erase(std::unique(fixed.begin(), fixed.end()), fixed.end());
+  size_t nodes = m->model.mesh.nodes.size();
+  size_t held = 0;
+  for (uint32_t n : fixed) held += n < nodes ? 1 : 0;
+  return 3 * (nodes - held);
+}
+
+uint64_t model_node_count(const sf_model* m) { return m->model.mesh.nodes.size(); }
+
+// The outcome and status of a study that left a batch.
+static sf_status batch_outcome(sf_study* m, sf_step_outcome* out) {
+  if (out) {
+    out->kind = m->status == ST_CONVERGED ? SF_OUTCOME_CONVERGED : SF_OUTCOME_RUNNING;
+    fill_progress(m->last, &out->progress);
+  }
+  if (m->status == ST_FAILED_NOT_PD) return SF_PCG_NOT_POSITIVE_DEFINITE;
+  if (m->status == ST_FAILED_NOT_CONVERGED) return SF_PCG_NOT_CONVERGED;
+  return SF_OK;
+}
+
+}  // namespace sf
+
+extern "C" {
+
+sf_status sf_study_solve_batch(sf_study** studies, uint64_t count, sf_step_outcome* outcomes, sf_status* statuses) {
+  if (!studies || count == 0) return fail(SF_INVALID_ARGUMENT, "an empty batch");
+  for (uint64_t i = 0; i < count; ++i) {
+    if (!studies[i]) return fail(SF_INVALID_ARGUMENT, "null study");
+    if (studies[i]->solver.device != studies[0]->solver.device)
+      return fail(SF_INVALID_ARGUMENT, "the studies of a batch must share their device");
+    for (uint64_t j = 0; j < i; ++j)
+      if (studies[j] == studies[i]) return fail(SF_INVALID_ARGUMENT, "a study appears twice in a batch");
+  }
+  BatchRunner run;
+  if (sf_status e = run.init(studies[0]->solver.device)) return e;
+  for (uint64_t i = 0; i < count; ++i) {
+    if (sf_status e = sf_study_resolve(studies[i], nullptr)) return e;
+    if (sf_status e = cuda_check(cudaStreamSynchronize(studies[i]->solver.stream), "batch start")) return e;
+    run.members.push_back(studies[i]);
+  }
+  std::vector<sf_study*> finished;
+  uint64_t chunk = 4;
+  while (!run.members.empty()) {
+    if (sf_status e = run.run_chunk(chunk, finished)) return e;
+    chunk = std::min<uint64_t>(16, chunk * 2);
+  }
+  for (uint64_t i = 0; i < count; ++i) {
+    sf_status st = batch_outcome(studies[i], outcomes ? outcomes + i : nullptr);
+    if (statuses) statuses[i] = st;
+  }
+  return SF_OK;
 }
 
 sf_status sf_study_displacements(const sf_study* s, double* out) {

@@ -29,6 +29,6 @@ def oracle_study(O, size, div, E, nu, options, clamp_axis=0, clamp_value=0.0, lo
     return O.Study(mesh, material or O.uniform(E, nu), options, fixed, faces, [list(traction)] * len(faces))
 
 
-def mg_options(precision, tolerance=1e-9, coarse_dofs=100, sell_min_rows=0, **kw):
-    return sf.StudyOptions(pcg=sf.PcgOptions(tolerance=tolerance), sell_min_rows=sell_min_rows,
+def mg_options(precision, tolerance=1e-9, coarse_dofs=100, sell_min_rows=0, batchable=False, **kw):
+    return sf.StudyOptions(pcg=sf.PcgOptions(tolerance=tolerance), sell_min_rows=sell_min_rows, batchable=batchable,
                            preconditioner=sf.MultigridOptions(coarse_dofs=coarse_dofs, precision=precision, **kw))
