@@ -339,6 +339,124 @@ def run_profile(args):
     return 0
 
 
+def percentile(values, q):
+    v = sorted(values)
+    if not v:
+        return None
+    k = (len(v) - 1) * q
+    lo, hi = int(k), min(int(k) + 1, len(v) - 1)
+    return v[lo] + (v[hi] - v[lo]) * (k - lo)
+
+
+def run_serving(args):
+    """The serving stream (512 mixed bar / tube / plate requests, Poisson arrivals at 20/s, seed 0)
+    through the serving loop, then the same stream through serial plain FP64 GPU solves."""
+    import concurrent.futures
+
+    import torch
+
+    import solidfem_b200 as sf
+    from solidfem_b200 import workloads as W
+
+    torch.cuda.set_device(0)
+    reqs = W.serving_stream(count=args.requests)
+    t0 = time.perf_counter()
+    with concurrent.futures.ThreadPoolExecutor(max_workers=8) as pool:
+        built = list(pool.map(W.build_model, reqs))
+    prep = time.perf_counter() - t0
+
+    def opts(precision):
+        return sf.StudyOptions(pcg=sf.PcgOptions(tolerance=TOLERANCE),
+                               preconditioner=sf.MultigridOptions(precision=precision))
+
+    # warm-up: context, module load
+    w = sf.StaticStudy.new(W.build_model(reqs[0])[1], opts(sf.Precision.MIXED))
+    w.solve()
+    del w
+    gc.collect()
+
+    def serve(models, paced):
+        server = sf.Server(sf.ServerOptions(build_threads=args.build_threads))
+        start = time.perf_counter()
+        ids = []
+        for r, (mesh, model) in zip(reqs, models):
+            delay = r.arrival - (time.perf_counter() - start)
+            if paced and delay > 0:
+                time.sleep(delay)
+            ids.append((server.submit(model, opts(sf.Precision.MIXED)), mesh.node_count()))
+        results = [server.wait(rid) for rid, _ in ids]
+        makespan = time.perf_counter() - start
+        stats = server.stats()
+        for rid, n in ids:
+            try:
+                server.take(rid, n)
+            except sf.SolidfemError:
+                pass
+        server.close()
+        return results, makespan, stats
+
+    results, makespan, stats = serve(built, True)
+    failed = sum(1 for r in results if r.status != sf.Status.OK)
+    lat = [r.latency_seconds for r in results]
+    mine = {"solves_per_s": len(reqs) / makespan, "makespan_s": makespan,
+            "p50_latency_s": percentile(lat, 0.5), "p99_latency_s": percentile(lat, 0.99),
+            "failed": failed, "batched_requests": stats["batched_requests"],
+            "mean_batch_size": stats["mean_batch_size"], "batches": stats["batches"],
+            "peak_reserved_gb": stats["peak_reserved_bytes"] / 1e9,
+            "iterations_mean": statistics.mean(r.outcome.progress.iteration for r in results),
+            "build_seconds_sum": sum(r.build_seconds for r in results),
+            "solve_seconds_sum": sum(r.solve_seconds for r in results),
+            "queue_seconds_mean": statistics.mean(r.queue_seconds for r in results),
+            "failures": sorted({f"{r.status.name}: {r.message}" for r in results if r.status != sf.Status.OK})}
+    del built
+    gc.collect()
+    # the same requests all submitted at once: the loop's capacity rather than the arrival rate
+    with concurrent.futures.ThreadPoolExecutor(max_workers=8) as pool:
+        built = list(pool.map(W.build_model, reqs))
+    sres, smake, sstats = serve(built, False)
+    slat = [r.latency_seconds for r in sres]
+    mine["saturated"] = {"solves_per_s": len(reqs) / smake, "makespan_s": smake,
+                         "p50_latency_s": percentile(slat, 0.5), "p99_latency_s": percentile(slat, 0.99),
+                         "failed": sum(1 for r in sres if r.status != sf.Status.OK),
+                         "mean_batch_size": sstats["mean_batch_size"],
+                         "peak_reserved_gb": sstats["peak_reserved_bytes"] / 1e9}
+    del built
+    gc.collect()
+
+    if args.no_serial:
+        print(json.dumps({"metric": "served solves/s", "value": mine["solves_per_s"], "mine": mine}))
+        return 0
+    # serial plain FP64 GPU solves of the same stream, one at a time in arrival order
+    with concurrent.futures.ThreadPoolExecutor(max_workers=8) as pool:
+        built = list(pool.map(W.build_model, reqs))
+    start = time.perf_counter()
+    lat, serial_failed = [], 0
+    for r, (mesh, model) in zip(reqs, built):
+        now = time.perf_counter() - start
+        if now < r.arrival:
+            time.sleep(r.arrival - now)
+        st = sf.StaticStudy.new(model, opts(sf.Precision.DOUBLE))
+        out = st.solve()
+        st.displacements()
+        serial_failed += out.kind != sf.Outcome.CONVERGED
+        del st
+        lat.append(time.perf_counter() - start - r.arrival)
+    makespan = time.perf_counter() - start
+    serial = {"solves_per_s": len(reqs) / makespan, "makespan_s": makespan,
+              "p50_latency_s": percentile(lat, 0.5), "p99_latency_s": percentile(lat, 0.99), "failed": serial_failed}
+    line = {"metric": "served solves/s (mixed-size stream, continuous batching)", "value": mine["solves_per_s"],
+            "unit": "solves/s", "n_gpus": 1, "higher_is_better": True,
+            "config": {"workload": f"serving stream: {len(reqs)} bar/tube/plate requests, Poisson 20/s, seed 0, "
+                                   "10k-600k DOF log-uniform, rel. residual 1e-8, HBM budget 150 GB, "
+                                   "requests under 100k DOF batched",
+                       "build_threads": args.build_threads, "model_prep_seconds": prep},
+            "mine": mine, "serial_fp64": serial,
+            "speedup_throughput": mine["solves_per_s"] / serial["solves_per_s"],
+            "data": "synthetic (seeded request stream)"}
+    print(json.dumps(line))
+    return 0
+
+
 def main():
     p = argparse.ArgumentParser(description=__doc__.splitlines()[0])
     p.add_argument("--gpus", type=int, default=1)
@@ -348,11 +466,18 @@ def main():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--profile", choices=["mixed", "double"], default=None,
                    help="run one resident solve for a profiler and exit")
+    p.add_argument("--workload", choices=["plate", "serving"], default="plate",
+                   help="plate: the 603k-DOF gate plate (default); serving: the mixed request stream")
+    p.add_argument("--requests", type=int, default=512, help="serving: requests in the stream")
+    p.add_argument("--build-threads", type=int, default=8, help="serving: host build threads")
+    p.add_argument("--no-serial", action="store_true", help="serving: skip the serial FP64 comparison")
     args = p.parse_args()
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
     if args.profile:
         return run_profile(args)
+    if args.workload == "serving":
+        return run_serving(args) if rank == 0 else 0
     if args.impl == "reference":
         return run_reference(args, rank, world)
     return run_mine(args, rank, world)

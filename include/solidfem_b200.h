@@ -394,14 +394,16 @@ sf_status sf_study_time_kernel(sf_study* study, int32_t kernel, uint64_t repeats
  * solved. Studies with fewer than `batch_max_dofs` free DOFs are built batchable and solved in
  * continuous batches: between chunks of iterations a batch drops the studies that stopped and
  * takes in the ones that became ready, and each step is one grid per kernel over all its studies
- * (sf_study_solve_batch). Larger studies solve on their own streams, overlapping on the device. */
+ * (sf_study_solve_batch). Larger studies solve on their own streams from solver threads,
+ * overlapping on the device with the batches and with each other. */
 typedef struct sf_server sf_server;
 typedef struct sf_server_options {
   int32_t device;
   uint64_t memory_budget;  /* bytes of device memory for admitted requests; 0: 150 GiB */
   uint64_t batch_max_dofs; /* requests with fewer free DOFs are batched; 100000 by default */
   uint64_t max_batch;      /* studies per batch; 0: 64 */
-  uint64_t build_threads;  /* host threads building (and solving unbatched) requests; 0: 4 */
+  uint64_t build_threads;  /* host threads building requests; 0: 8 */
+  uint64_t solve_threads;  /* host threads driving the solves too large to batch; 0: 4 */
   uint64_t setup_threads;  /* host threads inside one build when its options leave it 0; 0: 2 */
 } sf_server_options;
 void sf_server_options_default(sf_server_options* options);
@@ -418,6 +420,7 @@ typedef struct sf_request_result {
   sf_step_outcome outcome;
   uint64_t free_dofs, node_count, device_bytes;
   double queue_seconds, build_seconds, solve_seconds, latency_seconds; /* latency from submission */
+  char message[160]; /* the failure's sf_error message, empty on success */
 } sf_request_result;
 /* Waits up to timeout_ms (UINT64_MAX: until done) for a request; SF_NOT_FINISHED while it runs. */
 sf_status sf_server_wait(sf_server* server, uint64_t id, uint64_t timeout_ms, sf_request_result* out);

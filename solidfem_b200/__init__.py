@@ -109,14 +109,15 @@ class Kernel(enum.IntEnum):
 
 class _ServerOptions(C.Structure):
     _fields_ = [("device", C.c_int32), ("memory_budget", C.c_uint64), ("batch_max_dofs", C.c_uint64),
-                ("max_batch", C.c_uint64), ("build_threads", C.c_uint64), ("setup_threads", C.c_uint64)]
+                ("max_batch", C.c_uint64), ("build_threads", C.c_uint64), ("solve_threads", C.c_uint64),
+                ("setup_threads", C.c_uint64)]
 
 
 class _RequestResult(C.Structure):
     _fields_ = [("status", C.c_int32), ("finished", C.c_int32), ("batched", C.c_int32), ("batch_size", C.c_uint64),
                 ("outcome", _StepOutcome), ("free_dofs", C.c_uint64), ("node_count", C.c_uint64),
                 ("device_bytes", C.c_uint64), ("queue_seconds", C.c_double), ("build_seconds", C.c_double),
-                ("solve_seconds", C.c_double), ("latency_seconds", C.c_double)]
+                ("solve_seconds", C.c_double), ("latency_seconds", C.c_double), ("message", C.c_char * 160)]
 
 
 class _ServerStats(C.Structure):
@@ -740,12 +741,13 @@ class StaticStudy:
 @dataclass
 class ServerOptions:
     """sf_server_options: device, memory budget (bytes, 0: 150 GiB), the batching threshold in free DOFs,
-    studies per batch, build threads and setup threads per build."""
+    studies per batch, build threads, solver threads and setup threads per build."""
     device: int = 0
     memory_budget: int = 0
     batch_max_dofs: int = 100000
     max_batch: int = 64
-    build_threads: int = 4
+    build_threads: int = 8
+    solve_threads: int = 4
     setup_threads: int = 2
 
     def _c(self) -> _ServerOptions:
@@ -755,6 +757,7 @@ class ServerOptions:
         o.batch_max_dofs = self.batch_max_dofs
         o.max_batch = self.max_batch
         o.build_threads = self.build_threads
+        o.solve_threads = self.solve_threads
         o.setup_threads = self.setup_threads
         return o
 
@@ -773,6 +776,7 @@ class RequestResult:
     build_seconds: float
     solve_seconds: float
     latency_seconds: float
+    message: str = ""
 
 
 class Server:
@@ -802,7 +806,7 @@ class Server:
                              StepOutcome(Outcome(r.outcome.kind), Progress(p.iteration, p.relative_residual,
                                                                            bool(p.at_rounding_floor))),
                              r.free_dofs, r.node_count, r.device_bytes, r.queue_seconds, r.build_seconds,
-                             r.solve_seconds, r.latency_seconds)
+                             r.solve_seconds, r.latency_seconds, r.message.decode(errors="replace"))
 
     def take(self, rid: int, node_count: int) -> np.ndarray:
         out = np.empty((node_count, 3), dtype=np.float64)

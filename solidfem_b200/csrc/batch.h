@@ -17,8 +17,7 @@ struct BatchRunner {
   cudaStream_t stream = nullptr;
   std::vector<sf_study*> members;
   BatchIteration it;
-  PcgState* pinned = nullptr;
-  size_t pinned_cap = 0;
+  std::vector<void*> slots;  // pinned slots for the members' states
   bool dirty = true;
 
   ~BatchRunner();

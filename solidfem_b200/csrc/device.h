@@ -148,6 +148,14 @@ inline void copy_d2h(const DeviceSolver& s, void* dst, const void* src, size_t b
   cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, s.stream);
   s.d2h_bytes += bytes;
 }
+// Pinned host memory that is never freed (freeing pinned memory synchronizes the device): a
+// grow-only scratch buffer per host thread, and 512-byte slots for per-study state.
+static const size_t kPinnedSlotBytes = 512;
+double* pinned_scratch(size_t bytes);
+void* pinned_slot();
+void pinned_release(void* slot);
+static_assert(2 * sizeof(PcgState) <= kPinnedSlotBytes, "a slot holds two solver states");
+
 sf_status dev_alloc(DeviceSolver& s, void** ptr, size_t bytes);
 // Frees one allocation of dev_alloc before the solver ends (setup temporaries).
 void dev_free(DeviceSolver& s, void* ptr);

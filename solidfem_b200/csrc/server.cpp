@@ -7,9 +7,10 @@
 // depth share one). Between chunks of iterations a batch drops the studies that have stopped and
 // takes in the ones that became ready meanwhile, so requests that arrive while others are on the
 // GPU join as slots and memory free up; each step of a batch is one grid per kernel over all its
-// studies. Larger studies are solved by their build worker on the worker's stream, overlapping on
-// the device with the batches and with each other.
+// studies. Larger studies go to solver threads and solve on their own streams, overlapping on the
+// device with the batches and with each other while the build workers go on building.
 #include <algorithm>
+#include <cstdio>
 #include <condition_variable>
 #include <deque>
 #include <map>
@@ -42,6 +43,7 @@ struct Request {
   std::vector<double> displacements;
   uint64_t device_bytes = 0;
   uint64_t batch_peak = 0;  // the largest batch it ran in
+  char message[160] = {0};  // the failure's message
 };
 
 }  // namespace
@@ -58,8 +60,10 @@ struct sf_server {
   std::deque<sf::Request*> pending;      // submitted, not admitted
   std::deque<sf::Request*> admitted;     // waiting for a build worker
   std::vector<sf::Request*> ready;       // built, batchable, waiting for a batch
+  std::deque<sf::Request*> solving;      // built, too large to batch, waiting for a solver thread
+  uint64_t building = 0;                 // requests inside a build worker
   std::unordered_map<uint64_t, std::unique_ptr<sf::Request>> all;
-  std::vector<std::thread> workers;
+  std::vector<std::thread> workers, solvers;
   std::thread batcher;
   uint64_t completed = 0, batches_run = 0, batched_requests = 0, batch_member_sum = 0, batch_chunks = 0;
   std::unordered_map<sf_study*, sf::Request*> owners;  // batch thread only
@@ -83,6 +87,11 @@ struct sf_server {
   // Records a finished request: its displacements to the host, the study released. Caller does
   // not hold m.
   void complete(sf::Request* r, sf_status st) {
+    if (st) {
+      sf_error err;
+      sf_last_error(&err);
+      std::snprintf(r->message, sizeof r->message, "%s", err.message);
+    }
     if (r->study) {
       if (!st) {
         r->displacements.assign(r->node_count * 3, 0.0);
@@ -112,6 +121,7 @@ struct sf_server {
         if (admitted.empty()) return;
         r = admitted.front();
         admitted.pop_front();
+        ++building;
       }
       sf_study* st = nullptr;
       sf_model* model = r->model;
@@ -119,6 +129,10 @@ struct sf_server {
       sf_status e = sf_study_create(model, &r->options, nullptr, nullptr, &st);
       r->t_built = sf::now_seconds();
       if (e) {
+        {
+          std::lock_guard<std::mutex> lock(m);
+          --building;
+        }
         complete(r, e);
         continue;
       }
@@ -127,20 +141,35 @@ struct sf_server {
       {
         // The budget now holds the study's real footprint.
         std::lock_guard<std::mutex> lock(m);
+        --building;
         reserved = reserved - r->reserved + r->device_bytes;
         peak_reserved = std::max(peak_reserved, reserved);
         r->reserved = r->device_bytes;
         admit_locked();
         r->state = 2;
-        if (r->batchable) {
+        if (r->batchable)
           ready.push_back(r);
-          cv.notify_all();
-          continue;
-        }
+        else
+          solving.push_back(r);
       }
       cv.notify_all();
+    }
+  }
+
+  // Solves built studies too large to batch, each on its own stream, so the build workers keep
+  // building meanwhile; several solver threads overlap their studies on the device.
+  void solver_loop() {
+    for (;;) {
+      sf::Request* r = nullptr;
+      {
+        std::unique_lock<std::mutex> lock(m);
+        cv.wait(lock, [&] { return (stopping && admitted.empty() && building == 0) || !solving.empty(); });
+        if (solving.empty()) return;
+        r = solving.front();
+        solving.pop_front();
+      }
       sf_step_outcome out{};
-      e = sf_study_step(st, UINT64_MAX, nullptr, nullptr, &out);
+      sf_status e = sf_study_step(r->study, UINT64_MAX, nullptr, nullptr, &out);
       r->outcome = out;
       complete(r, e);
     }
@@ -156,7 +185,7 @@ struct sf_server {
         bool busy = false;
         for (auto& kv : runners) busy = busy || !kv.second->members.empty();
         cv.wait(lock, [&] { return stopping || !ready.empty() || busy; });
-        if (stopping && ready.empty() && !busy) return;
+        if (stopping && ready.empty() && !busy && admitted.empty() && building == 0) return;
         joining.swap(ready);
       }
       for (sf::Request* r : joining) {
@@ -234,7 +263,8 @@ void sf_server_options_default(sf_server_options* o) {
   o->memory_budget = 150ull << 30;
   o->batch_max_dofs = 100000;
   o->max_batch = 64;
-  o->build_threads = 4;
+  o->build_threads = 8;
+  o->solve_threads = 4;
   o->setup_threads = 2;
 }
 
@@ -245,7 +275,8 @@ sf_status sf_server_create(const sf_server_options* options, sf_server** out) {
   if (options) s->opt = *options;
   if (s->opt.memory_budget == 0) s->opt.memory_budget = 150ull << 30;
   if (s->opt.max_batch == 0) s->opt.max_batch = 64;
-  if (s->opt.build_threads == 0) s->opt.build_threads = 4;
+  if (s->opt.build_threads == 0) s->opt.build_threads = 8;
+  if (s->opt.solve_threads == 0) s->opt.solve_threads = 4;
   if (s->opt.setup_threads == 0) s->opt.setup_threads = 2;
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return sf::fail(SF_NO_DEVICE, "no CUDA device is visible");
@@ -255,6 +286,11 @@ sf_status sf_server_create(const sf_server_options* options, sf_server** out) {
     s->workers.emplace_back([raw] {
       cudaSetDevice(raw->opt.device);
       raw->worker_loop();
+    });
+  for (uint64_t i = 0; i < s->opt.solve_threads; ++i)
+    s->solvers.emplace_back([raw] {
+      cudaSetDevice(raw->opt.device);
+      raw->solver_loop();
     });
   s->batcher = std::thread([raw] {
     cudaSetDevice(raw->opt.device);
@@ -319,6 +355,7 @@ sf_status sf_server_wait(sf_server* s, uint64_t id, uint64_t timeout_ms, sf_requ
     out->build_seconds = r->t_built ? r->t_built - r->t_admit : 0.0;
     out->solve_seconds = r->state == 3 && r->t_built ? r->t_done - r->t_built : 0.0;
     out->latency_seconds = end - r->t_submit;
+    std::snprintf(out->message, sizeof out->message, "%s", r->message);
   }
   if (r->state != 3) return sf::fail(SF_NOT_FINISHED, "the request is still running");
   return SF_OK;
@@ -362,6 +399,11 @@ void sf_server_destroy(sf_server* s) {
     s->cv.notify_all();
   }
   for (auto& t : s->workers) t.join();
+  {
+    std::lock_guard<std::mutex> lock(s->m);
+    s->cv.notify_all();
+  }
+  for (auto& t : s->solvers) t.join();
   if (s->batcher.joinable()) s->batcher.join();
   for (auto& kv : s->all) {
     if (kv.second->model) sf_model_destroy(kv.second->model);

@@ -140,13 +140,8 @@ struct SetupMachine {
   Bsr prolongator, ap, coarse;
   sf_status failure = SF_OK;
   bool cancelled = false;
-  double* pinned = nullptr;  // host copy of a power iterate
-  size_t pinned_size = 0;
 
   explicit SetupMachine(DeviceSolver& d) : dev(d) {}
-  ~SetupMachine() {
-    if (pinned) cudaFreeHost(pinned);
-  }
 
   size_t level_index() const { return levels.size(); }
 
@@ -376,18 +371,16 @@ struct SetupMachine {
   }
 
   // Power iteration for lambda_max(D^-1 A) (setup.rs:390-449): the products on the device, the
-  // order-exact norms on the host from a pinned copy of each iterate.
+  // order-exact norms on the host from a pinned copy of each iterate (this thread's scratch).
   sf_status run_spectral() {
     size_t rb = current.rb, rows = current.rows, dofs = rows * rb;
     double *v = nullptr, *s2 = nullptr;
     sf_status e = dev_alloc(dev, (void**)&v, std::max<size_t>(1, dofs) * 8);
     if (!e) e = dev_alloc(dev, (void**)&s2, std::max<size_t>(1, dofs) * 8);
-    if (!e && pinned_size < dofs) {
-      if (pinned) cudaFreeHost(pinned);
-      pinned = nullptr;
-      pinned_size = 0;
-      e = cuda_check(cudaMallocHost((void**)&pinned, std::max<size_t>(1, dofs) * 8), "cudaMallocHost");
-      if (!e) pinned_size = dofs;
+    double* pinned = nullptr;
+    if (!e) {
+      pinned = pinned_scratch(std::max<size_t>(1, dofs) * 8);
+      if (!pinned) e = fail(SF_CUDA_ERROR, "cudaMallocHost failed");
     }
     double lm = 0.0;
     if (!e && dofs) {

@@ -1308,11 +1308,69 @@ sf_status cuda_check(cudaError_t e, const char* what) {
   return fail(SF_CUDA_ERROR, msg);
 }
 
+// Pinned host memory is never returned: freeing it synchronizes the whole device. Per host thread
+// a grow-only scratch buffer (earlier, smaller buffers stay allocated and valid), and a shared
+// pool of fixed 512-byte slots for per-study state read-backs.
+double* pinned_scratch(size_t bytes) {
+  thread_local double* buf = nullptr;
+  thread_local size_t cap = 0;
+  if (bytes > cap) {
+    size_t want = std::max(bytes, 2 * cap);
+    void* p = nullptr;
+    if (cudaMallocHost(&p, want) != cudaSuccess) return nullptr;
+    buf = (double*)p;
+    cap = want;
+  }
+  return buf;
+}
+
+namespace {
+std::mutex g_slot_mutex;
+std::vector<void*> g_free_slots;
+}  // namespace
+
+void* pinned_slot() {
+  std::lock_guard<std::mutex> lock(g_slot_mutex);
+  if (g_free_slots.empty()) {
+    const size_t n = 128;
+    void* p = nullptr;
+    if (cudaMallocHost(&p, n * kPinnedSlotBytes) != cudaSuccess) return nullptr;
+    for (size_t i = 0; i < n; ++i) g_free_slots.push_back((char*)p + i * kPinnedSlotBytes);
+  }
+  void* s = g_free_slots.back();
+  g_free_slots.pop_back();
+  return s;
+}
+
+void pinned_release(void* slot) {
+  if (!slot) return;
+  std::lock_guard<std::mutex> lock(g_slot_mutex);
+  g_free_slots.push_back(slot);
+}
+
+// Device memory comes from the device's stream-ordered pool: an allocation or a free is ordered on
+// the solver's stream and never waits for the rest of the device (cudaFree would synchronize the
+// whole device, stalling every other study in flight). The pool keeps freed memory for reuse
+// instead of returning it at each synchronization.
+void pool_setup(int device) {
+  static std::mutex mu;
+  static bool done[64] = {};
+  std::lock_guard<std::mutex> lock(mu);
+  if (device < 0 || device >= 64 || done[device]) return;
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+    uint64_t keep = UINT64_MAX;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  }
+  done[device] = true;
+}
+
 sf_status dev_alloc(DeviceSolver& s, void** ptr, size_t bytes) {
   // 64 bytes of slack: the staged loads read whole 16-byte chunks past an array's last value.
   size_t padded = bytes + 64;
-  cudaError_t e = cudaMalloc(ptr, padded);
-  if (e != cudaSuccess) return cuda_check(e, "cudaMalloc");
+  pool_setup(s.device);
+  cudaError_t e = cudaMallocAsync(ptr, padded, s.stream);
+  if (e != cudaSuccess) return cuda_check(e, "cudaMallocAsync");
   cudaMemsetAsync(*ptr, 0, padded, s.stream);
   s.owned.push_back({*ptr, padded});
   s.bytes += padded;
@@ -1323,7 +1381,7 @@ void dev_free(DeviceSolver& s, void* ptr) {
   if (!ptr) return;
   for (size_t i = 0; i < s.owned.size(); ++i)
     if (s.owned[i].first == ptr) {
-      cudaFree(ptr);
+      cudaFreeAsync(ptr, s.stream);
       s.bytes -= s.owned[i].second;
       s.owned[i] = s.owned.back();
       s.owned.pop_back();
@@ -1336,7 +1394,7 @@ void dev_free_all(DeviceSolver& s) {
   if (s.graph) cudaGraphDestroy(s.graph);
   s.graph_exec = nullptr;
   s.graph = nullptr;
-  for (auto& p : s.owned) cudaFree(p.first);
+  for (auto& p : s.owned) cudaFreeAsync(p.first, s.stream);
   s.owned.clear();
   s.bytes = 0;
 }
@@ -1734,18 +1792,24 @@ sf_status batch_build(const std::vector<DeviceSolver*>& inst, cudaStream_t strea
       per_warp = std::max(per_warp, rec[i][j].smem / std::max(1u, rec[i][j].block.x / 32));
       std::memcpy(host.data() + i * bytes, rec[i][j].pack.data(), bytes);
     }
+    if (per_warp > 0) {
+      // Fewer warps per block when the largest slot would not fit 200 KB of shared memory.
+      size_t warps = std::max<size_t>(1, std::min<size_t>(t.block.x / 32, (200 * 1024) / per_warp));
+      t.block.x = (unsigned)(32 * warps);
+    }
     t.smem = per_warp * (t.block.x / 32);
     if (t.smem > 200 * 1024) {
       batch_destroy(out);
-      return fail(SF_INVALID_ARGUMENT, "the studies of a batch need more shared memory per block than one SM holds");
+      return fail(SF_INVALID_ARGUMENT, "a study of the batch needs more shared memory per warp than one SM holds");
     }
-    cudaError_t e = cudaMalloc(&t.table, std::max<size_t>(host.size(), 16));
+    pool_setup(inst[0]->device);
+    cudaError_t e = cudaMallocAsync(&t.table, std::max<size_t>(host.size(), 16), stream);
     if (e != cudaSuccess) {
       batch_destroy(out);
       return cuda_check(e, "batch table");
     }
     out.tables.push_back(t.table);
-    e = cudaMemcpy(t.table, host.data(), host.size(), cudaMemcpyHostToDevice);
+    e = cudaMemcpyAsync(t.table, host.data(), host.size(), cudaMemcpyHostToDevice, stream);
     if (e == cudaSuccess && t.smem > 48 * 1024)
       e = cudaFuncSetAttribute(t.kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
     if (e != cudaSuccess) {
@@ -1799,7 +1863,7 @@ sf_status batch_replay(BatchIteration& b, uint64_t iterations) {
 void batch_destroy(BatchIteration& b) {
   if (b.exec) cudaGraphExecDestroy(b.exec);
   if (b.graph) cudaGraphDestroy(b.graph);
-  for (void* t : b.tables) cudaFree(t);
+  for (void* t : b.tables) cudaFreeAsync(t, b.stream);
   b.exec = nullptr;
   b.graph = nullptr;
   b.tables.clear();

@@ -361,7 +361,7 @@ struct sf_study {
   RecoveryDevice rec;
   bool recovered = false;  // rec holds the field of the converged displacements
   ~sf_study() {
-    if (pinned) cudaFreeHost(pinned);
+    pinned_release(pinned);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
     dev_free_all(solver);
@@ -788,6 +788,15 @@ static sf_status builder_assemble(sf_builder* b, uint64_t max_elements, sf_cance
                                                            : "the material at an integration point is not a stable solid");
   }
   b->next = end;
+  if (end == total) {
+    // The element stiffness buffer and the assembly map have served; free them for the solve.
+    AssemblyDevice& a = b->asmdev;
+    for (void* p : {(void*)a.ke, (void*)a.map, (void*)a.map_starts, (void*)a.cursor}) dev_free(s, p);
+    a.ke = nullptr;
+    a.map = a.map_starts = a.cursor = nullptr;
+    std::vector<uint32_t>().swap(b->pattern.map);
+    std::vector<uint32_t>().swap(b->pattern.map_starts);
+  }
   return SF_OK;
 }
 
@@ -947,7 +956,8 @@ sf_status sf_builder_finish(sf_builder* b, sf_study** out) {
   if (s->options.use_graphs) {
     if ((e = solver_capture_graph(d))) return e;
   }
-  cudaMallocHost((void**)&s->pinned, 2 * sizeof(PcgState));
+  s->pinned = (PcgState*)pinned_slot();
+  if (!s->pinned) return fail(SF_CUDA_ERROR, "cudaMallocHost failed");
   cudaEventCreate(&s->ev0);
   cudaEventCreate(&s->ev1);
   std::memset(&s->report, 0, sizeof(s->report));
@@ -1067,7 +1077,7 @@ namespace sf {
 
 BatchRunner::~BatchRunner() {
   batch_destroy(it);
-  if (pinned) cudaFreeHost(pinned);
+  for (void* p : slots) pinned_release(p);
   if (stream) cudaStreamDestroy(stream);
 }
 
@@ -1083,13 +1093,10 @@ sf_status BatchRunner::rebuild() {
   if (members.empty()) return SF_OK;
   std::vector<DeviceSolver*> inst;
   for (sf_study* m : members) inst.push_back(&m->solver);
-  if (pinned_cap < members.size()) {
-    if (pinned) cudaFreeHost(pinned);
-    pinned = nullptr;
-    pinned_cap = 0;
-    if (sf_status e = cuda_check(cudaMallocHost((void**)&pinned, members.size() * sizeof(PcgState)), "batch state"))
-      return e;
-    pinned_cap = members.size();
+  while (slots.size() < members.size()) {
+    void* p = pinned_slot();
+    if (!p) return fail(SF_CUDA_ERROR, "cudaMallocHost failed");
+    slots.push_back(p);
   }
   return batch_build(inst, stream, it);
 }
@@ -1102,7 +1109,7 @@ sf_status BatchRunner::run_chunk(uint64_t iterations, std::vector<sf_study*>& fi
   double t0 = now_seconds();
   if (sf_status e = batch_replay(it, iterations)) return e;
   for (size_t i = 0; i < members.size(); ++i) {
-    cudaMemcpyAsync(pinned + i, members[i]->solver.state, sizeof(PcgState), cudaMemcpyDeviceToHost, stream);
+    cudaMemcpyAsync(slots[i], members[i]->solver.state, sizeof(PcgState), cudaMemcpyDeviceToHost, stream);
     members[i]->solver.d2h_bytes += sizeof(PcgState);
     members[i]->solver.launches += it.sites * iterations;
   }
@@ -1111,7 +1118,7 @@ sf_status BatchRunner::run_chunk(uint64_t iterations, std::vector<sf_study*>& fi
   std::vector<sf_study*> keep;
   for (size_t i = 0; i < members.size(); ++i) {
     sf_study* m = members[i];
-    m->last = pinned[i];
+    m->last = *(const PcgState*)slots[i];
     m->status = m->last.status;
     m->report.solve_seconds += dt;
     m->report.iterations = m->last.iterations;
