@@ -1,0 +1,113 @@
+"""The benchmark configurations' correctness bar (needs a B200): displacements within 1e-8 relative
+L2 and nodal von Mises within 1e-6 of the oracle's own FP64 CPU solve (requested at 1e-12, or
+its rounding floor) on the same mesh, plus the closed-form cantilever check.
+
+Config 1: steel cantilever 100x10x10 mm, 20x4x4 hexes; config 2: thin plate 100x100x0.8 mm,
+60x60x2; a reduced printed block (60 mm cube, 15^3 hexes, shell within 2 mm of the surface).
+"""
+import numpy as np
+import pytest
+
+import solidfem_b200 as sf
+from tests.helpers import oracle_study, product_model
+
+pytestmark = pytest.mark.gpu
+
+L2_BAR = 1e-8
+VM_BAR = 1e-6
+
+
+def options(precision, tol):
+    return sf.StudyOptions(pcg=sf.PcgOptions(tolerance=tol), preconditioner=sf.MultigridOptions(precision=precision))
+
+
+def rel(a, b):
+    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
+def check_against_oracle(study, ref):
+    d, dr = study.displacements(), ref.displacements()
+    sol = study.solution()
+    _, vm_ref = ref.recover()
+    vm_err = float(np.max(np.abs(sol.nodal_von_mises - vm_ref)) / np.max(np.abs(vm_ref)))
+    return rel(d, dr), vm_err
+
+
+def test_config1_cantilever(oracle):
+    size, div, E, nu = (100.0, 10.0, 10.0), (20, 4, 4), 210000.0, 0.3
+    traction = (0.0, 0.0, -10.0)  # 1 kN over the 100 mm^2 end face
+    mesh, model = product_model(size, div, E, nu, traction=traction)
+    study = sf.StaticStudy.new(model, options(sf.Precision.DOUBLE, 1e-10))
+    assert study.solve().kind == sf.Outcome.CONVERGED
+    ref = oracle_study(oracle, size, div, E, nu, oracle.default_options(tolerance=1e-12, precision=oracle.DOUBLE),
+                       traction=traction)
+    ref.solve()
+    l2, vm = check_against_oracle(study, ref)
+    print(f"config 1: rel L2 {l2:.2e}, von Mises {vm:.2e}")
+    assert l2 <= L2_BAR and vm <= VM_BAR
+    # Timoshenko: F L^3 / (3 E I) + F L / (k G A) = 1.905 + 0.015 mm
+    nodes = mesh.nodes()
+    tip = np.abs(nodes[:, 0] - 100.0) < 1e-9
+    w = -float(study.displacements()[tip, 2].mean())
+    G, I, A = E / (2 * (1 + nu)), 10.0 ** 4 / 12.0, 100.0
+    beam = 1000.0 * 100.0 ** 3 / (3 * E * I) + 1000.0 * 100.0 / (5.0 / 6.0 * G * A)
+    print(f"config 1: tip deflection {w:.4f} mm, Timoshenko {beam:.4f} mm")
+    # 20 cells along the span sit 1.0% under beam theory; the reference's own check
+    # (cantilever.rs:40-80) holds 1% at 40 cells and shows convergence from below.
+    assert abs(w - beam) / beam < 0.015
+    _, fine_model = product_model(size, (40, 4, 4), E, nu, traction=traction)
+    fine = sf.StaticStudy.new(fine_model, options(sf.Precision.DOUBLE, 1e-10))
+    assert fine.solve().kind == sf.Outcome.CONVERGED
+    fine_nodes = fine_model.mesh.nodes()
+    w40 = -float(fine.displacements()[np.abs(fine_nodes[:, 0] - 100.0) < 1e-9, 2].mean())
+    print(f"config 1 at 40x4x4: tip deflection {w40:.4f} mm")
+    assert abs(w40 - beam) / beam < 0.01 and w < w40 <= beam * 1.001
+
+
+PLATE = ((100.0, 100.0, 0.8), (60, 60, 2), 2000.0, 0.35)
+PLATE_LOAD = dict(load_axis=2, load_value=0.8, traction=(0.0, 0.0, -0.01))
+
+
+@pytest.fixture(scope="module")
+def plate_oracle(oracle):
+    size, div, E, nu = PLATE
+    ref = oracle_study(oracle, size, div, E, nu, oracle.default_options(tolerance=1e-12, precision=oracle.DOUBLE),
+                       **PLATE_LOAD)
+    pr = ref.solve()
+    return ref, pr
+
+
+@pytest.mark.parametrize("precision", [sf.Precision.MIXED, sf.Precision.DOUBLE])
+def test_config2_thin_plate(plate_oracle, precision):
+    size, div, E, nu = PLATE
+    _, model = product_model(size, div, E, nu, **PLATE_LOAD)
+    study = sf.StaticStudy.new(model, options(precision, 1e-8))
+    out = study.solve()
+    assert out.kind == sf.Outcome.CONVERGED
+    ref, pr = plate_oracle
+    l2, vm = check_against_oracle(study, ref)
+    print(f"config 2 {precision.name}: {out.progress.iteration} iterations (floor {out.progress.at_rounding_floor}), "
+          f"oracle {pr.iteration} (floor {pr.at_rounding_floor}); rel L2 {l2:.2e}, von Mises {vm:.2e}")
+    assert l2 <= L2_BAR and vm <= VM_BAR
+
+
+def test_printed_block_reduced(oracle):
+    n = 15
+    size, div = (60.0, 60.0, 60.0), (n, n, n)
+    shell, core = (2400.0, 0.36), (800.0, 0.30)
+    lo, hi, depth = (0.0, 0.0, 0.0), size, 2.0
+    kw = dict(clamp_axis=2, clamp_value=0.0, load_axis=2, load_value=60.0, traction=(0.5, 0.0, 0.0))
+    material = sf.ShellCore(sf.Material(*shell), sf.Material(*core), lo, hi, depth)
+    _, model = product_model(size, div, 1.0, 0.0, material=material, **kw)
+    study = sf.StaticStudy.new(model, options(sf.Precision.MIXED, 1e-8))
+    assert study.solve().kind == sf.Outcome.CONVERGED
+    ref = oracle_study(oracle, size, div, 1.0, 0.0, oracle.default_options(tolerance=1e-12, precision=oracle.DOUBLE),
+                       material=oracle.shell_core(shell, core, lo, hi, depth), **kw)
+    # the two-material operator itself is bit-exact
+    rs, cols, vals = study.matrix()
+    ors, ocols, ovals = ref.matrix()
+    assert np.array_equal(cols, ocols) and np.array_equal(vals.view(np.uint64), ovals.view(np.uint64))
+    ref.solve()
+    l2, vm = check_against_oracle(study, ref)
+    print(f"printed block 15^3: rel L2 {l2:.2e}, von Mises {vm:.2e}")
+    assert l2 <= L2_BAR and vm <= VM_BAR
