@@ -2078,7 +2078,31 @@ struct orc_study {
   double seconds[4] = {0, 0, 0, 0};
   Recovered recovered;
   bool recovered_done = false;
+  vector<std::pair<size_t, double>> prescribed;           // (free dof, value), ascending dof
+  vector<std::array<double, 3>> prescribed_nodes;         // (node, axis, value) as doubles
 };
+
+// StudyBuilder::apply_prescribed (study.rs:564-593): each prescribed component in ascending
+// order moves what it forces on the unconstrained unknowns to the right-hand side, and its row
+// and column are emptied but for the diagonal; its right-hand side becomes diagonal x value.
+static void apply_prescribed(Csr& m, vector<double>& rhs, const vector<std::pair<size_t, double>>& prescribed) {
+  vector<char> constrained(rhs.size(), 0);
+  for (auto& p : prescribed) constrained[p.first] = 1;
+  for (auto& p : prescribed) {
+    size_t dof = p.first;
+    double value = p.second;
+    vector<std::pair<uint32_t, double>> entries;
+    for (size_t at = m.row_starts[dof]; at < m.row_starts[dof + 1]; ++at)
+      if (m.columns[at] != dof) entries.push_back({m.columns[at], m.values[at]});
+    for (auto& e : entries) {
+      size_t c = e.first;
+      if (!constrained[c]) rhs[c] -= e.second * value;
+      m.add(c, (uint32_t)dof, -e.second);
+      m.add(dof, e.first, -e.second);
+    }
+  }
+  for (auto& p : prescribed) rhs[p.first] = m.get(p.first, (uint32_t)p.first) * p.second;
+}
 
 extern "C" {
 
@@ -2152,10 +2176,28 @@ static double now_seconds() {
 }
 
 // StudyBuilder::new + step + finish (study.rs:419-656) in one call.
+int orc_study_new_prescribed(const orc_mesh* mesh, const orc_material* material, const orc_options* options,
+                             const uint32_t* fixed_nodes, uint64_t n_fixed, const orc_nodal_force* forces,
+                             uint64_t n_forces, const orc_face* faces, const double* tractions,
+                             uint64_t n_tractions, const orc_prescribed* prescribed, uint64_t n_prescribed,
+                             orc_study** out);
+
 int orc_study_new(const orc_mesh* mesh, const orc_material* material, const orc_options* options,
                   const uint32_t* fixed_nodes, uint64_t n_fixed, const orc_nodal_force* forces,
                   uint64_t n_forces, const orc_face* faces, const double* tractions,
                   uint64_t n_tractions, orc_study** out) {
+  return orc_study_new_prescribed(mesh, material, options, fixed_nodes, n_fixed, forces, n_forces, faces, tractions,
+                                  n_tractions, nullptr, 0, out);
+}
+
+// With prescribed components the reference checks the held DOFs' rank instead of the fixed
+// nodes (constraints.rs:162-256); the oracle leaves that refusal to the product's tests and
+// takes the model as held.
+int orc_study_new_prescribed(const orc_mesh* mesh, const orc_material* material, const orc_options* options,
+                             const uint32_t* fixed_nodes, uint64_t n_fixed, const orc_nodal_force* forces,
+                             uint64_t n_forces, const orc_face* faces, const double* tractions,
+                             uint64_t n_tractions, const orc_prescribed* prescribed, uint64_t n_prescribed,
+                             orc_study** out) {
   double t0 = now_seconds();
   const QuadMesh& q = mesh->q;
   size_t node_count = q.nodes.size();
@@ -2164,7 +2206,8 @@ int orc_study_new(const orc_mesh* mesh, const orc_material* material, const orc_
     if (fixed_nodes[i] >= node_count) return ORC_NODE_RANGE;
     is_fixed[fixed_nodes[i]] = 1;
   }
-  if (int c = check_constraints(q, is_fixed)) return c;
+  if (n_prescribed == 0)
+    if (int c = check_constraints(q, is_fixed)) return c;
   // build_load, study.rs:696-735
   vector<double> load(3 * node_count, 0.0);
   for (uint64_t i = 0; i < n_forces; ++i) {
@@ -2200,8 +2243,20 @@ int orc_study_new(const orc_mesh* mesh, const orc_material* material, const orc_
   for (size_t n = 0; n < node_count; ++n)
     if (s->free[n] != FIXED)
       for (int a = 0; a < 3; ++a) s->rhs.push_back(load[3 * n + a]);
+  // prescribed_dofs, study.rs:659-680
+  for (uint64_t i = 0; i < n_prescribed; ++i) {
+    const orc_prescribed& p = prescribed[i];
+    if (p.axis > 2 || !std::isfinite(p.value) || p.node >= node_count || s->free[p.node] == FIXED) {
+      delete s;
+      return ORC_BAD_PRESCRIBED;
+    }
+    s->prescribed.push_back({3 * (size_t)s->free[p.node] + p.axis, p.value});
+    s->prescribed_nodes.push_back({(double)p.node, (double)p.axis, p.value});
+  }
+  std::sort(s->prescribed.begin(), s->prescribed.end());
   bool all_zero = true;
   for (double v : s->rhs) all_zero = all_zero && v == 0.0;
+  for (auto& p : s->prescribed) all_zero = all_zero && p.second == 0.0;
   if (all_zero) {
     delete s;
     return ORC_NO_EFFECTIVE_LOAD;
@@ -2233,11 +2288,13 @@ int orc_study_new(const orc_mesh* mesh, const orc_material* material, const orc_
       }
     }
   }
+  if (!s->prescribed.empty()) apply_prescribed(s->matrix, s->rhs, s->prescribed);
   double t1 = now_seconds();
   s->seconds[0] = t1 - t0;
   s->use_mg = options->preconditioner == ORC_PRECONDITIONER_MULTIGRID;
   if (s->use_mg) {
     vector<double> modes = free_rigid_body_modes(q.nodes, s->free, s->free_count);
+    for (auto& p : s->prescribed) std::fill(modes.begin() + p.first * 6, modes.begin() + p.first * 6 + 6, 0.0);
     vector<P3> positions;
     for (size_t n = 0; n < node_count; ++n)
       if (s->free[n] != FIXED) positions.push_back(q.nodes[n]);
@@ -2303,6 +2360,8 @@ void orc_study_displacements(const orc_study* s, double* out) {
   for (size_t n = 0; n < s->free.size(); ++n)
     for (int a = 0; a < 3; ++a)
       out[3 * n + a] = s->free[n] == FIXED ? 0.0 : x[3 * (size_t)s->free[n] + a];
+  // A prescribed component is exact, not the solver's estimate of it (study.rs:233-236).
+  for (auto& p : s->prescribed_nodes) out[3 * (size_t)p[0] + (size_t)p[1]] = p[2];
 }
 
 // FNV-1a over the displacement bits, crates/solidfem/tests/validation/multigrid_precision.rs:216-226.

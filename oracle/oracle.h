@@ -27,6 +27,7 @@ enum {
   ORC_ELEMENT_INVERTED = 26,
   ORC_ELEMENT_MATERIAL = 27,
   ORC_JACOBI_DIAGONAL = 28,
+  ORC_BAD_PRESCRIBED = 31,
   ORC_MG_BLOCK_STRUCTURE = 40,
   ORC_MG_NEAR_NULL_LENGTH = 41,
   ORC_MG_NOT_POSITIVE_DEFINITE = 42,
@@ -100,6 +101,12 @@ typedef struct {
   double stress[6];
   double von_mises;
 } orc_point_stress;
+
+typedef struct {
+  uint32_t node;
+  uint32_t axis;
+  double value;
+} orc_prescribed;
 
 typedef struct orc_mesh orc_mesh;
 typedef struct orc_study orc_study;

@@ -39,6 +39,10 @@ class NodalForce(C.Structure):
     _fields_ = [("node", C.c_uint32), ("force", C.c_double * 3)]
 
 
+class Prescribed(C.Structure):
+    _fields_ = [("node", C.c_uint32), ("axis", C.c_uint32), ("value", C.c_double)]
+
+
 class Face(C.Structure):
     _fields_ = [("tet", C.c_uint32), ("face", C.c_uint32), ("nodes", C.c_uint32 * 6)]
 
@@ -95,6 +99,9 @@ def lib():
         L.orc_study_new.argtypes = [C.c_void_p, p(Material), p(Options), p(C.c_uint32), C.c_uint64,
                                     p(NodalForce), C.c_uint64, p(Face), p(C.c_double), C.c_uint64,
                                     p(C.c_void_p)]
+        L.orc_study_new_prescribed.argtypes = [C.c_void_p, p(Material), p(Options), p(C.c_uint32), C.c_uint64,
+                                               p(NodalForce), C.c_uint64, p(Face), p(C.c_double), C.c_uint64,
+                                               p(Prescribed), C.c_uint64, p(C.c_void_p)]
         L.orc_study_free.argtypes = [C.c_void_p]
         L.orc_study_step.argtypes = [C.c_void_p, C.c_uint64, p(Progress)]
         L.orc_study_displacements.argtypes = [C.c_void_p, p(C.c_double)]
@@ -211,7 +218,7 @@ class Study:
     """StaticStudy::new + step + solution of the oracle (study.rs)."""
 
     def __init__(self, mesh: Mesh, material: Material, options: Options, fixed,
-                 faces=(), tractions=(), forces=()):
+                 faces=(), tractions=(), forces=(), prescribed=()):
         self.mesh = mesh
         fixed = np.ascontiguousarray(fixed, dtype=np.uint32)
         nf = len(faces)
@@ -227,9 +234,10 @@ class Study:
             for k in range(3):
                 forr[i].force[k] = f[k]
         h = C.c_void_p()
-        code = lib().orc_study_new(mesh.h, C.byref(material), C.byref(options),
-                                   _ptr(fixed, C.c_uint32), len(fixed), forr, len(forces), farr,
-                                   _ptr(tr, C.c_double), nf, C.byref(h))
+        parr = (Prescribed * max(len(prescribed), 1))(*[Prescribed(int(n), int(a), float(v)) for n, a, v in prescribed])
+        code = lib().orc_study_new_prescribed(mesh.h, C.byref(material), C.byref(options),
+                                              _ptr(fixed, C.c_uint32), len(fixed), forr, len(forces), farr,
+                                              _ptr(tr, C.c_double), nf, parr, len(prescribed), C.byref(h))
         if code:
             raise ValueError(f"study refused: code {code}")
         self.h = h

@@ -173,6 +173,12 @@ sf_status setup_power_step(cudaStream_t st, uint32_t rows, int rb, const uint32_
                            const double* vals, const double* inv, const double* v, double* s2);
 sf_status setup_scale(cudaStream_t st, size_t n, const double* src, double d, double* v);
 sf_status setup_entry_rows(cudaStream_t st, uint32_t rows, const uint32_t* starts, uint32_t* out);
+// Listed blocks of len values out of / back into a block array; out[idx[i]] = vals[i].
+sf_status setup_gather_blocks(cudaStream_t st, size_t count, int len, const uint32_t* idx, const double* in,
+                              double* out);
+sf_status setup_scatter_blocks(cudaStream_t st, size_t count, int len, const uint32_t* idx, const double* in,
+                               double* out);
+sf_status setup_set_values(cudaStream_t st, size_t count, const uint32_t* idx, const double* vals, double* out);
 sf_status setup_smooth(cudaStream_t st, int rb, size_t entries, const uint32_t* entry_row, const uint32_t* p_cols,
                        const uint32_t* a_starts, const uint32_t* a_cols, const double* a_vals, const uint32_t* n_starts,
                        const uint32_t* n_cols, const uint32_t* aggregate, const double* t_vals, const double* inv,

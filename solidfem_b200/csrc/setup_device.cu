@@ -326,7 +326,44 @@ __global__ void sell_place_kernel(size_t blocks, const uint32_t* __restrict__ po
   }
 }
 
+// Copies listed blocks out of (gather) or back into (scatter) a block array.
+__global__ void gather_blocks_kernel(size_t count, int len, const uint32_t* __restrict__ idx,
+                                     const double* __restrict__ in, double* __restrict__ out) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < count * len; i += (size_t)gridDim.x * blockDim.x)
+    out[i] = in[(size_t)idx[i / len] * len + i % len];
+}
+__global__ void scatter_blocks_kernel(size_t count, int len, const uint32_t* __restrict__ idx,
+                                      const double* __restrict__ in, double* __restrict__ out) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < count * len; i += (size_t)gridDim.x * blockDim.x)
+    out[(size_t)idx[i / len] * len + i % len] = in[i];
+}
+__global__ void set_values_kernel(size_t count, const uint32_t* __restrict__ idx, const double* __restrict__ vals,
+                                  double* __restrict__ out) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < count; i += (size_t)gridDim.x * blockDim.x)
+    out[idx[i]] = vals[i];
+}
+
 }  // namespace
+
+sf_status setup_gather_blocks(cudaStream_t st, size_t count, int len, const uint32_t* idx, const double* in,
+                              double* out) {
+  if (count == 0) return SF_OK;
+  gather_blocks_kernel<<<grid_for(count * len), kT, 0, st>>>(count, len, idx, in, out);
+  return cuda_check(cudaGetLastError(), "gather blocks");
+}
+
+sf_status setup_scatter_blocks(cudaStream_t st, size_t count, int len, const uint32_t* idx, const double* in,
+                               double* out) {
+  if (count == 0) return SF_OK;
+  scatter_blocks_kernel<<<grid_for(count * len), kT, 0, st>>>(count, len, idx, in, out);
+  return cuda_check(cudaGetLastError(), "scatter blocks");
+}
+
+sf_status setup_set_values(cudaStream_t st, size_t count, const uint32_t* idx, const double* vals, double* out) {
+  if (count == 0) return SF_OK;
+  set_values_kernel<<<grid_for(count), kT, 0, st>>>(count, idx, vals, out);
+  return cuda_check(cudaGetLastError(), "set values");
+}
 
 sf_status setup_inverse_diagonal(cudaStream_t st, uint32_t rows, int rb, const uint32_t* starts, const uint32_t* cols,
                                  const double* vals, double* inv, unsigned long long* bad, double* pivots) {

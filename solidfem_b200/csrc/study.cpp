@@ -660,7 +660,6 @@ sf_status sf_builder_create(sf_model* model, const sf_study_options* options, sf
   for (double v : b->rhs) all_zero = all_zero && v == 0.0;
   for (auto& p : b->prescribed) all_zero = all_zero && p.second == 0.0;
   if (all_zero) return fail(SF_NO_EFFECTIVE_LOAD, "the model has no effective load");
-  if (!b->prescribed.empty()) return fail(SF_INVALID_ARGUMENT, "prescribed displacements are not supported on the device path yet");
   double t0 = now_seconds();
   build_pattern(mesh, b->free, b->free_count, b->threads, b->pattern);
   // Device set-up: mesh, element stiffness buffer, pattern and assembly map, system matrix.
@@ -754,6 +753,77 @@ void sf_builder_destroy(sf_builder* b) {
   delete b;
 }
 
+// StudyBuilder::apply_prescribed (study.rs:564-593) on the device-assembled matrix. Only the
+// prescribed block rows and their mirror blocks change, so those blocks are gathered to the host,
+// eliminated there in the reference's order, and written back: each prescribed component, by
+// ascending DOF, takes its row's off-diagonal entries by ascending column, moves entry x value off
+// every unconstrained right-hand side, and zeroes the entry and its transpose; then its own
+// right-hand side becomes diagonal x value.
+static sf_status apply_prescribed(sf_builder* b) {
+  if (b->prescribed.empty() || b->prescribed_applied) return SF_OK;
+  b->prescribed_applied = true;
+  DeviceSolver& s = b->solver;
+  const HostPattern& hp = b->pattern;
+  auto find = [&](uint32_t row, uint32_t col) -> uint32_t {
+    const uint32_t* lo = hp.cols.data() + hp.starts[row];
+    const uint32_t* hi = hp.cols.data() + hp.starts[row + 1];
+    return (uint32_t)(std::lower_bound(lo, hi, col) - hp.cols.data());
+  };
+  std::map<uint32_t, size_t> slot;
+  vector<uint32_t> list;
+  auto need = [&](uint32_t k) {
+    if (slot.emplace(k, list.size()).second) list.push_back(k);
+  };
+  for (auto& p : b->prescribed) {
+    uint32_t r = (uint32_t)(p.first / 3);
+    for (uint32_t k = hp.starts[r]; k < hp.starts[r + 1]; ++k) {
+      need(k);
+      need(find(hp.cols[k], r));
+    }
+  }
+  uint32_t* d_idx = nullptr;
+  double* d_vals = nullptr;
+  sf_status e = dev_alloc(s, (void**)&d_idx, list.size() * 4);
+  if (!e) e = dev_alloc(s, (void**)&d_vals, list.size() * 72);
+  vector<double> vals(list.size() * 9);
+  if (!e) {
+    copy_h2d(s, d_idx, list.data(), list.size() * 4);
+    e = setup_gather_blocks(s.stream, list.size(), 9, d_idx, (const double*)s.system.vals, d_vals);
+  }
+  if (!e) {
+    copy_d2h(s, vals.data(), d_vals, vals.size() * 8);
+    e = cuda_check(cudaStreamSynchronize(s.stream), "prescribed blocks");
+  }
+  if (e) return e;
+  auto at = [&](size_t i, size_t j) -> double& {
+    uint32_t k = find((uint32_t)(i / 3), (uint32_t)(j / 3));
+    return vals[slot[k] * 9 + (i % 3) * 3 + j % 3];
+  };
+  vector<char> constrained(b->rhs.size(), 0);
+  for (auto& p : b->prescribed) constrained[p.first] = 1;
+  for (auto& p : b->prescribed) {
+    const size_t dof = p.first, r = dof / 3, pr = dof % 3;
+    const double value = p.second;
+    for (uint32_t k = hp.starts[r]; k < hp.starts[r + 1]; ++k)
+      for (size_t q = 0; q < 3; ++q) {
+        size_t c = 3 * (size_t)hp.cols[k] + q;
+        if (c == dof) continue;
+        double& entry_ref = vals[slot[k] * 9 + pr * 3 + q];
+        double entry = entry_ref;
+        if (!constrained[c]) b->rhs[c] -= entry * value;
+        at(c, dof) += -entry;
+        entry_ref += -entry;
+      }
+  }
+  for (auto& p : b->prescribed) b->rhs[p.first] = at(p.first, p.first) * p.second;
+  copy_h2d(s, d_vals, vals.data(), vals.size() * 8);
+  e = setup_scatter_blocks(s.stream, list.size(), 9, d_idx, d_vals, (double*)s.system.vals);
+  if (!e) e = cuda_check(cudaStreamSynchronize(s.stream), "prescribed blocks");
+  dev_free(s, d_idx);
+  dev_free(s, d_vals);
+  return e;
+}
+
 static sf_status builder_assemble(sf_builder* b, uint64_t max_elements, sf_cancel_fn cancel, void* user) {
   size_t total = b->model.mesh.tets.size();
   if (b->next >= total) return SF_OK;
@@ -789,6 +859,10 @@ static sf_status builder_assemble(sf_builder* b, uint64_t max_elements, sf_cance
   }
   b->next = end;
   if (end == total) {
+    if (sf_status pe = apply_prescribed(b)) {
+      b->failure = pe;
+      return pe;
+    }
     // The element stiffness buffer and the assembly map have served; free them for the solve.
     AssemblyDevice& a = b->asmdev;
     for (void* p : {(void*)a.ke, (void*)a.map, (void*)a.map_starts, (void*)a.cursor}) dev_free(s, p);
@@ -815,6 +889,7 @@ static sf_status builder_setup(sf_builder* b, uint64_t budget, sf_cancel_fn canc
     fine.dev_starts = s.system.starts;
     fine.dev_cols = s.system.cols;
     vector<double> modes = rigid_modes(b->model.mesh.nodes, b->free, b->free_count);
+    for (auto& p : b->prescribed) std::fill(modes.begin() + p.first * 6, modes.begin() + p.first * 6 + 6, 0.0);
     vector<P3> positions;
     positions.reserve(b->free_count);
     for (size_t n = 0; n < b->free.size(); ++n)
@@ -1224,6 +1299,8 @@ sf_status sf_study_displacements(const sf_study* s, double* out) {
   if (sf_status e = cuda_check(cudaStreamSynchronize(d.stream), "read displacements")) return e;
   for (size_t n = 0; n < s->free.size(); ++n)
     for (int a = 0; a < 3; ++a) out[3 * n + a] = s->free[n] == FIXED ? 0.0 : x[3 * (size_t)s->free[n] + a];
+  // A prescribed component is exact, not the solver's estimate of it (study.rs:233-236).
+  for (auto& p : s->model.prescribed) out[3 * (size_t)p.first.first + p.first.second] = p.second;
   return SF_OK;
 }
 
@@ -1293,6 +1370,26 @@ static sf_status study_recover(sf_study* s) {
   unsigned long long none = ~0ull;
   copy_h2d(d, s->asmdev.error, &none, 8);
   sf_status e = launch_scatter_displacements(d.x, r, (uint32_t)nn, d.stream);
+  if (!e && !s->model.prescribed.empty()) {
+    // the prescribed components, exact
+    vector<uint32_t> idx;
+    vector<double> val;
+    for (auto& p : s->model.prescribed) {
+      idx.push_back(3 * p.first.first + p.first.second);
+      val.push_back(p.second);
+    }
+    uint32_t* d_idx = nullptr;
+    double* d_val = nullptr;
+    e = dev_alloc(d, (void**)&d_idx, idx.size() * 4);
+    if (!e) e = dev_alloc(d, (void**)&d_val, val.size() * 8);
+    if (!e) {
+      copy_h2d(d, d_idx, idx.data(), idx.size() * 4);
+      copy_h2d(d, d_val, val.data(), val.size() * 8);
+      e = setup_set_values(d.stream, idx.size(), d_idx, d_val, r.disp);
+    }
+    dev_free(d, d_idx);
+    dev_free(d, d_val);
+  }
   if (!e) e = launch_recovery(s->asmdev, s->model.material, r, (uint32_t)nn, (uint32_t)nv, d.stream);
   d.launches += 4;
   unsigned long long err = 0;
