@@ -62,6 +62,12 @@ __host__ __device__ inline size_t sell_value_offset(size_t q, int len, int chunk
 // the layout from host starts/columns, the values permuted on the device.
 sf_status make_sell_from_device(struct DeviceSolver& s, DevBsr& m, const uint32_t* starts, const uint32_t* cols);
 
+// Shared memory one warp of the row-group engine may stage (two groups); the launch opts in to
+// 200 KB per block.
+static const size_t kMaxStagePerWarp = 192 * 1024;
+// True when an operator runs in the SELL-32 layout: many rows, or a row group too long to stage.
+bool wants_sell(const DevBsr& m, uint64_t sell_min_rows);
+
 // Splits the rows of a block matrix into groups of at most `target` value bytes (a longer row is
 // a group of its own) and chooses the lanes per row from the mean blocks per row.
 sf_status make_row_groups(struct DeviceSolver& s, DevBsr& m, const uint32_t* host_starts, size_t value_bytes);

@@ -1377,6 +1377,14 @@ sf_status dev_alloc(DeviceSolver& s, void** ptr, size_t bytes) {
   return SF_OK;
 }
 
+bool wants_sell(const DevBsr& m, uint64_t sell_min_rows) {
+  // A warp stages two row groups at once; a group is at least one row, so an operator with rows
+  // too long to stage (the transposes of wide prolongators) runs one thread per row instead.
+  const size_t slot = ((m.group_bytes + 31) & ~15u) + ((m.group_blocks * 4 + 31) & ~15u) +
+                      (((m.group_rows + 1) * 4 + 31) & ~15u);
+  return m.rows >= sell_min_rows || 2 * slot > kMaxStagePerWarp;
+}
+
 void dev_free(DeviceSolver& s, void* ptr) {
   if (!ptr) return;
   for (size_t i = 0; i < s.owned.size(); ++i)
@@ -1554,7 +1562,7 @@ sf_status device_bsr(DeviceSolver& s, const Bsr& h, DevBsr& d, bool alias) {
     if (sf_status e = setup_convert<S>(s.stream, n, h.dev, (S*)d.vals)) return e;
   }
   if (sf_status e = make_row_groups(s, d, h.starts.data(), h.rb * h.cb * sizeof(S))) return e;
-  if (h.rows >= s.sell_min_rows)
+  if (wants_sell(d, s.sell_min_rows))
     if (sf_status e = make_sell_converted<S>(s, d, h.starts.data(), h.cols.data(), h.dev)) return e;
   return cuda_check(cudaGetLastError(), "level operator");
 }

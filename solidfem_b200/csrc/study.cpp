@@ -992,7 +992,7 @@ sf_status sf_builder_finish(sf_builder* b, sf_study** out) {
   if (e) return e;
   copy_h2d(d, d.rhs, s->rhs.data(), (size_t)d.n * 8);
   // The conjugate gradient's f64 product runs on a SELL copy when the system has many rows.
-  if (d.system.rows >= d.sell_min_rows)
+  if (wants_sell(d.system, d.sell_min_rows))
     if ((e = make_sell_from_device(d, d.system, s->pattern.starts.data(), s->pattern.cols.data()))) return e;
   if (mg) {
     s->levels = setup_take_levels(b->setup);
