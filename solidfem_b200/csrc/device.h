@@ -200,8 +200,11 @@ sf_status setup_convert(cudaStream_t st, size_t n, const double* in, S* out);
 template <typename S>
 sf_status setup_transpose_blocks(cudaStream_t st, size_t blocks, int rb, int cb, const uint32_t* src, const double* in,
                                  S* out);
+// The SELL-32 copy's columns and values (converted to S) from block CSR on the device.
 template <typename S>
-sf_status setup_sell_place(cudaStream_t st, size_t blocks, int len, const uint32_t* pos, const double* in, S* out);
+sf_status setup_sell_fill(cudaStream_t st, size_t slots, int len, const uint32_t* sell_rows, const uint32_t* sell_len,
+                          const uint32_t* sell_start, uint32_t nrows, const uint32_t* starts, const uint32_t* cols,
+                          const double* in, uint32_t* out_cols, S* out);
 
 // ------------------------------------------------------------------- assembly (assembly.cu)
 struct AssemblyDevice {

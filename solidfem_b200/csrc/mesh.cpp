@@ -248,14 +248,27 @@ vector<vector<uint32_t>> face_connected_bodies(const Mesh& mesh) {
     }
     return x;
   };
-  vector<std::pair<Key3, uint32_t>> keyed(n * 4);
+  // Tets sharing a face are joined: every face key goes into an open-addressing table, and a key
+  // met a second time joins its two tets. The partition, and so the body order below (by first
+  // tet), is the one a sort of the keys gives.
+  size_t cap = 16;
+  while (cap < 8 * n) cap <<= 1;
+  vector<Key3> keys(cap);
+  vector<uint32_t> owner(cap, 0xffffffffu);
   for (size_t t = 0; t < n; ++t)
-    for (int f = 0; f < 4; ++f) keyed[4 * t + f] = {face_key(mesh.corners[t], f), (uint32_t)t};
-  std::sort(keyed.begin(), keyed.end());
-  for (size_t i = 0; i + 1 < keyed.size(); ++i)
-    if (keyed[i].first == keyed[i + 1].first) {
-      size_t a = find(keyed[i].second), b = find(keyed[i + 1].second);
-      if (a != b) parent[std::max(a, b)] = std::min(a, b);
+    for (int f = 0; f < 4; ++f) {
+      Key3 k = face_key(mesh.corners[t], f);
+      uint64_t h = (uint64_t)k[0] * 0x9E3779B97F4A7C15ull ^ (uint64_t)k[1] * 0xC2B2AE3D27D4EB4Full ^
+                   (uint64_t)k[2] * 0x165667B19E3779F9ull;
+      size_t at = (size_t)(h >> 17) & (cap - 1);
+      while (owner[at] != 0xffffffffu && keys[at] != k) at = (at + 1) & (cap - 1);
+      if (owner[at] == 0xffffffffu) {
+        keys[at] = k;
+        owner[at] = (uint32_t)t;
+      } else {
+        size_t a = find(owner[at]), b = find(t);
+        if (a != b) parent[std::max(a, b)] = std::min(a, b);
+      }
     }
   vector<vector<uint32_t>> groups;
   vector<size_t> group_of(n, SIZE_MAX);

@@ -313,16 +313,25 @@ __global__ void transpose_blocks_kernel(size_t blocks, int rb, int cb, const uin
   }
 }
 
-// SELL placement with conversion from the f64 setup values.
+// Fills a SELL-32 copy from a block CSR matrix (f64 values, converted to S): one thread per slice
+// lane places its row's columns and values at their chunked positions; padding stays zero.
 template <typename S, int LEN>
-__global__ void sell_place_kernel(size_t blocks, const uint32_t* __restrict__ pos, const double* __restrict__ in,
-                                  S* __restrict__ out) {
+__global__ void sell_fill_kernel(size_t slots, const uint32_t* __restrict__ sell_rows, const uint32_t* __restrict__ sell_len,
+                                 const uint32_t* __restrict__ sell_start, uint32_t nrows,
+                                 const uint32_t* __restrict__ starts, const uint32_t* __restrict__ cols,
+                                 const double* __restrict__ in, uint32_t* __restrict__ out_cols, S* __restrict__ out) {
   constexpr int U = sell_chunk_blocks(LEN, (int)sizeof(S));
   constexpr int VEC = 16 / (int)sizeof(S);
-  for (size_t b = blockIdx.x * (size_t)blockDim.x + threadIdx.x; b < blocks; b += (size_t)gridDim.x * blockDim.x) {
-    const uint32_t q = pos[b];
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < slots; i += (size_t)gridDim.x * blockDim.x) {
+    const uint32_t row = sell_rows[i];
+    if (row >= nrows) continue;
+    const uint32_t s = (uint32_t)(i / 32), t = (uint32_t)(i % 32), n = sell_len[i], b0 = starts[row];
+    for (uint32_t k = 0; k < n; ++k) {
+      const size_t q = sell_start[s] + 32 * (k - k % U) + t * U + k % U;
+      out_cols[q] = cols[b0 + k];
 #pragma unroll
-    for (int e = 0; e < LEN; ++e) out[sell_value_offset(q, LEN, U, VEC, e)] = (S)in[b * LEN + e];
+      for (int e = 0; e < LEN; ++e) out[sell_value_offset(q, LEN, U, VEC, e)] = (S)in[(size_t)(b0 + k) * LEN + e];
+    }
   }
 }
 
@@ -466,17 +475,30 @@ template sf_status setup_transpose_blocks<float>(cudaStream_t, size_t, int, int,
 template sf_status setup_transpose_blocks<double>(cudaStream_t, size_t, int, int, const uint32_t*, const double*, double*);
 
 template <typename S>
-sf_status setup_sell_place(cudaStream_t st, size_t blocks, int len, const uint32_t* pos, const double* in, S* out) {
-  if (blocks == 0) return SF_OK;
+sf_status setup_sell_fill(cudaStream_t st, size_t slots, int len, const uint32_t* sell_rows, const uint32_t* sell_len,
+                          const uint32_t* sell_start, uint32_t nrows, const uint32_t* starts, const uint32_t* cols,
+                          const double* in, uint32_t* out_cols, S* out) {
+  if (slots == 0) return SF_OK;
   switch (len) {
-    case 9: sell_place_kernel<S, 9><<<grid_for(blocks), kT, 0, st>>>(blocks, pos, in, out); break;
-    case 18: sell_place_kernel<S, 18><<<grid_for(blocks), kT, 0, st>>>(blocks, pos, in, out); break;
-    case 36: sell_place_kernel<S, 36><<<grid_for(blocks), kT, 0, st>>>(blocks, pos, in, out); break;
+    case 9:
+      sell_fill_kernel<S, 9><<<grid_for(slots), kT, 0, st>>>(slots, sell_rows, sell_len, sell_start, nrows, starts, cols,
+                                                            in, out_cols, out);
+      break;
+    case 18:
+      sell_fill_kernel<S, 18><<<grid_for(slots), kT, 0, st>>>(slots, sell_rows, sell_len, sell_start, nrows, starts, cols,
+                                                             in, out_cols, out);
+      break;
+    case 36:
+      sell_fill_kernel<S, 36><<<grid_for(slots), kT, 0, st>>>(slots, sell_rows, sell_len, sell_start, nrows, starts, cols,
+                                                             in, out_cols, out);
+      break;
     default: return fail(SF_INVALID_ARGUMENT, "unsupported block size for the SELL layout");
   }
-  return cuda_check(cudaGetLastError(), "SELL placement");
+  return cuda_check(cudaGetLastError(), "SELL fill");
 }
-template sf_status setup_sell_place<float>(cudaStream_t, size_t, int, const uint32_t*, const double*, float*);
-template sf_status setup_sell_place<double>(cudaStream_t, size_t, int, const uint32_t*, const double*, double*);
+template sf_status setup_sell_fill<float>(cudaStream_t, size_t, int, const uint32_t*, const uint32_t*, const uint32_t*,
+                                          uint32_t, const uint32_t*, const uint32_t*, const double*, uint32_t*, float*);
+template sf_status setup_sell_fill<double>(cudaStream_t, size_t, int, const uint32_t*, const uint32_t*, const uint32_t*,
+                                           uint32_t, const uint32_t*, const uint32_t*, const double*, uint32_t*, double*);
 
 }  // namespace sf

@@ -869,19 +869,6 @@ __device__ __forceinline__ void sell_pcg_check_kernel(SellOp<double> A, const do
   }
 }
 
-// Places each block of a device-resident BSR matrix at its SELL position.
-template <typename S, int LEN>
-__global__ void sell_permute_kernel(size_t blocks, const uint32_t* __restrict__ pos, const S* __restrict__ in,
-                                    S* __restrict__ out) {
-  constexpr int U = sell_chunk_blocks(LEN, (int)sizeof(S));
-  constexpr int VEC = 16 / (int)sizeof(S);
-  for (size_t b = blockIdx.x * (size_t)blockDim.x + threadIdx.x; b < blocks; b += (size_t)gridDim.x * blockDim.x) {
-    const uint32_t q = pos[b];
-#pragma unroll
-    for (int e = 0; e < LEN; ++e) out[sell_value_offset(q, LEN, U, VEC, e)] = in[b * LEN + e];
-  }
-}
-
 // ap = A p with the curvature p.ap.
 template <int LPR>
 struct EpiDot {
@@ -1451,13 +1438,13 @@ namespace {
 
 struct SellLayout {
   uint32_t nslices = 0;
-  std::vector<uint32_t> rows, len, start, pos, cols;
+  std::vector<uint32_t> rows, len, start;
 };
 
 // Rows sorted by descending block count inside windows of kSellWindow rows (stable, so equal
 // lengths keep row order), cut into slices of 32, slice widths padded to chunks of `chunk`
-// blocks; pos[b] is the SELL slot (column index position) of BSR block b.
-SellLayout sell_layout(uint32_t nrows, const uint32_t* starts, const uint32_t* cols, uint32_t chunk) {
+// blocks. Only this row order is host work; the blocks are placed on the device.
+SellLayout sell_layout(uint32_t nrows, const uint32_t* starts, uint32_t chunk) {
   SellLayout L;
   L.nslices = (nrows + 31) / 32;
   std::vector<uint32_t> order(nrows);
@@ -1480,16 +1467,6 @@ SellLayout sell_layout(uint32_t nrows, const uint32_t* starts, const uint32_t* c
     width = (width + chunk - 1) / chunk * chunk;
     L.start[sl + 1] = L.start[sl] + 32 * width;
   }
-  L.pos.assign(starts[nrows], 0);
-  L.cols.assign(L.start[L.nslices], 0);
-  for (uint32_t i = 0; i < nrows; ++i) {
-    uint32_t r = order[i], sl = i / 32, t = i % 32;
-    for (uint32_t k = 0; k < rlen(r); ++k) {
-      uint32_t q = L.start[sl] + 32 * (k - k % chunk) + t * chunk + k % chunk;
-      L.pos[starts[r] + k] = q;
-      L.cols[q] = cols[starts[r] + k];
-    }
-  }
   return L;
 }
 
@@ -1499,13 +1476,13 @@ sf_status upload_sell_layout(DeviceSolver& s, DevBsr& m, const SellLayout& L, si
   if (!e) e = dev_alloc(s, (void**)&m.sell_rows, L.rows.size() * 4);
   if (!e) e = dev_alloc(s, (void**)&m.sell_len, L.len.size() * 4);
   if (!e) e = dev_alloc(s, (void**)&m.sell_start, L.start.size() * 4);
-  if (!e) e = dev_alloc(s, (void**)&m.sell_cols, std::max<size_t>(1, L.cols.size()) * 4);
-  if (!e) e = dev_alloc(s, &m.sell_vals, std::max<size_t>(1, L.cols.size()) * value_bytes);
+  const size_t slots = L.start[L.nslices];
+  if (!e) e = dev_alloc(s, (void**)&m.sell_cols, std::max<size_t>(1, slots) * 4);
+  if (!e) e = dev_alloc(s, &m.sell_vals, std::max<size_t>(1, slots) * value_bytes);
   if (e) return e;
   copy_h2d(s, m.sell_rows, L.rows.data(), L.rows.size() * 4);
   copy_h2d(s, m.sell_len, L.len.data(), L.len.size() * 4);
   copy_h2d(s, m.sell_start, L.start.data(), L.start.size() * 4);
-  if (!L.cols.empty()) copy_h2d(s, m.sell_cols, L.cols.data(), L.cols.size() * 4);
   return SF_OK;
 }
 
@@ -1516,29 +1493,18 @@ template <typename S>
 sf_status make_sell_converted(DeviceSolver& s, DevBsr& m, const uint32_t* starts, const uint32_t* cols,
                               const double* vals) {
   const int len = (int)(m.rb * m.cb);
-  SellLayout L = sell_layout(m.rows, starts, cols, (uint32_t)sell_chunk_blocks(len, (int)sizeof(S)));
+  SellLayout L = sell_layout(m.rows, starts, (uint32_t)sell_chunk_blocks(len, (int)sizeof(S)));
   if (sf_status e = upload_sell_layout(s, m, L, (size_t)len * sizeof(S))) return e;
-  uint32_t* pos = nullptr;
-  if (sf_status e = dev_alloc(s, (void**)&pos, std::max<size_t>(1, L.pos.size()) * 4)) return e;
-  if (!L.pos.empty()) copy_h2d(s, pos, L.pos.data(), L.pos.size() * 4);
-  sf_status e = setup_sell_place<S>(s.stream, L.pos.size(), len, pos, vals, (S*)m.sell_vals);
+  sf_status e = setup_sell_fill<S>(s.stream, (size_t)L.nslices * 32, len, m.sell_rows, m.sell_len, m.sell_start, m.rows,
+                                   m.starts, m.cols, vals, m.sell_cols, (S*)m.sell_vals);
   if (!e) e = cuda_check(cudaStreamSynchronize(s.stream), "SELL placement");
-  dev_free(s, pos);
   m.sell = true;
   return e;
 }
 
 sf_status make_sell_from_device(DeviceSolver& s, DevBsr& m, const uint32_t* starts, const uint32_t* cols) {
-  SellLayout L = sell_layout(m.rows, starts, cols, (uint32_t)sell_chunk_blocks(9, 8));
-  if (sf_status e = upload_sell_layout(s, m, L, 72)) return e;
-  uint32_t* pos = nullptr;
-  if (sf_status e = dev_alloc(s, (void**)&pos, std::max<size_t>(1, L.pos.size()) * 4)) return e;
-  if (!L.pos.empty()) copy_h2d(s, pos, L.pos.data(), L.pos.size() * 4);
-  sell_permute_kernel<double, 9><<<grid_for_elems(L.pos.size()), kThreads, 0, s.stream>>>(L.pos.size(), pos,
-                                                                                         (const double*)m.vals,
-                                                                                         (double*)m.sell_vals);
-  m.sell = true;
-  return cuda_check(cudaStreamSynchronize(s.stream), "SELL permute");
+  (void)cols;
+  return make_sell_converted<double>(s, m, starts, nullptr, (const double*)m.vals);
 }
 
 namespace {

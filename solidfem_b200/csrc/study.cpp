@@ -8,6 +8,7 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <numeric>
 #include <memory>
 
 #ifdef _OPENMP
@@ -69,12 +70,23 @@ sf_status check_constraints(const Mesh& m, const vector<char>& fixed) {
   auto bodies = face_connected_bodies(m);
   vector<vector<uint32_t>> body_nodes(bodies.size());
   vector<double> sizes(bodies.size());
+  vector<uint32_t> mark(m.nodes.size(), 0xffffffffu);
   for (size_t b = 0; b < bodies.size(); ++b) {
+    // The body's nodes, ascending: every node when the mesh is one body (a valid mesh uses every
+    // node), otherwise its tets' nodes deduplicated and sorted.
     vector<uint32_t>& nodes = body_nodes[b];
-    for (uint32_t t : bodies[b])
-      for (uint32_t n : m.tets[t]) nodes.push_back(n);
-    std::sort(nodes.begin(), nodes.end());
-    nodes.erase(std::unique(nodes.begin(), nodes.end()), nodes.end());
+    if (bodies.size() == 1) {
+      nodes.resize(m.nodes.size());
+      std::iota(nodes.begin(), nodes.end(), 0u);
+    } else {
+      for (uint32_t t : bodies[b])
+        for (uint32_t n : m.tets[t])
+          if (mark[n] != (uint32_t)b) {
+            mark[n] = (uint32_t)b;
+            nodes.push_back(n);
+          }
+      std::sort(nodes.begin(), nodes.end());
+    }
     P3 lo = {INFINITY, INFINITY, INFINITY}, hi = {-INFINITY, -INFINITY, -INFINITY};
     for (uint32_t n : nodes)
       for (int a = 0; a < 3; ++a) {
@@ -246,23 +258,32 @@ void build_pattern(const Mesh& m, const vector<uint32_t>& free, size_t free_coun
   vector<uint32_t> row_node(free_count);
   for (size_t n = 0; n < nn; ++n)
     if (free[n] != FIXED) row_node[free[n]] = (uint32_t)n;
+  // Per row: its distinct columns (a per-thread marker array stamped with the row) and its entry
+  // count, then the sorted columns and, per block, the entries in element order.
   vector<uint32_t> counts(free_count, 0), map_counts(free_count, 0);
 #ifdef _OPENMP
-#pragma omp parallel for schedule(dynamic, 1024) num_threads(threads)
+#pragma omp parallel num_threads(threads)
 #endif
-  for (long long r = 0; r < (long long)free_count; ++r) {
-    uint32_t node = row_node[r];
-    vector<uint32_t> cols;
-    uint32_t entries = 0;
-    for (uint32_t k = inc_start[node]; k < inc_start[node + 1]; ++k)
-      for (uint32_t n : m.tets[inc[k]])
-        if (free[n] != FIXED) {
-          cols.push_back(free[n]);
+  {
+    vector<uint32_t> mark(free_count, 0xffffffffu);
+#ifdef _OPENMP
+#pragma omp for schedule(dynamic, 1024)
+#endif
+    for (long long r = 0; r < (long long)free_count; ++r) {
+      uint32_t node = row_node[r], distinct = 0, entries = 0;
+      for (uint32_t k = inc_start[node]; k < inc_start[node + 1]; ++k)
+        for (uint32_t n : m.tets[inc[k]]) {
+          uint32_t fc = free[n];
+          if (fc == FIXED) continue;
           ++entries;
+          if (mark[fc] != (uint32_t)r) {
+            mark[fc] = (uint32_t)r;
+            ++distinct;
+          }
         }
-    std::sort(cols.begin(), cols.end());
-    counts[r] = (uint32_t)(std::unique(cols.begin(), cols.end()) - cols.begin());
-    map_counts[r] = entries;
+      counts[r] = distinct;
+      map_counts[r] = entries;
+    }
   }
   hp.starts.assign(free_count + 1, 0);
   vector<uint64_t> map_row(free_count + 1, 0);
@@ -274,40 +295,50 @@ void build_pattern(const Mesh& m, const vector<uint32_t>& free, size_t free_coun
   hp.map_starts.assign(hp.starts[free_count] + 1, 0);
   hp.map.assign(map_row[free_count], 0);
 #ifdef _OPENMP
-#pragma omp parallel for schedule(dynamic, 1024) num_threads(threads)
+#pragma omp parallel num_threads(threads)
 #endif
-  for (long long r = 0; r < (long long)free_count; ++r) {
-    uint32_t node = row_node[r];
-    vector<uint32_t> cols;
-    for (uint32_t k = inc_start[node]; k < inc_start[node + 1]; ++k)
-      for (uint32_t n : m.tets[inc[k]])
-        if (free[n] != FIXED) cols.push_back(free[n]);
-    std::sort(cols.begin(), cols.end());
-    cols.erase(std::unique(cols.begin(), cols.end()), cols.end());
-    uint32_t b0 = hp.starts[r];
-    std::copy(cols.begin(), cols.end(), hp.cols.begin() + b0);
-    // Per block of this row, its entry count, then the entries in element order.
-    vector<uint32_t> per(cols.size(), 0);
-    for (uint32_t k = inc_start[node]; k < inc_start[node + 1]; ++k)
-      for (uint32_t n : m.tets[inc[k]])
-        if (free[n] != FIXED) per[std::lower_bound(cols.begin(), cols.end(), free[n]) - cols.begin()] += 1;
-    uint64_t base = map_row[r];
-    vector<uint64_t> at(cols.size());
-    for (size_t j = 0; j < cols.size(); ++j) {
-      at[j] = base;
-      hp.map_starts[b0 + j] = (uint32_t)base;
-      base += per[j];
-    }
-    for (uint32_t k = inc_start[node]; k < inc_start[node + 1]; ++k) {
-      uint32_t e = inc[k];
-      const auto& t = m.tets[e];
-      int a = 0;
-      while (t[a] != node) ++a;
-      for (int b = 0; b < 10; ++b) {
-        uint32_t fc = free[t[b]];
-        if (fc == FIXED) continue;
-        size_t j = std::lower_bound(cols.begin(), cols.end(), fc) - cols.begin();
-        hp.map[at[j]++] = (e << 7) | (uint32_t)(10 * a + b);
+  {
+    vector<uint32_t> mark(free_count, 0xffffffffu), pos(free_count, 0), cols, per;
+    vector<uint64_t> at;
+#ifdef _OPENMP
+#pragma omp for schedule(dynamic, 1024)
+#endif
+    for (long long r = 0; r < (long long)free_count; ++r) {
+      uint32_t node = row_node[r];
+      cols.clear();
+      for (uint32_t k = inc_start[node]; k < inc_start[node + 1]; ++k)
+        for (uint32_t n : m.tets[inc[k]]) {
+          uint32_t fc = free[n];
+          if (fc != FIXED && mark[fc] != (uint32_t)r) {
+            mark[fc] = (uint32_t)r;
+            cols.push_back(fc);
+          }
+        }
+      std::sort(cols.begin(), cols.end());
+      uint32_t b0 = hp.starts[r];
+      std::copy(cols.begin(), cols.end(), hp.cols.begin() + b0);
+      per.assign(cols.size(), 0);
+      for (size_t j = 0; j < cols.size(); ++j) pos[cols[j]] = (uint32_t)j;
+      for (uint32_t k = inc_start[node]; k < inc_start[node + 1]; ++k)
+        for (uint32_t n : m.tets[inc[k]])
+          if (free[n] != FIXED) per[pos[free[n]]] += 1;
+      uint64_t base = map_row[r];
+      at.resize(cols.size());
+      for (size_t j = 0; j < cols.size(); ++j) {
+        at[j] = base;
+        hp.map_starts[b0 + j] = (uint32_t)base;
+        base += per[j];
+      }
+      for (uint32_t k = inc_start[node]; k < inc_start[node + 1]; ++k) {
+        uint32_t e = inc[k];
+        const auto& t = m.tets[e];
+        int a = 0;
+        while (t[a] != node) ++a;
+        for (int b = 0; b < 10; ++b) {
+          uint32_t fc = free[t[b]];
+          if (fc == FIXED) continue;
+          hp.map[at[pos[fc]]++] = (e << 7) | (uint32_t)(10 * a + b);
+        }
       }
     }
   }
