@@ -208,26 +208,15 @@ def run_mine(args, rank, world):
 
     import solidfem_b200 as sf
 
-    device = int(os.environ.get("LOCAL_RANK", 0))
-    torch.cuda.set_device(device)
-    dist = None
-    if world > 1:
-        import datetime
+    from solidfem_b200.replicas import ReplicaGroup
 
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=torch.device("cuda", device))
+    group = ReplicaGroup.from_env("nccl")
+    device = group.local_rank
+    torch.cuda.set_device(device)
 
     def barrier():
-        if dist:
-            dist.barrier()
+        group.barrier()
         torch.cuda.synchronize()
-
-    def max_over_ranks(x):
-        if not dist:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
 
     mesh, model = build_model(sf)
     # --- e2e through the public API with host buffers (model -> study -> solve -> displacements).
@@ -257,7 +246,9 @@ def run_mine(args, rank, world):
     barrier()
     # Median of the steps: host phases (pattern, aggregation, layouts) share the box's cores with
     # other tenants, and a step that met contention is listed in `samples` rather than averaged in.
-    e2e_sec = max_over_ranks(statistics.median(e2e_times))
+    e2e_local = statistics.median(e2e_times)
+    e2e_value = group.rate(1, e2e_local)
+    e2e_sec = group.max(e2e_local)
     rep = study.report()
 
     # --- value: device-resident solves of the mixed path.
@@ -271,10 +262,10 @@ def run_mine(args, rank, world):
         ms, its, out = timed_solves(torch, study, stream, args.steps)
     barrier()
     launches = study.device_timing()["kernel_launches"] - launches0
-    ms = max_over_ranks(ms)
+    value = group.rate(args.steps, ms / 1000.0)
+    ms = group.max(ms)
     clock = clocks.summary()
     ms_per_step = ms / args.steps
-    value = world * args.steps / (ms / 1000.0)
     x_mixed = study.displacements()
 
     # --- the plain FP64 path (Precision::Double semantics) for the mixed-vs-FP64 comparison.
@@ -284,7 +275,7 @@ def run_mine(args, rank, world):
     barrier()
     dms, dits, dout = timed_solves(torch, double, dstream, max(1, min(args.steps, 3)))
     barrier()
-    dms = max_over_ranks(dms) / max(1, min(args.steps, 3))
+    dms = group.max(dms) / max(1, min(args.steps, 3))
     x_double = double.displacements()
     diff = float(np.linalg.norm(x_mixed - x_double) / np.linalg.norm(x_double))
 
@@ -311,7 +302,7 @@ def run_mine(args, rank, world):
                          "peak_kind": peak_kind, "traffic": traffic,
                          "bytes_per_launch": kt["bytes_per_launch"], "ms_per_launch": kt["ms_per_launch"],
                          "system_product_gbs": st["bytes_per_launch"] / (st["ms_per_launch"] * 1e-3) / 1e9},
-            "e2e": {"value": world / e2e_sec, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "seconds_per_step": e2e_sec, "samples": [round(t, 4) for t in e2e_times]},
             "gpu_launches": launches, "clocks": clock}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -319,8 +310,7 @@ def run_mine(args, rank, world):
     if rank == 0:
         print(json.dumps(line), flush=True)
     del study, double
-    if dist:
-        dist.destroy_process_group()
+    group.close()
     return 0
 
 
@@ -413,24 +403,30 @@ def run_block(args):
 
 def run_serving(args):
     """The serving stream (512 mixed bar / tube / plate requests, Poisson arrivals at 20/s, seed 0)
-    through the serving loop, then the same stream through serial plain FP64 GPU solves."""
+    through the serving loop, then the same stream through serial plain FP64 GPU solves. Under
+    torchrun every rank serves its round-robin share of the stream on its own GPU (one server per
+    GPU, no collective on the data path); rates are over all ranks, latencies pooled."""
     import concurrent.futures
 
     import torch
 
     import solidfem_b200 as sf
     from solidfem_b200 import workloads as W
+    from solidfem_b200.replicas import ReplicaGroup
 
-    torch.cuda.set_device(0)
-    reqs = W.serving_stream(count=args.requests)
+    group = ReplicaGroup.from_env("nccl")
+    device = group.local_rank
+    torch.cuda.set_device(device)
+    stream = W.serving_stream(count=args.requests)
+    reqs = group.shard(stream)
     t0 = time.perf_counter()
     with concurrent.futures.ThreadPoolExecutor(max_workers=8) as pool:
         built = list(pool.map(W.build_model, reqs))
-    prep = time.perf_counter() - t0
+    prep = group.max(time.perf_counter() - t0)
 
     def opts(precision):
         return sf.StudyOptions(pcg=sf.PcgOptions(tolerance=TOLERANCE),
-                               preconditioner=sf.MultigridOptions(precision=precision))
+                               preconditioner=sf.MultigridOptions(precision=precision), device=device)
 
     # warm-up: context, module load
     w = sf.StaticStudy.new(W.build_model(reqs[0])[1], opts(sf.Precision.MIXED))
@@ -439,7 +435,8 @@ def run_serving(args):
     gc.collect()
 
     def serve(models, paced):
-        server = sf.Server(sf.ServerOptions(build_threads=args.build_threads))
+        server = sf.Server(sf.ServerOptions(device=device, build_threads=args.build_threads))
+        group.barrier()
         start = time.perf_counter()
         ids = []
         for r, (mesh, model) in zip(reqs, models):
@@ -458,40 +455,51 @@ def run_serving(args):
         server.close()
         return results, makespan, stats
 
+    def pooled(results, makespan, stats):
+        lat = group.gather([r.latency_seconds for r in results])
+        batches = group.sum(stats["batches"])
+        batched = group.sum(stats["batched_requests"])
+        return {"solves_per_s": group.rate(len(results), makespan), "makespan_s": group.max(makespan),
+                "p50_latency_s": percentile(lat, 0.5), "p99_latency_s": percentile(lat, 0.99),
+                "failed": int(group.sum(sum(1 for r in results if r.status != sf.Status.OK))),
+                "batched_requests": int(batched), "batches": int(batches),
+                "mean_batch_size": batched / batches if batches else 0.0,
+                "peak_reserved_gb": group.max(stats["peak_reserved_bytes"]) / 1e9}
+
     results, makespan, stats = serve(built, True)
-    failed = sum(1 for r in results if r.status != sf.Status.OK)
-    lat = [r.latency_seconds for r in results]
-    mine = {"solves_per_s": len(reqs) / makespan, "makespan_s": makespan,
-            "p50_latency_s": percentile(lat, 0.5), "p99_latency_s": percentile(lat, 0.99),
-            "failed": failed, "batched_requests": stats["batched_requests"],
-            "mean_batch_size": stats["mean_batch_size"], "batches": stats["batches"],
-            "peak_reserved_gb": stats["peak_reserved_bytes"] / 1e9,
-            "iterations_mean": statistics.mean(r.outcome.progress.iteration for r in results),
-            "build_seconds_sum": sum(r.build_seconds for r in results),
-            "solve_seconds_sum": sum(r.solve_seconds for r in results),
-            "queue_seconds_mean": statistics.mean(r.queue_seconds for r in results),
-            "failures": sorted({f"{r.status.name}: {r.message}" for r in results if r.status != sf.Status.OK})}
+    mine = pooled(results, makespan, stats)
+    mine.update({"iterations_mean": statistics.mean(group.gather([r.outcome.progress.iteration for r in results])),
+                 "build_seconds_sum": group.sum(sum(r.build_seconds for r in results)),
+                 "solve_seconds_sum": group.sum(sum(r.solve_seconds for r in results)),
+                 "queue_seconds_mean": statistics.mean(group.gather([r.queue_seconds for r in results])),
+                 "failures": sorted(set(group.gather(
+                     [f"{r.status.name}: {r.message}" for r in results if r.status != sf.Status.OK])))})
     del built
     gc.collect()
     # the same requests all submitted at once: the loop's capacity rather than the arrival rate
     with concurrent.futures.ThreadPoolExecutor(max_workers=8) as pool:
         built = list(pool.map(W.build_model, reqs))
-    sres, smake, sstats = serve(built, False)
-    slat = [r.latency_seconds for r in sres]
-    mine["saturated"] = {"solves_per_s": len(reqs) / smake, "makespan_s": smake,
-                         "p50_latency_s": percentile(slat, 0.5), "p99_latency_s": percentile(slat, 0.99),
-                         "failed": sum(1 for r in sres if r.status != sf.Status.OK),
-                         "mean_batch_size": sstats["mean_batch_size"],
-                         "peak_reserved_gb": sstats["peak_reserved_bytes"] / 1e9}
+    saturated = pooled(*serve(built, False))
+    mine["saturated"] = {k: saturated[k] for k in ("solves_per_s", "makespan_s", "p50_latency_s", "p99_latency_s",
+                                                   "failed", "mean_batch_size", "peak_reserved_gb")}
     del built
     gc.collect()
 
+    config = {"workload": f"serving stream: {len(stream)} bar/tube/plate requests, Poisson 20/s, seed 0, "
+                          "10k-600k DOF log-uniform, rel. residual 1e-8, HBM budget 150 GB, "
+                          "requests under 100k DOF batched",
+              "build_threads": args.build_threads, "model_prep_seconds": prep,
+              "parallelism": f"replicas: {group.world} server(s), round-robin request shares"}
     if args.no_serial:
-        print(json.dumps({"metric": "served solves/s", "value": mine["solves_per_s"], "mine": mine}))
+        if group.leader:
+            print(json.dumps({"metric": "served solves/s", "value": mine["solves_per_s"], "unit": "solves/s",
+                              "n_gpus": group.world, "config": config, "mine": mine}))
+        group.close()
         return 0
     # serial plain FP64 GPU solves of the same stream, one at a time in arrival order
     with concurrent.futures.ThreadPoolExecutor(max_workers=8) as pool:
         built = list(pool.map(W.build_model, reqs))
+    group.barrier()
     start = time.perf_counter()
     lat, serial_failed = [], 0
     for r, (mesh, model) in zip(reqs, built):
@@ -505,18 +513,18 @@ def run_serving(args):
         del st
         lat.append(time.perf_counter() - start - r.arrival)
     makespan = time.perf_counter() - start
-    serial = {"solves_per_s": len(reqs) / makespan, "makespan_s": makespan,
-              "p50_latency_s": percentile(lat, 0.5), "p99_latency_s": percentile(lat, 0.99), "failed": serial_failed}
+    lat = group.gather(lat)
+    serial = {"solves_per_s": group.rate(len(reqs), makespan), "makespan_s": group.max(makespan),
+              "p50_latency_s": percentile(lat, 0.5), "p99_latency_s": percentile(lat, 0.99),
+              "failed": int(group.sum(serial_failed))}
     line = {"metric": "served solves/s (mixed-size stream, continuous batching)", "value": mine["solves_per_s"],
-            "unit": "solves/s", "n_gpus": 1, "higher_is_better": True,
-            "config": {"workload": f"serving stream: {len(reqs)} bar/tube/plate requests, Poisson 20/s, seed 0, "
-                                   "10k-600k DOF log-uniform, rel. residual 1e-8, HBM budget 150 GB, "
-                                   "requests under 100k DOF batched",
-                       "build_threads": args.build_threads, "model_prep_seconds": prep},
-            "mine": mine, "serial_fp64": serial,
+            "unit": "solves/s", "n_gpus": group.world, "higher_is_better": True, "scaling": "strong",
+            "config": config, "mine": mine, "serial_fp64": serial,
             "speedup_throughput": mine["solves_per_s"] / serial["solves_per_s"],
             "data": "synthetic (seeded request stream)"}
-    print(json.dumps(line))
+    if group.leader:
+        print(json.dumps(line))
+    group.close()
     return 0
 
 
@@ -542,7 +550,7 @@ def main():
     if args.profile:
         return run_profile(args)
     if args.workload == "serving":
-        return run_serving(args) if rank == 0 else 0
+        return run_serving(args)
     if args.workload == "block":
         return run_block(args) if rank == 0 else 0
     if args.impl == "reference":
