@@ -36,6 +36,13 @@ struct DevBsr {
   // vals[Q0 * rb * cb + (i / VEC) * 32 VEC + t VEC + i % VEC] with VEC values per 16 bytes, so each
   // vector load of a warp is 512 contiguous bytes. Slice widths are padded to whole chunks.
   bool sell = false;
+  // Split-row copy (operators of 6-row blocks with many rows): the same slices, but each block
+  // row takes six lanes, one per scalar row, and a slice holds kSplitRowsPerSlice block rows
+  // (lanes 6 m .. 6 m + 5; lanes 30 and 31 idle). Lane t = 6 m + p reads row p of each block, so
+  // its "blocks" are 1 x cb: values as in SELL-32 with block length cb, U = sell_chunk_blocks(cb,
+  // value bytes). Columns are stored once per block row: chunk c of slice s keeps them at
+  // cols[(slice_start[s] / 32) * 5 + 5 U c + U m ..] for the six lanes of block row m to share.
+  bool split = false;
   uint32_t nslices = 0;
   uint32_t* sell_rows = nullptr;   // nslices * 32: the row of each lane (rows when padding)
   uint32_t* sell_len = nullptr;    // nslices * 32: its block count
@@ -45,6 +52,8 @@ struct DevBsr {
 };
 
 static const uint32_t kSellWindow = 2048;    // rows are sorted by length inside windows this long
+static const uint32_t kSplitRowsPerSlice = 5;  // block rows of six scalar rows per 32-lane slice
+static const uint32_t kSplitMinRows = 4096;    // 6-row block operators with this many rows split
 
 // Blocks per SELL lane chunk: 144 bytes of values, at least one block.
 constexpr int sell_chunk_blocks(int len, int value_bytes) {
@@ -67,6 +76,10 @@ sf_status make_sell_from_device(struct DeviceSolver& s, DevBsr& m, const uint32_
 static const size_t kMaxStagePerWarp = 192 * 1024;
 // True when an operator runs in the SELL-32 layout: many rows, or a row group too long to stage.
 bool wants_sell(const DevBsr& m, uint64_t sell_min_rows);
+// True when an operator of 6-row blocks runs split, one lane per scalar row: enough block rows
+// to fill the device with six lanes each (level 1 of an elasticity hierarchy and the transpose
+// restricting onto it), and launches whose kernel may depend on the size (not batchable).
+bool wants_split(const DevBsr& m, bool uniform_lanes);
 
 // Splits the rows of a block matrix into groups of at most `target` value bytes (a longer row is
 // a group of its own) and chooses the lanes per row from the mean blocks per row.
@@ -205,6 +218,11 @@ template <typename S>
 sf_status setup_sell_fill(cudaStream_t st, size_t slots, int len, const uint32_t* sell_rows, const uint32_t* sell_len,
                           const uint32_t* sell_start, uint32_t nrows, const uint32_t* starts, const uint32_t* cols,
                           const double* in, uint32_t* out_cols, S* out);
+// The split-row copy of a 6 x cb block CSR matrix (cb 3 or 6), converted to S.
+template <typename S>
+sf_status setup_split_fill(cudaStream_t st, size_t slots, int cb, const uint32_t* sell_rows, const uint32_t* sell_len,
+                           const uint32_t* sell_start, uint32_t nrows, const uint32_t* starts, const uint32_t* cols,
+                           const double* in, uint32_t* out_cols, S* out);
 
 // ------------------------------------------------------------------- assembly (assembly.cu)
 struct AssemblyDevice {

@@ -335,6 +335,33 @@ __global__ void sell_fill_kernel(size_t slots, const uint32_t* __restrict__ sell
   }
 }
 
+// Fills a split-row copy of a 6 x CB block CSR matrix: lane t = 6 m + p of a slice places row p
+// of each block of its block row as a 1 x CB block at its chunked SELL position; the lane with
+// p = 0 also places the block's column in the block row's shared column chunk.
+template <typename S, int CB>
+__global__ void split_fill_kernel(size_t slots, const uint32_t* __restrict__ sell_rows, const uint32_t* __restrict__ sell_len,
+                                  const uint32_t* __restrict__ sell_start, uint32_t nrows,
+                                  const uint32_t* __restrict__ starts, const uint32_t* __restrict__ cols,
+                                  const double* __restrict__ in, uint32_t* __restrict__ out_cols, S* __restrict__ out) {
+  constexpr int U = sell_chunk_blocks(CB, (int)sizeof(S));
+  constexpr int VEC = 16 / (int)sizeof(S);
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < slots; i += (size_t)gridDim.x * blockDim.x) {
+    const uint32_t row = sell_rows[i];
+    if (row >= nrows) continue;
+    const uint32_t s = (uint32_t)(i / 32), t = (uint32_t)(i % 32), m = t / 6, p = t % 6;
+    const uint32_t n = sell_len[i], b0 = starts[row];
+    const size_t cbase = (size_t)(sell_start[s] / 32) * kSplitRowsPerSlice + (size_t)m * U;
+    for (uint32_t k = 0; k < n; ++k) {
+      const uint32_t c = k / U, u = k % U;
+      const size_t q = sell_start[s] + 32 * (size_t)(c * U) + t * U + u;
+      if (p == 0) out_cols[cbase + (size_t)kSplitRowsPerSlice * U * c + u] = cols[b0 + k];
+#pragma unroll
+      for (int e = 0; e < CB; ++e)
+        out[sell_value_offset(q, CB, U, VEC, e)] = (S)in[(size_t)(b0 + k) * 6 * CB + p * CB + e];
+    }
+  }
+}
+
 // Copies listed blocks out of (gather) or back into (scatter) a block array.
 __global__ void gather_blocks_kernel(size_t count, int len, const uint32_t* __restrict__ idx,
                                      const double* __restrict__ in, double* __restrict__ out) {
@@ -496,6 +523,26 @@ sf_status setup_sell_fill(cudaStream_t st, size_t slots, int len, const uint32_t
   }
   return cuda_check(cudaGetLastError(), "SELL fill");
 }
+template <typename S>
+sf_status setup_split_fill(cudaStream_t st, size_t slots, int cb, const uint32_t* sell_rows, const uint32_t* sell_len,
+                           const uint32_t* sell_start, uint32_t nrows, const uint32_t* starts, const uint32_t* cols,
+                           const double* in, uint32_t* out_cols, S* out) {
+  if (slots == 0) return SF_OK;
+  if (cb == 3)
+    split_fill_kernel<S, 3><<<grid_for(slots), kT, 0, st>>>(slots, sell_rows, sell_len, sell_start, nrows, starts, cols,
+                                                           in, out_cols, out);
+  else if (cb == 6)
+    split_fill_kernel<S, 6><<<grid_for(slots), kT, 0, st>>>(slots, sell_rows, sell_len, sell_start, nrows, starts, cols,
+                                                           in, out_cols, out);
+  else
+    return fail(SF_INVALID_ARGUMENT, "unsupported block size for the split-row layout");
+  return cuda_check(cudaGetLastError(), "split fill");
+}
+template sf_status setup_split_fill<float>(cudaStream_t, size_t, int, const uint32_t*, const uint32_t*, const uint32_t*,
+                                           uint32_t, const uint32_t*, const uint32_t*, const double*, uint32_t*, float*);
+template sf_status setup_split_fill<double>(cudaStream_t, size_t, int, const uint32_t*, const uint32_t*, const uint32_t*,
+                                            uint32_t, const uint32_t*, const uint32_t*, const double*, uint32_t*, double*);
+
 template sf_status setup_sell_fill<float>(cudaStream_t, size_t, int, const uint32_t*, const uint32_t*, const uint32_t*,
                                           uint32_t, const uint32_t*, const uint32_t*, const double*, uint32_t*, float*);
 template sf_status setup_sell_fill<double>(cudaStream_t, size_t, int, const uint32_t*, const uint32_t*, const uint32_t*,

@@ -515,6 +515,11 @@ __device__ __forceinline__ void coarse_solve_kernel(uint32_t n, const double* __
 }
 
 // ------------------------------------------------------------ fixed-order reductions
+// The conjugate gradient's vector kernels walk [0, n) with a grid stride. A thread loads the
+// elements of kStrides consecutive strides before it uses any of them (one round trip to memory
+// instead of kStrides dependent ones) and then sums them in stride order: the same order, and so
+// the same bits, as the plain loop.
+constexpr int kStrides = 4;
 __device__ __forceinline__ double block_sum(double v, double* sh) {
   int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
@@ -778,6 +783,182 @@ __device__ __forceinline__ void sell_cheb_kernel(SellOp<S> A, const S* __restric
   sell_rows<S, V, RB, RB, false>(A, d_old, epi);
 }
 
+// ------------------------------------------------------------ split rows: one thread per scalar row
+// For operators of 6-row blocks with many block rows (level 1, and the transpose restricting onto
+// it): one lane per scalar row gives six times the threads of SELL-32 and a chain of chunks one
+// sixth as long per thread, with no shared memory. Lane t = 6 m + p of a slice owns scalar row p
+// of the slice's block row m; the six lanes of a block row read its shared column chunk (one
+// address per block row) and gather the same x entries. Each block's cb products are summed in
+// column order, a chunk's block sums pairwise, and the chunk sums in column order: a row of an
+// f32 level is summed about as accurately as the row-group engine's lane sums and butterfly
+// (a plain running sum over the row's ~100 products left the f32 cycle visibly noisier).
+template <int U>
+__device__ __forceinline__ void load_cols_shared(const uint32_t* p, uint32_t (&c)[U]) {
+  if constexpr (U % 4 == 0) {
+#pragma unroll
+    for (int k = 0; k < U / 4; ++k) {
+      uint4 w = __ldg(reinterpret_cast<const uint4*>(p) + k);
+      c[4 * k] = w.x;
+      c[4 * k + 1] = w.y;
+      c[4 * k + 2] = w.z;
+      c[4 * k + 3] = w.w;
+    }
+  } else if constexpr (U % 2 == 0) {
+#pragma unroll
+    for (int k = 0; k < U / 2; ++k) {
+      uint2 w = __ldg(reinterpret_cast<const uint2*>(p) + k);
+      c[2 * k] = w.x;
+      c[2 * k + 1] = w.y;
+    }
+  } else {
+#pragma unroll
+    for (int u = 0; u < U; ++u) c[u] = __ldg(p + u);
+  }
+}
+
+template <typename S, typename V, int CB, class Epi>
+__device__ __forceinline__ void split_rows(const SellOp<S>& A, const V* __restrict__ x, Epi& epi) {
+  constexpr int U = sell_chunk_blocks(CB, (int)sizeof(S));
+  constexpr int VEC = 16 / (int)sizeof(S);
+  constexpr int NV = U * CB / VEC;
+  static_assert((U * CB) % VEC == 0, "a lane chunk is whole 16-byte vectors");
+  typedef typename Vec16<S>::type W;
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t m = lane / 6, part = lane - 6 * m;
+  const uint32_t warps = blockDim.x >> 5;
+  for (uint32_t s = blockIdx.x * warps + (threadIdx.x >> 5); s < A.nslices; s += gridDim.x * warps) {
+    const uint32_t slot = s * 32 + lane;
+    const uint32_t row = A.rows[slot];
+    const uint32_t n = A.len[slot];
+    const bool live = row < A.nrows;
+    epi.pre(row, part, live);
+    V acc = V(0);
+    const uint32_t base = A.start[s];
+    const uint32_t* cp = A.cols + (size_t)(base >> 5) * kSplitRowsPerSlice + (size_t)m * U;
+    uint32_t cn[U];
+    S vn[U * CB];
+    if (n > 0) {
+      load_cols_shared<U>(cp, cn);
+      const W* vp = reinterpret_cast<const W*>(A.vals + (size_t)base * CB) + lane;
+#pragma unroll
+      for (int q = 0; q < NV; ++q) Vec16<S>::split(__ldcs(vp + 32 * q), vn + q * VEC);
+    }
+    for (uint32_t k0 = 0; k0 < n; k0 += U) {
+      uint32_t c[U];
+      S v[U * CB];
+#pragma unroll
+      for (int u = 0; u < U; ++u) c[u] = cn[u];
+#pragma unroll
+      for (int i = 0; i < U * CB; ++i) v[i] = vn[i];
+      if (k0 + U < n) {
+        load_cols_shared<U>(cp + (size_t)kSplitRowsPerSlice * (k0 + U), cn);
+        const W* vp = reinterpret_cast<const W*>(A.vals + ((size_t)base + 32 * (k0 + U)) * CB) + lane;
+#pragma unroll
+        for (int q = 0; q < NV; ++q) Vec16<S>::split(__ldcs(vp + 32 * q), vn + q * VEC);
+      }
+      V xv[U][CB];
+#pragma unroll
+      for (int u = 0; u < U; ++u)
+#pragma unroll
+        for (int q = 0; q < CB; ++q) xv[u][q] = k0 + u < n ? __ldg(x + (size_t)c[u] * CB + q) : V(0);
+      V bs[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        bs[u] = V(v[u * CB]) * xv[u][0];
+#pragma unroll
+        for (int q = 1; q < CB; ++q) bs[u] += V(v[u * CB + q]) * xv[u][q];
+      }
+#pragma unroll
+      for (int w = 1; w < U; w *= 2)
+#pragma unroll
+        for (int u = 0; u + w < U; u += 2 * w) bs[u] += bs[u + w];
+      acc += bs[0];
+    }
+    epi.post(row, part, live, acc);
+  }
+}
+
+template <typename V, int OP>
+struct SplitAxpy {
+  V* __restrict__ y;
+  const V* __restrict__ b;
+  V in;
+  __device__ __forceinline__ void pre(uint32_t row, uint32_t part, bool live) {
+    if (OP == OP_SET || !live) return;
+    const size_t i = (size_t)row * 6 + part;
+    in = OP == OP_RESIDUAL ? b[i] : y[i];
+  }
+  __device__ __forceinline__ void post(uint32_t row, uint32_t part, bool live, V acc) {
+    if (!live) return;
+    const size_t i = (size_t)row * 6 + part;
+    if (OP == OP_SET) y[i] = acc;
+    if (OP == OP_RESIDUAL) y[i] = in - acc;
+    if (OP == OP_ADD) y[i] = in + acc;
+  }
+};
+
+template <typename S, typename V, int CB, int OP>
+__device__ __forceinline__ void split_kernel(SellOp<S> A, const V* __restrict__ x, V* __restrict__ y,
+                                             const V* __restrict__ b, const int* __restrict__ status) {
+  if (*status != ST_ACTIVE) return;
+  SplitAxpy<V, OP> epi{y, b, V(0)};
+  split_rows<S, V, CB>(A, x, epi);
+}
+
+// The fused Chebyshev step with split rows. z = D^-1 r couples a block row's six components:
+// each lane's new residual reaches the other five lanes of its block row by shuffles (every
+// lane of the warp takes part; idle lanes carry zeros), then lane p forms row p of D^-1 r in
+// the order of cheb_step_kernel.
+template <typename S, typename V>
+struct SplitCheb {
+  const S* __restrict__ dinv;
+  const V* __restrict__ d_old;
+  V* __restrict__ d_new;
+  V* __restrict__ r;
+  V* __restrict__ x;
+  V* __restrict__ outer;
+  V keep, step;
+  __device__ __forceinline__ void pre(uint32_t, uint32_t, bool) {}
+  __device__ __forceinline__ void post(uint32_t row, uint32_t part, bool live, V acc) {
+    const size_t i = (size_t)row * 6 + part;
+    const V rn = live ? r[i] - acc : V(0);
+    const uint32_t first = (threadIdx.x & 31) - part;
+    V rq[6];
+#pragma unroll
+    for (int q = 0; q < 6; ++q) rq[q] = __shfl_sync(kFull, rn, (first + q) & 31);
+    if (!live) return;
+    V z = V(0);
+#pragma unroll
+    for (int q = 0; q < 6; ++q) z += V(dinv[i * 6 + q]) * rq[q];
+    const V dn = keep * d_old[i] + step * z;
+    r[i] = rn;
+    d_new[i] = dn;
+    const V xn = x[i] + dn;
+    if (outer)
+      outer[i] = outer[i] + xn;
+    else
+      x[i] = xn;
+  }
+};
+
+template <typename S, typename V>
+__device__ __forceinline__ void split_cheb_kernel(SellOp<S> A, const S* __restrict__ dinv,
+                                                  const V* __restrict__ d_old, V* __restrict__ d_new,
+                                                  V* __restrict__ r, V* __restrict__ x, V* __restrict__ outer,
+                                                  V keep, V step, const int* __restrict__ status) {
+  if (*status != ST_ACTIVE) return;
+  SplitCheb<S, V> epi;
+  epi.dinv = dinv;
+  epi.d_old = d_old;
+  epi.d_new = d_new;
+  epi.r = r;
+  epi.x = x;
+  epi.outer = outer;
+  epi.keep = keep;
+  epi.step = step;
+  split_rows<S, V, 6>(A, d_old, epi);
+}
+
 struct SellDot {
   const double* __restrict__ p;
   double* __restrict__ ap;
@@ -929,11 +1110,27 @@ __device__ __forceinline__ void pcg_update_kernel(uint32_t n, const double* __re
   if (st->status != ST_ACTIVE) return;
   double alpha = st->alpha, na = -alpha;
   double local = 0.0;
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    x[i] += alpha * p[i];
-    double rv = r[i] + na * ap[i];
-    r[i] = rv;
-    local += rv * rv;
+  const size_t stride = (size_t)gridDim.x * blockDim.x;
+  for (size_t i0 = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i0 < n; i0 += kStrides * stride) {
+    double pv[kStrides], av[kStrides], xv[kStrides], rv[kStrides];
+#pragma unroll
+    for (int k = 0; k < kStrides; ++k) {
+      const size_t i = i0 + k * stride;
+      const bool in = i < n;
+      pv[k] = in ? p[i] : 0.0;
+      av[k] = in ? ap[i] : 0.0;
+      xv[k] = in ? x[i] : 0.0;
+      rv[k] = in ? r[i] : 0.0;
+    }
+#pragma unroll
+    for (int k = 0; k < kStrides; ++k) {
+      const size_t i = i0 + k * stride;
+      if (i >= n) break;
+      x[i] = xv[k] + alpha * pv[k];
+      double rn = rv[k] + na * av[k];
+      r[i] = rn;
+      local += rn * rn;
+    }
   }
   double v[1] = {local}, total[1];
   if (finish_partials<1>(v, partials, &st->tickets[1], total) && threadIdx.x == 0) {
@@ -1017,10 +1214,23 @@ __device__ __forceinline__ void pcg_dot_rz_kernel(uint32_t n, const double* __re
   if (st->status != ST_ACTIVE) return;
   bool flex = st->flexible && st->mode == MODE_NORMAL;
   double rz = 0.0, apz = 0.0;
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    double zv = (double)z[i];
-    rz += r[i] * zv;
-    if (flex) apz += ap[i] * zv;
+  const size_t stride = (size_t)gridDim.x * blockDim.x;
+  for (size_t i0 = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i0 < n; i0 += kStrides * stride) {
+    double zv[kStrides], rv[kStrides], av[kStrides];
+#pragma unroll
+    for (int k = 0; k < kStrides; ++k) {
+      const size_t i = i0 + k * stride;
+      const bool in = i < n;
+      zv[k] = in ? (double)z[i] : 0.0;
+      rv[k] = in ? r[i] : 0.0;
+      av[k] = in && flex ? ap[i] : 0.0;
+    }
+#pragma unroll
+    for (int k = 0; k < kStrides; ++k) {
+      if (i0 + k * stride >= n) break;
+      rz += rv[k] * zv[k];
+      if (flex) apz += av[k] * zv[k];
+    }
   }
   double v[2] = {rz, apz}, total[2];
   if (finish_partials<2>(v, partials, &st->tickets[3], total) && threadIdx.x == 0) {
@@ -1043,9 +1253,22 @@ __device__ __forceinline__ void pcg_update_p_kernel(uint32_t n, const Z* __restr
   if (st->status != ST_ACTIVE) return;
   bool restart = st->mode == MODE_RESTART;
   double beta = st->beta;
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    double zv = (double)z[i];
-    p[i] = restart ? zv : zv + beta * p[i];
+  const size_t stride = (size_t)gridDim.x * blockDim.x;
+  for (size_t i0 = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i0 < n; i0 += kStrides * stride) {
+    double zv[kStrides], pv[kStrides];
+#pragma unroll
+    for (int k = 0; k < kStrides; ++k) {
+      const size_t i = i0 + k * stride;
+      const bool in = i < n;
+      zv[k] = in ? (double)z[i] : 0.0;
+      pv[k] = in && !restart ? p[i] : 0.0;
+    }
+#pragma unroll
+    for (int k = 0; k < kStrides; ++k) {
+      const size_t i = i0 + k * stride;
+      if (i >= n) break;
+      p[i] = restart ? zv[k] : zv[k] + beta * pv[k];
+    }
   }
 }
 
@@ -1151,8 +1374,20 @@ void launch_bsr(const DevBsr& m, const V* x, V* y, const V* b, const int* status
   }
 }
 
+template <typename S, typename V, int OP>
+void launch_split(const DevBsr& m, const V* x, V* y, const V* b, const int* status, cudaStream_t st) {
+  if (m.cb == 3)
+    launch_body<split_kernel<S, V, 3, OP>>(grid_for_slices(m.nslices), kThreads, 0, st, sell_of<S>(m), x, y, b, status);
+  else
+    launch_body<split_kernel<S, V, 6, OP>>(grid_for_slices(m.nslices), kThreads, 0, st, sell_of<S>(m), x, y, b, status);
+}
+
 template <typename S, typename V, int RB, int OP>
 void bsr_dispatch_cb(const DevBsr& m, const V* x, V* y, const V* b, const int* status, cudaStream_t st) {
+  if (RB == 6 && m.split) {
+    launch_split<S, V, OP>(m, x, y, b, status, st);
+    return;
+  }
   if (m.cb == 3)
     launch_bsr<S, V, RB, 3, OP>(m, x, y, b, status, st);
   else
@@ -1179,6 +1414,13 @@ void launch_cheb_step_lpr(const DevLevel& L, const V* d_old, V* d_new, V* r, V* 
 template <typename S, typename V, int RB>
 void launch_cheb_step(const DevLevel& L, const V* d_old, V* d_new, V* r, V* x, V* outer, double keep, double step,
                       const int* status, cudaStream_t st) {
+  if constexpr (RB == 6) {
+    if (L.a.split) {
+      launch_body<split_cheb_kernel<S, V>>(grid_for_slices(L.a.nslices), kThreads, 0, st, sell_of<S>(L.a),
+                                           (const S*)L.dinv, d_old, d_new, r, x, outer, (V)keep, (V)step, status);
+      return;
+    }
+  }
   if (L.a.sell) {
     launch_body<sell_cheb_kernel<S, V, RB>>(grid_for_slices(L.a.nslices), kThreads, 0, st,
         sell_of<S>(L.a), (const S*)L.dinv, d_old, d_new, r, x, outer, (V)keep, (V)step, status);
@@ -1372,6 +1614,10 @@ bool wants_sell(const DevBsr& m, uint64_t sell_min_rows) {
   return m.rows >= sell_min_rows || 2 * slot > kMaxStagePerWarp;
 }
 
+bool wants_split(const DevBsr& m, bool uniform_lanes) {
+  return !uniform_lanes && m.rb == 6 && (m.cb == 3 || m.cb == 6) && m.rows >= kSplitMinRows;
+}
+
 void dev_free(DeviceSolver& s, void* ptr) {
   if (!ptr) return;
   for (size_t i = 0; i < s.owned.size(); ++i)
@@ -1470,14 +1716,47 @@ SellLayout sell_layout(uint32_t nrows, const uint32_t* starts, uint32_t chunk) {
   return L;
 }
 
-sf_status upload_sell_layout(DeviceSolver& s, DevBsr& m, const SellLayout& L, size_t value_bytes) {
+// Block rows ordered as sell_layout orders rows, kSplitRowsPerSlice to a slice, six lanes each
+// (lane 6 m + p: scalar row p of the slice's block row m; lanes 30 and 31 idle), slice widths
+// padded to chunks of `chunk` blocks.
+SellLayout split_layout(uint32_t nrows, const uint32_t* starts, uint32_t chunk) {
+  SellLayout L;
+  L.nslices = (nrows + kSplitRowsPerSlice - 1) / kSplitRowsPerSlice;
+  std::vector<uint32_t> order(nrows);
+  for (uint32_t i = 0; i < nrows; ++i) order[i] = i;
+  auto rlen = [&](uint32_t r) { return starts[r + 1] - starts[r]; };
+  for (uint32_t w0 = 0; w0 < nrows; w0 += kSellWindow) {
+    uint32_t w1 = std::min(nrows, w0 + kSellWindow);
+    std::stable_sort(order.begin() + w0, order.begin() + w1, [&](uint32_t a, uint32_t b) { return rlen(a) > rlen(b); });
+  }
+  L.rows.assign((size_t)L.nslices * 32, nrows);
+  L.len.assign((size_t)L.nslices * 32, 0);
+  L.start.assign(L.nslices + 1, 0);
+  for (uint32_t i = 0; i < nrows; ++i) {
+    const size_t sl = i / kSplitRowsPerSlice, m = i % kSplitRowsPerSlice;
+    for (uint32_t p = 0; p < 6; ++p) {
+      L.rows[sl * 32 + 6 * m + p] = order[i];
+      L.len[sl * 32 + 6 * m + p] = rlen(order[i]);
+    }
+  }
+  for (uint32_t sl = 0; sl < L.nslices; ++sl) {
+    uint32_t width = 0;
+    for (uint32_t t = 0; t < 32; ++t) width = std::max(width, L.len[sl * 32 + t]);
+    width = (width + chunk - 1) / chunk * chunk;
+    L.start[sl + 1] = L.start[sl] + 32 * width;
+  }
+  return L;
+}
+
+sf_status upload_sell_layout(DeviceSolver& s, DevBsr& m, const SellLayout& L, size_t value_bytes, bool split) {
   m.nslices = L.nslices;
   sf_status e = SF_OK;
   if (!e) e = dev_alloc(s, (void**)&m.sell_rows, L.rows.size() * 4);
   if (!e) e = dev_alloc(s, (void**)&m.sell_len, L.len.size() * 4);
   if (!e) e = dev_alloc(s, (void**)&m.sell_start, L.start.size() * 4);
   const size_t slots = L.start[L.nslices];
-  if (!e) e = dev_alloc(s, (void**)&m.sell_cols, std::max<size_t>(1, slots) * 4);
+  const size_t col_slots = split ? slots / 32 * kSplitRowsPerSlice : slots;
+  if (!e) e = dev_alloc(s, (void**)&m.sell_cols, std::max<size_t>(1, col_slots) * 4);
   if (!e) e = dev_alloc(s, &m.sell_vals, std::max<size_t>(1, slots) * value_bytes);
   if (e) return e;
   copy_h2d(s, m.sell_rows, L.rows.data(), L.rows.size() * 4);
@@ -1494,11 +1773,23 @@ sf_status make_sell_converted(DeviceSolver& s, DevBsr& m, const uint32_t* starts
                               const double* vals) {
   const int len = (int)(m.rb * m.cb);
   SellLayout L = sell_layout(m.rows, starts, (uint32_t)sell_chunk_blocks(len, (int)sizeof(S)));
-  if (sf_status e = upload_sell_layout(s, m, L, (size_t)len * sizeof(S))) return e;
+  if (sf_status e = upload_sell_layout(s, m, L, (size_t)len * sizeof(S), false)) return e;
   sf_status e = setup_sell_fill<S>(s.stream, (size_t)L.nslices * 32, len, m.sell_rows, m.sell_len, m.sell_start, m.rows,
                                    m.starts, m.cols, vals, m.sell_cols, (S*)m.sell_vals);
   if (!e) e = cuda_check(cudaStreamSynchronize(s.stream), "SELL placement");
   m.sell = true;
+  return e;
+}
+
+// The split-row copy of a 6 x cb matrix from its f64 values on the device, converted to S.
+template <typename S>
+sf_status make_split_converted(DeviceSolver& s, DevBsr& m, const uint32_t* starts, const double* vals) {
+  SellLayout L = split_layout(m.rows, starts, (uint32_t)sell_chunk_blocks((int)m.cb, (int)sizeof(S)));
+  if (sf_status e = upload_sell_layout(s, m, L, (size_t)m.cb * sizeof(S), true)) return e;
+  sf_status e = setup_split_fill<S>(s.stream, (size_t)L.nslices * 32, (int)m.cb, m.sell_rows, m.sell_len, m.sell_start,
+                                    m.rows, m.starts, m.cols, vals, m.sell_cols, (S*)m.sell_vals);
+  if (!e) e = cuda_check(cudaStreamSynchronize(s.stream), "split-row placement");
+  m.split = true;
   return e;
 }
 
@@ -1528,8 +1819,11 @@ sf_status device_bsr(DeviceSolver& s, const Bsr& h, DevBsr& d, bool alias) {
     if (sf_status e = setup_convert<S>(s.stream, n, h.dev, (S*)d.vals)) return e;
   }
   if (sf_status e = make_row_groups(s, d, h.starts.data(), h.rb * h.cb * sizeof(S))) return e;
-  if (wants_sell(d, s.sell_min_rows))
+  if (wants_split(d, s.uniform_lanes)) {
+    if (sf_status e = make_split_converted<S>(s, d, h.starts.data(), h.dev)) return e;
+  } else if (wants_sell(d, s.sell_min_rows)) {
     if (sf_status e = make_sell_converted<S>(s, d, h.starts.data(), h.cols.data(), h.dev)) return e;
+  }
   return cuda_check(cudaGetLastError(), "level operator");
 }
 
