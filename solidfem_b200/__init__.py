@@ -46,7 +46,8 @@ class _Options(C.Structure):
                 ("neighbour_reach", C.c_double), ("coarse_dofs", C.c_uint64), ("max_levels", C.c_uint64),
                 ("smoother_degree", C.c_uint64), ("smoother_range", C.c_double), ("precision", C.c_int32),
                 ("threads", C.c_uint64), ("device", C.c_int32), ("use_graphs", C.c_int32),
-                ("device_memory_budget", C.c_uint64), ("sell_min_rows", C.c_uint64), ("batchable", C.c_int32)]
+                ("device_memory_budget", C.c_uint64), ("sell_min_rows", C.c_uint64), ("batchable", C.c_int32),
+                ("coarse_tail", C.c_int32)]
 
 
 class _BuildProgress(C.Structure):
@@ -92,7 +93,9 @@ class _LevelInfo(C.Structure):
 
 class _DeviceTiming(C.Structure):
     _fields_ = [("step_ms", C.c_double), ("assembly_ms", C.c_double), ("setup_ms", C.c_double),
-                ("kernel_launches", C.c_uint64), ("h2d_bytes", C.c_uint64), ("d2h_bytes", C.c_uint64)]
+                ("kernel_launches", C.c_uint64), ("h2d_bytes", C.c_uint64), ("d2h_bytes", C.c_uint64),
+                ("launches_per_iteration", C.c_uint64), ("coarse_tail_level", C.c_int32),
+                ("coarse_tail_cluster", C.c_uint32)]
 
 
 class _KernelTiming(C.Structure):
@@ -493,6 +496,7 @@ class StudyOptions:
     device_memory_budget: int = 0
     sell_min_rows: int = 0
     batchable: bool = False
+    coarse_tail: bool = False
 
     def _c(self) -> _Options:
         o = _Options()
@@ -516,6 +520,7 @@ class StudyOptions:
         o.device_memory_budget = self.device_memory_budget
         o.sell_min_rows = self.sell_min_rows
         o.batchable = 1 if self.batchable else 0
+        o.coarse_tail = 1 if self.coarse_tail else 0
         return o
 
 

@@ -144,6 +144,10 @@ struct DeviceSolver {
   mutable uint64_t h2d_bytes = 0, d2h_bytes = 0;
   uint64_t sell_min_rows = 32768;  // operators with at least this many rows use SELL-32
   bool uniform_lanes = false;      // lanes per row by block shape alone (batchable studies)
+  bool coarse_tail = false;        // fuse the last smoothed level and the coarse solve when they fit
+  int tail_level = -1;             // the level whose cycle runs as one cluster launch, or -1
+  unsigned tail_cluster = 0;       // CTAs of that cluster
+  size_t tail_smem = 0;            // shared memory of each of its CTAs
 };
 
 // One recorded kernel launch: the batched form of the kernel, its launch shape and the bytes of its
@@ -153,6 +157,7 @@ struct LaunchRecord {
   const void* batched = nullptr;
   dim3 grid, block;
   size_t smem = 0;
+  unsigned cluster = 0;  // CTAs per thread-block cluster (grid.x), 0 for a plain launch
   std::vector<unsigned char> pack;
 };
 extern thread_local std::vector<LaunchRecord>* g_recorder;

@@ -90,6 +90,19 @@ __global__ void __launch_bounds__(kThreads) batched_kernel(const PackT* __restri
   apply_pack<Body>(a);
 }
 
+// The same wrappers for a body launched with `Threads` threads per block (the coarse tail).
+template <auto Body, int Threads, typename... P>
+__global__ void __launch_bounds__(Threads) single_kernel_n(P... args) {
+  pdl_enter();
+  Body(args...);
+}
+template <auto Body, int Threads, typename PackT>
+__global__ void __launch_bounds__(Threads) batched_kernel_n(const PackT* __restrict__ table) {
+  pdl_enter();
+  const PackT a = table[blockIdx.y];
+  apply_pack<Body>(a);
+}
+
 template <typename F>
 struct BodyTraits;
 template <typename... P>
@@ -106,6 +119,14 @@ struct BodyTraits<void (*)(P...)> {
   template <auto Body>
   static const void* batched() {
     return (const void*)batched_kernel<Body, PackT>;
+  }
+  template <auto Body, int Threads>
+  static const void* single_n() {
+    return (const void*)single_kernel_n<Body, Threads, P...>;
+  }
+  template <auto Body, int Threads>
+  static const void* batched_n() {
+    return (const void*)batched_kernel_n<Body, Threads, PackT>;
   }
 };
 
@@ -156,6 +177,42 @@ void launch_body(dim3 grid, dim3 block, size_t smem, cudaStream_t st, A&&... arg
   void* argv[sizeof...(A) + 1];
   fill_argv(argv, pk);
   cudaLaunchKernelExC(&cfg, k, argv);
+}
+
+// A launch of `grid.x` CTAs of Threads threads forming one thread-block cluster per grid row (no
+// programmatic serialization: the launch waits for its predecessor in stream order).
+template <auto Body, int Threads, typename... A>
+void launch_body_cluster(dim3 grid, size_t smem, cudaStream_t st, A&&... args) {
+  typedef BodyTraits<decltype(Body)> T;
+  typename T::PackT pk = T::pack(std::forward<A>(args)...);
+  const dim3 block(Threads);
+  if (g_recorder) {
+    LaunchRecord r;
+    r.batched = T::template batched_n<Body, Threads>();
+    r.grid = grid;
+    r.block = block;
+    r.smem = smem;
+    r.cluster = grid.x;
+    r.pack.resize(sizeof(pk));
+    std::memcpy(r.pack.data(), &pk, sizeof(pk));
+    g_recorder->push_back(std::move(r));
+    return;
+  }
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = grid.x;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  void* argv[sizeof...(A) + 1];
+  fill_argv(argv, pk);
+  cudaLaunchKernelExC(&cfg, T::template single_n<Body, Threads>(), argv);
 }
 
 // ------------------------------------------------------------ asynchronous staging
@@ -959,6 +1016,515 @@ __device__ __forceinline__ void split_cheb_kernel(SellOp<S> A, const S* __restri
   split_rows<S, V, 6>(A, d_old, epi);
 }
 
+// ------------------------------------------------------------ the coarse tail: one cluster launch
+// The last smoothed level s and the coarsest level's direct solve run as ONE launch of one
+// thread-block cluster per instance (cycle.rs:461-539 for levels s and s + 1): smoother start,
+// Chebyshev steps, residual, restriction, coarse solve, prolongation, residual and post-smoother
+// are phases whose rows are split over the cluster's CTAs, which meet at the hardware cluster
+// barrier between phases (arrive.release / wait.acquire at cluster scope; no spin loop of ours).
+// A level this small runs each per-phase launch as a few waves of short warps, so the launches,
+// not the bytes, set its time. Each CTA stages its share of the rows (operator, prolongator,
+// restriction, D^-1, coarse inverse) in shared memory once; the vectors that phases gather live
+// as a replica in every CTA, and a phase stores each result into all replicas through distributed
+// shared memory, so a phase reads nothing but shared memory. Products use the row-group engine's
+// lanes per row, loop order and butterfly, and the epilogues restate EpiAxpy / EpiCheb /
+// cheb_start_kernel / coarse_solve_kernel term for term: the tail returns the bits of the
+// per-phase launches it replaces. Only the level's final x goes back to global memory.
+// Opt-in (sf_study_options.coarse_tail): measured on the 606k-DOF plate, the cluster launch takes
+// 44 us against about 37 us for the overlapped per-phase launches; its phases stall on
+// instruction fetch and on the cluster barriers rather than on memory.
+constexpr int kTailMaxSteps = 4;
+// Threads per CTA: 512 for f32 vectors, 256 for f64 (twice the registers per value).
+template <typename V>
+constexpr int tail_threads() {
+  return sizeof(V) == 4 ? 512 : 256;
+}
+constexpr uint32_t kTailMaxRows = 768;     // block rows of the fused level: a few rows per warp
+constexpr uint32_t kTailMaxCoarse = 1024;  // scalar rows of the coarsest level
+constexpr size_t kTailMaxSmem = 200 * 1024;
+
+__device__ __forceinline__ void cluster_barrier() {
+  __syncwarp();  // the barrier's .aligned form wants the warp converged
+  asm volatile("barrier.cluster.arrive.release.aligned;\n"
+               "barrier.cluster.wait.acquire.aligned;\n" ::: "memory");
+}
+
+template <typename S>
+struct TailMat {
+  const uint32_t* __restrict__ starts;
+  const uint32_t* __restrict__ cols;
+  const S* __restrict__ vals;
+  uint32_t rows;
+  int lanes;  // lanes per row of the operator's row-group launch
+};
+
+template <typename S, typename V>
+struct TailArgs {
+  TailMat<S> a, r, p;
+  const S* dinv;
+  const double* inv;  // coarsest level: n x n f64 inverse
+  uint32_t nc;
+  uint32_t nsteps;
+  V theta;
+  V keep[kTailMaxSteps], step[kTailMaxSteps];
+  const V* b;
+  V* x;
+  const int* status;
+};
+
+// The rows of a phase that CTA i of n takes: [share(rows, n, i), share(rows, n, i + 1)).
+__host__ __device__ inline uint32_t tail_share(uint32_t rows, uint32_t n, uint32_t i) {
+  return (uint32_t)(((uint64_t)rows * i) / n);
+}
+__host__ __device__ inline size_t tail_align(size_t bytes) { return (bytes + 15) & ~size_t(15); }
+
+// Shared memory the staged rows of one operator take (starts, columns, 6 x 6 blocks).
+__host__ __device__ inline size_t tail_mat_bytes(uint32_t rows, uint32_t blocks, size_t value_bytes) {
+  return tail_align((size_t)(rows + 1) * 4) + tail_align((size_t)blocks * 4) + tail_align((size_t)blocks * 36 * value_bytes);
+}
+
+// Rows [row0, row0 + rows) of an operator staged in this CTA's shared memory (starts from 0).
+template <typename S>
+struct LocalMat {
+  const uint32_t* starts;
+  const uint32_t* cols;
+  const S* vals;
+  uint32_t row0, rows;
+};
+
+// Copies n 16-byte words to shared memory, eight loads in flight per thread before any store.
+__device__ __forceinline__ void stage16(float4* __restrict__ dst, const float4* __restrict__ src, size_t n) {
+  for (size_t i0 = threadIdx.x; i0 < n; i0 += 8 * (size_t)blockDim.x) {
+    float4 w[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      const size_t i = i0 + (size_t)k * blockDim.x;
+      if (i < n) w[k] = __ldg(src + i);
+    }
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      const size_t i = i0 + (size_t)k * blockDim.x;
+      if (i < n) dst[i] = w[k];
+    }
+  }
+}
+
+template <typename S>
+__device__ __forceinline__ LocalMat<S> tail_stage(const TailMat<S>& A, uint32_t r0, uint32_t r1, unsigned char*& at) {
+  const uint32_t b0 = A.starts[r0], b1 = A.starts[r1];
+  uint32_t* st = reinterpret_cast<uint32_t*>(at);
+  at += tail_align((size_t)(r1 - r0 + 1) * 4);
+  uint32_t* cl = reinterpret_cast<uint32_t*>(at);
+  at += tail_align((size_t)(b1 - b0) * 4);
+  S* vl = reinterpret_cast<S*>(at);
+  at += tail_align((size_t)(b1 - b0) * 36 * sizeof(S));
+  for (uint32_t i = threadIdx.x; i <= r1 - r0; i += blockDim.x) st[i] = A.starts[r0 + i] - b0;
+  for (uint32_t i = threadIdx.x; i < b1 - b0; i += blockDim.x) cl[i] = __ldg(A.cols + b0 + i);
+  stage16(reinterpret_cast<float4*>(vl), reinterpret_cast<const float4*>(A.vals + (size_t)b0 * 36),
+          (size_t)(b1 - b0) * 36 * sizeof(S) / 16);
+  LocalMat<S> m;
+  m.starts = st;
+  m.cols = cl;
+  m.vals = vl;
+  m.row0 = r0;
+  m.rows = r1 - r0;
+  return m;
+}
+
+// Row p of a staged 6 x 6 block: 24 bytes (f32, 8-byte aligned) or 48 bytes (f64, 16-byte aligned).
+__device__ __forceinline__ void block_row(const float* src, float (&v)[6]) {
+  const float2* w = reinterpret_cast<const float2*>(src);
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    float2 t = w[i];
+    v[2 * i] = t.x;
+    v[2 * i + 1] = t.y;
+  }
+}
+__device__ __forceinline__ void block_row(const double* src, double (&v)[6]) {
+  const double2* w = reinterpret_cast<const double2*>(src);
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    double2 t = w[i];
+    v[2 * i] = t.x;
+    v[2 * i + 1] = t.y;
+  }
+}
+
+// One operator product over this CTA's staged rows with LPR lanes per row (run_groups' order: a
+// lane sums its blocks j, j + LPR, j + 2 LPR, ... then the team's butterfly). A block is read one
+// row at a time from shared memory, so only six values are live; x is this CTA's replica.
+template <typename S, typename V, int LPR, class Epi>
+__device__ __forceinline__ void tail_rows(const LocalMat<S>& A, const V* x, Epi& epi) {
+  constexpr int RB = 6, CB = 6, LEN = 36;
+  constexpr int TEAMS = 32 / LPR;
+  const int lane = threadIdx.x & 31;
+  const int team = lane / LPR, tl = lane % LPR;
+  const uint32_t warps = blockDim.x >> 5;
+  for (uint32_t l0 = (threadIdx.x >> 5) * TEAMS; l0 < A.rows; l0 += warps * TEAMS) {
+    const uint32_t lr = l0 + team;
+    const bool live = lr < A.rows;
+    const uint32_t row = A.row0 + lr;
+    epi.pre(row, live, tl);
+    V acc[RB];
+#pragma unroll
+    for (int p = 0; p < RB; ++p) acc[p] = V(0);
+    if (live) {
+      const uint32_t b0 = A.starts[lr], b1 = A.starts[lr + 1];
+      for (uint32_t j = b0 + tl; j < b1; j += LPR) {
+        const uint32_t c = A.cols[j];
+        V xa[CB];
+#pragma unroll
+        for (int q = 0; q < CB; ++q) xa[q] = x[(size_t)c * CB + q];
+        const S* blk = A.vals + (size_t)j * LEN;
+#pragma unroll
+        for (int p = 0; p < RB; ++p) {
+          S v[6];
+          block_row(blk + p * CB, v);
+#pragma unroll
+          for (int q = 0; q < CB; ++q) {
+            V t = V(v[q]) * xa[q];
+            acc[p] += t;
+          }
+        }
+      }
+    }
+    __syncwarp();
+#pragma unroll
+    for (int p = 0; p < RB; ++p)
+#pragma unroll
+      for (int o = LPR / 2; o > 0; o >>= 1) acc[p] += __shfl_xor_sync(kFull, acc[p], o);
+    epi.post(row, live, acc, tl);
+  }
+}
+
+// Where a phase reads and writes a level vector: this CTA's rows only (LOCAL, indexed from the
+// CTA's first row), the whole vector replicated in every CTA of the cluster (REPLICA: a store
+// goes to all CTAs' copies through distributed shared memory), or global memory (GLOBAL).
+enum { VEC_LOCAL = 0, VEC_REPLICA = 1, VEC_GLOBAL = 2 };
+
+__device__ __forceinline__ uint32_t cluster_rank() {
+  uint32_t r;
+  asm volatile("mov.u32 %0, %%cluster_ctarank;\n" : "=r"(r));
+  return r;
+}
+__device__ __forceinline__ void st_cluster(uint32_t addr, float v) {
+  asm volatile("st.shared::cluster.f32 [%0], %1;\n" ::"r"(addr), "f"(v) : "memory");
+}
+__device__ __forceinline__ void st_cluster(uint32_t addr, double v) {
+  asm volatile("st.shared::cluster.f64 [%0], %1;\n" ::"r"(addr), "d"(v) : "memory");
+}
+// Stores v at the same shared-memory offset in every CTA of the cluster (this one included).
+template <typename V>
+__device__ __forceinline__ void broadcast(V* local, V v) {
+  const uint32_t a = (uint32_t)__cvta_generic_to_shared(local);
+  const uint32_t n = gridDim.x;
+  for (uint32_t k = 0; k < n; ++k) {
+    uint32_t remote;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;\n" : "=r"(remote) : "r"(a), "r"(k));
+    st_cluster(remote, v);
+  }
+}
+
+template <typename V>
+struct Vref {
+  V* p;
+  uint32_t row0;  // LOCAL: the CTA's first row
+  int mode;
+  __device__ __forceinline__ size_t at(uint32_t row, int q) const {
+    return (size_t)(mode == VEC_LOCAL ? row - row0 : row) * 6 + q;
+  }
+  __device__ __forceinline__ V load(uint32_t row, int q) const {
+    return mode == VEC_GLOBAL ? __ldcg(p + at(row, q)) : p[at(row, q)];
+  }
+  __device__ __forceinline__ void store(uint32_t row, int q, V v) const {
+    if (mode == VEC_REPLICA)
+      broadcast(p + at(row, q), v);
+    else
+      p[at(row, q)] = v;
+  }
+};
+
+template <typename V>
+__device__ __forceinline__ Vref<V> vref(V* p, uint32_t row0, int mode) {
+  Vref<V> v;
+  v.p = p;
+  v.row0 = row0;
+  v.mode = mode;
+  return v;
+}
+
+// EpiAxpy through vector references.
+template <typename V, int LPR, int OP>
+struct TailAxpy {
+  static constexpr int N = Parts<6, LPR>::N;
+  Vref<V> y, b;
+  V in[N];
+  __device__ __forceinline__ void pre(uint32_t row, bool live, int tl) {
+    if (OP == OP_SET || !live) return;
+#pragma unroll
+    for (int k = 0; k < N; ++k) {
+      int p = tl + k * LPR;
+      if (p < 6) in[k] = OP == OP_RESIDUAL ? b.load(row, p) : y.load(row, p);
+    }
+  }
+  __device__ __forceinline__ void post(uint32_t row, bool live, const V (&acc)[6], int tl) {
+    if (!live) return;
+#pragma unroll
+    for (int k = 0; k < N; ++k) {
+      int p = tl + k * LPR;
+      if (p >= 6) continue;
+      V sum = pick<V, 6>(acc, p);
+      if (OP == OP_SET) y.store(row, p, sum);
+      if (OP == OP_RESIDUAL) y.store(row, p, in[k] - sum);
+      if (OP == OP_ADD) y.store(row, p, in[k] + sum);
+    }
+  }
+};
+
+// EpiCheb through vector references; D^-1 from the staged rows (first row `row0`). With
+// `has_outer` the step stores outer_out = outer_in + (x + d_new) instead of x.
+template <typename S, typename V, int LPR>
+struct TailCheb {
+  static constexpr int N = Parts<6, LPR>::N;
+  const S* dinv;
+  uint32_t row0;
+  Vref<V> d_old, d_new, r, x, outer_in, outer_out;
+  bool has_outer;
+  V keep, step;
+  V rv[6];
+  V dv[N], xv[N], ov[N];
+  S di[N][6];
+  __device__ __forceinline__ void pre(uint32_t row, bool live, int tl) {
+    if (!live) return;
+    const size_t local = (size_t)(row - row0) * 36;
+#pragma unroll
+    for (int q = 0; q < 6; ++q) rv[q] = r.load(row, q);
+#pragma unroll
+    for (int k = 0; k < N; ++k) {
+      int p = tl + k * LPR;
+      if (p >= 6) continue;
+#pragma unroll
+      for (int q = 0; q < 6; ++q) di[k][q] = dinv[local + p * 6 + q];
+      dv[k] = d_old.load(row, p);
+      xv[k] = x.load(row, p);
+      if (has_outer) ov[k] = outer_in.load(row, p);
+    }
+  }
+  __device__ __forceinline__ void post(uint32_t row, bool live, const V (&acc)[6], int tl) {
+    if (!live) return;
+    V rn[6];
+#pragma unroll
+    for (int q = 0; q < 6; ++q) rn[q] = rv[q] - acc[q];
+#pragma unroll
+    for (int k = 0; k < N; ++k) {
+      int p = tl + k * LPR;
+      if (p >= 6) continue;
+      V z = V(0);
+#pragma unroll
+      for (int q = 0; q < 6; ++q) z += V(di[k][q]) * rn[q];
+      V dn = keep * dv[k] + step * z;
+      r.store(row, p, pick<V, 6>(rn, p));
+      d_new.store(row, p, dn);
+      V xn = xv[k] + dn;
+      if (has_outer)
+        outer_out.store(row, p, ov[k] + xn);
+      else
+        x.store(row, p, xn);
+    }
+  }
+};
+
+// This CTA's staged data and vectors: its rows of the level operator, prolongator and D^-1, its
+// rows of the restriction and of the coarse inverse; replicas of the gathered vectors (d0, d1, x,
+// res, and the coarse b and x); its own rows of r, post_x, tmp and b.
+template <typename S, typename V>
+struct TailLocal {
+  LocalMat<S> a, p, r;
+  const S* dinv;
+  const double* inv;
+  uint32_t c0, c1;  // coarse rows of the inverse
+  V *d0, *d1, *x, *res, *cb, *cx;  // replicas
+  V *r_own, *post_x, *tmp, *b;     // own rows
+};
+
+template <typename V, int OP, typename S>
+__device__ __forceinline__ void tail_axpy(const LocalMat<S>& A, int lanes, const V* x, Vref<V> y, Vref<V> b) {
+  switch (lanes) {
+    case 4: { TailAxpy<V, 4, OP> e{y, b, {}}; tail_rows<S, V, 4>(A, x, e); break; }
+    case 8: { TailAxpy<V, 8, OP> e{y, b, {}}; tail_rows<S, V, 8>(A, x, e); break; }
+    case 16: { TailAxpy<V, 16, OP> e{y, b, {}}; tail_rows<S, V, 16>(A, x, e); break; }
+    default: { TailAxpy<V, 32, OP> e{y, b, {}}; tail_rows<S, V, 32>(A, x, e); break; }
+  }
+}
+
+template <typename S, typename V, int LPR>
+__device__ __forceinline__ void tail_cheb_lpr(const TailLocal<S, V>& l, V* d_old, V* d_new, Vref<V> x, bool has_outer,
+                                              Vref<V> outer_in, Vref<V> outer_out, V keep, V step) {
+  TailCheb<S, V, LPR> e;
+  e.dinv = l.dinv;
+  e.row0 = l.a.row0;
+  e.d_old = vref(d_old, 0, VEC_REPLICA);
+  e.d_new = vref(d_new, 0, VEC_REPLICA);
+  e.r = vref(l.r_own, l.a.row0, VEC_LOCAL);
+  e.x = x;
+  e.outer_in = outer_in;
+  e.outer_out = outer_out;
+  e.has_outer = has_outer;
+  e.keep = keep;
+  e.step = step;
+  tail_rows<S, V, LPR>(l.a, d_old, e);
+}
+
+template <typename S, typename V>
+__device__ __forceinline__ void tail_cheb(int lanes, const TailLocal<S, V>& l, V* d_old, V* d_new, Vref<V> x,
+                                          bool has_outer, Vref<V> outer_in, Vref<V> outer_out, V keep, V step) {
+  switch (lanes) {
+    case 4: tail_cheb_lpr<S, V, 4>(l, d_old, d_new, x, has_outer, outer_in, outer_out, keep, step); break;
+    case 8: tail_cheb_lpr<S, V, 8>(l, d_old, d_new, x, has_outer, outer_in, outer_out, keep, step); break;
+    case 16: tail_cheb_lpr<S, V, 16>(l, d_old, d_new, x, has_outer, outer_in, outer_out, keep, step); break;
+    default: tail_cheb_lpr<S, V, 32>(l, d_old, d_new, x, has_outer, outer_in, outer_out, keep, step); break;
+  }
+}
+
+// The smoother of enqueue_smooth on level s: the start (cheb_start_kernel, term for term) on the
+// CTA's rows of b into x, then the steps; with an outer vector the last step stores
+// outer_out = outer_in + x. Every phase that stores into replicas ends at a cluster barrier, so
+// no CTA leaves while another may still store into its shared memory.
+template <typename S, typename V>
+__device__ __forceinline__ void tail_smooth(const TailArgs<S, V>& t, const TailLocal<S, V>& l, const V* b_own,
+                                            Vref<V> x, bool has_outer, Vref<V> outer_in, Vref<V> outer_out) {
+  for (uint32_t lr = threadIdx.x; lr < l.a.rows; lr += blockDim.x) {
+    const uint32_t row = l.a.row0 + lr;
+    const S* di = l.dinv + (size_t)lr * 36;
+    V bv[6];
+#pragma unroll
+    for (int q = 0; q < 6; ++q) {
+      bv[q] = b_own[(size_t)lr * 6 + q];
+      l.r_own[(size_t)lr * 6 + q] = bv[q];
+    }
+#pragma unroll
+    for (int p = 0; p < 6; ++p) {
+      V z = V(0);
+#pragma unroll
+      for (int q = 0; q < 6; ++q) z += V(di[p * 6 + q]) * bv[q];
+      V dv = z / t.theta;
+      broadcast(l.d0 + (size_t)row * 6 + p, dv);
+      x.store(row, p, dv);
+    }
+  }
+  cluster_barrier();
+  for (uint32_t k = 0; k < t.nsteps; ++k) {
+    const bool last = k + 1 == t.nsteps;
+    V* d_old = (k & 1) ? l.d1 : l.d0;
+    V* d_new = (k & 1) ? l.d0 : l.d1;
+    tail_cheb<S, V>(t.a.lanes, l, d_old, d_new, x, last && has_outer, outer_in, outer_out, t.keep[k], t.step[k]);
+    cluster_barrier();
+  }
+  if (has_outer && t.nsteps == 0) {
+    for (uint32_t i = threadIdx.x; i < l.a.rows * 6; i += blockDim.x) {
+      const uint32_t row = l.a.row0 + i / 6;
+      const int q = (int)(i % 6);
+      outer_out.store(row, q, outer_in.load(row, q) + x.load(row, q));
+    }
+    cluster_barrier();
+  }
+}
+
+template <typename S, typename V>
+__device__ __forceinline__ void tail_kernel(TailArgs<S, V> t) {
+  if (*t.status != ST_ACTIVE) return;  // one word for the whole cluster: every CTA leaves or none
+  // Lay out this CTA's shared memory (the layout tail_cta_bytes sizes on the host) and stage its
+  // rows. The replicas come first, so a store into another CTA's replica lands at the same offset.
+  extern __shared__ __align__(16) unsigned char tail_smem[];
+  const uint32_t n = gridDim.x, i = cluster_rank();
+  const uint32_t a0 = tail_share(t.a.rows, n, i), a1 = tail_share(t.a.rows, n, i + 1);
+  const uint32_t r0 = tail_share(t.r.rows, n, i), r1 = tail_share(t.r.rows, n, i + 1);
+  const uint32_t nv = t.a.rows * 6;
+  TailLocal<S, V> l;
+  l.c0 = tail_share(t.nc, n, i);
+  l.c1 = tail_share(t.nc, n, i + 1);
+  unsigned char* at = tail_smem;
+  auto take = [&](size_t count) {
+    V* p = reinterpret_cast<V*>(at);
+    at += tail_align(count * sizeof(V));
+    return p;
+  };
+  l.d0 = take(nv);
+  l.d1 = take(nv);
+  l.x = take(nv);
+  l.res = take(nv);
+  l.cb = take(t.nc);
+  l.cx = take(t.nc);
+  l.a = tail_stage(t.a, a0, a1, at);
+  l.p = tail_stage(t.p, a0, a1, at);
+  l.r = tail_stage(t.r, r0, r1, at);
+  {
+    S* d = reinterpret_cast<S*>(at);
+    at += tail_align((size_t)(a1 - a0) * 36 * sizeof(S));
+    stage16(reinterpret_cast<float4*>(d), reinterpret_cast<const float4*>(t.dinv + (size_t)a0 * 36),
+            (size_t)(a1 - a0) * 36 * sizeof(S) / 16);
+    l.dinv = d;
+    double* v = reinterpret_cast<double*>(at);
+    at += tail_align((size_t)(l.c1 - l.c0) * t.nc * 8);
+    for (size_t k = threadIdx.x; k < (size_t)(l.c1 - l.c0) * t.nc; k += blockDim.x)
+      v[k] = __ldg(t.inv + (size_t)l.c0 * t.nc + k);
+    l.inv = v;
+  }
+  const size_t own = (size_t)(a1 - a0) * 6;
+  l.r_own = take(own);
+  l.post_x = take(own);
+  l.tmp = take(own);
+  l.b = take(own);
+  for (size_t k = threadIdx.x; k < own; k += blockDim.x) l.b[k] = __ldcg(t.b + (size_t)a0 * 6 + k);
+  __syncthreads();
+  // Every CTA of the cluster is running and laid out before any store reaches another's replicas.
+  cluster_barrier();
+
+  const Vref<V> x_rep = vref(l.x, 0, VEC_REPLICA), none = vref((V*)nullptr, 0, VEC_LOCAL);
+  tail_smooth<S, V>(t, l, l.b, x_rep, false, none, none);
+  tail_axpy<V, OP_RESIDUAL>(l.a, t.a.lanes, l.x, vref(l.res, 0, VEC_REPLICA), vref(l.b, a0, VEC_LOCAL));
+  cluster_barrier();
+  tail_axpy<V, OP_SET>(l.r, t.r.lanes, l.res, vref(l.cb, 0, VEC_REPLICA), none);
+  cluster_barrier();
+  {
+    // coarse_solve_kernel, term for term
+    const uint32_t warps = blockDim.x >> 5;
+    const int lane = threadIdx.x & 31;
+    for (uint32_t lr = threadIdx.x >> 5; lr < l.c1 - l.c0; lr += warps) {
+      const double* a = l.inv + (size_t)lr * t.nc;
+      double s = 0.0;
+      for (uint32_t j = lane; j < t.nc; j += 32) s += a[j] * (double)l.cb[j];
+      for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(kFull, s, o);
+      if (lane == 0) broadcast(l.cx + l.c0 + lr, V(s));
+    }
+  }
+  cluster_barrier();
+  tail_axpy<V, OP_ADD>(l.p, t.p.lanes, l.cx, x_rep, none);
+  cluster_barrier();
+  tail_axpy<V, OP_RESIDUAL>(l.a, t.a.lanes, l.x, vref(l.tmp, a0, VEC_LOCAL), vref(l.b, a0, VEC_LOCAL));
+  cluster_barrier();
+  tail_smooth<S, V>(t, l, l.tmp, vref(l.post_x, a0, VEC_LOCAL), true, x_rep, vref(t.x, 0, VEC_GLOBAL));
+}
+
+// Shared memory CTA i of n needs (the layout of tail_kernel), from the host row starts of the
+// level operator, prolongator and restriction.
+inline size_t tail_cta_bytes(const std::vector<uint32_t>& a_starts, const std::vector<uint32_t>& p_starts,
+                             const std::vector<uint32_t>& r_starts, uint32_t nc, uint32_t n, uint32_t i,
+                             size_t value_bytes, size_t vector_bytes) {
+  const uint32_t rows = (uint32_t)a_starts.size() - 1, crows = (uint32_t)r_starts.size() - 1;
+  const uint32_t a0 = tail_share(rows, n, i), a1 = tail_share(rows, n, i + 1);
+  const uint32_t r0 = tail_share(crows, n, i), r1 = tail_share(crows, n, i + 1);
+  const uint32_t c0 = tail_share(nc, n, i), c1 = tail_share(nc, n, i + 1);
+  const size_t nv = (size_t)rows * 6, own = (size_t)(a1 - a0) * 6;
+  return 4 * tail_align(nv * vector_bytes) + 2 * tail_align((size_t)nc * vector_bytes) +
+         tail_mat_bytes(a1 - a0, a_starts[a1] - a_starts[a0], value_bytes) +
+         tail_mat_bytes(a1 - a0, p_starts[a1] - p_starts[a0], value_bytes) +
+         tail_mat_bytes(r1 - r0, r_starts[r1] - r_starts[r0], value_bytes) +
+         tail_align((size_t)(a1 - a0) * 36 * value_bytes) + tail_align((size_t)(c1 - c0) * nc * 8) +
+         4 * tail_align(own * vector_bytes);
+}
+
 struct SellDot {
   const double* __restrict__ p;
   double* __restrict__ ap;
@@ -1468,10 +2034,93 @@ void enqueue_smooth(DeviceSolver& s, DevLevel& L, const B* b_in, V* b_out, V* x,
   }
 }
 
+template <typename S>
+TailMat<S> tail_mat(const DevBsr& m) {
+  TailMat<S> t;
+  t.starts = m.starts;
+  t.cols = m.cols;
+  t.vals = (const S*)m.vals;
+  t.rows = m.rows;
+  t.lanes = m.lanes_per_row;
+  return t;
+}
+
+// Levels li and li + 1 (the coarsest, factored) as one cluster launch of tail_kernel.
+template <typename S, typename V>
+void enqueue_tail(DeviceSolver& s, size_t li, const int* status) {
+  DevLevel& L = s.levels[li];
+  DevLevel& C = s.levels[li + 1];
+  TailArgs<S, V> t = {};
+  t.a = tail_mat<S>(L.a);
+  t.r = tail_mat<S>(L.r);
+  t.p = tail_mat<S>(L.p);
+  t.dinv = (const S*)L.dinv;
+  t.inv = C.coarse_inverse;
+  t.nc = C.n;
+  t.nsteps = (uint32_t)L.steps.size();
+  t.theta = (V)L.theta;
+  for (size_t k = 0; k < L.steps.size(); ++k) {
+    t.keep[k] = (V)L.steps[k].first;
+    t.step[k] = (V)L.steps[k].second;
+  }
+  t.b = (const V*)L.b;
+  t.x = (V*)L.x;
+  t.status = status;
+  launch_body_cluster<tail_kernel<S, V>, tail_threads<V>()>(dim3(s.tail_cluster), s.tail_smem, s.stream, t);
+  s.launches_per_iteration++;
+}
+
+// CTAs of the tail's cluster on this device and their shared memory: 16 (a non-portable size)
+// when each CTA's share fits kTailMaxSmem and the device can place such a cluster, else 8, else
+// 0 (no tail). `hs` is the fused level, `hc` the coarsest.
+template <typename S, typename V>
+unsigned tail_cluster_size(const HostLevel& hs, const HostLevel& hc, size_t* smem) {
+  typedef BodyTraits<decltype(&tail_kernel<S, V>)> T;
+  const void* single = T::template single_n<tail_kernel<S, V>, tail_threads<V>()>();
+  const void* batched = T::template batched_n<tail_kernel<S, V>, tail_threads<V>()>();
+  // restriction row starts: the prolongator's blocks counted per coarse row
+  std::vector<uint32_t> r_starts(hc.a.rows + 1, 0);
+  for (uint32_t c : hs.p.cols) r_starts[c + 1] += 1;
+  for (size_t i = 0; i < hc.a.rows; ++i) r_starts[i + 1] += r_starts[i];
+  const uint32_t nc = (uint32_t)(hc.a.rows * hc.a.rb);
+  cudaFuncSetAttribute(single, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+  cudaFuncSetAttribute(batched, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+  for (unsigned c : {16u, 8u}) {
+    size_t bytes = 0;
+    for (unsigned i = 0; i < c; ++i)
+      bytes = std::max(bytes, tail_cta_bytes(hs.a.starts, hs.p.starts, r_starts, nc, c, i, sizeof(S), sizeof(V)));
+    if (bytes > kTailMaxSmem) continue;
+    cudaFuncSetAttribute(single, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    cudaFuncSetAttribute(batched, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    cudaLaunchAttribute attr;
+    attr.id = cudaLaunchAttributeClusterDimension;
+    attr.val.clusterDim.x = c;
+    attr.val.clusterDim.y = 1;
+    attr.val.clusterDim.z = 1;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(c);
+    cfg.blockDim = dim3(tail_threads<V>());
+    cfg.dynamicSmemBytes = bytes;
+    cfg.attrs = &attr;
+    cfg.numAttrs = 1;
+    int clusters = 0;
+    if (cudaOccupancyMaxActiveClusters(&clusters, single, &cfg) == cudaSuccess && clusters > 0) {
+      *smem = bytes;
+      return c;
+    }
+    cudaGetLastError();
+  }
+  return 0;
+}
+
 // One V-cycle from level `li` (cycle.rs:461-539). B is the type of the right-hand side; an f64
 // right-hand side reaching an f32 level is rounded into b_store first.
 template <typename S, typename V, typename B>
 void enqueue_cycle(DeviceSolver& s, size_t li, const B* rhs, V* b_store, V* x, const int* status) {
+  if ((int)li == s.tail_level) {
+    enqueue_tail<S, V>(s, li, status);
+    return;
+  }
   DevLevel& L = s.levels[li];
   cudaStream_t st = s.stream;
   if (!L.has_p) {
@@ -1924,6 +2573,30 @@ sf_status solver_upload_hierarchy(DeviceSolver& s, const std::vector<HostLevel>&
   }
   if (s.vector_single)
     if (sf_status e = dev_alloc(s, (void**)&s.z32, (size_t)s.n * 4)) return e;
+  // The coarse tail: the last smoothed level (6-row blocks) and the factored coarsest level,
+  // small enough that one cluster beats a launch per phase. Batchable studies keep per-phase
+  // launches (their kernel sequence must not depend on sizes).
+  s.tail_level = -1;
+  s.tail_cluster = 0;
+  s.tail_smem = 0;
+  if (s.coarse_tail && !s.uniform_lanes && s.levels.size() >= 3) {
+    const size_t li = s.levels.size() - 2;
+    const DevLevel& L = s.levels[li];
+    const DevLevel& C = s.levels[li + 1];
+    if (L.has_p && C.has_factor && L.a.rb == 6 && L.a.cb == 6 && L.p.rb == 6 && L.p.cb == 6 && L.r.rb == 6 &&
+        L.r.cb == 6 && L.a.rows <= kTailMaxRows && C.n <= kTailMaxCoarse && L.steps.size() <= (size_t)kTailMaxSteps) {
+      size_t smem = 0;
+      const HostLevel &hs = levels[li], &hc = levels[li + 1];
+      unsigned c = !s.storage_single ? tail_cluster_size<double, double>(hs, hc, &smem)
+                   : !s.vector_single ? tail_cluster_size<float, double>(hs, hc, &smem)
+                                      : tail_cluster_size<float, float>(hs, hc, &smem);
+      if (c) {
+        s.tail_level = (int)li;
+        s.tail_cluster = c;
+        s.tail_smem = smem;
+      }
+    }
+  }
   return cuda_check(cudaStreamSynchronize(s.stream), "hierarchy upload");
 }
 
@@ -2027,6 +2700,7 @@ sf_status batch_build(const std::vector<DeviceSolver*>& inst, cudaStream_t strea
       at = j;
       if (rec[i][j].batched != rec[0][j].batched) why = "a different kernel";
       else if (rec[i][j].pack.size() != rec[0][j].pack.size()) why = "different arguments";
+      else if (rec[i][j].cluster != rec[0][j].cluster) why = "a different cluster size";
     }
     if (why) {
       char msg[200];
@@ -2040,6 +2714,7 @@ sf_status batch_build(const std::vector<DeviceSolver*>& inst, cudaStream_t strea
     dim3 grid, block;
     size_t smem;
     void* table;
+    unsigned cluster;
   };
   std::vector<Site> list(sites);
   for (size_t j = 0; j < sites; ++j) {
@@ -2048,6 +2723,7 @@ sf_status batch_build(const std::vector<DeviceSolver*>& inst, cudaStream_t strea
     t.block = rec[0][j].block;
     t.grid = dim3(1, (unsigned)inst.size(), 1);
     t.smem = 0;
+    t.cluster = rec[0][j].cluster;
     const size_t bytes = rec[0][j].pack.size();
     std::vector<unsigned char> host(bytes * inst.size());
     // Block sizes may differ (a row-group kernel's warps per block follow its largest group); the
@@ -2058,14 +2734,17 @@ sf_status batch_build(const std::vector<DeviceSolver*>& inst, cudaStream_t strea
       t.grid.x = std::max(t.grid.x, rec[i][j].grid.x);
       t.block.x = std::max(t.block.x, rec[i][j].block.x);
       per_warp = std::max(per_warp, rec[i][j].smem / std::max(1u, rec[i][j].block.x / 32));
+      if (t.cluster) t.smem = std::max(t.smem, rec[i][j].smem);
       std::memcpy(host.data() + i * bytes, rec[i][j].pack.data(), bytes);
     }
-    if (per_warp > 0) {
+    if (t.cluster) {
+      // a cluster kernel keeps its block (launch bounds) and the largest instance's shared memory
+    } else if (per_warp > 0) {
       // Fewer warps per block when the largest slot would not fit 200 KB of shared memory.
       size_t warps = std::max<size_t>(1, std::min<size_t>(t.block.x / 32, (200 * 1024) / per_warp));
       t.block.x = (unsigned)(32 * warps);
     }
-    t.smem = per_warp * (t.block.x / 32);
+    if (!t.cluster) t.smem = per_warp * (t.block.x / 32);
     if (t.smem > 200 * 1024) {
       batch_destroy(out);
       return fail(SF_INVALID_ARGUMENT, "a study of the batch needs more shared memory per warp than one SM holds");
@@ -2094,8 +2773,17 @@ sf_status batch_build(const std::vector<DeviceSolver*>& inst, cudaStream_t strea
   cudaError_t launch = cudaSuccess;
   for (Site& t : list) {
     cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    if (t.cluster) {
+      // one cluster per instance: grid.x is the cluster, blockIdx.y the instance
+      t.grid.x = t.cluster;
+      attr[0].id = cudaLaunchAttributeClusterDimension;
+      attr[0].val.clusterDim.x = t.cluster;
+      attr[0].val.clusterDim.y = 1;
+      attr[0].val.clusterDim.z = 1;
+    } else {
+      attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+      attr[0].val.programmaticStreamSerializationAllowed = 1;
+    }
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = t.grid;
     cfg.blockDim = t.block;

@@ -601,6 +601,7 @@ void sf_study_options_default(sf_study_options* o) {
   o->device_memory_budget = 0;
   o->sell_min_rows = 0;
   o->batchable = 0;
+  o->coarse_tail = 0;
 }
 
 // ------------------------------------------------------------------------------ builder
@@ -703,6 +704,7 @@ sf_status sf_builder_create(sf_model* model, const sf_study_options* options, sf
   s.sell_min_rows = b->options.sell_min_rows ? b->options.sell_min_rows : 32768;
   s.uniform_lanes = b->options.batchable != 0;
   if (s.uniform_lanes) s.sell_min_rows = UINT64_MAX;
+  s.coarse_tail = b->options.coarse_tail != 0;
   if (sf_status e = cuda_check(cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking), "stream")) return e;
   AssemblyDevice& a = b->asmdev;
   a.tet_count = (uint32_t)mesh.tets.size();
@@ -1627,6 +1629,9 @@ sf_status sf_study_device_timing(const sf_study* s, sf_device_timing* out) {
   out->kernel_launches = s->solver.launches;
   out->h2d_bytes = s->solver.h2d_bytes;
   out->d2h_bytes = s->solver.d2h_bytes;
+  out->launches_per_iteration = s->solver.launches_per_iteration;
+  out->coarse_tail_level = s->solver.tail_level;
+  out->coarse_tail_cluster = s->solver.tail_cluster;
   return SF_OK;
 }
 
