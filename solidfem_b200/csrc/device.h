@@ -176,6 +176,12 @@ inline void copy_d2h(const DeviceSolver& s, void* dst, const void* src, size_t b
 // grow-only scratch buffer per host thread, and 512-byte slots for per-study state.
 static const size_t kPinnedSlotBytes = 512;
 double* pinned_scratch(size_t bytes);
+// A process-wide pool of page-locked host buffers that are never freed (cudaFreeHost would
+// synchronize the whole device): pinned_acquire returns the smallest free buffer of at least
+// `bytes` (or a new one), pinned_return hands it back. Unlike the per-thread scratch, a buffer
+// belongs to its holder until it is returned, so it may live across resumable steps.
+void* pinned_acquire(size_t bytes);
+void pinned_return(void* buffer);
 void* pinned_slot();
 void pinned_release(void* slot);
 static_assert(2 * sizeof(PcgState) <= kPinnedSlotBytes, "a slot holds two solver states");

@@ -248,28 +248,33 @@ vector<vector<uint32_t>> face_connected_bodies(const Mesh& mesh) {
     }
     return x;
   };
-  // Tets sharing a face are joined: every face key goes into an open-addressing table, and a key
-  // met a second time joins its two tets. The partition, and so the body order below (by first
+  // Tets sharing a face are joined. Faces are bucketed by their smallest corner (a counting sort:
+  // a shared face has the same sorted key in both tets, so both copies land in one bucket of a
+  // few faces, and buckets follow node order, which keeps the passes cache-friendly); inside a
+  // bucket, equal keys join their tets. The partition, and so the body order below (by first
   // tet), is the one a sort of the keys gives.
-  size_t cap = 16;
-  while (cap < 8 * n) cap <<= 1;
-  vector<Key3> keys(cap);
-  vector<uint32_t> owner(cap, 0xffffffffu);
+  const size_t nodes = mesh.nodes.size();
+  vector<uint32_t> start(nodes + 1, 0);
+  for (size_t t = 0; t < n; ++t)
+    for (int f = 0; f < 4; ++f) start[face_key(mesh.corners[t], f)[0] + 1] += 1;
+  for (size_t i = 0; i < nodes; ++i) start[i + 1] += start[i];
+  vector<uint32_t> cursor(start.begin(), start.end() - 1);
+  vector<uint32_t> item(4 * n);
+  vector<uint64_t> rest(4 * n);  // the key's two larger corners
   for (size_t t = 0; t < n; ++t)
     for (int f = 0; f < 4; ++f) {
       Key3 k = face_key(mesh.corners[t], f);
-      uint64_t h = (uint64_t)k[0] * 0x9E3779B97F4A7C15ull ^ (uint64_t)k[1] * 0xC2B2AE3D27D4EB4Full ^
-                   (uint64_t)k[2] * 0x165667B19E3779F9ull;
-      size_t at = (size_t)(h >> 17) & (cap - 1);
-      while (owner[at] != 0xffffffffu && keys[at] != k) at = (at + 1) & (cap - 1);
-      if (owner[at] == 0xffffffffu) {
-        keys[at] = k;
-        owner[at] = (uint32_t)t;
-      } else {
-        size_t a = find(owner[at]), b = find(t);
-        if (a != b) parent[std::max(a, b)] = std::min(a, b);
-      }
+      uint32_t at = cursor[k[0]]++;
+      item[at] = (uint32_t)t;
+      rest[at] = ((uint64_t)k[1] << 32) | k[2];
     }
+  for (size_t c = 0; c < nodes; ++c)
+    for (uint32_t i = start[c]; i < start[c + 1]; ++i)
+      for (uint32_t j = i + 1; j < start[c + 1]; ++j)
+        if (rest[i] == rest[j]) {
+          size_t a = find(item[i]), b = find(item[j]);
+          if (a != b) parent[std::max(a, b)] = std::min(a, b);
+        }
   vector<vector<uint32_t>> groups;
   vector<size_t> group_of(n, SIZE_MAX);
   for (size_t t = 0; t < n; ++t) {

@@ -123,7 +123,7 @@ struct SetupMachine {
   vector<HostLevel> levels;
   // per-level state
   double* inv = nullptr;  // device inverse diagonal
-  vector<double> norms;   // host copy of the block norms (join pass)
+  double* norms = nullptr;  // host copy of the block norms (join pass), a pooled pinned buffer
   bool is_coarsest = false;
   double reach = 3.0;
   size_t retries = 0;
@@ -133,7 +133,7 @@ struct SetupMachine {
   size_t aggregates = 0;
   vector<uint32_t> member_starts, members;
   vector<P3> coarse_positions;
-  vector<double> tentative;  // rows x rb x 6, host (uploaded for smoothing)
+  double* tentative = nullptr;  // rows x rb x 6, a pooled pinned buffer (uploaded for smoothing)
   vector<double> coarse_null;
   double lambda_max = 0;
   vector<uint32_t> filter_starts, filter_cols;
@@ -142,6 +142,10 @@ struct SetupMachine {
   bool cancelled = false;
 
   explicit SetupMachine(DeviceSolver& d) : dev(d) {}
+  ~SetupMachine() {
+    pinned_return(norms);
+    pinned_return(tentative);
+  }
 
   size_t level_index() const { return levels.size(); }
 
@@ -207,8 +211,10 @@ struct SetupMachine {
     size_t blocks = current.cols.size();
     if ((e = dev_alloc(dev, (void**)&d_norms, std::max<size_t>(1, blocks) * 8))) return e;
     e = setup_block_norms(dev.stream, blocks, (int)(rb * current.cb), current.dev, d_norms);
-    norms.assign(blocks, 0.0);
-    if (!e && blocks) copy_d2h(dev, norms.data(), d_norms, blocks * 8);
+    pinned_return(norms);
+    norms = (double*)pinned_acquire(blocks * 8);
+    if (!e && !norms) e = fail(SF_CUDA_ERROR, "cudaMallocHost failed");
+    if (!e && blocks) copy_d2h(dev, norms, d_norms, blocks * 8);
     if (!e) e = sync("block norms");
     dev_free(dev, d_norms);
     if (e) return e;
@@ -327,9 +333,12 @@ struct SetupMachine {
   }
 
   // Tentative prolongator by two-pass Gram-Schmidt per aggregate (transfer.rs:19-68).
-  void run_tentative() {
+  sf_status run_tentative() {
     size_t rb = current.rb, rows = current.rows, block = rb * MODES;
-    tentative.assign(rows * block, 0.0);
+    // Every row belongs to one aggregate, which writes its whole block row: no fill needed.
+    pinned_return(tentative);
+    tentative = (double*)pinned_acquire(rows * block * 8);
+    if (!tentative) return fail(SF_CUDA_ERROR, "cudaMallocHost failed");
     coarse_null.assign(aggregates * 36, 0.0);
     rows_parallel(aggregates, opt.threads, [&](size_t a) {
       size_t count = member_starts[a + 1] - member_starts[a];
@@ -365,9 +374,10 @@ struct SetupMachine {
         }
       }
       for (size_t m = 0; m < count; ++m)
-        std::copy(local.begin() + m * block, local.begin() + (m + 1) * block, tentative.begin() + (size_t)mem[m] * block);
+        std::copy(local.begin() + m * block, local.begin() + (m + 1) * block, tentative + (size_t)mem[m] * block);
     });
     phase = SPECTRAL;
+    return SF_OK;
   }
 
   // Power iteration for lambda_max(D^-1 A) (setup.rs:390-449): the products on the device, the
@@ -485,7 +495,9 @@ struct SetupMachine {
     if (!e) e = upload(ns, &n_starts);
     if (!e) e = upload(nc, &n_cols);
     if (!e) e = upload(aggregate, &agg);
-    if (!e) e = upload(tentative, &t);
+    const size_t tentative_bytes = rows * rb * MODES * 8;
+    if (!e) e = dev_alloc(dev, (void**)&t, std::max<size_t>(1, tentative_bytes));
+    if (!e && tentative_bytes) copy_h2d(dev, t, tentative, tentative_bytes);
     if (!e) e = dev_alloc(dev, (void**)&prolongator.dev, std::max<size_t>(1, entries) * rb * MODES * 8);
     if (!e) e = entry_rows(prolongator, &rows_of);
     if (!e)
@@ -494,8 +506,8 @@ struct SetupMachine {
     if (!e) e = sync("smooth");
     for (void* p : {(void*)n_starts, (void*)n_cols, (void*)agg, (void*)rows_of, (void*)t}) dev_free(dev, p);
     if (e) return e;
-    tentative.clear();
-    tentative.shrink_to_fit();
+    pinned_return(tentative);  // the copy above completed at the sync
+    tentative = nullptr;
     phase = PRODUCT;
     return SF_OK;
   }
@@ -588,7 +600,8 @@ struct SetupMachine {
     prolongator = Bsr();
     near_null = std::move(coarse_null);
     positions = std::move(coarse_positions);
-    norms.clear();
+    pinned_return(norms);
+    norms = nullptr;
     reach = opt.reach;
     retries = 0;
     is_coarsest = false;
@@ -694,7 +707,7 @@ sf_status setup_step(SetupMachine* m, size_t budget, sf_cancel_fn cancel, void* 
       case DIAGONAL: s = m->run_diagonal(); break;
       case STRENGTH: m->run_strength(); break;
       case AGGREGATE: m->run_aggregate(); break;
-      case TENTATIVE: m->run_tentative(); break;
+      case TENTATIVE: s = m->run_tentative(); break;
       case SPECTRAL:
         s = m->run_spectral();
         rows *= 20;

@@ -2205,7 +2205,40 @@ double* pinned_scratch(size_t bytes) {
 namespace {
 std::mutex g_slot_mutex;
 std::vector<void*> g_free_slots;
+std::mutex g_pool_mutex;
+std::vector<std::pair<void*, size_t>> g_pool_free;    // returned buffers
+std::vector<std::pair<void*, size_t>> g_pool_sizes;   // every buffer made
 }  // namespace
+
+void* pinned_acquire(size_t bytes) {
+  bytes = std::max<size_t>(bytes, 1);
+  std::lock_guard<std::mutex> lock(g_pool_mutex);
+  size_t best = SIZE_MAX;
+  for (size_t i = 0; i < g_pool_free.size(); ++i)
+    if (g_pool_free[i].second >= bytes && (best == SIZE_MAX || g_pool_free[i].second < g_pool_free[best].second))
+      best = i;
+  if (best != SIZE_MAX) {
+    void* p = g_pool_free[best].first;
+    g_pool_free[best] = g_pool_free.back();
+    g_pool_free.pop_back();
+    return p;
+  }
+  const size_t want = (bytes + ((size_t)1 << 20) - 1) & ~(((size_t)1 << 20) - 1);  // whole MiB
+  void* p = nullptr;
+  if (cudaMallocHost(&p, want) != cudaSuccess) return nullptr;
+  g_pool_sizes.push_back({p, want});
+  return p;
+}
+
+void pinned_return(void* buffer) {
+  if (!buffer) return;
+  std::lock_guard<std::mutex> lock(g_pool_mutex);
+  for (auto& b : g_pool_sizes)
+    if (b.first == buffer) {
+      g_pool_free.push_back(b);
+      return;
+    }
+}
 
 void* pinned_slot() {
   std::lock_guard<std::mutex> lock(g_slot_mutex);

@@ -239,9 +239,33 @@ vector<double> rigid_modes(const vector<P3>& nodes, const vector<uint32_t>& free
   return modes;
 }
 
+// An allocator whose resize leaves new elements uninitialised: the pattern's large arrays are
+// written in full by the parallel pass that fills them, so a zero fill first (single-threaded,
+// and the page faults of tens of MB with it) is pure cost.
+template <typename T>
+struct NoInit : std::allocator<T> {
+  template <typename U>
+  struct rebind {
+    typedef NoInit<U> other;
+  };
+  NoInit() = default;
+  template <typename U>
+  NoInit(const NoInit<U>&) {}
+  template <typename U>
+  void construct(U* p) noexcept {
+    ::new (static_cast<void*>(p)) U;
+  }
+  template <typename U, typename... A>
+  void construct(U* p, A&&... a) {
+    ::new (static_cast<void*>(p)) U(std::forward<A>(a)...);
+  }
+};
+typedef vector<uint32_t, NoInit<uint32_t>> RawU32;
+
 struct HostPattern {
-  vector<uint32_t> starts, cols;           // block rows over free nodes
-  vector<uint32_t> map_starts, map;        // per block: (element << 7) | (10 a + b), ascending
+  vector<uint32_t> starts;                 // block rows over free nodes
+  RawU32 cols;
+  RawU32 map_starts, map;                  // per block: (element << 7) | (10 a + b), ascending
 };
 
 // The free-node block pattern (assembly.rs:55-81, csr.rs:19-71) and, for each block, the
@@ -291,9 +315,9 @@ void build_pattern(const Mesh& m, const vector<uint32_t>& free, size_t free_coun
     hp.starts[r + 1] = hp.starts[r] + counts[r];
     map_row[r + 1] = map_row[r] + map_counts[r];
   }
-  hp.cols.assign(hp.starts[free_count], 0);
-  hp.map_starts.assign(hp.starts[free_count] + 1, 0);
-  hp.map.assign(map_row[free_count], 0);
+  hp.cols.resize(hp.starts[free_count]);
+  hp.map_starts.resize(hp.starts[free_count] + 1);
+  hp.map.resize(map_row[free_count]);
 #ifdef _OPENMP
 #pragma omp parallel num_threads(threads)
 #endif
@@ -901,8 +925,8 @@ static sf_status builder_assemble(sf_builder* b, uint64_t max_elements, sf_cance
     for (void* p : {(void*)a.ke, (void*)a.map, (void*)a.map_starts, (void*)a.cursor}) dev_free(s, p);
     a.ke = nullptr;
     a.map = a.map_starts = a.cursor = nullptr;
-    std::vector<uint32_t>().swap(b->pattern.map);
-    std::vector<uint32_t>().swap(b->pattern.map_starts);
+    RawU32().swap(b->pattern.map);
+    RawU32().swap(b->pattern.map_starts);
   }
   return SF_OK;
 }
@@ -917,7 +941,7 @@ static sf_status builder_setup(sf_builder* b, uint64_t budget, sf_cancel_fn canc
     fine.rows = b->free_count;
     fine.rb = fine.cb = 3;
     fine.starts = b->pattern.starts;
-    fine.cols = b->pattern.cols;
+    fine.cols.assign(b->pattern.cols.begin(), b->pattern.cols.end());
     fine.dev = (double*)s.system.vals;
     fine.dev_starts = s.system.starts;
     fine.dev_cols = s.system.cols;
