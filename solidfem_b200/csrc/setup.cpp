@@ -14,6 +14,7 @@
 #include <algorithm>
 #include <atomic>
 #include <cmath>
+#include <future>
 #include <limits>
 #include <memory>
 
@@ -140,9 +141,16 @@ struct SetupMachine {
   Bsr prolongator, ap, coarse;
   sf_status failure = SF_OK;
   bool cancelled = false;
+  // The power iteration needs only the level operator and D^-1, so it runs on a helper thread
+  // from the end of the diagonal phase while this thread builds the strength graph, the aggregates
+  // and the tentative prolongator (host work that touches neither the device nor these buffers);
+  // the spectral phase takes its result. Declared last, so it is waited for first.
+  double *power_v = nullptr, *power_s = nullptr;
+  std::future<std::pair<sf_status, double>> power;
 
   explicit SetupMachine(DeviceSolver& d) : dev(d) {}
   ~SetupMachine() {
+    if (power.valid()) power.wait();
     pinned_return(norms);
     pinned_return(tentative);
   }
@@ -217,6 +225,7 @@ struct SetupMachine {
     if (!e && blocks) copy_d2h(dev, norms, d_norms, blocks * 8);
     if (!e) e = sync("block norms");
     dev_free(dev, d_norms);
+    if (!e) e = start_power();
     if (e) return e;
     phase = STRENGTH;
     return SF_OK;
@@ -381,19 +390,17 @@ struct SetupMachine {
   }
 
   // Power iteration for lambda_max(D^-1 A) (setup.rs:390-449): the products on the device, the
-  // order-exact norms on the host from a pinned copy of each iterate (this thread's scratch).
-  sf_status run_spectral() {
-    size_t rb = current.rb, rows = current.rows, dofs = rows * rb;
-    double *v = nullptr, *s2 = nullptr;
-    sf_status e = dev_alloc(dev, (void**)&v, std::max<size_t>(1, dofs) * 8);
-    if (!e) e = dev_alloc(dev, (void**)&s2, std::max<size_t>(1, dofs) * 8);
-    double* pinned = nullptr;
-    if (!e) {
-      pinned = pinned_scratch(std::max<size_t>(1, dofs) * 8);
-      if (!pinned) e = fail(SF_CUDA_ERROR, "cudaMallocHost failed");
-    }
+  // order-exact norms on the host from a pinned copy of each iterate. Returns the last norm.
+  std::pair<sf_status, double> power_iteration() {
+    cudaSetDevice(dev.device);  // a helper thread starts on device 0
+    const size_t rb = current.rb, rows = current.rows, dofs = rows * rb;
+    double* pinned = (double*)pinned_acquire(std::max<size_t>(1, dofs) * 8);
+    if (!pinned) return {SF_CUDA_ERROR, 0.0};
+    sf_status e = SF_OK;
     double lm = 0.0;
-    if (!e && dofs) {
+    if (dofs) {
+      double* v = power_v;
+      double* s2 = power_s;
       for (size_t i = 0; i < dofs; ++i) pinned[i] = start_value(i);
       double n0 = norm2(pinned, dofs);
       for (size_t i = 0; i < dofs; ++i) pinned[i] /= n0;
@@ -413,10 +420,29 @@ struct SetupMachine {
       }
       if (!e) e = sync("power iteration");
     }
-    dev_free(dev, v);
-    dev_free(dev, s2);
+    pinned_return(pinned);  // every copy from it completed at the syncs
+    return {e, lm};
+  }
+
+  sf_status start_power() {
+    const size_t dofs = current.rows * current.rb;
+    sf_status e = dev_alloc(dev, (void**)&power_v, std::max<size_t>(1, dofs) * 8);
+    if (!e) e = dev_alloc(dev, (void**)&power_s, std::max<size_t>(1, dofs) * 8);
     if (e) return e;
-    lambda_max = lm * SPECTRAL_MARGIN;
+    power = std::async(std::launch::async, [this] { return power_iteration(); });
+    return SF_OK;
+  }
+
+  sf_status run_spectral() {
+    const size_t rb = current.rb, rows = current.rows;
+    if (!power.valid())
+      if (sf_status e = start_power()) return e;
+    std::pair<sf_status, double> r = power.get();
+    dev_free(dev, power_v);
+    dev_free(dev, power_s);
+    power_v = power_s = nullptr;
+    if (r.first) return fail(r.first, "the power iteration for the largest eigenvalue failed");
+    lambda_max = r.second * SPECTRAL_MARGIN;
     if (is_coarsest) {
       phase = (rows * rb <= DENSE_LIMIT) ? FACTOR : DONE;
       if (phase == DONE) push_final(false);

@@ -806,6 +806,9 @@ sf_status sf_builder_create(sf_model* model, const sf_study_options* options, sf
 
 void sf_builder_destroy(sf_builder* b) {
   if (!b) return;
+  // The setup first: it waits for any device work of its own still in flight.
+  if (b->setup) setup_destroy(b->setup);
+  b->setup = nullptr;
   release_builder_device(b);
   delete b;
 }
