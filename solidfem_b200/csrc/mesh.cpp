@@ -251,30 +251,74 @@ vector<vector<uint32_t>> face_connected_bodies(const Mesh& mesh) {
   // Tets sharing a face are joined. Faces are bucketed by their smallest corner (a counting sort:
   // a shared face has the same sorted key in both tets, so both copies land in one bucket of a
   // few faces, and buckets follow node order, which keeps the passes cache-friendly); inside a
-  // bucket, equal keys join their tets. The partition, and so the body order below (by first
-  // tet), is the one a sort of the keys gives.
-  const size_t nodes = mesh.nodes.size();
-  vector<uint32_t> start(nodes + 1, 0);
-  for (size_t t = 0; t < n; ++t)
-    for (int f = 0; f < 4; ++f) start[face_key(mesh.corners[t], f)[0] + 1] += 1;
-  for (size_t i = 0; i < nodes; ++i) start[i + 1] += start[i];
-  vector<uint32_t> cursor(start.begin(), start.end() - 1);
-  vector<uint32_t> item(4 * n);
-  vector<uint64_t> rest(4 * n);  // the key's two larger corners
-  for (size_t t = 0; t < n; ++t)
+  // bucket, equal keys pair their tets. Keys, bucket counts and pairs are found in parallel, the
+  // joins run in one thread. Joining makes the smallest tet of a body its root, so the partition
+  // and the body order below (by first tet) do not depend on the order of the joins: they are the
+  // ones a sort of the keys gives.
+  const size_t nodes = mesh.nodes.size(), faces = 4 * n;
+  int threads = 1;
+#ifdef _OPENMP
+  threads = n < 16384 ? 1 : std::max(1, std::min(omp_get_max_threads(), 16));
+#endif
+  vector<uint32_t> low(faces);
+  vector<uint64_t> key(faces);  // the key's two larger corners
+#ifdef _OPENMP
+#pragma omp parallel for num_threads(threads) schedule(static)
+#endif
+  for (long long t = 0; t < (long long)n; ++t)
     for (int f = 0; f < 4; ++f) {
       Key3 k = face_key(mesh.corners[t], f);
-      uint32_t at = cursor[k[0]]++;
-      item[at] = (uint32_t)t;
-      rest[at] = ((uint64_t)k[1] << 32) | k[2];
+      low[4 * t + f] = k[0];
+      key[4 * t + f] = ((uint64_t)k[1] << 32) | k[2];
     }
-  for (size_t c = 0; c < nodes; ++c)
-    for (uint32_t i = start[c]; i < start[c + 1]; ++i)
-      for (uint32_t j = i + 1; j < start[c + 1]; ++j)
-        if (rest[i] == rest[j]) {
-          size_t a = find(item[i]), b = find(item[j]);
-          if (a != b) parent[std::max(a, b)] = std::min(a, b);
-        }
+  // per-thread counts over contiguous face ranges, then each thread's place inside every bucket
+  vector<vector<uint32_t>> counts(threads, vector<uint32_t>(nodes + 1, 0));
+#ifdef _OPENMP
+#pragma omp parallel for num_threads(threads) schedule(static, 1)
+#endif
+  for (int c = 0; c < threads; ++c) {
+    const size_t b0 = faces * c / threads, b1 = faces * (c + 1) / threads;
+    for (size_t i = b0; i < b1; ++i) counts[c][low[i]] += 1;
+  }
+  vector<uint32_t> start(nodes + 1, 0);
+  for (size_t v = 0; v < nodes; ++v) {
+    uint32_t at = start[v];
+    for (int c = 0; c < threads; ++c) {
+      const uint32_t k = counts[c][v];
+      counts[c][v] = at;
+      at += k;
+    }
+    start[v + 1] = at;
+  }
+  vector<uint32_t> item(faces);
+  vector<uint64_t> rest(faces);
+#ifdef _OPENMP
+#pragma omp parallel for num_threads(threads) schedule(static, 1)
+#endif
+  for (int c = 0; c < threads; ++c) {
+    const size_t b0 = faces * c / threads, b1 = faces * (c + 1) / threads;
+    for (size_t i = b0; i < b1; ++i) {
+      const uint32_t at = counts[c][low[i]]++;
+      item[at] = (uint32_t)(i / 4);
+      rest[at] = key[i];
+    }
+  }
+  vector<vector<std::pair<uint32_t, uint32_t>>> pairs(threads);
+#ifdef _OPENMP
+#pragma omp parallel for num_threads(threads) schedule(static, 1)
+#endif
+  for (int c = 0; c < threads; ++c) {
+    const size_t v0 = nodes * c / threads, v1 = nodes * (c + 1) / threads;
+    for (size_t v = v0; v < v1; ++v)
+      for (uint32_t i = start[v]; i < start[v + 1]; ++i)
+        for (uint32_t j = i + 1; j < start[v + 1]; ++j)
+          if (rest[i] == rest[j]) pairs[c].push_back({item[i], item[j]});
+  }
+  for (auto& list : pairs)
+    for (auto& pr : list) {
+      size_t a = find(pr.first), b = find(pr.second);
+      if (a != b) parent[std::max(a, b)] = std::min(a, b);
+    }
   vector<vector<uint32_t>> groups;
   vector<size_t> group_of(n, SIZE_MAX);
   for (size_t t = 0; t < n; ++t) {

@@ -262,15 +262,55 @@ struct NoInit : std::allocator<T> {
 };
 typedef vector<uint32_t, NoInit<uint32_t>> RawU32;
 
+// An uninitialised page-locked host array from the pinned pool (never freed, so dropping it does
+// not synchronize the device): the assembly map is written straight into memory the upload can
+// read at full link speed, and handed back to the pool once it is on the device.
+struct PinnedU32 {
+  uint32_t* p = nullptr;
+  size_t n = 0;
+  PinnedU32() = default;
+  PinnedU32(const PinnedU32&) = delete;
+  PinnedU32& operator=(const PinnedU32&) = delete;
+  PinnedU32(PinnedU32&& o) noexcept : p(o.p), n(o.n) { o.p = nullptr, o.n = 0; }
+  PinnedU32& operator=(PinnedU32&& o) noexcept {
+    if (this != &o) {
+      release();
+      p = o.p;
+      n = o.n;
+      o.p = nullptr;
+      o.n = 0;
+    }
+    return *this;
+  }
+  ~PinnedU32() { release(); }
+  bool resize(size_t count) {
+    release();
+    p = (uint32_t*)pinned_acquire(std::max<size_t>(1, count) * 4);
+    n = p ? count : 0;
+    return p != nullptr;
+  }
+  void release() {
+    pinned_return(p);
+    p = nullptr;
+    n = 0;
+  }
+  uint32_t* data() { return p; }
+  const uint32_t* data() const { return p; }
+  size_t size() const { return n; }
+  bool empty() const { return n == 0; }
+  uint32_t& operator[](size_t i) { return p[i]; }
+  const uint32_t& operator[](size_t i) const { return p[i]; }
+};
+
 struct HostPattern {
   vector<uint32_t> starts;                 // block rows over free nodes
   RawU32 cols;
-  RawU32 map_starts, map;                  // per block: (element << 7) | (10 a + b), ascending
+  PinnedU32 map_starts, map;               // per block: (element << 7) | (10 a + b), ascending
 };
 
 // The free-node block pattern (assembly.rs:55-81, csr.rs:19-71) and, for each block, the
 // elements that add to it in ascending order, built row-parallel from node-to-element incidence.
-void build_pattern(const Mesh& m, const vector<uint32_t>& free, size_t free_count, int threads, HostPattern& hp) {
+bool build_pattern(const Mesh& m, const vector<uint32_t>& free, size_t free_count, int threads, HostPattern& hp) {
   size_t nn = m.nodes.size(), ne = m.tets.size();
   vector<uint32_t> inc_start(nn + 1, 0);
   for (auto& t : m.tets)
@@ -316,8 +356,7 @@ void build_pattern(const Mesh& m, const vector<uint32_t>& free, size_t free_coun
     map_row[r + 1] = map_row[r] + map_counts[r];
   }
   hp.cols.resize(hp.starts[free_count]);
-  hp.map_starts.resize(hp.starts[free_count] + 1);
-  hp.map.resize(map_row[free_count]);
+  if (!hp.map_starts.resize(hp.starts[free_count] + 1) || !hp.map.resize(map_row[free_count])) return false;
 #ifdef _OPENMP
 #pragma omp parallel num_threads(threads)
 #endif
@@ -367,6 +406,7 @@ void build_pattern(const Mesh& m, const vector<uint32_t>& free, size_t free_coun
     }
   }
   hp.map_starts[hp.starts[free_count]] = (uint32_t)map_row[free_count];
+  return true;
 }
 
 }  // namespace
@@ -717,7 +757,8 @@ sf_status sf_builder_create(sf_model* model, const sf_study_options* options, sf
   for (auto& p : b->prescribed) all_zero = all_zero && p.second == 0.0;
   if (all_zero) return fail(SF_NO_EFFECTIVE_LOAD, "the model has no effective load");
   double t0 = now_seconds();
-  build_pattern(mesh, b->free, b->free_count, b->threads, b->pattern);
+  if (!build_pattern(mesh, b->free, b->free_count, b->threads, b->pattern))
+    return fail(SF_CUDA_ERROR, "cudaMallocHost failed for the assembly map");
   // Device set-up: mesh, element stiffness buffer, pattern and assembly map, system matrix.
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(SF_NO_DEVICE, "no CUDA device is visible");
@@ -762,7 +803,8 @@ sf_status sf_builder_create(sf_model* model, const sf_study_options* options, sf
   copy_h2d(s, a.map_starts, b->pattern.map_starts.data(), (blocks + 1) * 4);
   if (!b->pattern.map.empty())
     copy_h2d(s, a.map, b->pattern.map.data(), b->pattern.map.size() * 4);
-  copy_h2d(s, a.cursor, b->pattern.map_starts.data(), blocks * 4);
+  // the gather's per-block cursors start at the map starts: a copy on the device
+  cudaMemcpyAsync(a.cursor, a.map_starts, blocks * 4, cudaMemcpyDeviceToDevice, s.stream);
   unsigned long long none = ~0ull;
   copy_h2d(s, a.error, &none, 8);
   copy_h2d(s, s.system.starts, b->pattern.starts.data(), (b->free_count + 1) * 4);
@@ -799,6 +841,9 @@ sf_status sf_builder_create(sf_model* model, const sf_study_options* options, sf
     release_builder_device(b.get());
     return e;
   }
+  // The map is on the device now: its host copy goes back to the pool.
+  b->pattern.map.release();
+  b->pattern.map_starts.release();
   b->assembly_seconds = now_seconds() - t0;
   *out = b.release();
   return SF_OK;
@@ -928,8 +973,8 @@ static sf_status builder_assemble(sf_builder* b, uint64_t max_elements, sf_cance
     for (void* p : {(void*)a.ke, (void*)a.map, (void*)a.map_starts, (void*)a.cursor}) dev_free(s, p);
     a.ke = nullptr;
     a.map = a.map_starts = a.cursor = nullptr;
-    RawU32().swap(b->pattern.map);
-    RawU32().swap(b->pattern.map_starts);
+    b->pattern.map.release();
+    b->pattern.map_starts.release();
   }
   return SF_OK;
 }
