@@ -203,6 +203,12 @@ sf_status setup_power_step(cudaStream_t st, uint32_t rows, int rb, const uint32_
                            const double* vals, const double* inv, const double* v, double* s2);
 sf_status setup_scale(cudaStream_t st, size_t n, const double* src, double d, double* v);
 sf_status setup_entry_rows(cudaStream_t st, uint32_t rows, const uint32_t* starts, uint32_t* out);
+// One pass of a union pattern (symbolic product): out_starts null counts each row's distinct
+// columns into out[row]; otherwise writes them, ascending, at out[out_starts[row] ..]. Columns
+// are below `width`.
+sf_status setup_union_rows(cudaStream_t st, uint32_t rows, uint32_t width, const uint32_t* outer_starts,
+                           const uint32_t* outer_idx, bool self, const uint32_t* inner_starts,
+                           const uint32_t* inner_cols, const uint32_t* out_starts, uint32_t* out);
 // Listed blocks of len values out of / back into a block array; out[idx[i]] = vals[i].
 sf_status setup_gather_blocks(cudaStream_t st, size_t count, int len, const uint32_t* idx, const double* in,
                               double* out);

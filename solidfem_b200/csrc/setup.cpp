@@ -182,6 +182,35 @@ struct SetupMachine {
   }
   sf_status sync(const char* what) { return cuda_check(cudaStreamSynchronize(dev.stream), what); }
 
+  // True when a union pattern of `width` columns runs on the device (one warp's bitmap of the
+  // columns fits shared memory); wider ones take symbolic_rows on the host.
+  static bool union_on_device(size_t width) { return (width + 31) / 32 * 4 <= 200 * 1024; }
+
+  // A union pattern (the symbolic_rows of a product) on the device: a count pass, the row starts
+  // by a prefix sum here, a fill pass. `out` gets the device starts and columns and the same
+  // arrays on the host, equal to what symbolic_rows gives (each row's distinct columns, sorted).
+  sf_status device_union(size_t rows, size_t width, const uint32_t* d_outer_starts, const uint32_t* d_outer_idx,
+                         bool self, const uint32_t* d_inner_starts, const uint32_t* d_inner_cols, Bsr& out) {
+    sf_status e = dev_alloc(dev, (void**)&out.dev_starts, (rows + 1) * 4);
+    if (!e)
+      e = setup_union_rows(dev.stream, (uint32_t)rows, (uint32_t)width, d_outer_starts, d_outer_idx, self,
+                           d_inner_starts, d_inner_cols, nullptr, out.dev_starts);
+    out.starts.assign(rows + 1, 0);
+    if (!e && rows) copy_d2h(dev, out.starts.data() + 1, out.dev_starts, rows * 4);
+    if (!e) e = sync("union pattern counts");
+    if (e) return e;
+    for (size_t r = 0; r < rows; ++r) out.starts[r + 1] += out.starts[r];
+    copy_h2d(dev, out.dev_starts, out.starts.data(), (rows + 1) * 4);
+    const size_t total = out.starts[rows];
+    if ((e = dev_alloc(dev, (void**)&out.dev_cols, std::max<size_t>(1, total) * 4))) return e;
+    e = setup_union_rows(dev.stream, (uint32_t)rows, (uint32_t)width, d_outer_starts, d_outer_idx, self,
+                         d_inner_starts, d_inner_cols, out.dev_starts, out.dev_cols);
+    out.cols.resize(total);
+    if (!e && total) copy_d2h(dev, out.cols.data(), out.dev_cols, total * 4);
+    if (!e) e = sync("union pattern");
+    return e;
+  }
+
   // setup.rs:269-321 on the device; the block norms for the join pass come back to the host.
   sf_status run_diagonal() {
     const size_t rb = current.rb, rows = current.rows;
@@ -507,20 +536,25 @@ struct SetupMachine {
     prolongator.rows = rows;
     prolongator.rb = rb;
     prolongator.cb = MODES;
-    symbolic_rows(
-        rows, aggregates, opt.threads,
-        [&](size_t row, auto&& emit) {
-          emit(aggregate[row]);
-          for (uint32_t k = ns[row]; k < ns[row + 1]; ++k) emit(aggregate[nc[k]]);
-        },
-        prolongator.starts, prolongator.cols);
     uint32_t *n_starts = nullptr, *n_cols = nullptr, *agg = nullptr, *rows_of = nullptr;
     double* t = nullptr;
-    size_t entries = prolongator.cols.size();
-    sf_status e = upload_pattern(prolongator);
-    if (!e) e = upload(ns, &n_starts);
+    sf_status e = upload(ns, &n_starts);
     if (!e) e = upload(nc, &n_cols);
     if (!e) e = upload(aggregate, &agg);
+    if (!e && union_on_device(aggregates)) {
+      // the row's own aggregate and its neighbours' aggregates
+      e = device_union(rows, aggregates, n_starts, n_cols, true, nullptr, agg, prolongator);
+    } else if (!e) {
+      symbolic_rows(
+          rows, aggregates, opt.threads,
+          [&](size_t row, auto&& emit) {
+            emit(aggregate[row]);
+            for (uint32_t k = ns[row]; k < ns[row + 1]; ++k) emit(aggregate[nc[k]]);
+          },
+          prolongator.starts, prolongator.cols);
+      e = upload_pattern(prolongator);
+    }
+    size_t entries = prolongator.cols.size();
     const size_t tentative_bytes = rows * rb * MODES * 8;
     if (!e) e = dev_alloc(dev, (void**)&t, std::max<size_t>(1, tentative_bytes));
     if (!e && tentative_bytes) copy_h2d(dev, t, tentative, tentative_bytes);
@@ -545,19 +579,25 @@ struct SetupMachine {
     ap.rows = rows;
     ap.rb = rb;
     ap.cb = MODES;
-    symbolic_rows(
-        rows, aggregates, opt.threads,
-        [&](size_t row, auto&& emit) {
-          for (uint32_t at = current.starts[row]; at < current.starts[row + 1]; ++at) {
-            uint32_t col = current.cols[at];
-            for (uint32_t in = prolongator.starts[col]; in < prolongator.starts[col + 1]; ++in)
-              emit(prolongator.cols[in]);
-          }
-        },
-        ap.starts, ap.cols);
+    sf_status e = SF_OK;
+    if (union_on_device(aggregates)) {
+      e = device_union(rows, aggregates, current.dev_starts, current.dev_cols, false, prolongator.dev_starts,
+                       prolongator.dev_cols, ap);
+    } else {
+      symbolic_rows(
+          rows, aggregates, opt.threads,
+          [&](size_t row, auto&& emit) {
+            for (uint32_t at = current.starts[row]; at < current.starts[row + 1]; ++at) {
+              uint32_t col = current.cols[at];
+              for (uint32_t in = prolongator.starts[col]; in < prolongator.starts[col + 1]; ++in)
+                emit(prolongator.cols[in]);
+            }
+          },
+          ap.starts, ap.cols);
+      e = upload_pattern(ap);
+    }
     uint32_t* rows_of = nullptr;
     size_t entries = ap.cols.size();
-    sf_status e = upload_pattern(ap);
     if (!e) e = dev_alloc(dev, (void**)&ap.dev, std::max<size_t>(1, entries) * rb * MODES * 8);
     if (!e) e = entry_rows(ap, &rows_of);
     if (!e)
@@ -587,21 +627,25 @@ struct SetupMachine {
     coarse = Bsr();
     coarse.rows = aggregates;
     coarse.rb = coarse.cb = cdim;
-    symbolic_rows(
-        aggregates, aggregates, opt.threads,
-        [&](size_t c, auto&& emit) {
-          for (uint32_t k = pt_starts[c]; k < pt_starts[c + 1]; ++k) {
-            uint32_t fine_row = pt_rows[k];
-            for (uint32_t in = ap.starts[fine_row]; in < ap.starts[fine_row + 1]; ++in) emit(ap.cols[in]);
-          }
-        },
-        coarse.starts, coarse.cols);
     uint32_t *d_pt_starts = nullptr, *d_pt_rows = nullptr, *d_pt_at = nullptr, *rows_of = nullptr;
-    size_t entries = coarse.cols.size();
-    sf_status e = upload_pattern(coarse);
-    if (!e) e = upload(pt_starts, &d_pt_starts);
+    sf_status e = upload(pt_starts, &d_pt_starts);
     if (!e) e = upload(pt_rows, &d_pt_rows);
     if (!e) e = upload(pt_at, &d_pt_at);
+    if (!e && union_on_device(aggregates)) {
+      e = device_union(aggregates, aggregates, d_pt_starts, d_pt_rows, false, ap.dev_starts, ap.dev_cols, coarse);
+    } else if (!e) {
+      symbolic_rows(
+          aggregates, aggregates, opt.threads,
+          [&](size_t c, auto&& emit) {
+            for (uint32_t k = pt_starts[c]; k < pt_starts[c + 1]; ++k) {
+              uint32_t fine_row = pt_rows[k];
+              for (uint32_t in = ap.starts[fine_row]; in < ap.starts[fine_row + 1]; ++in) emit(ap.cols[in]);
+            }
+          },
+          coarse.starts, coarse.cols);
+      e = upload_pattern(coarse);
+    }
+    size_t entries = coarse.cols.size();
     if (!e) e = dev_alloc(dev, (void**)&coarse.dev, std::max<size_t>(1, entries) * cdim * cdim * 8);
     if (!e) e = entry_rows(coarse, &rows_of);
     if (!e)

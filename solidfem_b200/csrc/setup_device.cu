@@ -168,6 +168,63 @@ __global__ void power_step_kernel(uint32_t rows, const uint32_t* __restrict__ st
   }
 }
 
+// Row r of a union pattern: the sorted distinct columns inner_cols[k] over the inner rows j of r's
+// outer list (j = r itself first when `self`); with inner_starts null each j has the one column
+// inner_cols[j]. A warp per row sets the columns' bits in its own bitmap of `words` words in shared
+// memory, then walks the bitmap in order: 32 words at a time, a warp prefix sum of their popcounts
+// places each word's set bits. The count pass (out_starts null) writes the row's column count to
+// out[r]; the fill pass writes the columns at out[out_starts[r] ..]. Every bit is cleared after use.
+__global__ void union_rows_kernel(uint32_t rows, uint32_t words, const uint32_t* __restrict__ outer_starts,
+                                  const uint32_t* __restrict__ outer_idx, int self,
+                                  const uint32_t* __restrict__ inner_starts, const uint32_t* __restrict__ inner_cols,
+                                  const uint32_t* __restrict__ out_starts, uint32_t* __restrict__ out) {
+  extern __shared__ uint32_t union_bits[];
+  const unsigned full = 0xffffffffu;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, warps = blockDim.x >> 5;
+  uint32_t* bm = union_bits + (size_t)warp * words;
+  for (uint32_t i = lane; i < words; i += 32) bm[i] = 0;
+  __syncwarp();
+  for (uint32_t r = blockIdx.x * warps + warp; r < rows; r += gridDim.x * warps) {
+    const uint32_t o0 = outer_starts[r], n = outer_starts[r + 1] - o0 + (self ? 1u : 0u);
+    for (uint32_t t = lane; t < n; t += 32) {
+      const uint32_t j = self ? (t == 0 ? r : outer_idx[o0 + t - 1]) : outer_idx[o0 + t];
+      if (inner_starts) {
+        for (uint32_t k = inner_starts[j]; k < inner_starts[j + 1]; ++k) {
+          const uint32_t c = inner_cols[k];
+          atomicOr(&bm[c >> 5], 1u << (c & 31));
+        }
+      } else {
+        const uint32_t c = inner_cols[j];
+        atomicOr(&bm[c >> 5], 1u << (c & 31));
+      }
+    }
+    __syncwarp();
+    const uint32_t base = out_starts ? out_starts[r] : 0u;
+    uint32_t total = 0;
+    for (uint32_t w0 = 0; w0 < words; w0 += 32) {
+      const uint32_t w = w0 + lane;
+      uint32_t bits = w < words ? bm[w] : 0u;
+      const uint32_t cnt = (uint32_t)__popc(bits);
+      uint32_t inc = cnt;
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t v = __shfl_up_sync(full, inc, o);
+        if (lane >= o) inc += v;
+      }
+      if (out_starts) {
+        uint32_t at = base + total + (inc - cnt);
+        while (bits) {
+          out[at++] = w * 32u + (uint32_t)(__ffs(bits) - 1);
+          bits &= bits - 1;
+        }
+      }
+      if (w < words) bm[w] = 0u;
+      total += __shfl_sync(full, inc, 31);
+    }
+    if (!out_starts && lane == 0) out[r] = total;
+    __syncwarp();
+  }
+}
+
 // The block row of each entry of a block pattern.
 __global__ void entry_rows_kernel(uint32_t rows, const uint32_t* __restrict__ starts, uint32_t* __restrict__ out) {
   for (uint32_t row = blockIdx.x * blockDim.x + threadIdx.x; row < rows; row += gridDim.x * blockDim.x)
@@ -434,6 +491,24 @@ sf_status setup_scale(cudaStream_t st, size_t n, const double* src, double d, do
   if (n == 0) return SF_OK;
   scale_kernel<<<grid_for(n), kT, 0, st>>>(n, src, d, v);
   return cuda_check(cudaGetLastError(), "scale");
+}
+
+sf_status setup_union_rows(cudaStream_t st, uint32_t rows, uint32_t width, const uint32_t* outer_starts,
+                           const uint32_t* outer_idx, bool self, const uint32_t* inner_starts,
+                           const uint32_t* inner_cols, const uint32_t* out_starts, uint32_t* out) {
+  const uint32_t words = (width + 31) / 32;
+  const size_t per_warp = (size_t)std::max<uint32_t>(words, 1) * 4;
+  const size_t limit = 200 * 1024;
+  if (per_warp > limit) return fail(SF_INVALID_ARGUMENT, "union pattern wider than one warp's bitmap");
+  const int warps = (int)std::max<size_t>(1, std::min<size_t>(8, limit / per_warp));
+  const size_t smem = per_warp * warps;
+  if (rows == 0) return SF_OK;
+  const void* k = (const void*)union_rows_kernel;
+  if (smem > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)limit);
+  const int grid = (int)std::max<size_t>(1, std::min<size_t>((rows + warps - 1) / warps, 148 * 16));
+  union_rows_kernel<<<grid, 32 * warps, smem, st>>>(rows, words, outer_starts, outer_idx, self ? 1 : 0, inner_starts,
+                                                    inner_cols, out_starts, out);
+  return cuda_check(cudaGetLastError(), "union pattern");
 }
 
 sf_status setup_entry_rows(cudaStream_t st, uint32_t rows, const uint32_t* starts, uint32_t* out) {
