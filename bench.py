@@ -60,9 +60,10 @@ def build_model(sf):
     nodes = mesh.nodes()
     model = sf.Model(mesh, sf.Material(YOUNGS, POISSON))
     model.fix_nodes(np.nonzero(np.abs(nodes[:, 0]) < 1e-9)[0])
-    for f in mesh.boundary_faces():
-        if all(abs(nodes[n][2] - SIZE[2]) < 1e-9 for n in list(f.nodes)[:3]):
-            model.add_traction(f, (0.0, 0.0, -PRESSURE))
+    # the top faces (all three corners at z = thickness), as one array in boundary-face order
+    faces = mesh.boundary_face_array()
+    top = np.all(np.abs(nodes[faces["nodes"][:, :3], 2] - SIZE[2]) < 1e-9, axis=1)
+    model.add_face_tractions(faces[top], (0.0, 0.0, -PRESSURE))
     return mesh, model
 
 
