@@ -180,33 +180,92 @@ __global__ void point_positions_kernel(const double* __restrict__ nodes, const u
   }
 }
 
-// Adds, for every block of the pattern, the contributions of its elements below `end`, resuming
-// where the previous slice stopped.
-__global__ void gather_kernel(size_t blocks, const uint32_t* __restrict__ map_starts, const uint32_t* __restrict__ map,
-                              const double* __restrict__ ke, uint32_t* __restrict__ cursor, uint32_t end,
-                              double* __restrict__ vals) {
-  size_t blk = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
-  if (blk >= blocks) return;
-  uint32_t j = cursor[blk], stop = map_starts[blk + 1];
-  if (j == stop) return;
-  double v[9];
-  for (int k = 0; k < 9; ++k) v[k] = vals[blk * 9 + k];
-  for (; j < stop; ++j) {
-    uint32_t packed = map[j];
-    uint32_t e = packed >> 7;
-    if (e >= end) break;
-    int ab = packed & 127, a = ab / 10, b = ab % 10;
-    if (a <= b) {
-      const double* src = ke + (size_t)e * 495 + (size_t)c_pair[a][b] * 9;
-      for (int k = 0; k < 9; ++k) v[k] += src[k];
-    } else {
-      const double* src = ke + (size_t)e * 495 + (size_t)c_pair[b][a] * 9;
-      for (int i = 0; i < 3; ++i)
-        for (int k = 0; k < 3; ++k) v[i * 3 + k] += src[k * 3 + i];
+// Adds to every block of the pattern the contributions of its elements below `end`, resuming
+// where the previous slice stopped: one warp per block row (free node). The warp stages up to 32
+// of the node's elements (ascending, from the row's cursor) with their ten nodes and the node's
+// place in each; lane j then walks them in order for block j of the row and, where an element
+// also holds the block's column node, adds that element's (a, b) block. Each block therefore
+// sums its elements in ascending order, the order of the reference's element loop
+// (assembly.rs:87-130); no per-block list of contributions exists.
+constexpr int kGatherWarps = 8;
+constexpr int kGatherStage = 32;
+
+__global__ void __launch_bounds__(32 * kGatherWarps)
+    gather_kernel(uint32_t rows, const uint32_t* __restrict__ starts, const uint32_t* __restrict__ cols,
+                  const uint32_t* __restrict__ row_node, const uint32_t* __restrict__ inc_start,
+                  const uint32_t* __restrict__ inc, const uint32_t* __restrict__ tets,
+                  const double* __restrict__ ke, uint32_t* __restrict__ cursor, uint32_t end,
+                  double* __restrict__ vals) {
+  __shared__ uint32_t s_nodes[kGatherWarps][kGatherStage][10];
+  __shared__ uint32_t s_elem[kGatherWarps][kGatherStage];
+  __shared__ int s_place[kGatherWarps][kGatherStage];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const unsigned full = 0xffffffffu;
+  for (uint32_t r = blockIdx.x * kGatherWarps + warp; r < rows; r += gridDim.x * kGatherWarps) {
+    const uint32_t node = row_node[r], k0 = cursor[r], k1 = inc_start[node + 1];
+    const uint32_t b0 = starts[r], nb = starts[r + 1] - b0;
+    uint32_t k_end = k0;
+    for (uint32_t jb = 0; jb < nb; jb += 32) {
+      const uint32_t j = jb + lane;
+      const bool live = j < nb;
+      const uint32_t col_node = live ? row_node[cols[b0 + j]] : 0xffffffffu;
+      double v[9];
+#pragma unroll
+      for (int q = 0; q < 9; ++q) v[q] = live ? vals[(size_t)(b0 + j) * 9 + q] : 0.0;
+      uint32_t k = k0;
+      for (;;) {
+        // stage the next elements below `end` (they are ascending: the first at or past `end`
+        // ends the row's work for this slice)
+        const uint32_t kk = k + lane;
+        const uint32_t e = kk < k1 ? inc[kk] : 0xffffffffu;
+        const bool take = kk < k1 && e < end;
+        const unsigned mask = __ballot_sync(full, take);
+        const int count = __popc(mask);  // a prefix: elements ascend
+        if (take) {
+          s_elem[warp][lane] = e;
+          int place = 0;
+#pragma unroll
+          for (int q = 0; q < 10; ++q) {
+            const uint32_t n = tets[(size_t)e * 10 + q];
+            s_nodes[warp][lane][q] = n;
+            if (n == node) place = q;
+          }
+          s_place[warp][lane] = place;
+        }
+        __syncwarp();
+        if (live) {
+          for (int t = 0; t < count; ++t) {
+            int b = -1;
+#pragma unroll
+            for (int q = 0; q < 10; ++q)
+              if (s_nodes[warp][t][q] == col_node) b = q;
+            if (b < 0) continue;
+            const int a = s_place[warp][t];
+            const size_t el = s_elem[warp][t];
+            if (a <= b) {
+              const double* src = ke + el * 495 + (size_t)c_pair[a][b] * 9;
+#pragma unroll
+              for (int q = 0; q < 9; ++q) v[q] += src[q];
+            } else {
+              const double* src = ke + el * 495 + (size_t)c_pair[b][a] * 9;
+#pragma unroll
+              for (int i = 0; i < 3; ++i)
+#pragma unroll
+                for (int q = 0; q < 3; ++q) v[i * 3 + q] += src[q * 3 + i];
+            }
+          }
+        }
+        __syncwarp();
+        k += (uint32_t)count;
+        if (count < 32) break;
+      }
+      k_end = k;
+      if (live)
+#pragma unroll
+        for (int q = 0; q < 9; ++q) vals[(size_t)(b0 + j) * 9 + q] = v[q];
     }
+    if (lane == 0) cursor[r] = k_end;
   }
-  cursor[blk] = j;
-  for (int k = 0; k < 9; ++k) vals[blk * 9 + k] = v[k];
 }
 
 // The rules' points (crates/solidfem-elastic/src/quadrature.rs:111-144) and the Tet10 shape
@@ -314,10 +373,12 @@ sf_status launch_point_positions(const AssemblyDevice& a, cudaStream_t stream) {
 }
 
 sf_status launch_gather(const AssemblyDevice& a, DevBsr& system, uint32_t end, cudaStream_t stream) {
-  if (system.blocks == 0) return SF_OK;
+  if (system.blocks == 0 || system.rows == 0) return SF_OK;
   if (sf_status s = ensure_tables(a.quadrature, stream)) return s;
-  gather_kernel<<<(unsigned)((system.blocks + 255) / 256), 256, 0, stream>>>(
-      system.blocks, a.map_starts, a.map, a.ke, a.cursor, end, (double*)system.vals);
+  const unsigned grid = (unsigned)std::min<size_t>((system.rows + kGatherWarps - 1) / kGatherWarps, 148 * 64);
+  gather_kernel<<<grid, 32 * kGatherWarps, 0, stream>>>(system.rows, system.starts, system.cols, a.row_node,
+                                                        a.inc_start, a.inc, a.tets, a.ke, a.cursor, end,
+                                                        (double*)system.vals);
   return cuda_check(cudaGetLastError(), "gather");
 }
 

@@ -248,9 +248,10 @@ struct AssemblyDevice {
   double* ke = nullptr;           // 495 x tet_count upper-triangle element stiffness
   double* point_material = nullptr;  // tet_count x points x 2 (E, nu) when a callback supplies it
   double* positions = nullptr;    // tet_count x points x 3, integration point positions
-  uint32_t* map_starts = nullptr; // blocks + 1
-  uint32_t* map = nullptr;        // (element << 7) | (10 a + b), ascending element per block
-  uint32_t* cursor = nullptr;     // blocks: next map entry to add
+  uint32_t* inc_start = nullptr;  // node_count + 1: each node's elements in inc, ascending
+  uint32_t* inc = nullptr;        // 10 x tet_count
+  uint32_t* row_node = nullptr;   // per free block row: its node
+  uint32_t* cursor = nullptr;     // per free block row: the next of its node's elements to add
   unsigned long long* error = nullptr;  // (tet << 32) | (point << 8) | kind, min over faults
   uint32_t tet_count = 0;
   int quadrature = 0;

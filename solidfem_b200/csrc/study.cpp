@@ -262,69 +262,35 @@ struct NoInit : std::allocator<T> {
 };
 typedef vector<uint32_t, NoInit<uint32_t>> RawU32;
 
-// An uninitialised page-locked host array from the pinned pool (never freed, so dropping it does
-// not synchronize the device): the assembly map is written straight into memory the upload can
-// read at full link speed, and handed back to the pool once it is on the device.
-struct PinnedU32 {
-  uint32_t* p = nullptr;
-  size_t n = 0;
-  PinnedU32() = default;
-  PinnedU32(const PinnedU32&) = delete;
-  PinnedU32& operator=(const PinnedU32&) = delete;
-  PinnedU32(PinnedU32&& o) noexcept : p(o.p), n(o.n) { o.p = nullptr, o.n = 0; }
-  PinnedU32& operator=(PinnedU32&& o) noexcept {
-    if (this != &o) {
-      release();
-      p = o.p;
-      n = o.n;
-      o.p = nullptr;
-      o.n = 0;
-    }
-    return *this;
-  }
-  ~PinnedU32() { release(); }
-  bool resize(size_t count) {
-    release();
-    p = (uint32_t*)pinned_acquire(std::max<size_t>(1, count) * 4);
-    n = p ? count : 0;
-    return p != nullptr;
-  }
-  void release() {
-    pinned_return(p);
-    p = nullptr;
-    n = 0;
-  }
-  uint32_t* data() { return p; }
-  const uint32_t* data() const { return p; }
-  size_t size() const { return n; }
-  bool empty() const { return n == 0; }
-  uint32_t& operator[](size_t i) { return p[i]; }
-  const uint32_t& operator[](size_t i) const { return p[i]; }
-};
-
 struct HostPattern {
   vector<uint32_t> starts;                 // block rows over free nodes
   RawU32 cols;
-  PinnedU32 map_starts, map;               // per block: (element << 7) | (10 a + b), ascending
+  // Node-to-element incidence (each node's elements ascending) and each free row's node: the
+  // device gather walks them, so no per-block list of contributions is built on the host.
+  vector<uint32_t> inc_start, inc, row_node;
 };
 
-// The free-node block pattern (assembly.rs:55-81, csr.rs:19-71) and, for each block, the
-// elements that add to it in ascending order, built row-parallel from node-to-element incidence.
+// The free-node block pattern (assembly.rs:55-81, csr.rs:19-71), built row-parallel from
+// node-to-element incidence, which is kept for the device assembly.
 bool build_pattern(const Mesh& m, const vector<uint32_t>& free, size_t free_count, int threads, HostPattern& hp) {
   size_t nn = m.nodes.size(), ne = m.tets.size();
-  vector<uint32_t> inc_start(nn + 1, 0);
+  vector<uint32_t>& inc_start = hp.inc_start;
+  inc_start.assign(nn + 1, 0);
   for (auto& t : m.tets)
     for (uint32_t n : t) inc_start[n + 1] += 1;
   for (size_t i = 0; i < nn; ++i) inc_start[i + 1] += inc_start[i];
-  vector<uint32_t> fill(inc_start.begin(), inc_start.end() - 1), inc(inc_start[nn]);
+  vector<uint32_t> fill(inc_start.begin(), inc_start.end() - 1);
+  vector<uint32_t>& inc = hp.inc;
+  inc.resize(inc_start[nn]);
   for (size_t e = 0; e < ne; ++e)
     for (uint32_t n : m.tets[e]) inc[fill[n]++] = (uint32_t)e;
-  vector<uint32_t> row_node(free_count);
+  vector<uint32_t>& row_node = hp.row_node;
+  row_node.resize(free_count);
   for (size_t n = 0; n < nn; ++n)
     if (free[n] != FIXED) row_node[free[n]] = (uint32_t)n;
-  // Per row: its distinct columns (a per-thread marker array stamped with the row) and its entry
-  // count, then the sorted columns and, per block, the entries in element order.
-  vector<uint32_t> counts(free_count, 0), map_counts(free_count, 0);
+  // Per row its distinct columns (a per-thread marker array stamped with the row), then the
+  // sorted columns.
+  vector<uint32_t> counts(free_count, 0);
 #ifdef _OPENMP
 #pragma omp parallel num_threads(threads)
 #endif
@@ -334,35 +300,26 @@ bool build_pattern(const Mesh& m, const vector<uint32_t>& free, size_t free_coun
 #pragma omp for schedule(dynamic, 1024)
 #endif
     for (long long r = 0; r < (long long)free_count; ++r) {
-      uint32_t node = row_node[r], distinct = 0, entries = 0;
+      uint32_t node = row_node[r], distinct = 0;
       for (uint32_t k = inc_start[node]; k < inc_start[node + 1]; ++k)
         for (uint32_t n : m.tets[inc[k]]) {
           uint32_t fc = free[n];
-          if (fc == FIXED) continue;
-          ++entries;
-          if (mark[fc] != (uint32_t)r) {
+          if (fc != FIXED && mark[fc] != (uint32_t)r) {
             mark[fc] = (uint32_t)r;
             ++distinct;
           }
         }
       counts[r] = distinct;
-      map_counts[r] = entries;
     }
   }
   hp.starts.assign(free_count + 1, 0);
-  vector<uint64_t> map_row(free_count + 1, 0);
-  for (size_t r = 0; r < free_count; ++r) {
-    hp.starts[r + 1] = hp.starts[r] + counts[r];
-    map_row[r + 1] = map_row[r] + map_counts[r];
-  }
+  for (size_t r = 0; r < free_count; ++r) hp.starts[r + 1] = hp.starts[r] + counts[r];
   hp.cols.resize(hp.starts[free_count]);
-  if (!hp.map_starts.resize(hp.starts[free_count] + 1) || !hp.map.resize(map_row[free_count])) return false;
 #ifdef _OPENMP
 #pragma omp parallel num_threads(threads)
 #endif
   {
-    vector<uint32_t> mark(free_count, 0xffffffffu), pos(free_count, 0), cols, per;
-    vector<uint64_t> at;
+    vector<uint32_t> mark(free_count, 0xffffffffu), cols;
 #ifdef _OPENMP
 #pragma omp for schedule(dynamic, 1024)
 #endif
@@ -378,34 +335,9 @@ bool build_pattern(const Mesh& m, const vector<uint32_t>& free, size_t free_coun
           }
         }
       std::sort(cols.begin(), cols.end());
-      uint32_t b0 = hp.starts[r];
-      std::copy(cols.begin(), cols.end(), hp.cols.begin() + b0);
-      per.assign(cols.size(), 0);
-      for (size_t j = 0; j < cols.size(); ++j) pos[cols[j]] = (uint32_t)j;
-      for (uint32_t k = inc_start[node]; k < inc_start[node + 1]; ++k)
-        for (uint32_t n : m.tets[inc[k]])
-          if (free[n] != FIXED) per[pos[free[n]]] += 1;
-      uint64_t base = map_row[r];
-      at.resize(cols.size());
-      for (size_t j = 0; j < cols.size(); ++j) {
-        at[j] = base;
-        hp.map_starts[b0 + j] = (uint32_t)base;
-        base += per[j];
-      }
-      for (uint32_t k = inc_start[node]; k < inc_start[node + 1]; ++k) {
-        uint32_t e = inc[k];
-        const auto& t = m.tets[e];
-        int a = 0;
-        while (t[a] != node) ++a;
-        for (int b = 0; b < 10; ++b) {
-          uint32_t fc = free[t[b]];
-          if (fc == FIXED) continue;
-          hp.map[at[pos[fc]]++] = (e << 7) | (uint32_t)(10 * a + b);
-        }
-      }
+      std::copy(cols.begin(), cols.end(), hp.cols.begin() + hp.starts[r]);
     }
   }
-  hp.map_starts[hp.starts[free_count]] = (uint32_t)map_row[free_count];
   return true;
 }
 
@@ -757,8 +689,7 @@ sf_status sf_builder_create(sf_model* model, const sf_study_options* options, sf
   for (auto& p : b->prescribed) all_zero = all_zero && p.second == 0.0;
   if (all_zero) return fail(SF_NO_EFFECTIVE_LOAD, "the model has no effective load");
   double t0 = now_seconds();
-  if (!build_pattern(mesh, b->free, b->free_count, b->threads, b->pattern))
-    return fail(SF_CUDA_ERROR, "cudaMallocHost failed for the assembly map");
+  build_pattern(mesh, b->free, b->free_count, b->threads, b->pattern);
   // Device set-up: mesh, element stiffness buffer, pattern and assembly map, system matrix.
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(SF_NO_DEVICE, "no CUDA device is visible");
@@ -777,16 +708,18 @@ sf_status sf_builder_create(sf_model* model, const sf_study_options* options, sf
   a.points = md.quadrature == SF_QUADRATURE_FOURTEEN_POINT ? 14 : 4;
   size_t blocks = b->pattern.cols.size();
   size_t budget = b->options.device_memory_budget;
-  size_t need = nn * 24 + mesh.tets.size() * 40 + mesh.tets.size() * 495 * 8 + blocks * (4 + 72 + 8) +
-                b->pattern.map.size() * 4;
+  const HostPattern& hp = b->pattern;
+  size_t need = nn * 24 + mesh.tets.size() * 40 + mesh.tets.size() * 495 * 8 + blocks * (4 + 72) +
+                (hp.inc_start.size() + hp.inc.size() + 2 * hp.row_node.size()) * 4;
   if (budget && need > budget) return fail(SF_DEVICE_MEMORY_BUDGET, "the assembly does not fit the device memory budget");
   sf_status e = SF_OK;
   if (!e) e = dev_alloc(s, (void**)&a.nodes, nn * 24);
   if (!e) e = dev_alloc(s, (void**)&a.tets, mesh.tets.size() * 40);
   if (!e) e = dev_alloc(s, (void**)&a.ke, mesh.tets.size() * 495 * 8);
-  if (!e) e = dev_alloc(s, (void**)&a.map_starts, (blocks + 1) * 4);
-  if (!e) e = dev_alloc(s, (void**)&a.map, std::max<size_t>(1, b->pattern.map.size()) * 4);
-  if (!e) e = dev_alloc(s, (void**)&a.cursor, std::max<size_t>(1, blocks) * 4);
+  if (!e) e = dev_alloc(s, (void**)&a.inc_start, hp.inc_start.size() * 4);
+  if (!e) e = dev_alloc(s, (void**)&a.inc, std::max<size_t>(1, hp.inc.size()) * 4);
+  if (!e) e = dev_alloc(s, (void**)&a.row_node, std::max<size_t>(1, hp.row_node.size()) * 4);
+  if (!e) e = dev_alloc(s, (void**)&a.cursor, std::max<size_t>(1, hp.row_node.size()) * 4);
   if (!e) e = dev_alloc(s, (void**)&a.error, 8);
   s.system.rows = (uint32_t)b->free_count;
   s.system.rb = s.system.cb = 3;
@@ -800,11 +733,15 @@ sf_status sf_builder_create(sf_model* model, const sf_study_options* options, sf
   }
   copy_h2d(s, a.nodes, mesh.nodes.data(), nn * 24);
   copy_h2d(s, a.tets, mesh.tets.data(), mesh.tets.size() * 40);
-  copy_h2d(s, a.map_starts, b->pattern.map_starts.data(), (blocks + 1) * 4);
-  if (!b->pattern.map.empty())
-    copy_h2d(s, a.map, b->pattern.map.data(), b->pattern.map.size() * 4);
-  // the gather's per-block cursors start at the map starts: a copy on the device
-  cudaMemcpyAsync(a.cursor, a.map_starts, blocks * 4, cudaMemcpyDeviceToDevice, s.stream);
+  // each row's cursor starts at its node's first element
+  vector<uint32_t> cursor(hp.row_node.size());
+  for (size_t r = 0; r < cursor.size(); ++r) cursor[r] = hp.inc_start[hp.row_node[r]];
+  copy_h2d(s, a.inc_start, hp.inc_start.data(), hp.inc_start.size() * 4);
+  if (!hp.inc.empty()) copy_h2d(s, a.inc, hp.inc.data(), hp.inc.size() * 4);
+  if (!cursor.empty()) {
+    copy_h2d(s, a.row_node, hp.row_node.data(), cursor.size() * 4);
+    copy_h2d(s, a.cursor, cursor.data(), cursor.size() * 4);
+  }
   unsigned long long none = ~0ull;
   copy_h2d(s, a.error, &none, 8);
   copy_h2d(s, s.system.starts, b->pattern.starts.data(), (b->free_count + 1) * 4);
@@ -841,9 +778,10 @@ sf_status sf_builder_create(sf_model* model, const sf_study_options* options, sf
     release_builder_device(b.get());
     return e;
   }
-  // The map is on the device now: its host copy goes back to the pool.
-  b->pattern.map.release();
-  b->pattern.map_starts.release();
+  // The incidence is on the device now.
+  vector<uint32_t>().swap(b->pattern.inc_start);
+  vector<uint32_t>().swap(b->pattern.inc);
+  vector<uint32_t>().swap(b->pattern.row_node);
   b->assembly_seconds = now_seconds() - t0;
   *out = b.release();
   return SF_OK;
@@ -970,11 +908,10 @@ static sf_status builder_assemble(sf_builder* b, uint64_t max_elements, sf_cance
     }
     // The element stiffness buffer and the assembly map have served; free them for the solve.
     AssemblyDevice& a = b->asmdev;
-    for (void* p : {(void*)a.ke, (void*)a.map, (void*)a.map_starts, (void*)a.cursor}) dev_free(s, p);
+    for (void* p : {(void*)a.ke, (void*)a.inc_start, (void*)a.inc, (void*)a.row_node, (void*)a.cursor})
+      dev_free(s, p);
     a.ke = nullptr;
-    a.map = a.map_starts = a.cursor = nullptr;
-    b->pattern.map.release();
-    b->pattern.map_starts.release();
+    a.inc_start = a.inc = a.row_node = a.cursor = nullptr;
   }
   return SF_OK;
 }
