@@ -172,10 +172,9 @@ inline void copy_d2h(const DeviceSolver& s, void* dst, const void* src, size_t b
   cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, s.stream);
   s.d2h_bytes += bytes;
 }
-// Pinned host memory that is never freed (freeing pinned memory synchronizes the device): a
-// grow-only scratch buffer per host thread, and 512-byte slots for per-study state.
+// Pinned host memory that is never freed (freeing pinned memory synchronizes the device):
+// pooled buffers, and 512-byte slots for per-study state.
 static const size_t kPinnedSlotBytes = 512;
-double* pinned_scratch(size_t bytes);
 // A process-wide pool of page-locked host buffers that are never freed (cudaFreeHost would
 // synchronize the whole device): pinned_acquire returns the smallest free buffer of at least
 // `bytes` (or a new one), pinned_return hands it back. Unlike the per-thread scratch, a buffer

@@ -90,7 +90,7 @@ struct sf_server {
     if (st) {
       sf_error err;
       sf_last_error(&err);
-      std::snprintf(r->message, sizeof r->message, "%s", err.message);
+      std::snprintf(r->message, sizeof r->message, "%.159s", err.message);
     }
     if (r->study) {
       if (!st) {

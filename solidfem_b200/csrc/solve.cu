@@ -1261,11 +1261,13 @@ struct TailAxpy {
   Vref<V> y, b;
   V in[N];
   __device__ __forceinline__ void pre(uint32_t row, bool live, int tl) {
-    if (OP == OP_SET || !live) return;
+    if constexpr (OP != OP_SET) {
+      if (!live) return;
 #pragma unroll
-    for (int k = 0; k < N; ++k) {
-      int p = tl + k * LPR;
-      if (p < 6) in[k] = OP == OP_RESIDUAL ? b.load(row, p) : y.load(row, p);
+      for (int k = 0; k < N; ++k) {
+        int p = tl + k * LPR;
+        if (p < 6) in[k] = OP == OP_RESIDUAL ? b.load(row, p) : y.load(row, p);
+      }
     }
   }
   __device__ __forceinline__ void post(uint32_t row, bool live, const V (&acc)[6], int tl) {
@@ -2189,19 +2191,6 @@ sf_status cuda_check(cudaError_t e, const char* what) {
 // Pinned host memory is never returned: freeing it synchronizes the whole device. Per host thread
 // a grow-only scratch buffer (earlier, smaller buffers stay allocated and valid), and a shared
 // pool of fixed 512-byte slots for per-study state read-backs.
-double* pinned_scratch(size_t bytes) {
-  thread_local double* buf = nullptr;
-  thread_local size_t cap = 0;
-  if (bytes > cap) {
-    size_t want = std::max(bytes, 2 * cap);
-    void* p = nullptr;
-    if (cudaMallocHost(&p, want) != cudaSuccess) return nullptr;
-    buf = (double*)p;
-    cap = want;
-  }
-  return buf;
-}
-
 namespace {
 std::mutex g_slot_mutex;
 std::vector<void*> g_free_slots;
