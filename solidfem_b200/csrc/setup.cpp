@@ -266,31 +266,38 @@ struct SetupMachine {
     closest.assign(rows, 0.0);
     double limit_scale = reach * reach;
     vector<uint32_t> counts(rows, 0);
+    // One distance per entry: the row's distances are kept while its closest one is found, and
+    // each entry's verdict is marked for the fill pass.
+    vector<unsigned char> strong(current.cols.size());
     rows_parallel(rows, opt.threads, [&](size_t row) {
+      thread_local vector<double> dist;
+      const uint32_t a0 = current.starts[row], a1 = current.starts[row + 1];
+      dist.resize(a1 - a0);
       double c = std::numeric_limits<double>::max();
-      for (uint32_t at = current.starts[row]; at < current.starts[row + 1]; ++at) {
+      for (uint32_t at = a0; at < a1; ++at) {
         uint32_t col = current.cols[at];
-        if (col != row) c = std::min(c, squared_distance(positions, row, col));
+        if (col != row) {
+          dist[at - a0] = squared_distance(positions, row, col);
+          c = std::min(c, dist[at - a0]);
+        }
       }
       closest[row] = c;
       double limit = limit_scale * c;
       uint32_t n = 0;
-      for (uint32_t at = current.starts[row]; at < current.starts[row + 1]; ++at) {
-        uint32_t col = current.cols[at];
-        if (col != row && squared_distance(positions, row, col) <= limit) ++n;
+      for (uint32_t at = a0; at < a1; ++at) {
+        const bool s = current.cols[at] != row && dist[at - a0] <= limit;
+        strong[at] = s;
+        n += s;
       }
       counts[row] = n;
     });
     strong_starts.assign(rows + 1, 0);
     for (size_t r = 0; r < rows; ++r) strong_starts[r + 1] = strong_starts[r] + counts[r];
-    strong_cols.assign(strong_starts[rows], 0);
+    strong_cols.resize(strong_starts[rows]);
     rows_parallel(rows, opt.threads, [&](size_t row) {
-      double limit = limit_scale * closest[row];
       uint32_t w = strong_starts[row];
-      for (uint32_t at = current.starts[row]; at < current.starts[row + 1]; ++at) {
-        uint32_t col = current.cols[at];
-        if (col != row && squared_distance(positions, row, col) <= limit) strong_cols[w++] = col;
-      }
+      for (uint32_t at = current.starts[row]; at < current.starts[row + 1]; ++at)
+        if (strong[at]) strong_cols[w++] = current.cols[at];
     });
     phase = AGGREGATE;
   }
@@ -315,15 +322,17 @@ struct SetupMachine {
         seeded[strong_cols[k]] = 1;
       }
     }
+    // join pass: a row's strong neighbours are stamped with the row (the same test as a search
+    // of its strong list)
+    vector<uint32_t> stamp(rows, NO_AGGREGATE);
     for (size_t row = 0; row < rows; ++row) {
       if (aggregate[row] != NO_AGGREGATE) continue;
-      const uint32_t* nb = strong_cols.data() + strong_starts[row];
-      const uint32_t* ne = strong_cols.data() + strong_starts[row + 1];
+      for (uint32_t k = strong_starts[row]; k < strong_starts[row + 1]; ++k) stamp[strong_cols[k]] = (uint32_t)row;
       double best = 0.0;
       uint32_t chosen = NO_AGGREGATE;
       for (uint32_t at = current.starts[row]; at < current.starts[row + 1]; ++at) {
         uint32_t col = current.cols[at];
-        if (!std::binary_search(nb, ne, col) || !seeded[col]) continue;
+        if (stamp[col] != (uint32_t)row || !seeded[col]) continue;
         double n = norms[at];
         if (n > best) {
           best = n;
