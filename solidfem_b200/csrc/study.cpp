@@ -637,19 +637,24 @@ sf_status sf_builder_create(sf_model* model, const sf_study_options* options, sf
     for (int a = 0; a < 3; ++a) load[3 * (size_t)f.first + a] += f.second[a];
   }
   if (!md.tractions.empty()) {
-    auto key = [](const sf_boundary_face& f) {
-      std::array<uint32_t, 8> k;
-      k[0] = f.tet;
-      k[1] = f.face;
-      for (int i = 0; i < 6; ++i) k[2 + i] = f.nodes[i];
-      return k;
+    // A boundary face is fixed by its (tet, face): a per-tet mask of boundary faces, and the
+    // face's nodes compared with the mesh's own entry, decide membership in the boundary list.
+    vector<unsigned char> boundary_mask(mesh.tets.size(), 0);
+    vector<uint32_t> entry(mesh.tets.size() * 4, 0);
+    for (size_t i = 0; i < mesh.faces.size(); ++i) {
+      const sf_boundary_face& f = mesh.faces[i];
+      boundary_mask[f.tet] |= (unsigned char)(1u << f.face);
+      entry[(size_t)f.tet * 4 + f.face] = (uint32_t)i;
+    }
+    auto on_boundary = [&](const sf_boundary_face& f) {
+      if (f.tet >= mesh.tets.size() || f.face >= 4 || !(boundary_mask[f.tet] & (1u << f.face))) return false;
+      const sf_boundary_face& g = mesh.faces[entry[(size_t)f.tet * 4 + f.face]];
+      for (int i = 0; i < 6; ++i)
+        if (g.nodes[i] != f.nodes[i]) return false;
+      return true;
     };
-    vector<std::array<uint32_t, 8>> boundary;
-    boundary.reserve(mesh.faces.size());
-    for (auto& f : mesh.faces) boundary.push_back(key(f));
-    std::sort(boundary.begin(), boundary.end());
     for (auto& tr : md.tractions) {
-      if (!std::binary_search(boundary.begin(), boundary.end(), key(tr.first))) {
+      if (!on_boundary(tr.first)) {
         error_slot().tet = tr.first.tet;
         error_slot().face = tr.first.face;
         return fail(SF_FACE_NOT_ON_BOUNDARY, "a traction face is not on the mesh boundary");
