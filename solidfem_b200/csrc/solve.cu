@@ -1527,6 +1527,135 @@ inline size_t tail_cta_bytes(const std::vector<uint32_t>& a_starts, const std::v
          4 * tail_align(own * vector_bytes);
 }
 
+// ------------------------------------------------------------ smoother starts fused into products
+// A level's smoother starts from zero on a right-hand side that a product has just made: the
+// residual b - A x before the post-smoother, the restriction R r before a coarser level's
+// pre-smoother. The start (cheb_start_kernel, term for term: r = b; d = (D^-1 b) / theta; x = d)
+// is done in that product's epilogue, from the row's freshly summed values, so the start needs
+// no launch of its own and the post-smoother's right-hand side never goes to memory.
+template <typename S, typename V>
+struct StartArgs {
+  const S* dinv;
+  V* b_out;  // the right-hand side, when the level reads it again (the restricted b); or null
+  V* r;
+  V* d;
+  V* x;
+  V theta;
+};
+
+// Component p of a block row's start from the row's right-hand side values bv.
+template <typename S, typename V, int RB>
+__device__ __forceinline__ void start_part(const StartArgs<S, V>& a, uint32_t row, int p, const V (&bv)[RB]) {
+  const size_t base = (size_t)row * RB;
+  if (a.b_out) a.b_out[base + p] = bv[p];
+  a.r[base + p] = bv[p];
+  V z = V(0);
+#pragma unroll
+  for (int q = 0; q < RB; ++q) z += V(a.dinv[base * RB + p * RB + q]) * bv[q];
+  V dv = z / a.theta;
+  a.d[base + p] = dv;
+  a.x[base + p] = dv;
+}
+
+// SELL-32 (one thread per block row).
+template <typename S, typename V, int RB, int OP>
+struct SellStart {
+  StartArgs<S, V> a;
+  const V* __restrict__ b;
+  V in[RB];
+  __device__ __forceinline__ void pre(uint32_t row, bool live) {
+    if (OP != OP_RESIDUAL || !live) return;
+#pragma unroll
+    for (int q = 0; q < RB; ++q) in[q] = b[(size_t)row * RB + q];
+  }
+  __device__ __forceinline__ void post(uint32_t row, bool live, uint32_t, const V (&acc)[RB], const V (&)[RB]) {
+    if (!live) return;
+    V bv[RB];
+#pragma unroll
+    for (int q = 0; q < RB; ++q) bv[q] = OP == OP_RESIDUAL ? in[q] - acc[q] : acc[q];
+#pragma unroll
+    for (int p = 0; p < RB; ++p) start_part<S, V, RB>(a, row, p, bv);
+  }
+};
+
+template <typename S, typename V, int RB, int CB, int OP>
+__device__ __forceinline__ void sell_start_kernel(SellOp<S> A, const V* __restrict__ x, const V* __restrict__ b,
+                                                  StartArgs<S, V> a, const int* __restrict__ status) {
+  if (*status != ST_ACTIVE) return;
+  SellStart<S, V, RB, OP> epi;
+  epi.a = a;
+  epi.b = b;
+  sell_rows<S, V, RB, CB, false>(A, x, epi);
+}
+
+// Split rows (lane 6 m + p: scalar row p of block row m); the six values of a block row meet by
+// shuffles, as in SplitCheb.
+template <typename S, typename V, int OP>
+struct SplitStart {
+  StartArgs<S, V> a;
+  const V* __restrict__ b;
+  V in;
+  __device__ __forceinline__ void pre(uint32_t row, uint32_t part, bool live) {
+    if (OP == OP_RESIDUAL && live) in = b[(size_t)row * 6 + part];
+  }
+  __device__ __forceinline__ void post(uint32_t row, uint32_t part, bool live, V acc) {
+    const V t = live ? (OP == OP_RESIDUAL ? in - acc : acc) : V(0);
+    const uint32_t first = (threadIdx.x & 31) - part;
+    V bv[6];
+#pragma unroll
+    for (int q = 0; q < 6; ++q) bv[q] = __shfl_sync(kFull, t, (first + q) & 31);
+    if (!live) return;
+    start_part<S, V, 6>(a, row, (int)part, bv);
+  }
+};
+
+template <typename S, typename V, int CB, int OP>
+__device__ __forceinline__ void split_start_kernel(SellOp<S> A, const V* __restrict__ x, const V* __restrict__ b,
+                                                   StartArgs<S, V> a, const int* __restrict__ status) {
+  if (*status != ST_ACTIVE) return;
+  SplitStart<S, V, OP> epi;
+  epi.a = a;
+  epi.b = b;
+  epi.in = V(0);
+  split_rows<S, V, CB>(A, x, epi);
+}
+
+// Row groups (LPR lanes per row): after the butterfly every lane holds the whole row.
+template <typename S, typename V, int RB, int LPR, int OP>
+struct EpiStart {
+  StartArgs<S, V> a;
+  const V* __restrict__ b;
+  V in[RB];
+  __device__ __forceinline__ void pre(uint32_t row, bool live, int) {
+    if (OP != OP_RESIDUAL || !live) return;
+#pragma unroll
+    for (int q = 0; q < RB; ++q) in[q] = b[(size_t)row * RB + q];
+  }
+  __device__ __forceinline__ void post(uint32_t row, bool live, const V (&acc)[RB], const V (&)[RB], int tl) {
+    if (!live) return;
+    V bv[RB];
+#pragma unroll
+    for (int q = 0; q < RB; ++q) bv[q] = OP == OP_RESIDUAL ? in[q] - acc[q] : acc[q];
+#pragma unroll
+    for (int k = 0; k < Parts<RB, LPR>::N; ++k) {
+      const int p = tl + k * LPR;
+      if (p < RB) start_part<S, V, RB>(a, row, p, bv);
+    }
+  }
+};
+
+template <typename S, typename V, int RB, int CB, int LPR, int OP>
+__device__ __forceinline__ void bsr_start_kernel(Op<S> A, const V* __restrict__ x, const V* __restrict__ b,
+                                                 StartArgs<S, V> a, const int* __restrict__ status) {
+  if (*status != ST_ACTIVE) return;
+  extern __shared__ __align__(16) char smem[];
+  char* wbase = smem + (threadIdx.x >> 5) * 2 * slot_bytes(A);
+  EpiStart<S, V, RB, LPR, OP> epi;
+  epi.a = a;
+  epi.b = b;
+  run_groups<S, V, RB, CB, LPR, false>(A, x, wbase, epi);
+}
+
 struct SellDot {
   const double* __restrict__ p;
   double* __restrict__ ap;
@@ -2009,18 +2138,71 @@ void launch_cheb_start(const DevLevel& L, const B* b_in, V* b_out, V* r, V* d, V
       L.a.rows, (const S*)L.dinv, b_in, b_out, r, d, x, (V)theta, status);
 }
 
+// The product of `m` (a residual b - m x or a restriction m x) with the smoother start of the
+// level that reads its result fused in (sell_start_kernel / split_start_kernel / bsr_start_kernel).
+template <typename S, typename V, int RB, int CB, int OP>
+void launch_start_rb(const DevBsr& m, const V* x, const V* b, const StartArgs<S, V>& a, const int* status,
+                     cudaStream_t st) {
+  if constexpr (RB == 6) {
+    if (m.split) {
+      launch_body<split_start_kernel<S, V, CB, OP>>(grid_for_slices(m.nslices), kThreads, 0, st, sell_of<S>(m), x, b,
+                                                    a, status);
+      return;
+    }
+  }
+  if (m.sell) {
+    launch_body<sell_start_kernel<S, V, RB, CB, OP>>(grid_for_slices(m.nslices), kThreads, 0, st, sell_of<S>(m), x, b,
+                                                     a, status);
+    return;
+  }
+  Op<S> A = op_of<S>(m);
+  Shape sh = shape_of(A, false);
+  switch (m.lanes_per_row) {
+    case 4: launch_body<bsr_start_kernel<S, V, RB, CB, 4, OP>>(sh.grid, sh.threads, sh.smem, st, A, x, b, a, status); break;
+    case 8: launch_body<bsr_start_kernel<S, V, RB, CB, 8, OP>>(sh.grid, sh.threads, sh.smem, st, A, x, b, a, status); break;
+    case 16: launch_body<bsr_start_kernel<S, V, RB, CB, 16, OP>>(sh.grid, sh.threads, sh.smem, st, A, x, b, a, status); break;
+    default: launch_body<bsr_start_kernel<S, V, RB, CB, 32, OP>>(sh.grid, sh.threads, sh.smem, st, A, x, b, a, status); break;
+  }
+}
+
+template <typename S, typename V, int OP>
+void launch_start_product(const DevBsr& m, const V* x, const V* b, const StartArgs<S, V>& a, const int* status,
+                          cudaStream_t st) {
+  if (m.rb == 3)
+    launch_start_rb<S, V, 3, 3, OP>(m, x, b, a, status, st);
+  else if (m.cb == 3)
+    launch_start_rb<S, V, 6, 3, OP>(m, x, b, a, status, st);
+  else
+    launch_start_rb<S, V, 6, 6, OP>(m, x, b, a, status, st);
+}
+
+template <typename S, typename V>
+StartArgs<S, V> start_args(const DevLevel& L, V* b_out, V* x) {
+  StartArgs<S, V> a;
+  a.dinv = (const S*)L.dinv;
+  a.b_out = b_out;
+  a.r = (V*)L.res;
+  a.d = (V*)L.d0;
+  a.x = x;
+  a.theta = (V)L.theta;
+  return a;
+}
+
 // The smoother from a zero guess on right-hand side b into x (cycle.rs:570-651). `outer`, when
 // given, receives x += (smoothed x) at the last step instead of storing x.
 template <typename S, typename V, typename B>
-void enqueue_smooth(DeviceSolver& s, DevLevel& L, const B* b_in, V* b_out, V* x, V* outer, const int* status) {
+void enqueue_smooth(DeviceSolver& s, DevLevel& L, const B* b_in, V* b_out, V* x, V* outer, const int* status,
+                    bool started = false) {
   cudaStream_t st = s.stream;
   V* r = (V*)L.res;
   V* d[2] = {(V*)L.d0, (V*)L.d1};
-  if (L.a.rb == 3)
-    launch_cheb_start<S, V, B, 3>(L, b_in, b_out, r, d[0], x, L.theta, status, st);
-  else
-    launch_cheb_start<S, V, B, 6>(L, b_in, b_out, r, d[0], x, L.theta, status, st);
-  s.launches_per_iteration++;
+  if (!started) {  // else the product that made b_in did the start
+    if (L.a.rb == 3)
+      launch_cheb_start<S, V, B, 3>(L, b_in, b_out, r, d[0], x, L.theta, status, st);
+    else
+      launch_cheb_start<S, V, B, 6>(L, b_in, b_out, r, d[0], x, L.theta, status, st);
+    s.launches_per_iteration++;
+  }
   for (size_t k = 0; k < L.steps.size(); ++k) {
     bool last = k + 1 == L.steps.size();
     V* o = last ? outer : nullptr;
@@ -2118,7 +2300,8 @@ unsigned tail_cluster_size(const HostLevel& hs, const HostLevel& hc, size_t* sme
 // One V-cycle from level `li` (cycle.rs:461-539). B is the type of the right-hand side; an f64
 // right-hand side reaching an f32 level is rounded into b_store first.
 template <typename S, typename V, typename B>
-void enqueue_cycle(DeviceSolver& s, size_t li, const B* rhs, V* b_store, V* x, const int* status) {
+void enqueue_cycle(DeviceSolver& s, size_t li, const B* rhs, V* b_store, V* x, const int* status,
+                   bool started = false) {
   if ((int)li == s.tail_level) {
     enqueue_tail<S, V>(s, li, status);
     return;
@@ -2136,21 +2319,30 @@ void enqueue_cycle(DeviceSolver& s, size_t li, const B* rhs, V* b_store, V* x, c
       launch_body<coarse_solve_kernel<V>>(grid_for_rows(L.n), kThreads, 0, st, L.n, L.coarse_inverse, bv, x, status);
       s.launches_per_iteration++;
     } else {
-      enqueue_smooth<S, V, B>(s, L, rhs, b_store, x, nullptr, status);
+      enqueue_smooth<S, V, B>(s, L, rhs, b_store, x, nullptr, status, started);
     }
     return;
   }
-  enqueue_smooth<S, V, B>(s, L, rhs, b_store, x, nullptr, status);
+  enqueue_smooth<S, V, B>(s, L, rhs, b_store, x, nullptr, status, started);
   const V* b = b_store ? (const V*)b_store : (const V*)rhs;
   DevLevel& C = s.levels[li + 1];
   bsr_dispatch<S, V, OP_RESIDUAL>(L.a, x, (V*)L.res, b, status, st);
-  bsr_dispatch<S, V, OP_SET>(L.r, (const V*)L.res, (V*)C.b, nullptr, status, st);
+  // The restriction; when the coarser level starts with its smoother, that start is fused in.
+  const bool fuse = (int)(li + 1) != s.tail_level && (C.has_p || !C.has_factor);
+  if (fuse)
+    launch_start_product<S, V, OP_SET>(L.r, (const V*)L.res, (const V*)nullptr,
+                                       start_args<S, V>(C, (V*)C.b, (V*)C.x), status, st);
+  else
+    bsr_dispatch<S, V, OP_SET>(L.r, (const V*)L.res, (V*)C.b, nullptr, status, st);
   s.launches_per_iteration += 2;
-  enqueue_cycle<S, V, V>(s, li + 1, (const V*)C.b, nullptr, (V*)C.x, status);
+  enqueue_cycle<S, V, V>(s, li + 1, (const V*)C.b, nullptr, (V*)C.x, status, fuse);
   bsr_dispatch<S, V, OP_ADD>(L.p, (const V*)C.x, x, nullptr, status, st);
-  bsr_dispatch<S, V, OP_RESIDUAL>(L.a, x, (V*)L.tmp, b, status, st);
+  // The residual b - A x with the post-smoother's start fused in (its right-hand side stays in
+  // registers).
+  launch_start_product<S, V, OP_RESIDUAL>(L.a, (const V*)x, b, start_args<S, V>(L, (V*)nullptr, (V*)L.post_x),
+                                          status, st);
   s.launches_per_iteration += 2;
-  enqueue_smooth<S, V, V>(s, L, (const V*)L.tmp, nullptr, (V*)L.post_x, x, status);
+  enqueue_smooth<S, V, V>(s, L, (const V*)nullptr, nullptr, (V*)L.post_x, x, status, true);
 }
 
 // z = M r for the solver's r (f64) into z (f64) or z32.
