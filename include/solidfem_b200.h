@@ -325,7 +325,9 @@ sf_status sf_study_system_multiply(sf_study* study, const double* x, double* y);
  *
  * - count at most 8; a larger count is refused with SF_INVALID_ARGUMENT before any work. count 0
  *   does nothing. x, y and energy: 8-byte-aligned device (or managed) memory of the study's
- *   device, not overlapping; x and y hold count * free_dofs doubles, energy count doubles.
+ *   device, not overlapping; x and y hold count * free_dofs doubles, energy count doubles, each
+ *   range inside one allocation (a range that runs past the end of its allocation is refused).
+ * - The calling thread's current device is the same after the call as before it.
  * - Asynchronous: the kernel is enqueued on the study's stream (sf_study_stream); read y and
  *   energy after that stream has reached it.
  * - The first call on a device looks up the scratch's address with that device current, which can
@@ -336,7 +338,10 @@ sf_status sf_study_system_multiply(sf_study* study, const double* x, double* y);
  *   it needs an initial value.
  * - Every study on a device shares the one scratch array: two calls whose kernels can run at the
  *   same time (different streams, studies or host threads) race and give wrong results. Order
- *   them, for example on one stream. */
+ *   them, for example on one stream.
+ * - The scratch's address is kept per device for the life of the process. Studies and this address
+ *   do not survive cudaDeviceReset: destroy every study of a device before resetting it, and do not
+ *   call this entry point on that device afterwards. */
 sf_status sf_study_energy_products(sf_study* study, const double* x, double* y, double* energy,
                                    uint64_t count);
 

@@ -15,6 +15,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <mutex>
@@ -159,10 +160,18 @@ void launch_body(dim3 grid, dim3 block, size_t smem, cudaStream_t st, A&&... arg
     return;
   }
   const void* k = T::template single<Body>();
-  static bool opted = false;
-  if (smem > 48 * 1024 && !opted) {
-    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    opted = true;
+  if (smem > 48 * 1024) {
+    // The opt-in above 48 KB is a per-device attribute of the kernel: set it once per device
+    // ordinal (a bit per device, atomically, since studies on different host threads and devices
+    // launch the same kernels).
+    static std::atomic<uint64_t> opted{0};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const uint64_t bit = dev < 64 ? 1ull << dev : 0;
+    if (!bit || !(opted.load(std::memory_order_acquire) & bit)) {
+      cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+      opted.fetch_or(bit, std::memory_order_acq_rel);
+    }
   }
   cudaLaunchAttribute attr[1];
   attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;

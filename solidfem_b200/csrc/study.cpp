@@ -12,6 +12,7 @@
 #include <memory>
 
 #ifdef _OPENMP
+#include <cuda.h>
 #include <omp.h>
 #endif
 
@@ -1603,16 +1604,41 @@ sf_status sf_study_system_multiply(sf_study* s, const double* x, double* y) {
 }
 
 namespace {
-// A device (or managed) pointer of the study's device, aligned for doubles.
-bool on_study_device(const void* p, int device) {
+typedef CUresult (*AddressRangeFn)(CUdeviceptr*, size_t*, CUdeviceptr);
+
+// The driver's cuMemGetAddressRange, looked up through the runtime (the library does not link the
+// driver library itself); null where the driver does not offer it.
+AddressRangeFn address_range_fn() {
+  static AddressRangeFn fn = [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPointByVersion("cuMemGetAddressRange", &f, 12000, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess) {
+      cudaGetLastError();
+      return (AddressRangeFn) nullptr;
+    }
+    return (AddressRangeFn)f;
+  }();
+  return fn;
+}
+
+// `bytes` of device (or managed) memory of the study's device from p, aligned for doubles and
+// inside one allocation, so a kernel given the range stays in bounds.
+bool on_study_device(const void* p, size_t bytes, int device) {
   if ((uintptr_t)p % alignof(double) != 0) return false;
   cudaPointerAttributes attr{};
   if (cudaPointerGetAttributes(&attr, p) != cudaSuccess) {
     cudaGetLastError();
     return false;
   }
-  if (attr.type == cudaMemoryTypeManaged) return true;
-  return attr.type == cudaMemoryTypeDevice && attr.device == device;
+  if (attr.type != cudaMemoryTypeManaged && !(attr.type == cudaMemoryTypeDevice && attr.device == device))
+    return false;
+  AddressRangeFn range = address_range_fn();
+  if (!range) return false;
+  CUdeviceptr base = 0;
+  size_t size = 0;
+  if (range(&base, &size, (CUdeviceptr)(uintptr_t)p) != CUDA_SUCCESS) return false;
+  return (uintptr_t)p + bytes <= (uintptr_t)base + size;
 }
 bool overlaps(const void* a, size_t abytes, const void* b, size_t bbytes) {
   uintptr_t a0 = (uintptr_t)a, b0 = (uintptr_t)b;
@@ -1626,10 +1652,19 @@ sf_status sf_study_energy_products(sf_study* s, const double* x, double* y, doub
   if (count > solver_energy_max_vectors()) return solver_energy_products(d, x, y, energy, count);
   if (count == 0) return SF_OK;
   if (!x || !y || !energy) return fail(SF_INVALID_ARGUMENT, "null argument");
+  // The caller's current device is put back on every return.
+  int caller_device = 0;
+  if (sf_status e = cuda_check(cudaGetDevice(&caller_device), "cudaGetDevice")) return e;
+  struct Restore {
+    int device;
+    ~Restore() { cudaSetDevice(device); }
+  } restore{caller_device};
   if (sf_status e = cuda_check(cudaSetDevice(d.device), "cudaSetDevice")) return e;
-  if (!on_study_device(x, d.device) || !on_study_device(y, d.device) || !on_study_device(energy, d.device))
-    return fail(SF_INVALID_ARGUMENT, "x, y and energy must be 8-byte aligned device memory of the study's device");
   const size_t vbytes = (size_t)count * d.n * sizeof(double), ebytes = (size_t)count * sizeof(double);
+  if (!on_study_device(x, vbytes, d.device) || !on_study_device(y, vbytes, d.device) ||
+      !on_study_device(energy, ebytes, d.device))
+    return fail(SF_INVALID_ARGUMENT, "x, y and energy must be 8-byte aligned device memory of the study's device, "
+                                     "each range inside one allocation");
   if (overlaps(x, vbytes, y, vbytes) || overlaps(x, vbytes, energy, ebytes) || overlaps(y, vbytes, energy, ebytes))
     return fail(SF_INVALID_ARGUMENT, "x, y and energy must not overlap");
   return solver_energy_products(d, x, y, energy, count);

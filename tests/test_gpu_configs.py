@@ -3,8 +3,13 @@ L2 and nodal von Mises within 1e-6 of the oracle's own FP64 CPU solve (requested
 its rounding floor) on the same mesh, plus the closed-form cantilever check.
 
 Config 1: steel cantilever 100x10x10 mm, 20x4x4 hexes; config 2: thin plate 100x100x0.8 mm,
-60x60x2; a reduced printed block (60 mm cube, 15^3 hexes, shell within 2 mm of the surface).
+60x60x2; config 3: the 606k-DOF gate plate, 100x100x0.8 mm on 100x100x2 hexes (603,000 free DOFs),
+mixed and FP64; config 4 at two sizes: a 15^3-hex printed block (operator bit-exact) and a 40^3
+one (1.6M free DOFs; shell within 2 mm of the surface, core inside). The large oracle solves run
+on every host core: the oracle's row threading changes no bit.
 """
+import os
+
 import numpy as np
 import pytest
 
@@ -68,31 +73,61 @@ PLATE = ((100.0, 100.0, 0.8), (60, 60, 2), 2000.0, 0.35)
 PLATE_LOAD = dict(load_axis=2, load_value=0.8, traction=(0.0, 0.0, -0.01))
 
 
-@pytest.fixture(scope="module")
-def plate_oracle(oracle):
-    size, div, E, nu = PLATE
+GATE = ((100.0, 100.0, 0.8), (100, 100, 2), 2000.0, 0.35)
+
+
+def all_cores(oracle):
+    oracle.set_threads(len(os.sched_getaffinity(0)))
+
+
+def plate_reference(oracle, plate):
+    size, div, E, nu = plate
+    all_cores(oracle)
     ref = oracle_study(oracle, size, div, E, nu, oracle.default_options(tolerance=1e-12, precision=oracle.DOUBLE),
                        **PLATE_LOAD)
     pr = ref.solve()
     return ref, pr
 
 
-@pytest.mark.parametrize("precision", [sf.Precision.MIXED, sf.Precision.DOUBLE])
-def test_config2_thin_plate(plate_oracle, precision):
-    size, div, E, nu = PLATE
+@pytest.fixture(scope="module")
+def plate_oracle(oracle):
+    return plate_reference(oracle, PLATE)
+
+
+@pytest.fixture(scope="module")
+def gate_oracle(oracle):
+    return plate_reference(oracle, GATE)
+
+
+def check_plate(plate, ref_pr, precision, label):
+    size, div, E, nu = plate
     _, model = product_model(size, div, E, nu, **PLATE_LOAD)
     study = sf.StaticStudy.new(model, options(precision, 1e-8))
     out = study.solve()
     assert out.kind == sf.Outcome.CONVERGED
-    ref, pr = plate_oracle
+    ref, pr = ref_pr
     l2, vm = check_against_oracle(study, ref)
-    print(f"config 2 {precision.name}: {out.progress.iteration} iterations (floor {out.progress.at_rounding_floor}), "
-          f"oracle {pr.iteration} (floor {pr.at_rounding_floor}); rel L2 {l2:.2e}, von Mises {vm:.2e}")
+    print(f"{label} {precision.name}: {out.progress.iteration} iterations, residual {out.progress.relative_residual:.3e} "
+          f"(floor {out.progress.at_rounding_floor}); oracle {pr.iteration} (floor {pr.at_rounding_floor}, residual "
+          f"{pr.relative_residual:.3e}); rel L2 {l2:.2e}, von Mises {vm:.2e}")
+    # Both requested 1e-8; where f64 cannot resolve it the solver stops at its rounding floor.
+    assert out.progress.relative_residual <= 1e-8 or out.progress.at_rounding_floor
     assert l2 <= L2_BAR and vm <= VM_BAR
 
 
-def test_printed_block_reduced(oracle):
-    n = 15
+@pytest.mark.parametrize("precision", [sf.Precision.MIXED, sf.Precision.DOUBLE])
+def test_config2_thin_plate(plate_oracle, precision):
+    check_plate(PLATE, plate_oracle, precision, "config 2")
+
+
+@pytest.mark.parametrize("precision", [sf.Precision.MIXED, sf.Precision.DOUBLE])
+def test_config3_gate_plate(gate_oracle, precision):
+    """The headline workload: 606k DOFs, mixed and FP64, against the oracle's FP64 solve."""
+    check_plate(GATE, gate_oracle, precision, "config 3")
+
+
+@pytest.mark.parametrize("n", [15, 40])
+def test_printed_block(oracle, n):
     size, div = (60.0, 60.0, 60.0), (n, n, n)
     shell, core = (2400.0, 0.36), (800.0, 0.30)
     lo, hi, depth = (0.0, 0.0, 0.0), size, 2.0
@@ -101,13 +136,15 @@ def test_printed_block_reduced(oracle):
     _, model = product_model(size, div, 1.0, 0.0, material=material, **kw)
     study = sf.StaticStudy.new(model, options(sf.Precision.MIXED, 1e-8))
     assert study.solve().kind == sf.Outcome.CONVERGED
+    all_cores(oracle)
     ref = oracle_study(oracle, size, div, 1.0, 0.0, oracle.default_options(tolerance=1e-12, precision=oracle.DOUBLE),
                        material=oracle.shell_core(shell, core, lo, hi, depth), **kw)
-    # the two-material operator itself is bit-exact
-    rs, cols, vals = study.matrix()
-    ors, ocols, ovals = ref.matrix()
-    assert np.array_equal(cols, ocols) and np.array_equal(vals.view(np.uint64), ovals.view(np.uint64))
+    if n <= 20:
+        # the two-material operator itself is bit-exact
+        rs, cols, vals = study.matrix()
+        ors, ocols, ovals = ref.matrix()
+        assert np.array_equal(cols, ocols) and np.array_equal(vals.view(np.uint64), ovals.view(np.uint64))
     ref.solve()
     l2, vm = check_against_oracle(study, ref)
-    print(f"printed block 15^3: rel L2 {l2:.2e}, von Mises {vm:.2e}")
+    print(f"printed block {n}^3 ({study.report()['free_dofs']} free DOFs): rel L2 {l2:.2e}, von Mises {vm:.2e}")
     assert l2 <= L2_BAR and vm <= VM_BAR

@@ -11,7 +11,7 @@ import pytest
 import torch.multiprocessing as mp
 
 from solidfem_b200 import workloads as W
-from solidfem_b200.replicas import ReplicaGroup
+from replicas import ReplicaGroup
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
@@ -77,6 +77,7 @@ def test_reference_arm_non_leader_exits_without_work(monkeypatch):
 
     def fail(*a, **k):
         raise AssertionError("a non-leader rank ran the CPU sample")
-    monkeypatch.setattr(bench, "cpu_baseline_sample", fail)
+    monkeypatch.setattr(bench, "oracle_solve", fail)
+    monkeypatch.setattr(bench, "_oracle", fail)
     args = types.SimpleNamespace(warmup=3, steps=2, gpus=2)
     assert bench.run_reference(args, 1, 2) == 0

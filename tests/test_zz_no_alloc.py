@@ -82,3 +82,25 @@ def test_energy_products_refusals():
         study.energy_products(x.data_ptr(), x.data_ptr(), e.data_ptr(), 1)
     assert err.value.status == sf.Status.INVALID_ARGUMENT
     study.energy_products(x.data_ptr(), y.data_ptr(), e.data_ptr(), 0)  # nothing to do
+
+
+def test_energy_products_refuse_a_short_buffer_and_keep_the_current_device():
+    import torch
+
+    study = make_study(False)
+    n = study.report()["free_dofs"]
+    x = torch.zeros((2, n), dtype=torch.float64, device="cuda:0")
+    short = torch.zeros(2 * n - 1, dtype=torch.float64, device="cuda:0")  # one entry short of two vectors
+    e = torch.zeros(2, dtype=torch.float64, device="cuda:0")
+    torch.cuda.synchronize()
+    before = torch.cuda.current_device()
+    with pytest.raises(sf.SolidfemError) as err:
+        study.energy_products(x.data_ptr(), short.data_ptr(), e.data_ptr(), 2)
+    assert err.value.status == sf.Status.INVALID_ARGUMENT
+    with pytest.raises(sf.SolidfemError) as err:
+        study.energy_products(x.data_ptr(), x[1].data_ptr(), e.data_ptr(), 1)  # overlapping x and y
+    assert err.value.status == sf.Status.INVALID_ARGUMENT
+    y = torch.zeros((2, n), dtype=torch.float64, device="cuda:0")
+    study.energy_products(x.data_ptr(), y.data_ptr(), e.data_ptr(), 2)
+    torch.cuda.synchronize()
+    assert torch.cuda.current_device() == before
