@@ -22,7 +22,7 @@
 extern "C" {
 #endif
 
-#define SF_ABI_VERSION 1
+#define SF_ABI_VERSION 2
 
 /* Status codes. Named refusals mirror MeshError (crates/solidfem-mesh/src/error.rs),
  * ModelError (crates/solidfem-elastic/src/error.rs:23-119), MultigridError
@@ -72,6 +72,7 @@ typedef struct sf_error {
   int32_t status;
   uint32_t tet, node, face, point, axis;
   uint64_t row, level, block, iteration, rank;
+  uint64_t expected, found; /* the lengths of NearNullLength and PositionLength */
   double pivot, curvature, relative_residual, determinant, value;
   char message[256];
 } sf_error;
@@ -195,7 +196,9 @@ typedef struct sf_study_options {
 /* StudyOptions::default with the reference's defaults (Jacobi preconditioner). */
 void sf_study_options_default(sf_study_options* options);
 
-/* Returns nonzero to cancel. Read per element, per setup row and per solver iteration. */
+/* Returns nonzero to cancel. Read before each slice of assembly, each phase of each multigrid
+ * setup level, each solver iteration and each recovery launch (the reference reads it per element,
+ * per setup row and per iteration; the device does those in larger launches). */
 typedef int32_t (*sf_cancel_fn)(void* user);
 
 /* ---------------------------------------------------------------- build -------------------- */
@@ -243,7 +246,10 @@ typedef struct sf_step_outcome {
  * however the solve is sliced. */
 sf_status sf_study_step(sf_study* study, uint64_t max_iterations, sf_cancel_fn cancel, void* user,
                         sf_step_outcome* outcome);
-/* StaticStudy::displacements (study.rs:219-238): node_count x 3, zero at fixed nodes. */
+/* Pcg::progress (pcg.rs:200-207) of the study's solve: iterations, relative residual, floor. */
+sf_status sf_study_progress(const sf_study* study, sf_progress* out);
+/* StaticStudy::displacements (study.rs:219-238): node_count x 3, zero at fixed nodes. The estimate
+ * so far (Pcg::estimate, pcg.rs:192-194) while the solve runs: a preview, not an answer. */
 sf_status sf_study_displacements(const sf_study* study, double* out);
 
 /* Report, study.rs:151-176. */
@@ -276,12 +282,69 @@ typedef struct sf_point_stress {
 } sf_point_stress;
 
 /* StaticStudy::solution (study.rs:246-260), recovered on the device: refuses with
- * SF_NOT_FINISHED before convergence. Any output pointer may be NULL. displacements:
- * node_count x 3; nodal_stress: node_count x 6; nodal_von_mises: node_count; points:
- * tet_count x points_per_element. */
-sf_status sf_study_solution(sf_study* study, double* displacements, double* nodal_stress,
-                            double* nodal_von_mises, sf_point_stress* points);
+ * SF_NOT_FINISHED before convergence. `cancel` is read between slices of 65,536 units of recovery
+ * work (SF_CANCELLED); the recovered field is kept, so later calls only copy it out. Any output
+ * pointer may be NULL. displacements: node_count x 3; nodal_stress: node_count x 6;
+ * nodal_von_mises: node_count; points: tet_count x points_per_element. */
+sf_status sf_study_solution(sf_study* study, sf_cancel_fn cancel, void* user, double* displacements,
+                            double* nodal_stress, double* nodal_von_mises, sf_point_stress* points);
+
+/* Recovery (crates/solidfem-elastic/src/results.rs:97-124): a resumable stress recovery of one
+ * snapshot of a study's displacements, with its own device buffers. Destroy it before its study. */
+typedef struct sf_recovery sf_recovery;
+/* StaticStudy::begin_recovery (study.rs:262-274): snapshots the current displacements on the
+ * device: the converged answer, or a preview of a solve still running. */
+sf_status sf_study_begin_recovery(sf_study* study, sf_recovery** out);
+/* StaticStudy::continue_recovery (study.rs:276-296): up to max_units more units of work (each
+ * element, then each vertex's patch fit, in order, on the device); *finished (may be NULL) is
+ * set once all are done. `cancel` is read before each launch (SF_CANCELLED; the recovery can be
+ * continued later). Any slicing gives the bits of one call. An inverted element or invalid
+ * material is refused by name (tet, point). */
+sf_status sf_study_continue_recovery(sf_study* study, sf_recovery* recovery, uint64_t max_units,
+                                     sf_cancel_fn cancel, void* user, int32_t* finished);
+/* StaticStudy::finish_recovery (study.rs:298-304): the recovered field (RecoveredField,
+ * results.rs:126-139), outputs as sf_study_solution; SF_NOT_FINISHED while units remain. */
+sf_status sf_study_finish_recovery(sf_study* study, sf_recovery* recovery, double* displacements,
+                                   double* nodal_stress, double* nodal_von_mises, sf_point_stress* points);
+void sf_recovery_destroy(sf_recovery* recovery);
 void sf_study_destroy(sf_study* study);
+
+/* ------------------------------------------------------------- raw systems ---------------- */
+/* The solver crate's seam without a mesh: a symmetric matrix in scalar CSR (CsrMatrix,
+ * crates/solidfem-solve/src/csr.rs:6-13) and a right-hand side, solved on the device by the
+ * conjugate gradient of Pcg::new / step / estimate / progress (pcg.rs:133-213). options->
+ * preconditioner picks Jacobi::new (preconditioner.rs:49-79) or the multigrid of
+ * MultigridSetup::new + step + finish (multigrid/setup.rs:129-215, run to the end inside create,
+ * `cancel` read before each phase of each level); the other options are the study's (tolerance, cap, multigrid
+ * settings, precision, device, graphs). */
+typedef struct sf_system sf_system;
+
+/* n unknowns; row_starts n + 1, columns and values row_starts[n] each (every row's columns
+ * strictly ascending and below n: SF_INVALID_ARGUMENT otherwise); rhs n. For multigrid,
+ * near_null holds near_null_count = 6 n values ((row, mode) at 6 row + mode) and positions
+ * position_count = n / 3 points (x, y, z), one per block row; wrong lengths are refused as
+ * SF_MG_NEAR_NULL_LENGTH / SF_MG_POSITION_LENGTH (expected, found in sf_error), a matrix whose
+ * rows do not group into 3x3 blocks as SF_MG_BLOCK_STRUCTURE (row), a diagonal block that is not
+ * positive definite as SF_MG_NOT_POSITIVE_DEFINITE (level, block, pivot). For Jacobi they are
+ * ignored, n is any size, and a diagonal entry that is not positive and finite is refused as
+ * SF_JACOBI_DIAGONAL (row, value). options NULL: the defaults (Jacobi). A zero right-hand side
+ * is converged at once. */
+sf_status sf_system_create(uint64_t n, const uint64_t* row_starts, const uint32_t* columns, const double* values,
+                           const double* rhs, const double* near_null, uint64_t near_null_count,
+                           const double* positions, uint64_t position_count, const sf_study_options* options,
+                           sf_cancel_fn cancel, void* user, sf_system** out);
+/* Pcg::step (pcg.rs:167-190): up to max_iterations iterations, the same bits however sliced;
+ * SF_PCG_NOT_POSITIVE_DEFINITE (iteration, curvature) or SF_PCG_NOT_CONVERGED (iteration,
+ * relative_residual) once the solve has failed, for this call and every later one. */
+sf_status sf_system_step(sf_system* system, uint64_t max_iterations, sf_cancel_fn cancel, void* user,
+                         sf_step_outcome* outcome);
+/* Pcg::estimate (pcg.rs:192-194): the current estimate, n values. */
+sf_status sf_system_estimate(const sf_system* system, double* out);
+/* Pcg::progress (pcg.rs:200-207). */
+sf_status sf_system_progress(const sf_system* system, sf_progress* out);
+/* Multigrid::level_sizes().len() (cycle.rs:333-339); 0 under Jacobi. */
+uint64_t sf_system_level_count(const sf_system* system);
+void sf_system_destroy(sf_system* system);
 
 /* ------------------------------------------------------------- inspection ----------------- */
 /* The assembled free-DOF system as scalar CSR (csr.rs:6-13), copied from the device:
@@ -440,6 +503,12 @@ sf_status sf_server_wait(sf_server* server, uint64_t id, uint64_t timeout_ms, sf
 /* Copies a finished request's displacements (node_count x 3, may be NULL) and forgets the request;
  * returns the request's own failure status if it failed. */
 sf_status sf_server_take(sf_server* server, uint64_t id, double* displacements);
+
+/* Cancels a request: one still queued is dropped at once; one being built or solved stops at its
+ * next cancel check (a batched one leaves its batch between chunks of iterations, the other
+ * members going on). It then finishes with status SF_CANCELLED. A finished request is left as it
+ * is. */
+sf_status sf_server_cancel(sf_server* server, uint64_t id);
 
 typedef struct sf_server_stats {
   uint64_t completed, pending, reserved_bytes, peak_reserved_bytes, batches, batched_requests;

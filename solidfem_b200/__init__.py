@@ -80,7 +80,8 @@ class PointStress(C.Structure):
 class _Error(C.Structure):
     _fields_ = [("status", C.c_int32), ("tet", C.c_uint32), ("node", C.c_uint32), ("face", C.c_uint32),
                 ("point", C.c_uint32), ("axis", C.c_uint32), ("row", C.c_uint64), ("level", C.c_uint64),
-                ("block", C.c_uint64), ("iteration", C.c_uint64), ("rank", C.c_uint64), ("pivot", C.c_double),
+                ("block", C.c_uint64), ("iteration", C.c_uint64), ("rank", C.c_uint64), ("expected", C.c_uint64),
+                ("found", C.c_uint64), ("pivot", C.c_double),
                 ("curvature", C.c_double), ("relative_residual", C.c_double), ("determinant", C.c_double),
                 ("value", C.c_double), ("message", C.c_char * 256)]
 
@@ -167,9 +168,14 @@ SIGNATURES = {
     "sf_builder_destroy": (None, [_V]),
     "sf_study_create": (C.c_int, [_V, _P(_Options), _CANCEL, _V, _P(_V)]),
     "sf_study_step": (C.c_int, [_V, C.c_uint64, _CANCEL, _V, _P(_StepOutcome)]),
+    "sf_study_progress": (C.c_int, [_V, _P(_Progress)]),
     "sf_study_displacements": (C.c_int, [_V, _P(C.c_double)]),
     "sf_study_report": (C.c_int, [_V, _P(_Report)]),
-    "sf_study_solution": (C.c_int, [_V, _P(C.c_double), _P(C.c_double), _P(C.c_double), _P(PointStress)]),
+    "sf_study_solution": (C.c_int, [_V, _CANCEL, _V, _P(C.c_double), _P(C.c_double), _P(C.c_double), _P(PointStress)]),
+    "sf_study_begin_recovery": (C.c_int, [_V, _P(_V)]),
+    "sf_study_continue_recovery": (C.c_int, [_V, _V, C.c_uint64, _CANCEL, _V, _P(C.c_int32)]),
+    "sf_study_finish_recovery": (C.c_int, [_V, _V, _P(C.c_double), _P(C.c_double), _P(C.c_double), _P(PointStress)]),
+    "sf_recovery_destroy": (None, [_V]),
     "sf_study_destroy": (None, [_V]),
     "sf_study_matrix": (C.c_int, [_V, _P(C.c_uint64), _P(C.c_uint32), _P(C.c_double)]),
     "sf_study_rhs": (C.c_int, [_V, _P(C.c_double)]),
@@ -187,11 +193,20 @@ SIGNATURES = {
     "sf_server_wait": (C.c_int, [_V, C.c_uint64, C.c_uint64, _P(_RequestResult)]),
     "sf_server_take": (C.c_int, [_V, C.c_uint64, _P(C.c_double)]),
     "sf_server_statistics": (C.c_int, [_V, _P(_ServerStats)]),
+    "sf_server_cancel": (C.c_int, [_V, C.c_uint64]),
     "sf_server_destroy": (None, [_V]),
     "sf_study_device_timing": (C.c_int, [_V, _P(_DeviceTiming)]),
     "sf_study_resolve": (C.c_int, [_V, _P(C.c_double)]),
     "sf_study_stream": (C.c_uint64, [_V]),
     "sf_study_time_kernel": (C.c_int, [_V, C.c_int32, C.c_uint64, _P(_KernelTiming)]),
+    "sf_system_create": (C.c_int, [C.c_uint64, _P(C.c_uint64), _P(C.c_uint32), _P(C.c_double), _P(C.c_double),
+                                   _P(C.c_double), C.c_uint64, _P(C.c_double), C.c_uint64, _P(_Options), _CANCEL, _V,
+                                   _P(_V)]),
+    "sf_system_step": (C.c_int, [_V, C.c_uint64, _CANCEL, _V, _P(_StepOutcome)]),
+    "sf_system_estimate": (C.c_int, [_V, _P(C.c_double)]),
+    "sf_system_progress": (C.c_int, [_V, _P(_Progress)]),
+    "sf_system_level_count": (C.c_uint64, [_V]),
+    "sf_system_destroy": (None, [_V]),
 }
 
 _lib = None
@@ -643,22 +658,38 @@ class StaticStudy:
                 return o
 
     def displacements(self) -> np.ndarray:
+        """The current estimate (a preview until converged), node_count x 3, zero at fixed nodes."""
         out = np.empty((self.mesh.node_count(), 3))
         _check(library().sf_study_displacements(self._h, _dptr(out)))
         return out
 
-    def solution(self) -> Solution:
-        """StaticStudy::solution (study.rs:246-260): displacements and the stress field recovered on
-        the device; refuses (NOT_FINISHED) until the solve has converged."""
+    def progress(self) -> Progress:
+        """Pcg::progress (pcg.rs:200-207)."""
+        p = _Progress()
+        _check(library().sf_study_progress(self._h, C.byref(p)))
+        return Progress(p.iteration, p.relative_residual, bool(p.at_rounding_floor))
+
+    def _field_buffers(self):
         n = self.mesh.node_count()
         q = 14 if self._quadrature == Quadrature.FOURTEEN_POINT else 4
-        d = np.empty((n, 3))
-        s6 = np.empty((n, 6))
-        vm = np.empty(n)
-        pts = np.empty(self.mesh.tet_count() * q, dtype=POINT_STRESS_DTYPE)
-        _check(library().sf_study_solution(self._h, _dptr(d), _dptr(s6), _dptr(vm),
+        return (np.empty((n, 3)), np.empty((n, 6)), np.empty(n),
+                np.empty(self.mesh.tet_count() * q, dtype=POINT_STRESS_DTYPE))
+
+    def solution(self, cancel: Optional[Callable[[], bool]] = None) -> Solution:
+        """StaticStudy::solution (study.rs:246-260): displacements and the stress field recovered on
+        the device; refuses (NOT_FINISHED) until the solve has converged, CANCELLED when `cancel`
+        returns true between slices of the recovery."""
+        d, s6, vm, pts = self._field_buffers()
+        _check(library().sf_study_solution(self._h, _cancel_fn(cancel), None, _dptr(d), _dptr(s6), _dptr(vm),
                                            pts.ctypes.data_as(C.POINTER(PointStress))))
         return Solution(d, pts, s6, vm, self.report())
+
+    def begin_recovery(self) -> "Recovery":
+        """StaticStudy::begin_recovery (study.rs:262-274): a resumable recovery of the current
+        displacements (the answer once converged, else a preview)."""
+        h = C.c_void_p()
+        _check(library().sf_study_begin_recovery(self._h, C.byref(h)))
+        return Recovery(self, h)
 
     def report(self) -> dict:
         r = _Report()
@@ -744,6 +775,43 @@ class StaticStudy:
 
 
 @dataclass
+class RecoveredField:
+    """RecoveredField (crates/solidfem-elastic/src/results.rs:126-139)."""
+    displacements: np.ndarray
+    point_stresses: np.ndarray
+    nodal_stress: np.ndarray
+    nodal_von_mises: np.ndarray
+
+
+class Recovery:
+    """A resumable stress recovery on the device (Recovery, results.rs:97-124): continue() does up to
+    max_units more elements, then vertex patch fits; finish() returns the field."""
+
+    def __init__(self, study: StaticStudy, handle):
+        self._study = study  # the study outlives its recoveries
+        self._h = handle
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            library().sf_recovery_destroy(self._h)
+            self._h = None
+
+    def continue_(self, max_units: int, cancel: Optional[Callable[[], bool]] = None) -> bool:
+        """StaticStudy::continue_recovery (study.rs:276-296): True once every unit is done."""
+        done = C.c_int32()
+        _check(library().sf_study_continue_recovery(self._study._h, self._h, max_units, _cancel_fn(cancel), None,
+                                                    C.byref(done)))
+        return bool(done.value)
+
+    def finish(self) -> RecoveredField:
+        """StaticStudy::finish_recovery (study.rs:298-304); NOT_FINISHED while units remain."""
+        d, s6, vm, pts = self._study._field_buffers()
+        _check(library().sf_study_finish_recovery(self._study._h, self._h, _dptr(d), _dptr(s6), _dptr(vm),
+                                                  pts.ctypes.data_as(C.POINTER(PointStress))))
+        return RecoveredField(d, pts, s6, vm)
+
+
+@dataclass
 class ServerOptions:
     """sf_server_options: device, memory budget (bytes, 0: 150 GiB), the batching threshold in free DOFs,
     studies per batch, build threads, solver threads and setup threads per build."""
@@ -813,6 +881,10 @@ class Server:
                              r.free_dofs, r.node_count, r.device_bytes, r.queue_seconds, r.build_seconds,
                              r.solve_seconds, r.latency_seconds, r.message.decode(errors="replace"))
 
+    def cancel(self, rid: int) -> None:
+        """Stops a request at its next cancel check; it finishes as CANCELLED (sf_server_cancel)."""
+        _check(library().sf_server_cancel(self._h, rid))
+
     def take(self, rid: int, node_count: int) -> np.ndarray:
         out = np.empty((node_count, 3), dtype=np.float64)
         try:
@@ -836,6 +908,70 @@ class Server:
         self.close()
 
 
+def _outcome(o: _StepOutcome) -> StepOutcome:
+    p = o.progress
+    return StepOutcome(Outcome(o.kind), Progress(p.iteration, p.relative_residual, bool(p.at_rounding_floor)))
+
+
+class System:
+    """A raw symmetric system solved on the device: CsrMatrix + Pcg (crates/solidfem-solve/src/pcg.rs)
+    under Jacobi or the multigrid of MultigridSetup (multigrid/setup.rs), without a mesh.
+
+    ``row_starts``/``columns``/``values`` are scalar CSR (each row's columns ascending); for multigrid
+    ``near_null`` holds 6 values per unknown and ``positions`` one point per block row of three."""
+
+    def __init__(self, row_starts, columns, values, rhs, options: Optional[StudyOptions] = None,
+                 near_null=None, positions=None, cancel: Optional[Callable[[], bool]] = None):
+        rs = np.ascontiguousarray(row_starts, dtype=np.uint64)
+        cols = np.ascontiguousarray(columns, dtype=np.uint32)
+        vals = np.ascontiguousarray(values, dtype=np.float64)
+        b = np.ascontiguousarray(rhs, dtype=np.float64)
+        n = len(rs) - 1
+        if len(b) != n:
+            raise ValueError(f"rhs has {len(b)} values for {n} rows")
+        nn = None if near_null is None else np.ascontiguousarray(near_null, dtype=np.float64).reshape(-1)
+        pos = None if positions is None else np.ascontiguousarray(positions, dtype=np.float64).reshape(-1, 3)
+        self.n = n
+        h = C.c_void_p()
+        _check(library().sf_system_create(
+            n, rs.ctypes.data_as(C.POINTER(C.c_uint64)), _uptr(cols), _dptr(vals), _dptr(b),
+            None if nn is None else _dptr(nn), 0 if nn is None else len(nn),
+            None if pos is None else _dptr(pos), 0 if pos is None else len(pos),
+            C.byref((options or StudyOptions())._c()), _cancel_fn(cancel), None, C.byref(h)))
+        self._h = h
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            library().sf_system_destroy(self._h)
+            self._h = None
+
+    def step(self, max_iterations: int, cancel: Optional[Callable[[], bool]] = None) -> StepOutcome:
+        """Pcg::step: raises SolidfemError (PCG_NOT_POSITIVE_DEFINITE / PCG_NOT_CONVERGED) once failed."""
+        o = _StepOutcome()
+        _check(library().sf_system_step(self._h, max_iterations, _cancel_fn(cancel), None, C.byref(o)))
+        return _outcome(o)
+
+    def solve(self, slice_iterations: int = 2**62) -> StepOutcome:
+        while True:
+            o = self.step(slice_iterations)
+            if o.kind != Outcome.RUNNING:
+                return o
+
+    def estimate(self) -> np.ndarray:
+        """Pcg::estimate: the current estimate of x."""
+        out = np.empty(self.n)
+        _check(library().sf_system_estimate(self._h, _dptr(out)))
+        return out
+
+    def progress(self) -> Progress:
+        p = _Progress()
+        _check(library().sf_system_progress(self._h, C.byref(p)))
+        return Progress(p.iteration, p.relative_residual, bool(p.at_rounding_floor))
+
+    def level_count(self) -> int:
+        return int(library().sf_system_level_count(self._h))
+
+
 def solve_batch(studies) -> list:
     """Solves resident studies together, one grid per kernel over all of them (sf_study_solve_batch).
     Returns (StepOutcome, Status) per study."""
@@ -856,5 +992,5 @@ __all__ = [
     "FACE_DTYPE", "BoundaryFace", "Mesh", "box_tet_mesh", "Material", "ShellCore", "Quadrature", "Model", "Precision",
     "PcgOptions", "MultigridOptions", "Jacobi", "StudyOptions", "StudyBuilder", "StaticStudy", "StepOutcome",
     "Outcome", "Progress", "BuildProgress", "PointStress", "SolidfemError", "Status", "library", "SIGNATURES", "Kernel", "Solution",
-    "solve_batch", "Server", "ServerOptions", "RequestResult",
+    "solve_batch", "Server", "ServerOptions", "RequestResult", "System", "Recovery", "RecoveredField",
 ]

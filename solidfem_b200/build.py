@@ -29,7 +29,7 @@ CU_SOURCES = {
     "assembly.cu": ["-fmad=false", "-prec-div=true", "-prec-sqrt=true"],
     "setup_device.cu": ["-fmad=false", "-prec-div=true", "-prec-sqrt=true"],
 }
-CPP_SOURCES = ["mesh.cpp", "setup.cpp", "study.cpp", "server.cpp"]
+CPP_SOURCES = ["mesh.cpp", "setup.cpp", "study.cpp", "server.cpp", "system.cpp"]
 CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-fopenmp", "-ffp-contract=off", "-fno-fast-math", "-Wall",
              "-Wno-unused-function", "-Wno-unused-variable", "-I" + os.path.join(CUDA, "include")]
 

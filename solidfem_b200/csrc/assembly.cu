@@ -499,11 +499,12 @@ __device__ __forceinline__ double stress_of(const double (&g)[10][3], const doub
 // Per element: stress at every integration point, and at every element node with the element's own
 // material (results.rs:494-523).
 __global__ void recover_elements_kernel(const double* __restrict__ nodes, const uint32_t* __restrict__ tets,
-                                        const double* __restrict__ disp, uint32_t count, int points, FieldArgs field,
+                                        const double* __restrict__ disp, uint32_t first, uint32_t count, int points,
+                                        FieldArgs field,
                                         const double* __restrict__ point_material, double* __restrict__ pstress,
                                         double* __restrict__ pvm, double* __restrict__ ppos, double* __restrict__ pmat,
                                         double* __restrict__ cand, unsigned long long* error) {
-  uint32_t e = blockIdx.x * blockDim.x + threadIdx.x;
+  uint32_t e = first + blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= count) return;
   double x[10][3], u[10][3];
   for (int a = 0; a < 10; ++a) {
@@ -594,11 +595,11 @@ __device__ bool patch_solve(double (&m)[4][4], double (&rhs)[4][6]) {
 
 // The linear patch fit at every mesh vertex over its elements' integration points, in element
 // order; a patch of more than one material is left unfitted (results.rs:438-466, patch.rs:37-66).
-__global__ void patch_fit_kernel(const double* __restrict__ nodes, uint32_t vertices, int points,
+__global__ void patch_fit_kernel(const double* __restrict__ nodes, uint32_t first, uint32_t vertices, int points,
                                  const uint32_t* __restrict__ offsets, const uint32_t* __restrict__ incident,
                                  const double* __restrict__ pstress, const double* __restrict__ ppos,
                                  const double* __restrict__ pmat, double* __restrict__ fits, int* __restrict__ has_fit) {
-  uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
+  uint32_t v = first + blockIdx.x * blockDim.x + threadIdx.x;
   if (v >= vertices) return;
   double c[3] = {nodes[(size_t)v * 3], nodes[(size_t)v * 3 + 1], nodes[(size_t)v * 3 + 2]};
   uint32_t o0 = offsets[v], o1 = offsets[v + 1];
@@ -720,21 +721,33 @@ sf_status launch_scatter_displacements(const double* x, RecoveryDevice& r, uint3
   return cuda_check(cudaGetLastError(), "scatter displacements");
 }
 
-sf_status launch_recovery(const AssemblyDevice& a, const MaterialSpec& m, RecoveryDevice& r, uint32_t node_count,
-                          uint32_t vertex_count, cudaStream_t stream) {
+sf_status launch_recovery_elements(const AssemblyDevice& a, const MaterialSpec& m, RecoveryDevice& r, uint32_t first,
+                                   uint32_t end, cudaStream_t stream) {
+  if (end <= first) return SF_OK;
   if (sf_status s = ensure_tables(a.quadrature, stream)) return s;
   if (sf_status s = ensure_node_table(a.quadrature, stream)) return s;
-  recover_elements_kernel<<<(a.tet_count + 127) / 128, 128, 0, stream>>>(
-      a.nodes, a.tets, r.disp, a.tet_count, a.points, field_args(m), a.point_material, r.point_stress, r.point_vm,
+  recover_elements_kernel<<<(end - first + 127) / 128, 128, 0, stream>>>(
+      a.nodes, a.tets, r.disp, first, end, a.points, field_args(m), a.point_material, r.point_stress, r.point_vm,
       r.point_pos, r.point_mat, r.node_candidate, a.error);
-  patch_fit_kernel<<<(vertex_count + 127) / 128, 128, 0, stream>>>(a.nodes, vertex_count, a.points, r.vertex_offsets,
-                                                                   r.vertex_incident, r.point_stress, r.point_pos,
-                                                                   r.point_mat, r.fits, r.has_fit);
+  return cuda_check(cudaGetLastError(), "recovery elements");
+}
+
+sf_status launch_recovery_fits(const AssemblyDevice& a, RecoveryDevice& r, uint32_t first, uint32_t end,
+                               cudaStream_t stream) {
+  if (end <= first) return SF_OK;
+  patch_fit_kernel<<<(end - first + 127) / 128, 128, 0, stream>>>(a.nodes, first, end, a.points, r.vertex_offsets,
+                                                                  r.vertex_incident, r.point_stress, r.point_pos,
+                                                                  r.point_mat, r.fits, r.has_fit);
+  return cuda_check(cudaGetLastError(), "recovery patch fits");
+}
+
+sf_status launch_recovery_field(const AssemblyDevice& a, RecoveryDevice& r, uint32_t node_count,
+                                uint32_t vertex_count, cudaStream_t stream) {
   nodal_field_kernel<<<(node_count + 127) / 128, 128, 0, stream>>>(a.nodes, a.tets, node_count, vertex_count,
                                                                    r.node_offsets, r.node_incident, r.node_candidate,
                                                                    r.fits, r.has_fit, r.midside_first, r.nodal_stress,
                                                                    r.nodal_vm);
-  return cuda_check(cudaGetLastError(), "recovery");
+  return cuda_check(cudaGetLastError(), "recovery field");
 }
 
 }  // namespace sf

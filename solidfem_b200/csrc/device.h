@@ -291,9 +291,16 @@ struct RecoveryDevice {
   bool ready = false;             // incidence uploaded
 };
 // Device stress recovery of the displacements in r.disp (crates/solidfem-elastic/src/results.rs:
-// 470-539 and 376-410, patch.rs:37-120), bit-identical to the reference's serial recovery.
-sf_status launch_recovery(const AssemblyDevice& a, const MaterialSpec& m, RecoveryDevice& r,
-                          uint32_t node_count, uint32_t vertex_count, cudaStream_t stream);
+// 470-539 and 376-410, patch.rs:37-120), bit-identical to the reference's serial recovery, in
+// the reference's units of work: elements [first, end) (point stresses and each element's values
+// at its nodes), then vertices [first, end) (patch fits), then the nodal field once both are done.
+// Every unit is independent of the others, so any slicing gives the bits of one pass.
+sf_status launch_recovery_elements(const AssemblyDevice& a, const MaterialSpec& m, RecoveryDevice& r, uint32_t first,
+                                   uint32_t end, cudaStream_t stream);
+sf_status launch_recovery_fits(const AssemblyDevice& a, RecoveryDevice& r, uint32_t first, uint32_t end,
+                               cudaStream_t stream);
+sf_status launch_recovery_field(const AssemblyDevice& a, RecoveryDevice& r, uint32_t node_count,
+                                uint32_t vertex_count, cudaStream_t stream);
 // The displacement of every mesh node from the free-DOF solution (zero at fixed nodes).
 sf_status launch_scatter_displacements(const double* x, RecoveryDevice& r, uint32_t node_count, cudaStream_t stream);
 
@@ -311,6 +318,12 @@ sf_status solver_precondition(DeviceSolver& s, const double* d_in, double* d_out
 sf_status solver_system_multiply(DeviceSolver& s, const double* d_in, double* d_out);
 sf_status solver_capture_graph(DeviceSolver& s);
 sf_status solver_read_state(DeviceSolver& s, PcgState* out);
+// Pcg::step on the device (study.cpp): up to max_iterations iterations replayed in chunks with one
+// state read-back per chunk into `pinned`; updates last, status and cancelled.
+sf_status run_iterations(DeviceSolver& d, bool use_graphs, uint64_t max_iterations, sf_cancel_fn cancel, void* user,
+                         PcgState* pinned, PcgState& last, int& status, bool& cancelled);
+// The step outcome of a solve in `status` and its PcgError, if it failed, as the returned status.
+sf_status step_result(int status, bool cancelled, const PcgState& last, sf_step_outcome* out);
 // Restarts the solve from x = 0 with the resident right-hand side (Pcg::new).
 sf_status solver_restart(DeviceSolver& s, double tolerance, uint64_t max_iterations);
 // Mean device milliseconds per launch of one solver kernel and its algorithmic bytes per launch.

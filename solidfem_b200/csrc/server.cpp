@@ -10,6 +10,7 @@
 // studies. Larger studies go to solver threads and solve on their own streams, overlapping on the
 // device with the batches and with each other while the build workers go on building.
 #include <algorithm>
+#include <atomic>
 #include <cstdio>
 #include <condition_variable>
 #include <deque>
@@ -44,7 +45,11 @@ struct Request {
   uint64_t device_bytes = 0;
   uint64_t batch_peak = 0;  // the largest batch it ran in
   char message[160] = {0};  // the failure's message
+  std::atomic<bool> cancel{false};  // sf_server_cancel asked for it
 };
+
+// The cancel callback of a request's build and solve.
+int32_t request_cancelled(void* user) { return static_cast<Request*>(user)->cancel.load() ? 1 : 0; }
 
 }  // namespace
 
@@ -126,7 +131,7 @@ struct sf_server {
       sf_study* st = nullptr;
       sf_model* model = r->model;
       r->model = nullptr;
-      sf_status e = sf_study_create(model, &r->options, nullptr, nullptr, &st);
+      sf_status e = sf_study_create(model, &r->options, sf::request_cancelled, r, &st);
       r->t_built = sf::now_seconds();
       if (e) {
         {
@@ -169,10 +174,27 @@ struct sf_server {
         solving.pop_front();
       }
       sf_step_outcome out{};
-      sf_status e = sf_study_step(r->study, UINT64_MAX, nullptr, nullptr, &out);
+      sf_status e = sf_study_step(r->study, UINT64_MAX, sf::request_cancelled, r, &out);
       r->outcome = out;
+      if (!e && out.kind == SF_OUTCOME_CANCELLED) e = sf::fail(SF_CANCELLED, "the request was cancelled");
       complete(r, e);
     }
+  }
+
+  // Members of a batch whose requests were cancelled leave it between chunks; the others go on.
+  void drop_cancelled(sf::BatchRunner& run) {
+    std::vector<sf_study*> keep;
+    for (sf_study* st : run.members) {
+      sf::Request* r = owners[st];
+      if (!r->cancel.load()) {
+        keep.push_back(st);
+        continue;
+      }
+      owners.erase(st);
+      run.dirty = true;
+      complete(r, sf::fail(SF_CANCELLED, "the request was cancelled"));
+    }
+    run.members.swap(keep);
   }
 
   void batch_loop() {
@@ -189,6 +211,10 @@ struct sf_server {
         joining.swap(ready);
       }
       for (sf::Request* r : joining) {
+        if (r->cancel.load()) {
+          complete(r, sf::fail(SF_CANCELLED, "the request was cancelled"));
+          continue;
+        }
         uint64_t sig = sf::study_signature(r->study);
         auto& run = runners[sig];
         if (!run) {
@@ -209,6 +235,7 @@ struct sf_server {
       }
       for (auto& kv : runners) {
         sf::BatchRunner& run = *kv.second;
+        drop_cancelled(run);
         if (run.members.empty()) continue;
         // A batch holds at most max_batch studies; the rest wait in the ready list.
         if (run.members.size() > opt.max_batch) {
@@ -374,6 +401,36 @@ sf_status sf_server_take(sf_server* s, uint64_t id, double* displacements) {
   }
   if (r->status) return sf::fail(r->status, "the request failed");
   if (displacements) std::memcpy(displacements, r->displacements.data(), r->displacements.size() * 8);
+  return SF_OK;
+}
+
+sf_status sf_server_cancel(sf_server* s, uint64_t id) {
+  if (!s) return sf::fail(SF_INVALID_ARGUMENT, "null argument");
+  sf::Request* dropped = nullptr;
+  {
+    std::lock_guard<std::mutex> lock(s->m);
+    auto it = s->all.find(id);
+    if (it == s->all.end()) return sf::fail(SF_INVALID_ARGUMENT, "no such request");
+    sf::Request* r = it->second.get();
+    if (r->state == 3) return SF_OK;  // finished already: nothing to cancel
+    r->cancel.store(true);
+    // Not yet taken by a worker: it leaves the queue here. Later stages read the flag.
+    for (auto* q : {&s->pending, &s->admitted}) {
+      auto at = std::find(q->begin(), q->end(), r);
+      if (at != q->end()) {
+        q->erase(at);
+        dropped = r;
+        break;
+      }
+    }
+  }
+  if (dropped) {
+    if (dropped->model) {
+      sf_model_destroy(dropped->model);
+      dropped->model = nullptr;
+    }
+    s->complete(dropped, sf::fail(SF_CANCELLED, "the request was cancelled"));
+  }
   return SF_OK;
 }
 

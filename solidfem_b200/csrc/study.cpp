@@ -386,9 +386,11 @@ struct sf_study {
   double assembly_ms = 0;
   PcgState* pinned = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-  RecoveryDevice rec;
-  bool recovered = false;  // rec holds the field of the converged displacements
+  RecoveryDevice rec;              // the incidence tables every recovery of this study reads
+  sf_recovery* answer = nullptr;   // the finished recovery of the converged displacements
+  void release_answer();
   ~sf_study() {
+    release_answer();
     pinned_release(pinned);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
@@ -396,6 +398,26 @@ struct sf_study {
     if (solver.stream) cudaStreamDestroy(solver.stream);
   }
 };
+
+// A resumable stress recovery of one snapshot of a study's displacements (Recovery,
+// results.rs:97-124): its own device buffers, the study's incidence tables, and how far it got
+// (elements first, then one patch fit per vertex).
+struct sf_recovery {
+  sf_study* study = nullptr;
+  RecoveryDevice dev;
+  uint64_t next_element = 0, next_vertex = 0;
+  bool converged = false;  // a snapshot of the converged answer, not a preview
+  vector<void*> owned;     // dev's own buffers
+};
+
+extern "C" {
+static void recovery_free(sf_recovery* r);  // defined with the recovery entry points
+}
+
+void sf_study::release_answer() {
+  if (answer) recovery_free(answer);
+  answer = nullptr;
+}
 
 static void release_builder_device(sf_builder* b) {
   dev_free_all(b->solver);
@@ -1120,53 +1142,30 @@ static void fill_progress(const PcgState& st, sf_progress* p) {
   p->at_rounding_floor = st.at_floor;
 }
 
-sf_status sf_study_step(sf_study* s, uint64_t max_iterations, sf_cancel_fn cancel, void* user, sf_step_outcome* out) {
-  if (!s) return fail(SF_INVALID_ARGUMENT, "null argument");
-  DeviceSolver& d = s->solver;
-  cudaSetDevice(d.device);
-  auto finish = [&](int kind) -> sf_status {
-    s->report.iterations = s->last.iterations;
-    s->report.relative_residual = s->last.rel;
-    s->report.at_rounding_floor = s->last.at_floor;
-    if (out) {
-      out->kind = kind;
-      fill_progress(s->last, &out->progress);
-    }
-    if (s->status == ST_FAILED_NOT_PD) {
-      error_slot().iteration = s->last.fail_iteration;
-      error_slot().curvature = s->last.curvature;
-      return fail(SF_PCG_NOT_POSITIVE_DEFINITE, "the system is not positive definite along the search direction");
-    }
-    if (s->status == ST_FAILED_NOT_CONVERGED) {
-      error_slot().iteration = s->last.iterations;
-      error_slot().relative_residual = s->last.rel;
-      return fail(SF_PCG_NOT_CONVERGED, "the iteration cap ran out before the tolerance");
-    }
-    return SF_OK;
-  };
-  if (s->cancelled) return finish(SF_OUTCOME_CANCELLED);
-  if (s->status == ST_CONVERGED) return finish(SF_OUTCOME_CONVERGED);
-  if (s->status != ST_ACTIVE) return finish(SF_OUTCOME_RUNNING);
-  double t0 = now_seconds();
-  cudaEventRecord(s->ev0, d.stream);
-  // Iterations are enqueued in chunks; every kernel of an iteration after the solve ends returns
-  // at once, so the state is read back once per chunk, with one chunk in flight ahead.
+}  // extern "C"
+
+namespace sf {
+
+// Pcg::step (pcg.rs:167-190) on the device: up to max_iterations iterations, enqueued in chunks;
+// every kernel of an iteration after the solve ends returns at once, so the state is read back
+// once per chunk, with one chunk in flight ahead. `cancel` is read before every iteration.
+sf_status run_iterations(DeviceSolver& d, bool use_graphs, uint64_t max_iterations, sf_cancel_fn cancel, void* user,
+                         PcgState* pinned, PcgState& last, int& status, bool& cancelled) {
   uint64_t done = 0;
   const uint64_t chunk_max = 16;
   uint64_t chunk = 4;
   bool stop = false;
-  int kind = SF_OUTCOME_RUNNING;
   while (!stop && done < max_iterations) {
     uint64_t k = std::min<uint64_t>(chunk, max_iterations - done);
     uint64_t launched = 0;
     for (; launched < k; ++launched) {
       if (cancel && cancel(user)) {
-        s->cancelled = true;
+        cancelled = true;
         stop = true;
         break;
       }
       sf_status e = SF_OK;
-      if (s->options.use_graphs) {
+      if (use_graphs) {
         e = cuda_check(cudaGraphLaunch(d.graph_exec, d.stream), "graph launch");
         d.launches += d.graph_kernels;
       } else {
@@ -1176,22 +1175,71 @@ sf_status sf_study_step(sf_study* s, uint64_t max_iterations, sf_cancel_fn cance
       if (e) return e;
     }
     done += launched;
-    copy_d2h(d, s->pinned, d.state, sizeof(PcgState));
+    copy_d2h(d, pinned, d.state, sizeof(PcgState));
     if (sf_status e = cuda_check(cudaStreamSynchronize(d.stream), "solver step")) return e;
-    s->last = *s->pinned;
-    s->status = s->last.status;
-    if (s->status != ST_ACTIVE) stop = true;
+    last = *pinned;
+    status = last.status;
+    if (status != ST_ACTIVE) stop = true;
     chunk = std::min(chunk_max, chunk * 2);
   }
+  return SF_OK;
+}
+
+// The StepOutcome of a step that ended with `status` (pcg.rs:47-57, 216-275): the kind and the
+// progress, and for a failed solve its PcgError as the returned status with its payload.
+sf_status step_result(int status, bool cancelled, const PcgState& last, sf_step_outcome* out) {
+  if (out) {
+    out->kind = cancelled ? SF_OUTCOME_CANCELLED : status == ST_CONVERGED ? SF_OUTCOME_CONVERGED : SF_OUTCOME_RUNNING;
+    fill_progress(last, &out->progress);
+  }
+  if (cancelled) return SF_OK;
+  if (status == ST_FAILED_NOT_PD) {
+    error_slot().iteration = last.fail_iteration;
+    error_slot().curvature = last.curvature;
+    return fail(SF_PCG_NOT_POSITIVE_DEFINITE, "the system is not positive definite along the search direction");
+  }
+  if (status == ST_FAILED_NOT_CONVERGED) {
+    error_slot().iteration = last.iterations;
+    error_slot().relative_residual = last.rel;
+    return fail(SF_PCG_NOT_CONVERGED, "the iteration cap ran out before the tolerance");
+  }
+  return SF_OK;
+}
+
+}  // namespace sf
+
+extern "C" {
+
+sf_status sf_study_step(sf_study* s, uint64_t max_iterations, sf_cancel_fn cancel, void* user, sf_step_outcome* out) {
+  if (!s) return fail(SF_INVALID_ARGUMENT, "null argument");
+  DeviceSolver& d = s->solver;
+  cudaSetDevice(d.device);
+  auto finish = [&]() -> sf_status {
+    s->report.iterations = s->last.iterations;
+    s->report.relative_residual = s->last.rel;
+    s->report.at_rounding_floor = s->last.at_floor;
+    return step_result(s->status, s->cancelled, s->last, out);
+  };
+  if (s->cancelled || s->status != ST_ACTIVE) return finish();
+  double t0 = now_seconds();
+  cudaEventRecord(s->ev0, d.stream);
+  if (sf_status e = run_iterations(d, s->options.use_graphs != 0, max_iterations, cancel, user, s->pinned, s->last,
+                                   s->status, s->cancelled))
+    return e;
   cudaEventRecord(s->ev1, d.stream);
   cudaEventSynchronize(s->ev1);
   float ms = 0;
   cudaEventElapsedTime(&ms, s->ev0, s->ev1);
   s->step_ms = ms;
   s->report.solve_seconds += now_seconds() - t0;
-  if (s->cancelled) kind = SF_OUTCOME_CANCELLED;
-  else if (s->status == ST_CONVERGED) kind = SF_OUTCOME_CONVERGED;
-  return finish(kind);
+  return finish();
+}
+
+/* Pcg::progress (pcg.rs:200-207) of a study's solve. */
+sf_status sf_study_progress(const sf_study* s, sf_progress* out) {
+  if (!s || !out) return fail(SF_INVALID_ARGUMENT, "null argument");
+  fill_progress(s->last, out);
+  return SF_OK;
 }
 
 }  // extern "C"
@@ -1358,66 +1406,93 @@ sf_status sf_study_report(const sf_study* s, sf_report* out) {
   return SF_OK;
 }
 
-// Device stress recovery of the current displacements (Recovery, results.rs:97-124): the
-// incidence lists are built once on the host, the three recovery kernels run on the study stream.
-static sf_status study_recover(sf_study* s) {
-  if (s->recovered) return SF_OK;
-  DeviceSolver& d = s->solver;
+// Device stress recovery (Recovery, results.rs:97-124, 376-539). The incidence lists every
+// recovery of a study reads are built once on the host; a recovery snapshots the displacements on
+// the device and advances in the reference's units of work (each element, then each vertex's
+// patch fit); the nodal field is made when both are done.
+static sf_status recovery_tables(sf_study* s) {
   RecoveryDevice& r = s->rec;
+  if (r.ready) return SF_OK;
+  DeviceSolver& d = s->solver;
+  const Mesh& m = s->model.mesh;
+  const size_t nn = m.nodes.size(), ne = m.tets.size(), nv = m.vertex_count;
+  // Elements touching each vertex through a corner, and (element, local node) per node, both in
+  // element order (results.rs:414-435); the first element reaching each midside node.
+  vector<uint32_t> voff(nv + 1, 0), noff(nn + 1, 0);
+  for (auto& t : m.tets) {
+    for (int c = 0; c < 4; ++c) voff[t[c] + 1] += 1;
+    for (int a = 0; a < 10; ++a) noff[t[a] + 1] += 1;
+  }
+  for (size_t i = 0; i < nv; ++i) voff[i + 1] += voff[i];
+  for (size_t i = 0; i < nn; ++i) noff[i + 1] += noff[i];
+  vector<uint32_t> vinc(voff[nv]), ninc(noff[nn]);
+  vector<uint32_t> vf(voff.begin(), voff.end() - 1), nf(noff.begin(), noff.end() - 1);
+  vector<uint32_t> mid(nn - nv, 0xffffffffu);
+  for (size_t e = 0; e < ne; ++e) {
+    const auto& t = m.tets[e];
+    for (int c = 0; c < 4; ++c) vinc[vf[t[c]]++] = (uint32_t)e;
+    for (int a = 0; a < 10; ++a) ninc[nf[t[a]]++] = ((uint32_t)e << 4) | (uint32_t)a;
+    for (int k = 0; k < 6; ++k)
+      if (mid[t[4 + k] - nv] == 0xffffffffu) mid[t[4 + k] - nv] = ((uint32_t)e << 3) | (uint32_t)k;
+  }
+  sf_status e = SF_OK;
+  if (!e) e = dev_alloc(d, (void**)&r.free, nn * 4);
+  if (!e) e = dev_alloc(d, (void**)&r.vertex_offsets, (nv + 1) * 4);
+  if (!e) e = dev_alloc(d, (void**)&r.vertex_incident, std::max<size_t>(1, vinc.size()) * 4);
+  if (!e) e = dev_alloc(d, (void**)&r.node_offsets, (nn + 1) * 4);
+  if (!e) e = dev_alloc(d, (void**)&r.node_incident, std::max<size_t>(1, ninc.size()) * 4);
+  if (!e) e = dev_alloc(d, (void**)&r.midside_first, std::max<size_t>(1, mid.size()) * 4);
+  if (e) return e;
+  copy_h2d(d, r.free, s->free.data(), nn * 4);
+  copy_h2d(d, r.vertex_offsets, voff.data(), voff.size() * 4);
+  if (!vinc.empty()) copy_h2d(d, r.vertex_incident, vinc.data(), vinc.size() * 4);
+  copy_h2d(d, r.node_offsets, noff.data(), noff.size() * 4);
+  if (!ninc.empty()) copy_h2d(d, r.node_incident, ninc.data(), ninc.size() * 4);
+  if (!mid.empty()) copy_h2d(d, r.midside_first, mid.data(), mid.size() * 4);
+  if ((e = cuda_check(cudaStreamSynchronize(d.stream), "recovery set-up"))) return e;
+  r.ready = true;
+  return SF_OK;
+}
+
+static void recovery_free(sf_recovery* r) {
+  if (!r) return;
+  DeviceSolver& d = r->study->solver;
+  cudaSetDevice(d.device);
+  cudaStreamSynchronize(d.stream);
+  for (void* p : r->owned) dev_free(d, p);
+  delete r;
+}
+
+// Recovery::new (results.rs:103-124) on the device: a snapshot of the current displacements
+// (prescribed components exact, fixed nodes zero) and the buffers of the work to come.
+static sf_status recovery_begin(sf_study* s, sf_recovery** out) {
+  if (sf_status e = recovery_tables(s)) return e;
+  DeviceSolver& d = s->solver;
   const Mesh& m = s->model.mesh;
   const size_t nn = m.nodes.size(), ne = m.tets.size(), nv = m.vertex_count;
   const size_t pts = (size_t)s->asmdev.points * ne;
-  double t0 = now_seconds();
-  if (!r.ready) {
-    // Elements touching each vertex through a corner, and (element, local node) per node, both in
-    // element order (results.rs:414-435); the first element reaching each midside node.
-    vector<uint32_t> voff(nv + 1, 0), noff(nn + 1, 0);
-    for (auto& t : m.tets) {
-      for (int c = 0; c < 4; ++c) voff[t[c] + 1] += 1;
-      for (int a = 0; a < 10; ++a) noff[t[a] + 1] += 1;
-    }
-    for (size_t i = 0; i < nv; ++i) voff[i + 1] += voff[i];
-    for (size_t i = 0; i < nn; ++i) noff[i + 1] += noff[i];
-    vector<uint32_t> vinc(voff[nv]), ninc(noff[nn]);
-    vector<uint32_t> vf(voff.begin(), voff.end() - 1), nf(noff.begin(), noff.end() - 1);
-    vector<uint32_t> mid(nn - nv, 0xffffffffu);
-    for (size_t e = 0; e < ne; ++e) {
-      const auto& t = m.tets[e];
-      for (int c = 0; c < 4; ++c) vinc[vf[t[c]]++] = (uint32_t)e;
-      for (int a = 0; a < 10; ++a) ninc[nf[t[a]]++] = ((uint32_t)e << 4) | (uint32_t)a;
-      for (int k = 0; k < 6; ++k)
-        if (mid[t[4 + k] - nv] == 0xffffffffu) mid[t[4 + k] - nv] = ((uint32_t)e << 3) | (uint32_t)k;
-    }
-    sf_status e = SF_OK;
-    if (!e) e = dev_alloc(d, (void**)&r.disp, nn * 24);
-    if (!e) e = dev_alloc(d, (void**)&r.free, nn * 4);
-    if (!e) e = dev_alloc(d, (void**)&r.point_stress, pts * 48);
-    if (!e) e = dev_alloc(d, (void**)&r.point_vm, pts * 8);
-    if (!e) e = dev_alloc(d, (void**)&r.point_pos, pts * 24);
-    if (!e) e = dev_alloc(d, (void**)&r.point_mat, pts * 16);
-    if (!e) e = dev_alloc(d, (void**)&r.node_candidate, ne * 10 * 56);
-    if (!e) e = dev_alloc(d, (void**)&r.vertex_offsets, (nv + 1) * 4);
-    if (!e) e = dev_alloc(d, (void**)&r.vertex_incident, std::max<size_t>(1, vinc.size()) * 4);
-    if (!e) e = dev_alloc(d, (void**)&r.node_offsets, (nn + 1) * 4);
-    if (!e) e = dev_alloc(d, (void**)&r.node_incident, std::max<size_t>(1, ninc.size()) * 4);
-    if (!e) e = dev_alloc(d, (void**)&r.fits, nv * 28 * 8);
-    if (!e) e = dev_alloc(d, (void**)&r.has_fit, nv * 4);
-    if (!e) e = dev_alloc(d, (void**)&r.midside_first, std::max<size_t>(1, mid.size()) * 4);
-    if (!e) e = dev_alloc(d, (void**)&r.nodal_stress, nn * 48);
-    if (!e) e = dev_alloc(d, (void**)&r.nodal_vm, nn * 8);
-    if (e) return e;
-    copy_h2d(d, r.free, s->free.data(), nn * 4);
-    copy_h2d(d, r.vertex_offsets, voff.data(), voff.size() * 4);
-    if (!vinc.empty()) copy_h2d(d, r.vertex_incident, vinc.data(), vinc.size() * 4);
-    copy_h2d(d, r.node_offsets, noff.data(), noff.size() * 4);
-    if (!ninc.empty()) copy_h2d(d, r.node_incident, ninc.data(), ninc.size() * 4);
-    if (!mid.empty()) copy_h2d(d, r.midside_first, mid.data(), mid.size() * 4);
-    if ((e = cuda_check(cudaStreamSynchronize(d.stream), "recovery set-up"))) return e;
-    r.ready = true;
-  }
-  unsigned long long none = ~0ull;
-  copy_h2d(d, s->asmdev.error, &none, 8);
-  sf_status e = launch_scatter_displacements(d.x, r, (uint32_t)nn, d.stream);
+  std::unique_ptr<sf_recovery> rec(new sf_recovery);
+  rec->study = s;
+  rec->converged = s->status == ST_CONVERGED;
+  RecoveryDevice& r = rec->dev;
+  r = s->rec;  // the shared tables
+  auto alloc = [&](void** p, size_t bytes) -> sf_status {
+    if (sf_status e = dev_alloc(d, p, std::max<size_t>(bytes, 8))) return e;
+    rec->owned.push_back(*p);
+    return SF_OK;
+  };
+  sf_status e = SF_OK;
+  if (!e) e = alloc((void**)&r.disp, nn * 24);
+  if (!e) e = alloc((void**)&r.point_stress, pts * 48);
+  if (!e) e = alloc((void**)&r.point_vm, pts * 8);
+  if (!e) e = alloc((void**)&r.point_pos, pts * 24);
+  if (!e) e = alloc((void**)&r.point_mat, pts * 16);
+  if (!e) e = alloc((void**)&r.node_candidate, ne * 10 * 56);
+  if (!e) e = alloc((void**)&r.fits, nv * 28 * 8);
+  if (!e) e = alloc((void**)&r.has_fit, nv * 4);
+  if (!e) e = alloc((void**)&r.nodal_stress, nn * 48);
+  if (!e) e = alloc((void**)&r.nodal_vm, nn * 8);
+  if (!e) e = launch_scatter_displacements(d.x, r, (uint32_t)nn, d.stream);
   if (!e && !s->model.prescribed.empty()) {
     // the prescribed components, exact
     vector<uint32_t> idx;
@@ -1435,50 +1510,86 @@ static sf_status study_recover(sf_study* s) {
       copy_h2d(d, d_val, val.data(), val.size() * 8);
       e = setup_set_values(d.stream, idx.size(), d_idx, d_val, r.disp);
     }
+    if (!e) e = cuda_check(cudaStreamSynchronize(d.stream), "recovery snapshot");
     dev_free(d, d_idx);
     dev_free(d, d_val);
   }
-  if (!e) e = launch_recovery(s->asmdev, s->model.material, r, (uint32_t)nn, (uint32_t)nv, d.stream);
-  d.launches += 4;
-  unsigned long long err = 0;
-  if (!e) copy_d2h(d, &err, s->asmdev.error, 8);
-  if (!e) e = cuda_check(cudaStreamSynchronize(d.stream), "recovery");
-  if (e) return e;
-  if (err != ~0ull) {
-    error_slot().tet = (uint32_t)(err >> 32);
-    error_slot().point = (uint32_t)((err >> 8) & 0xff);
-    return fail((err & 0xff) == FAULT_INVERTED ? SF_ELEMENT_INVERTED_JACOBIAN : SF_ELEMENT_INVALID_MATERIAL,
-                "recovery met an inverted element or an invalid material");
+  d.launches += 1;
+  if (e) {
+    recovery_free(rec.release());
+    return e;
   }
-  s->report.recovery_seconds += now_seconds() - t0;
-  s->recovered = true;
+  *out = rec.release();
   return SF_OK;
 }
 
-sf_status sf_study_solution(sf_study* s, double* displacements, double* nodal_stress, double* nodal_von_mises,
-                            sf_point_stress* points) {
-  if (!s) return fail(SF_INVALID_ARGUMENT, "null argument");
-  if (s->status != ST_CONVERGED) return fail(SF_NOT_FINISHED, "the solve has not converged");
+// Recovery::advance (results.rs:470-539): up to `budget` more units, elements first, then patch
+// fits; `cancel` is read before each launch. Returns the element fault the reference would name.
+static sf_status recovery_advance(sf_study* s, sf_recovery* rec, uint64_t budget, sf_cancel_fn cancel, void* user) {
   DeviceSolver& d = s->solver;
-  cudaSetDevice(d.device);
-  if (displacements)
-    if (sf_status e = sf_study_displacements(s, displacements)) return e;
-  if (!nodal_stress && !nodal_von_mises && !points) return SF_OK;
-  if (sf_status e = study_recover(s)) return e;
-  const size_t nn = s->model.mesh.nodes.size(), ne = s->model.mesh.tets.size();
+  const uint64_t ne = s->model.mesh.tets.size(), nv = s->model.mesh.vertex_count;
+  double t0 = now_seconds();
+  sf_status e = SF_OK;
+  if (rec->next_element < ne && budget > 0) {
+    if (cancel && cancel(user)) return fail(SF_CANCELLED, "the recovery was cancelled");
+    const uint64_t end = std::min<uint64_t>(ne, rec->next_element + budget);
+    unsigned long long none = ~0ull, err = 0;
+    copy_h2d(d, s->asmdev.error, &none, 8);
+    e = launch_recovery_elements(s->asmdev, s->model.material, rec->dev, (uint32_t)rec->next_element, (uint32_t)end,
+                                 d.stream);
+    d.launches += 1;
+    if (!e) copy_d2h(d, &err, s->asmdev.error, 8);
+    if (!e) e = cuda_check(cudaStreamSynchronize(d.stream), "recovery");
+    if (e) return e;
+    if (err != ~0ull) {
+      error_slot().tet = (uint32_t)(err >> 32);
+      error_slot().point = (uint32_t)((err >> 8) & 0xff);
+      return fail((err & 0xff) == FAULT_INVERTED ? SF_ELEMENT_INVERTED_JACOBIAN : SF_ELEMENT_INVALID_MATERIAL,
+                  "recovery met an inverted element or an invalid material");
+    }
+    budget -= end - rec->next_element;
+    rec->next_element = end;
+  }
+  if (rec->next_element == ne && rec->next_vertex < nv && budget > 0) {
+    if (cancel && cancel(user)) return fail(SF_CANCELLED, "the recovery was cancelled");
+    const uint64_t end = std::min<uint64_t>(nv, rec->next_vertex + budget);
+    e = launch_recovery_fits(s->asmdev, rec->dev, (uint32_t)rec->next_vertex, (uint32_t)end, d.stream);
+    d.launches += 1;
+    if (!e) e = cuda_check(cudaStreamSynchronize(d.stream), "recovery");
+    if (e) return e;
+    rec->next_vertex = end;
+  }
+  s->report.recovery_seconds += now_seconds() - t0;
+  return SF_OK;
+}
+
+static bool recovery_finished(const sf_study* s, const sf_recovery* r) {
+  return r->next_element == s->model.mesh.tets.size() && r->next_vertex == s->model.mesh.vertex_count;
+}
+
+// Recovery::into_field (results.rs:376-410) and the copies out: any output may be null.
+static sf_status recovery_outputs(sf_study* s, sf_recovery* rec, double* displacements, double* nodal_stress,
+                                  double* nodal_von_mises, sf_point_stress* points) {
+  DeviceSolver& d = s->solver;
+  const Mesh& m = s->model.mesh;
+  const size_t nn = m.nodes.size(), ne = m.tets.size();
   const size_t q = (size_t)s->asmdev.points, pts = q * ne;
-  if (nodal_stress) copy_d2h(d, nodal_stress, s->rec.nodal_stress, nn * 48);
-  if (nodal_von_mises) copy_d2h(d, nodal_von_mises, s->rec.nodal_vm, nn * 8);
+  sf_status e = launch_recovery_field(s->asmdev, rec->dev, (uint32_t)nn, (uint32_t)m.vertex_count, d.stream);
+  d.launches += 1;
+  if (e) return e;
+  if (displacements) copy_d2h(d, displacements, rec->dev.disp, nn * 24);
+  if (nodal_stress) copy_d2h(d, nodal_stress, rec->dev.nodal_stress, nn * 48);
+  if (nodal_von_mises) copy_d2h(d, nodal_von_mises, rec->dev.nodal_vm, nn * 8);
   vector<double> ps, pv, pp;
   if (points) {
     ps.resize(pts * 6);
     pv.resize(pts);
     pp.resize(pts * 3);
-    copy_d2h(d, ps.data(), s->rec.point_stress, pts * 48);
-    copy_d2h(d, pv.data(), s->rec.point_vm, pts * 8);
-    copy_d2h(d, pp.data(), s->rec.point_pos, pts * 24);
+    copy_d2h(d, ps.data(), rec->dev.point_stress, pts * 48);
+    copy_d2h(d, pv.data(), rec->dev.point_vm, pts * 8);
+    copy_d2h(d, pp.data(), rec->dev.point_pos, pts * 24);
   }
-  if (sf_status e = cuda_check(cudaStreamSynchronize(d.stream), "read recovery")) return e;
+  if ((e = cuda_check(cudaStreamSynchronize(d.stream), "read recovery"))) return e;
   if (points)
     for (size_t i = 0; i < pts; ++i) {
       points[i].tet = (uint32_t)(i / q);
@@ -1489,6 +1600,57 @@ sf_status sf_study_solution(sf_study* s, double* displacements, double* nodal_st
     }
   return SF_OK;
 }
+
+// Units of recovery work per launch when the caller gives no budget (sf_study_solution): the
+// cancel callback is read between such slices.
+static const uint64_t kRecoverySlice = 1u << 16;
+
+sf_status sf_study_solution(sf_study* s, sf_cancel_fn cancel, void* user, double* displacements,
+                            double* nodal_stress, double* nodal_von_mises, sf_point_stress* points) {
+  if (!s) return fail(SF_INVALID_ARGUMENT, "null argument");
+  if (s->status != ST_CONVERGED) return fail(SF_NOT_FINISHED, "the solve has not converged");
+  DeviceSolver& d = s->solver;
+  cudaSetDevice(d.device);
+  if (!nodal_stress && !nodal_von_mises && !points) return sf_study_displacements(s, displacements);
+  if (!s->answer) {
+    sf_recovery* rec = nullptr;
+    if (sf_status e = recovery_begin(s, &rec)) return e;
+    while (!recovery_finished(s, rec)) {
+      if (sf_status e = recovery_advance(s, rec, kRecoverySlice, cancel, user)) {
+        recovery_free(rec);
+        return e;
+      }
+    }
+    s->answer = rec;
+  }
+  return recovery_outputs(s, s->answer, displacements, nodal_stress, nodal_von_mises, points);
+}
+
+sf_status sf_study_begin_recovery(sf_study* s, sf_recovery** out) {
+  if (!s || !out) return fail(SF_INVALID_ARGUMENT, "null argument");
+  *out = nullptr;
+  cudaSetDevice(s->solver.device);
+  return recovery_begin(s, out);
+}
+
+sf_status sf_study_continue_recovery(sf_study* s, sf_recovery* r, uint64_t max_units, sf_cancel_fn cancel, void* user,
+                                     int32_t* finished) {
+  if (!s || !r || r->study != s) return fail(SF_INVALID_ARGUMENT, "a recovery of another study");
+  cudaSetDevice(s->solver.device);
+  sf_status e = recovery_advance(s, r, max_units, cancel, user);
+  if (finished) *finished = recovery_finished(s, r) ? 1 : 0;
+  return e;
+}
+
+sf_status sf_study_finish_recovery(sf_study* s, sf_recovery* r, double* displacements, double* nodal_stress,
+                                   double* nodal_von_mises, sf_point_stress* points) {
+  if (!s || !r || r->study != s) return fail(SF_INVALID_ARGUMENT, "a recovery of another study");
+  if (!recovery_finished(s, r)) return fail(SF_NOT_FINISHED, "elements or patch fits remain");
+  cudaSetDevice(s->solver.device);
+  return recovery_outputs(s, r, displacements, nodal_stress, nodal_von_mises, points);
+}
+
+void sf_recovery_destroy(sf_recovery* r) { recovery_free(r); }
 
 void sf_study_destroy(sf_study* s) { delete s; }
 
@@ -1693,7 +1855,7 @@ sf_status sf_study_resolve(sf_study* s, const double* rhs) {
     copy_h2d(d, d.rhs, rhs, (size_t)d.n * 8);
   }
   if (sf_status e = solver_restart(d, s->options.tolerance, s->options.max_iterations)) return e;
-  s->recovered = false;
+  s->release_answer();
   s->cancelled = false;
   std::memset(&s->last, 0, sizeof(s->last));
   s->status = ST_ACTIVE;

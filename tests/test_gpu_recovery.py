@@ -76,3 +76,74 @@ def test_solution_refused_before_convergence():
     with pytest.raises(sf.SolidfemError) as e:
         study.solution()
     assert e.value.status == sf.Status.NOT_FINISHED
+
+
+def field_bits(f):
+    return [np.ascontiguousarray(a).view(np.uint8) for a in
+            (f.displacements, f.nodal_stress, f.nodal_von_mises, f.point_stresses)]
+
+
+def assert_same_field(a, b):
+    for x, y in zip(field_bits(a), field_bits(b)):
+        assert np.array_equal(x, y)
+
+
+def recover_in_slices(study, budget, cancel_at=None):
+    rec = study.begin_recovery()
+    calls = 0
+    while True:
+        calls += 1
+        if cancel_at is not None and calls == cancel_at:
+            with pytest.raises(sf.SolidfemError) as err:
+                rec.continue_(budget, cancel=lambda: True)
+            assert err.value.status == sf.Status.CANCELLED
+            continue
+        if rec.continue_(budget):
+            return rec.finish()
+
+
+@pytest.mark.parametrize("budget", [1, 97, 1000, 2**40])
+def test_sliced_recovery_gives_the_bits_of_one_call(budget):
+    """continue_recovery in any slices (results.rs:97-124: a recovery resumed in slices gives
+    exactly the bits of one run), with a cancelled call in the middle that changes nothing."""
+    _, model = product_model((10.0, 1.0, 1.0), (12, 3, 3), 200000.0, 0.3)
+    study = sf.StaticStudy.new(model, mg_options(sf.Precision.MIXED))
+    assert study.solve().kind == sf.Outcome.CONVERGED
+    whole = study.solution()
+    sliced = recover_in_slices(study, budget, cancel_at=2 if budget < 2**40 else None)
+    assert_same_field(whole, sliced)
+
+
+def test_a_preview_recovery_runs_before_convergence_and_matches_the_oracle(oracle):
+    """begin_recovery on a solve still running recovers the estimate so far (a preview), bit-exact
+    with the oracle's recovery of those displacements; solution() still refuses."""
+    size, div = (20.0, 20.0, 1.0), (8, 8, 2)
+    _, model = product_model(size, div, 200000.0, 0.3)
+    study = sf.StaticStudy.new(model, mg_options(sf.Precision.DOUBLE))
+    assert study.step(5).kind == sf.Outcome.RUNNING
+    rec = study.begin_recovery()
+    with pytest.raises(sf.SolidfemError) as err:
+        rec.finish()
+    assert err.value.status == sf.Status.NOT_FINISHED
+    while not rec.continue_(500):
+        pass
+    field = rec.finish()
+    assert np.array_equal(field.displacements.view(np.uint64), study.displacements().view(np.uint64))
+    ref = oracle_study(oracle, size, div, 200000.0, 0.3, oracle.default_options(tolerance=1e-9, coarse_dofs=100))
+    s6, vm = ref.recover_with(field.displacements)
+    assert np.array_equal(field.nodal_stress.view(np.uint64), s6.view(np.uint64))
+    assert np.array_equal(field.nodal_von_mises.view(np.uint64), vm.view(np.uint64))
+    with pytest.raises(sf.SolidfemError) as err:
+        study.solution()
+    assert err.value.status == sf.Status.NOT_FINISHED
+
+
+def test_solution_can_be_cancelled():
+    _, model = product_model((10.0, 1.0, 1.0), (12, 3, 3), 200000.0, 0.3)
+    study = sf.StaticStudy.new(model, mg_options(sf.Precision.DOUBLE))
+    assert study.solve().kind == sf.Outcome.CONVERGED
+    with pytest.raises(sf.SolidfemError) as err:
+        study.solution(cancel=lambda: True)
+    assert err.value.status == sf.Status.CANCELLED
+    sol = study.solution()  # nothing was kept from the cancelled call
+    assert np.all(np.isfinite(sol.nodal_von_mises))
