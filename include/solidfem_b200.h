@@ -290,7 +290,9 @@ sf_status sf_study_solution(sf_study* study, sf_cancel_fn cancel, void* user, do
                             double* nodal_stress, double* nodal_von_mises, sf_point_stress* points);
 
 /* Recovery (crates/solidfem-elastic/src/results.rs:97-124): a resumable stress recovery of one
- * snapshot of a study's displacements, with its own device buffers. Destroy it before its study. */
+ * snapshot of a study's displacements, with its own device buffers. Its study may be destroyed
+ * first: the recovery's device memory then goes with the study, and the handle only accepts
+ * sf_recovery_destroy. */
 typedef struct sf_recovery sf_recovery;
 /* StaticStudy::begin_recovery (study.rs:262-274): snapshots the current displacements on the
  * device: the converged answer, or a preview of a solve still running. */
@@ -373,6 +375,33 @@ sf_status sf_study_aggregates(const sf_study* study, uint64_t level, uint32_t* o
 /* Preconditioner::apply (preconditioner.rs:10-20): one device V-cycle (or Jacobi scaling) of
  * `residual` into `output`, free_dofs each, host buffers. */
 sf_status sf_study_precondition(sf_study* study, const double* residual, double* output);
+/* The stages of one level of the device V-cycle (cycle.rs:461-539 and its device form,
+ * gpu/reference.rs:17-240), each run by exactly the launches the cycle makes for it, in the
+ * study's storage and vector precision (host f64 buffers; inputs are rounded to the vector type,
+ * outputs widened): the hand-off the reference's device tests compare stage by stage
+ * (tests/solver/gpu_hierarchy_execution.rs:434-557). n is the level's scalar rows, nc the next
+ * coarser level's.
+ *   SMOOTH          in0 b (n) -> out0 the smoother from zero (n)
+ *   SMOOTH_ADD      in0 b, in1 x (n) -> out0 x + smoother (the post-smoother's final add)
+ *   START           in0 b (n) -> out0 (D^-1 b) / theta (the smoother's first iterate)
+ *   RESIDUAL        in0 b, in1 x (n) -> out0 b - A x
+ *   RESTRICT        in0 r (n) -> out0 R r (nc)
+ *   PROLONG         in0 e (nc), in1 x (n) -> out0 x + P e
+ *   RESTRICT_START  in0 r (n) -> out0 R r (nc), out1 the coarser level's start from it (nc)
+ *   RESIDUAL_START  in0 b, in1 x (n) -> out0 b - A x, out1 the start from it (n)
+ * The stage overwrites the level's work vectors: call it between solver steps, not during one. */
+enum {
+  SF_STAGE_SMOOTH = 0,
+  SF_STAGE_RESIDUAL = 1,
+  SF_STAGE_RESTRICT = 2,
+  SF_STAGE_PROLONG = 3,
+  SF_STAGE_START = 4,
+  SF_STAGE_SMOOTH_ADD = 5,
+  SF_STAGE_RESTRICT_START = 6,
+  SF_STAGE_RESIDUAL_START = 7
+};
+sf_status sf_study_level_stage(sf_study* study, uint64_t level, int32_t stage, const double* in0,
+                               const double* in1, double* out0, double* out1);
 /* CsrMatrix::multiply (csr.rs:112-120) on the device, FP64, host buffers. */
 sf_status sf_study_system_multiply(sf_study* study, const double* x, double* y);
 
@@ -389,7 +418,9 @@ sf_status sf_study_system_multiply(sf_study* study, const double* x, double* y);
  * - count at most 8; a larger count is refused with SF_INVALID_ARGUMENT before any work. count 0
  *   does nothing. x, y and energy: 8-byte-aligned device (or managed) memory of the study's
  *   device, not overlapping; x and y hold count * free_dofs doubles, energy count doubles, each
- *   range inside one allocation (a range that runs past the end of its allocation is refused).
+ *   range inside one allocation (a range that runs past the end of its allocation is refused;
+ *   the driver sees allocations only, so a sub-allocator's piece is checked against the whole
+ *   allocation it was carved from).
  * - The calling thread's current device is the same after the call as before it.
  * - Asynchronous: the kernel is enqueued on the study's stream (sf_study_stream); read y and
  *   energy after that stream has reached it.

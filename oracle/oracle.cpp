@@ -13,6 +13,7 @@
 
 #include <algorithm>
 #include <array>
+#include <cfloat>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -2433,6 +2434,246 @@ void orc_precondition(orc_study* s, const double* r, double* z) { s->pcg.precond
 void orc_system_multiply(orc_study* s, const double* x, double* y) { s->pcg.system_multiply(x, y); }
 double orc_multiply_rounding_bound(const orc_study* s, const double* x) {
   return s->matrix.multiply_rounding_bound(x);
+}
+
+// ---------------------------------------------------------------------------------------------
+// Stages of one level of the V-cycle in the study's precision, with the per-entry rounding bounds
+// the reference's device tests assert against (crates/solidfem-solve/src/gpu/reference.rs:256-355;
+// tests/solver/gpu_cycle_execution.rs:253-267): a device stage and this one each lie within the
+// bound of the exact value of the same rounded inputs, so they differ by at most twice the bound.
+// Inputs arrive in f64 and are rounded to the cycle's vector type; outputs are widened to f64.
+// ---------------------------------------------------------------------------------------------
+}  // extern "C"
+
+namespace {
+
+// |M| |v| for a block matrix, in f64.
+template <class S>
+vector<double> abs_product(const BlockCsr<S>& m, const vector<double>& v) {
+  const size_t rb = m.row_block, cb = m.col_block;
+  vector<double> out(m.rows * rb, 0.0);
+  for (size_t row = 0; row < m.rows; ++row)
+    for (size_t at = m.starts[row]; at < m.starts[row + 1]; ++at) {
+      const S* b = m.block(at);
+      const size_t col = (size_t)m.columns[at] * cb;
+      for (size_t p = 0; p < rb; ++p)
+        for (size_t q = 0; q < cb; ++q) out[row * rb + p] += std::fabs((double)b[p * cb + q]) * std::fabs(v[col + q]);
+    }
+  return out;
+}
+
+// reference.rs:256-274: terms * unit * sum |a_ij x_j| per scalar row.
+template <class S>
+vector<double> multiply_bound(const BlockCsr<S>& m, const vector<double>& x, double unit) {
+  vector<double> out = abs_product(m, x);
+  for (size_t row = 0; row < m.rows; ++row) {
+    const double terms = (double)(m.starts[row + 1] - m.starts[row]) * (double)m.col_block;
+    for (size_t p = 0; p < m.row_block; ++p) out[row * m.row_block + p] *= terms * unit;
+  }
+  return out;
+}
+
+// The transpose of a block matrix (the stored restriction), values widened to f64.
+template <class S>
+BlockCsr<double> transpose(const BlockCsr<S>& m, size_t out_rows) {
+  BlockCsr<double> t;
+  t.rows = out_rows;
+  t.row_block = m.col_block;
+  t.col_block = m.row_block;
+  t.starts.assign(out_rows + 1, 0);
+  for (uint32_t c : m.columns) t.starts[c + 1] += 1;
+  for (size_t i = 0; i < out_rows; ++i) t.starts[i + 1] += t.starts[i];
+  vector<size_t> at(t.starts.begin(), t.starts.end() - 1);
+  t.columns.resize(m.columns.size());
+  t.values.resize(m.values.size());
+  const size_t rb = m.row_block, cb = m.col_block;
+  for (size_t row = 0; row < m.rows; ++row)
+    for (size_t k = m.starts[row]; k < m.starts[row + 1]; ++k) {
+      const size_t slot = at[m.columns[k]]++;
+      t.columns[slot] = (uint32_t)row;
+      for (size_t p = 0; p < rb; ++p)
+        for (size_t q = 0; q < cb; ++q) t.values[slot * rb * cb + q * rb + p] = (double)m.block(k)[p * cb + q];
+    }
+  return t;
+}
+
+// y = blockdiag(d) x, f64.
+void block_apply(const vector<double>& d, size_t n, const vector<double>& x, vector<double>& y) {
+  y.assign(x.size(), 0.0);
+  for (size_t row = 0; row < x.size() / n; ++row)
+    for (size_t p = 0; p < n; ++p) {
+      double sum = 0.0;
+      for (size_t q = 0; q < n; ++q) sum += d[(row * n + p) * n + q] * x[row * n + q];
+      y[row * n + p] = sum;
+    }
+}
+
+// reference.rs:276-355: a first-order bound on |computed - exact| of the smoother from zero on
+// right-hand side b (already in the vector type), with the scalars rounded to that type; the
+// division by theta allowed 2.5 units of rounding.
+template <class S, class V>
+vector<double> smoother_bound(const SLevel<S>& lv, size_t degree, const vector<double>& b, double unit) {
+  const BlockCsr<S>& a = lv.a;
+  const size_t n = a.row_block, len = a.rows * n;
+  vector<double> diag(lv.inv.size()), abs_diag(lv.inv.size());
+  for (size_t i = 0; i < diag.size(); ++i) {
+    diag[i] = (double)lv.inv[i];
+    abs_diag[i] = std::fabs(diag[i]);
+  }
+  const double theta0 = 0.5 * (lv.lambda_max + lv.lambda_min), delta = 0.5 * (lv.lambda_max - lv.lambda_min);
+  const double sigma = theta0 / delta;
+  double rho = 1.0 / sigma;
+  const double theta = (double)(V)theta0;
+  vector<double> abs_b(len), z, abs_bb, work, abs_work, propagated;
+  for (size_t i = 0; i < len; ++i) abs_b[i] = std::fabs(b[i]);
+  block_apply(abs_diag, n, abs_b, abs_bb);
+  block_apply(diag, n, b, z);
+  vector<double> residual(b), direction(len), solution(len), error_d(len), error_r(len, 0.0);
+  for (size_t i = 0; i < len; ++i) {
+    error_d[i] = ((double)n * unit * abs_bb[i]) / std::fabs(theta) + 2.5 * unit * std::fabs(z[i] / theta);
+    direction[i] = z[i] / theta;
+    solution[i] = direction[i];
+  }
+  vector<double> error_x(error_d), terms(len);
+  for (size_t row = 0; row < a.rows; ++row)
+    for (size_t p = 0; p < n; ++p) terms[row * n + p] = (double)(a.starts[row + 1] - a.starts[row]) * (double)a.col_block;
+  vector<double> abs_direction(len), ad(len), abs_residual(len);
+  for (size_t s = 1; s < degree; ++s) {
+    const double next = 1.0 / (2.0 * sigma - rho);
+    const double c1 = (double)(V)(next * rho), c2 = (double)(V)(2.0 * next / delta);
+    rho = next;
+    for (size_t i = 0; i < len; ++i) abs_direction[i] = std::fabs(direction[i]);
+    abs_work = abs_product(a, abs_direction);
+    propagated = abs_product(a, error_d);
+    for (size_t row = 0; row < a.rows; ++row) {  // residual -= A direction, exact enough in f64
+      double out[8];
+      a.multiply_row(row, direction.data(), out);
+      for (size_t p = 0; p < n; ++p) residual[row * n + p] -= out[p];
+    }
+    for (size_t i = 0; i < len; ++i)
+      error_r[i] += terms[i] * unit * abs_work[i] + propagated[i] + unit * std::fabs(residual[i]);
+    block_apply(diag, n, residual, z);
+    for (size_t i = 0; i < len; ++i) abs_residual[i] = std::fabs(residual[i]);
+    block_apply(abs_diag, n, abs_residual, abs_work);
+    block_apply(abs_diag, n, error_r, work);
+    for (size_t i = 0; i < len; ++i) {
+      const double error_z = (double)n * unit * abs_work[i] + work[i];
+      const double d = c1 * direction[i] + c2 * z[i];
+      error_d[i] = std::fabs(c1) * error_d[i] + std::fabs(c2) * error_z +
+                   3.0 * unit * (std::fabs(c1 * direction[i]) + std::fabs(c2 * z[i]));
+      direction[i] = d;
+      solution[i] += d;
+      error_x[i] += error_d[i] + unit * std::fabs(solution[i]);
+    }
+  }
+  return error_x;
+}
+
+template <class S, class V>
+int level_stage(Cycle<S, V>& c, size_t li, int stage, const double* in0, const double* in1, double* out,
+                double* bound) {
+  if (li >= c.levels.size()) return 1;
+  SLevel<S>& lv = c.levels[li];
+  auto& w = c.work[li];
+  const size_t n = lv.a.dofs(), rb = lv.a.row_block;
+  const double unit = std::is_same<V, float>::value ? (double)FLT_EPSILON : DBL_EPSILON;
+  auto rounded = [](const double* p, size_t len) {
+    vector<V> v(len);
+    for (size_t i = 0; i < len; ++i) v[i] = (V)p[i];
+    return v;
+  };
+  auto widened = [](const vector<V>& v) { return vector<double>(v.begin(), v.end()); };
+  switch (stage) {
+    case ORC_STAGE_SMOOTH:
+    case ORC_STAGE_SMOOTH_ADD: {
+      if (lv.factor && !lv.has_p) return 1;
+      vector<V> b = rounded(in0, n), x(n);
+      c.smooth(li, b.data(), x.data());
+      vector<double> e = smoother_bound<S, V>(lv, c.degree, widened(b), unit);
+      if (stage == ORC_STAGE_SMOOTH_ADD) {
+        vector<V> base = rounded(in1, n);
+        for (size_t i = 0; i < n; ++i) {
+          x[i] = base[i] + x[i];
+          e[i] += unit * std::fabs((double)x[i]);
+        }
+      }
+      for (size_t i = 0; i < n; ++i) {
+        out[i] = (double)x[i];
+        bound[i] = e[i];
+      }
+      return 0;
+    }
+    case ORC_STAGE_START: {  // cycle.rs:591-610: d = (D^-1 b) / theta, the smoother's first x
+      vector<V> b = rounded(in0, n), z(n);
+      const V first = (V)(0.5 * (lv.lambda_max + lv.lambda_min));
+      vector<double> abs_b(n), abs_bb, zz;
+      for (size_t row = 0; row < lv.a.rows; ++row) c.apply_inverse_diagonal(lv, row, b.data(), z.data());
+      vector<double> diag(lv.inv.size());
+      for (size_t i = 0; i < diag.size(); ++i) diag[i] = std::fabs((double)lv.inv[i]);
+      for (size_t i = 0; i < n; ++i) abs_b[i] = std::fabs((double)b[i]);
+      block_apply(diag, rb, abs_b, abs_bb);
+      for (size_t i = 0; i < n; ++i) {
+        const V d = z[i] / first;
+        out[i] = (double)d;
+        bound[i] = ((double)rb * unit * abs_bb[i]) / std::fabs((double)first) + 2.5 * unit * std::fabs((double)d);
+      }
+      return 0;
+    }
+    case ORC_STAGE_RESIDUAL: {  // cycle.rs:548-564; bound as gpu_cycle_execution.rs:253-267
+      vector<V> b = rounded(in0, n), x = rounded(in1, n), r(n);
+      c.residual(li, b.data(), x.data(), r.data());
+      vector<double> xd = widened(x), e = multiply_bound(lv.a, xd, unit), ax = abs_product(lv.a, xd);
+      for (size_t i = 0; i < n; ++i) {
+        out[i] = (double)r[i];
+        bound[i] = e[i] + unit * (std::fabs((double)b[i]) + ax[i]);
+      }
+      return 0;
+    }
+    case ORC_STAGE_RESTRICT: {  // block.rs:157-172 (the reference's device restricts by the stored transpose)
+      if (!lv.has_p) return 1;
+      const size_t cn = c.levels[li + 1].a.dofs();
+      vector<V> r = rounded(in0, n), y(cn);
+      lv.p.multiply_transpose(r.data(), y.data(), cn);
+      BlockCsr<double> t = transpose(lv.p, c.levels[li + 1].a.rows);
+      vector<double> e = multiply_bound(t, widened(r), unit);
+      for (size_t i = 0; i < cn; ++i) {
+        out[i] = (double)y[i];
+        bound[i] = e[i];
+      }
+      return 0;
+    }
+    case ORC_STAGE_PROLONG: {  // cycle.rs:512-521: x += P e
+      if (!lv.has_p) return 1;
+      const size_t cn = c.levels[li + 1].a.dofs();
+      vector<V> e = rounded(in0, cn), x = rounded(in1, n), pe(rb);
+      vector<double> ed = widened(e), eb = multiply_bound(lv.p, ed, unit), ap = abs_product(lv.p, ed);
+      for (size_t row = 0; row < lv.a.rows; ++row) {
+        lv.p.multiply_row(row, e.data(), pe.data());
+        for (size_t p = 0; p < rb; ++p) {
+          const size_t i = row * rb + p;
+          out[i] = (double)(V)(x[i] + pe[p]);
+          bound[i] = eb[i] + unit * (std::fabs((double)x[i]) + ap[i]);
+        }
+      }
+      return 0;
+    }
+  }
+  (void)w;
+  return 1;
+}
+
+}  // namespace
+
+extern "C" {
+
+int orc_level_stage(orc_study* s, uint64_t level, int stage, const double* in0, const double* in1, double* out,
+                    double* bound) {
+  if (!s->use_mg) return 1;
+  switch (s->mg.precision) {
+    case ORC_PRECISION_DOUBLE: return level_stage(s->mg.dd, level, stage, in0, in1, out, bound);
+    case ORC_PRECISION_SINGLE_STORAGE: return level_stage(s->mg.fd, level, stage, in0, in1, out, bound);
+    default: return level_stage(s->mg.ff, level, stage, in0, in1, out, bound);
+  }
 }
 
 // StaticStudy::solution, study.rs:246-260: recovery of the current displacements.

@@ -108,6 +108,10 @@ typedef struct {
   double value;
 } orc_prescribed;
 
+// Stages of one V-cycle level (orc_level_stage): smoother from zero; x + smoother; the start
+// (D^-1 b) / theta; b - A x; P^T r; x + P e.
+enum { ORC_STAGE_SMOOTH = 0, ORC_STAGE_RESIDUAL = 1, ORC_STAGE_RESTRICT = 2, ORC_STAGE_PROLONG = 3,
+       ORC_STAGE_START = 4, ORC_STAGE_SMOOTH_ADD = 5 };
 typedef struct orc_mesh orc_mesh;
 typedef struct orc_study orc_study;
 

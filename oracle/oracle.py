@@ -16,6 +16,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_build", "liboracle.so")
 
 ACTIVE, CONVERGED, FAILED_NOT_PD, FAILED_NOT_CONVERGED = 0, 1, 2, 3
+STAGE_SMOOTH, STAGE_RESIDUAL, STAGE_RESTRICT, STAGE_PROLONG, STAGE_START, STAGE_SMOOTH_ADD = range(6)
 DOUBLE, SINGLE_STORAGE, SINGLE = 0, 1, 2
 JACOBI, MULTIGRID = 0, 1
 UNIFORM, SHELL_CORE = 0, 1
@@ -133,6 +134,8 @@ def lib():
         L.orc_study_point_count.restype = C.c_uint64
         L.orc_study_point_stresses.argtypes = [C.c_void_p, p(PointStress)]
         L.orc_element_stiffness.argtypes = [p(C.c_double), p(Material), C.c_int, p(C.c_double)]
+        L.orc_level_stage.argtypes = [C.c_void_p, C.c_uint64, C.c_int, p(C.c_double), p(C.c_double), p(C.c_double),
+                                      p(C.c_double)]
         _lib = L
     return _lib
 
@@ -332,6 +335,18 @@ class Study:
         y = np.empty_like(x)
         lib().orc_system_multiply(self.h, _ptr(x, C.c_double), _ptr(y, C.c_double))
         return y
+
+    def level_stage(self, level, stage, in0, in1=None, out_len=None):
+        """One stage of a level's V-cycle in the study's precision and its per-entry rounding bound
+        (gpu/reference.rs:256-355): returns (out, bound)."""
+        a = np.ascontiguousarray(in0, dtype=np.float64)
+        b = np.ascontiguousarray(in1 if in1 is not None else np.zeros(1), dtype=np.float64)
+        n = out_len or len(a)
+        out, bound = np.empty(n), np.empty(n)
+        if lib().orc_level_stage(self.h, level, stage, _ptr(a, C.c_double), _ptr(b, C.c_double),
+                                 _ptr(out, C.c_double), _ptr(bound, C.c_double)):
+            raise ValueError(f"stage {stage} does not apply to level {level}")
+        return out, bound
 
     def recover(self):
         code = lib().orc_study_recover(self.h)

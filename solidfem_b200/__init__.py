@@ -103,6 +103,18 @@ class _KernelTiming(C.Structure):
     _fields_ = [("ms_per_launch", C.c_double), ("bytes_per_launch", C.c_double), ("launches", C.c_uint64)]
 
 
+class Stage(enum.IntEnum):
+    """Stages of one level of the device V-cycle (SF_STAGE_*)."""
+    SMOOTH = 0
+    RESIDUAL = 1
+    RESTRICT = 2
+    PROLONG = 3
+    START = 4
+    SMOOTH_ADD = 5
+    RESTRICT_START = 6
+    RESIDUAL_START = 7
+
+
 class Kernel(enum.IntEnum):
     """Solver kernels that can be timed in isolation (SF_KERNEL_*)."""
     CHEBYSHEV_STEP = 0
@@ -185,6 +197,8 @@ SIGNATURES = {
     "sf_study_aggregates": (C.c_int, [_V, C.c_uint64, _P(C.c_uint32)]),
     "sf_study_precondition": (C.c_int, [_V, _P(C.c_double), _P(C.c_double)]),
     "sf_study_system_multiply": (C.c_int, [_V, _P(C.c_double), _P(C.c_double)]),
+    "sf_study_level_stage": (C.c_int, [_V, C.c_uint64, C.c_int32, _P(C.c_double), _P(C.c_double), _P(C.c_double),
+                                       _P(C.c_double)]),
     "sf_study_energy_products": (C.c_int, [_V, _V, _V, _V, C.c_uint64]),
     "sf_study_solve_batch": (C.c_int, [_P(_V), C.c_uint64, _P(_StepOutcome), _P(C.c_int)]),
     "sf_server_options_default": (None, [_P(_ServerOptions)]),
@@ -740,6 +754,20 @@ class StaticStudy:
         _check(library().sf_study_precondition(self._h, _dptr(r), _dptr(z)))
         return z
 
+    def level_stage(self, level: int, stage: "Stage", in0, in1=None, out_len: Optional[int] = None):
+        """One stage of a level's device V-cycle (sf_study_level_stage): returns out0, or (out0, out1)
+        for the fused-start stages. out_len is the output length (the coarser level's for the
+        restrictions)."""
+        a = np.ascontiguousarray(in0, dtype=np.float64)
+        b = None if in1 is None else np.ascontiguousarray(in1, dtype=np.float64)
+        n = out_len or len(a)
+        o0, o1 = np.empty(n), np.empty(n)
+        _check(library().sf_study_level_stage(self._h, level, int(stage), _dptr(a), None if b is None else _dptr(b),
+                                              _dptr(o0), _dptr(o1)))
+        if stage in (Stage.RESTRICT_START, Stage.RESIDUAL_START):
+            return o0, o1
+        return o0
+
     def system_multiply(self, x: np.ndarray) -> np.ndarray:
         x = np.ascontiguousarray(x, dtype=np.float64)
         y = np.empty_like(x)
@@ -992,5 +1020,5 @@ __all__ = [
     "FACE_DTYPE", "BoundaryFace", "Mesh", "box_tet_mesh", "Material", "ShellCore", "Quadrature", "Model", "Precision",
     "PcgOptions", "MultigridOptions", "Jacobi", "StudyOptions", "StudyBuilder", "StaticStudy", "StepOutcome",
     "Outcome", "Progress", "BuildProgress", "PointStress", "SolidfemError", "Status", "library", "SIGNATURES", "Kernel", "Solution",
-    "solve_batch", "Server", "ServerOptions", "RequestResult", "System", "Recovery", "RecoveredField",
+    "solve_batch", "Server", "ServerOptions", "RequestResult", "System", "Recovery", "RecoveredField", "Stage",
 ]

@@ -313,6 +313,9 @@ sf_status solver_init_pcg(DeviceSolver& s, double tolerance, uint64_t max_iterat
 sf_status solver_enqueue_iteration(DeviceSolver& s);
 // Enqueues z = M r for the current r (reset_direction, pcg.rs:278-282) and rz.
 sf_status solver_enqueue_reset(DeviceSolver& s);
+// One stage of a level's V-cycle (SF_STAGE_*) on f64 device buffers (inspection entry point).
+sf_status solver_level_stage(DeviceSolver& s, size_t level, int stage, const double* in0, const double* in1,
+                             double* out0, double* out1);
 // One standalone preconditioner application / system product (inspection entry points).
 sf_status solver_precondition(DeviceSolver& s, const double* d_in, double* d_out);
 sf_status solver_system_multiply(DeviceSolver& s, const double* d_in, double* d_out);

@@ -3145,6 +3145,107 @@ sf_status solver_time_kernel(DeviceSolver& s, int kernel, uint64_t repeats, doub
   return time_level0<float, float>(s, kernel, repeats, ms, bytes);
 }
 
+namespace {
+
+// One stage of level li's V-cycle on the level's own buffers, through the launches the cycle
+// makes (same layouts, same fused epilogues): inputs in f64 device memory are rounded to the
+// vector type first, outputs widened to f64. The stages and their buffers:
+//   SMOOTH          b -> L.b;  smoother from zero into L.x
+//   SMOOTH_ADD      b -> L.b, x -> L.tmp;  L.tmp += smoother (the post-smoother's last step)
+//   START           b -> L.b;  the start kernel: L.x = (D^-1 b) / theta
+//   RESIDUAL        b -> L.b, x -> L.x;  L.res = b - A x
+//   RESTRICT        r -> L.res;  C.b = R r
+//   PROLONG         e -> C.x, x -> L.x;  L.x += P e
+//   RESTRICT_START  r -> L.res;  C.b = R r with the coarser level's start fused in (C.x)
+//   RESIDUAL_START  b -> L.b, x -> L.x;  L.res = b - A x with the start fused in (L.post_x)
+template <typename S, typename V>
+sf_status level_stage(DeviceSolver& s, size_t li, int stage, const double* in0, const double* in1, double* out0,
+                      double* out1) {
+  DevLevel& L = s.levels[li];
+  const bool coarse = li + 1 < s.levels.size();
+  DevLevel* C = coarse ? &s.levels[li + 1] : nullptr;
+  cudaStream_t st = s.stream;
+  const int* on = s.always_active;
+  auto to_v = [&](const double* src, void* dst, uint32_t n) {
+    launch_body<convert_kernel<double, V>>(grid_for_elems(n), kThreads, 0, st, n, src, (V*)dst, on);
+  };
+  auto from_v = [&](const void* src, double* dst, uint32_t n) {
+    launch_body<convert_kernel<V, double>>(grid_for_elems(n), kThreads, 0, st, n, (const V*)src, dst, on);
+  };
+  const bool smoothed = L.has_p || !L.has_factor;
+  switch (stage) {
+    case SF_STAGE_SMOOTH:
+    case SF_STAGE_SMOOTH_ADD:
+    case SF_STAGE_START:
+      if (!smoothed) return fail(SF_INVALID_ARGUMENT, "the coarsest level is factored, not smoothed");
+      to_v(in0, L.b, L.n);
+      if (stage == SF_STAGE_START) {
+        if (L.a.rb == 3)
+          launch_cheb_start<S, V, V, 3>(L, (const V*)L.b, nullptr, (V*)L.res, (V*)L.d0, (V*)L.x, L.theta, on, st);
+        else
+          launch_cheb_start<S, V, V, 6>(L, (const V*)L.b, nullptr, (V*)L.res, (V*)L.d0, (V*)L.x, L.theta, on, st);
+        from_v(L.x, out0, L.n);
+      } else if (stage == SF_STAGE_SMOOTH) {
+        enqueue_smooth<S, V, V>(s, L, (const V*)L.b, nullptr, (V*)L.x, nullptr, on);
+        from_v(L.x, out0, L.n);
+      } else {
+        to_v(in1, L.tmp, L.n);
+        enqueue_smooth<S, V, V>(s, L, (const V*)L.b, nullptr, (V*)L.post_x, (V*)L.tmp, on);
+        from_v(L.tmp, out0, L.n);
+      }
+      break;
+    case SF_STAGE_RESIDUAL:
+    case SF_STAGE_RESIDUAL_START:
+      to_v(in0, L.b, L.n);
+      to_v(in1, L.x, L.n);
+      if (stage == SF_STAGE_RESIDUAL) {
+        bsr_dispatch<S, V, OP_RESIDUAL>(L.a, (const V*)L.x, (V*)L.res, (const V*)L.b, on, st);
+      } else {
+        if (!smoothed) return fail(SF_INVALID_ARGUMENT, "the coarsest level is factored, not smoothed");
+        launch_start_product<S, V, OP_RESIDUAL>(L.a, (const V*)L.x, (const V*)L.b,
+                                                start_args<S, V>(L, (V*)nullptr, (V*)L.post_x), on, st);
+        from_v(L.post_x, out1, L.n);
+      }
+      from_v(L.res, out0, L.n);
+      break;
+    case SF_STAGE_RESTRICT:
+    case SF_STAGE_RESTRICT_START:
+      if (!L.has_p) return fail(SF_INVALID_ARGUMENT, "the level has no coarser level");
+      to_v(in0, L.res, L.n);
+      if (stage == SF_STAGE_RESTRICT) {
+        bsr_dispatch<S, V, OP_SET>(L.r, (const V*)L.res, (V*)C->b, nullptr, on, st);
+      } else {
+        if (!C->has_p && C->has_factor) return fail(SF_INVALID_ARGUMENT, "the coarser level is factored, not smoothed");
+        launch_start_product<S, V, OP_SET>(L.r, (const V*)L.res, (const V*)nullptr,
+                                           start_args<S, V>(*C, (V*)C->b, (V*)C->x), on, st);
+        from_v(C->x, out1, C->n);
+      }
+      from_v(C->b, out0, C->n);
+      break;
+    case SF_STAGE_PROLONG:
+      if (!L.has_p) return fail(SF_INVALID_ARGUMENT, "the level has no coarser level");
+      to_v(in0, C->x, C->n);
+      to_v(in1, L.x, L.n);
+      bsr_dispatch<S, V, OP_ADD>(L.p, (const V*)C->x, (V*)L.x, nullptr, on, st);
+      from_v(L.x, out0, L.n);
+      break;
+    default:
+      return fail(SF_INVALID_ARGUMENT, "unknown stage");
+  }
+  s.launches += 4;
+  return cuda_check(cudaStreamSynchronize(st), "level stage");
+}
+
+}  // namespace
+
+sf_status solver_level_stage(DeviceSolver& s, size_t level, int stage, const double* in0, const double* in1,
+                             double* out0, double* out1) {
+  if (!s.multigrid || level >= s.levels.size()) return fail(SF_INVALID_ARGUMENT, "no such multigrid level");
+  if (!s.storage_single) return level_stage<double, double>(s, level, stage, in0, in1, out0, out1);
+  if (!s.vector_single) return level_stage<float, double>(s, level, stage, in0, in1, out0, out1);
+  return level_stage<float, float>(s, level, stage, in0, in1, out0, out1);
+}
+
 sf_status solver_precondition(DeviceSolver& s, const double* d_in, double* d_out) {
   enqueue_precondition(s, d_in, d_out, s.z32, s.always_active);
   if (s.vector_single && s.multigrid)

@@ -388,9 +388,12 @@ struct sf_study {
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   RecoveryDevice rec;              // the incidence tables every recovery of this study reads
   sf_recovery* answer = nullptr;   // the finished recovery of the converged displacements
+  vector<sf_recovery*> recoveries; // every live recovery of this study, `answer` included
   void release_answer();
+  void orphan_recoveries();
   ~sf_study() {
     release_answer();
+    orphan_recoveries();
     pinned_release(pinned);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
@@ -417,6 +420,16 @@ static void recovery_free(sf_recovery* r);  // defined with the recovery entry p
 void sf_study::release_answer() {
   if (answer) recovery_free(answer);
   answer = nullptr;
+}
+
+// The study goes first: its recoveries keep their handles (which the caller still destroys) but
+// lose their device memory, which goes with the study's own.
+void sf_study::orphan_recoveries() {
+  for (sf_recovery* r : recoveries) {
+    r->study = nullptr;
+    r->owned.clear();
+  }
+  recoveries.clear();
 }
 
 static void release_builder_device(sf_builder* b) {
@@ -1456,10 +1469,13 @@ static sf_status recovery_tables(sf_study* s) {
 
 static void recovery_free(sf_recovery* r) {
   if (!r) return;
-  DeviceSolver& d = r->study->solver;
-  cudaSetDevice(d.device);
-  cudaStreamSynchronize(d.stream);
-  for (void* p : r->owned) dev_free(d, p);
+  if (sf_study* s = r->study) {
+    DeviceSolver& d = s->solver;
+    cudaSetDevice(d.device);
+    cudaStreamSynchronize(d.stream);
+    for (void* p : r->owned) dev_free(d, p);
+    s->recoveries.erase(std::remove(s->recoveries.begin(), s->recoveries.end(), r), s->recoveries.end());
+  }
   delete r;
 }
 
@@ -1515,6 +1531,7 @@ static sf_status recovery_begin(sf_study* s, sf_recovery** out) {
     dev_free(d, d_val);
   }
   d.launches += 1;
+  s->recoveries.push_back(rec.get());
   if (e) {
     recovery_free(rec.release());
     return e;
@@ -1741,6 +1758,41 @@ sf_status sf_study_precondition(sf_study* s, const double* residual, double* out
   }
   cudaFree(din);
   cudaFree(dout);
+  return e;
+}
+
+sf_status sf_study_level_stage(sf_study* s, uint64_t level, int32_t stage, const double* in0, const double* in1,
+                               double* out0, double* out1) {
+  if (!s || !in0 || !out0) return fail(SF_INVALID_ARGUMENT, "null argument");
+  DeviceSolver& d = s->solver;
+  if (!d.multigrid || level >= d.levels.size()) return fail(SF_INVALID_ARGUMENT, "no such multigrid level");
+  const bool two_in = stage == SF_STAGE_SMOOTH_ADD || stage == SF_STAGE_RESIDUAL || stage == SF_STAGE_PROLONG ||
+                      stage == SF_STAGE_RESIDUAL_START;
+  const bool two_out = stage == SF_STAGE_RESTRICT_START || stage == SF_STAGE_RESIDUAL_START;
+  if ((two_in && !in1) || (two_out && !out1)) return fail(SF_INVALID_ARGUMENT, "null argument");
+  const bool has_coarse = level + 1 < d.levels.size();
+  const size_t n = d.levels[level].n, cn = has_coarse ? d.levels[level + 1].n : 0;
+  // lengths: the coarse level's for the prolongation's e and the restrictions' outputs
+  const size_t n_in0 = stage == SF_STAGE_PROLONG ? cn : n;
+  const size_t n_out = stage == SF_STAGE_RESTRICT || stage == SF_STAGE_RESTRICT_START ? cn : n;
+  if ((n_in0 == 0 || n_out == 0)) return fail(SF_INVALID_ARGUMENT, "the level has no coarser level");
+  cudaSetDevice(d.device);
+  double *di0 = nullptr, *di1 = nullptr, *do0 = nullptr, *do1 = nullptr;
+  sf_status e = dev_alloc(d, (void**)&di0, n_in0 * 8);
+  if (!e) e = dev_alloc(d, (void**)&di1, n * 8);
+  if (!e) e = dev_alloc(d, (void**)&do0, n_out * 8);
+  if (!e) e = dev_alloc(d, (void**)&do1, n_out * 8);
+  if (!e) {
+    copy_h2d(d, di0, in0, n_in0 * 8);
+    if (two_in) copy_h2d(d, di1, in1, n * 8);
+    e = solver_level_stage(d, level, stage, di0, di1, do0, do1);
+  }
+  if (!e) {
+    copy_d2h(d, out0, do0, n_out * 8);
+    if (two_out) copy_d2h(d, out1, do1, n_out * 8);
+    e = cuda_check(cudaStreamSynchronize(d.stream), "level stage");
+  }
+  for (double* p : {di0, di1, do0, do1}) dev_free(d, p);
   return e;
 }
 

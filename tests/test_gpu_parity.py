@@ -159,3 +159,28 @@ def test_jacobi_tension_bar_is_exact():
     tip = np.abs(nodes[:, 0] - length) < 1e-9
     expected = force * length / E
     assert abs(d[tip, 0].mean() - expected) / expected < 1e-5
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_fourteen_point_assembly_and_recovery_are_bit_exact(oracle, name):
+    """The 14-point rule (quadrature.rs:53-161) through device assembly and recovery, to the bit
+    against the oracle; on these straight-sided elements it also agrees with the 4-point rule to
+    rounding (the integrand is quadratic: element/rigid_body.rs:129-139)."""
+    size, div, E, nu = CASES[name]
+    mesh, model = product_model(size, div, E, nu)
+    model.set_quadrature(sf.Quadrature.FOURTEEN_POINT)
+    study = sf.StaticStudy.new(model, mg_options(sf.Precision.DOUBLE))
+    ref = oracle_study(oracle, size, div, E, nu, oracle.default_options(tolerance=1e-9, coarse_dofs=100,
+                                                                        precision=oracle.DOUBLE, quadrature=1))
+    _, _, vals = study.matrix()
+    _, _, ovals = ref.matrix()
+    assert np.array_equal(vals.view(np.uint64), ovals.view(np.uint64))
+    _, four = product_model(size, div, E, nu)
+    _, _, vals4 = sf.StaticStudy.new(four, mg_options(sf.Precision.DOUBLE)).matrix()
+    assert np.abs(vals - vals4).max() < 1e-12 * np.abs(vals4).max()
+    assert study.solve().kind == sf.Outcome.CONVERGED
+    sol = study.solution()
+    assert len(sol.point_stresses) == 14 * mesh.tet_count()
+    s6, vm = ref.recover_with(sol.displacements)
+    assert np.array_equal(sol.nodal_stress.view(np.uint64), s6.view(np.uint64))
+    assert np.array_equal(sol.nodal_von_mises.view(np.uint64), vm.view(np.uint64))

@@ -147,3 +147,17 @@ def test_solution_can_be_cancelled():
     assert err.value.status == sf.Status.CANCELLED
     sol = study.solution()  # nothing was kept from the cancelled call
     assert np.all(np.isfinite(sol.nodal_von_mises))
+
+
+def test_a_recovery_outliving_its_study_can_still_be_destroyed():
+    """Destroying the study first (as a garbage collector may) leaves the recovery handle valid for
+    sf_recovery_destroy only."""
+    _, model = product_model((10.0, 1.0, 1.0), (12, 3, 3), 200000.0, 0.3)
+    study = sf.StaticStudy.new(model, mg_options(sf.Precision.DOUBLE))
+    assert study.solve().kind == sf.Outcome.CONVERGED
+    rec = study.begin_recovery()
+    lib = sf.library()
+    lib.sf_study_destroy(study._h)  # the study goes first
+    study._h = None
+    lib.sf_recovery_destroy(rec._h)
+    rec._h = None

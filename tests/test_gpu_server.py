@@ -15,10 +15,11 @@ pytestmark = pytest.mark.gpu
 
 TOL = 1e-8
 BATCH_MAX_DOFS = 30_000
-# A request alone and in the mix runs the same arithmetic per row; the mix only changes which
-# rows share a thread block in the batched grids, which reorders the partial sums of the dot
-# products (about 1e-16 relative each).
-MIX_BAR = 1e-9
+# A request alone and in the mix runs the same arithmetic per row, and every reduction has a fixed
+# grid per study, so the answers come out with the same bits (measured); the bar leaves room only
+# for a batch whose members' thread blocks differ in shape, which would regroup the partial sums
+# of a dot product (about 1e-16 relative each).
+MIX_BAR = 1e-12
 
 
 def options(batchable=False):

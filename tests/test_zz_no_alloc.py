@@ -85,18 +85,26 @@ def test_energy_products_refusals():
 
 
 def test_energy_products_refuse_a_short_buffer_and_keep_the_current_device():
+    """A range must lie inside one device allocation. The driver knows allocations, not a
+    sub-allocator's pieces of them (torch's caching allocator carves tensors out of larger
+    allocations), so the short buffer here is its own cudaMalloc, one entry short of two vectors."""
     import torch
+    from cuda.bindings import runtime as rt
 
     study = make_study(False)
     n = study.report()["free_dofs"]
     x = torch.zeros((2, n), dtype=torch.float64, device="cuda:0")
-    short = torch.zeros(2 * n - 1, dtype=torch.float64, device="cuda:0")  # one entry short of two vectors
     e = torch.zeros(2, dtype=torch.float64, device="cuda:0")
     torch.cuda.synchronize()
     before = torch.cuda.current_device()
-    with pytest.raises(sf.SolidfemError) as err:
-        study.energy_products(x.data_ptr(), short.data_ptr(), e.data_ptr(), 2)
-    assert err.value.status == sf.Status.INVALID_ARGUMENT
+    err_code, short = rt.cudaMalloc((2 * n - 1) * 8)
+    assert err_code == rt.cudaError_t.cudaSuccess
+    try:
+        with pytest.raises(sf.SolidfemError) as err:
+            study.energy_products(x.data_ptr(), int(short), e.data_ptr(), 2)
+        assert err.value.status == sf.Status.INVALID_ARGUMENT
+    finally:
+        rt.cudaFree(short)
     with pytest.raises(sf.SolidfemError) as err:
         study.energy_products(x.data_ptr(), x[1].data_ptr(), e.data_ptr(), 1)  # overlapping x and y
     assert err.value.status == sf.Status.INVALID_ARGUMENT
