@@ -214,6 +214,21 @@ sf_status setup_gather_blocks(cudaStream_t st, size_t count, int len, const uint
 sf_status setup_scatter_blocks(cudaStream_t st, size_t count, int len, const uint32_t* idx, const double* in,
                                double* out);
 sf_status setup_set_values(cudaStream_t st, size_t count, const uint32_t* idx, const double* vals, double* out);
+// The free nodes' rigid-body modes (rows x 3 x 6) about `center`, scaled (rigid_modes.rs:36-83);
+// row_node maps each free block row to its mesh node, nodes are the mesh's positions.
+sf_status setup_rigid_modes(cudaStream_t st, uint32_t rows, const uint32_t* row_node, const double* nodes,
+                            const double center[3], double scale, double* modes);
+// The coarsest level's dense Cholesky factor (in `work`, n x n) and explicit inverse L^-T L^-1 (in
+// `inverse`), bit-identical to DenseCholesky's column loop (block.rs:307-374) and the host's
+// inverse; `li` is n x n scratch. A non-positive pivot stops the factor: its column goes to *bad
+// (which must hold ~0 before) and its value to *pivot; the inverse is then not meaningful.
+sf_status setup_dense_inverse(cudaStream_t st, uint32_t rows, int rb, const uint32_t* starts, const uint32_t* cols,
+                              const double* vals, size_t n, double* work, double* li, double* inverse,
+                              unsigned long long* bad, double* pivot);
+// The tentative prolongator of every aggregate into t (rows x rb x 6 at the members' rows) and the
+// coarse near-null space (aggregates x 36), bit-identical to the host loops (transfer.rs:19-68).
+sf_status setup_tentative(cudaStream_t st, size_t aggregates, int rb, const uint32_t* member_starts,
+                          const uint32_t* members, const double* near_null, double* t, double* coarse);
 sf_status setup_smooth(cudaStream_t st, int rb, size_t entries, const uint32_t* entry_row, const uint32_t* p_cols,
                        const uint32_t* a_starts, const uint32_t* a_cols, const double* a_vals, const uint32_t* n_starts,
                        const uint32_t* n_cols, const uint32_t* aggregate, const double* t_vals, const double* inv,

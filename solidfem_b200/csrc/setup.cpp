@@ -4,10 +4,11 @@
 // reference's aggregates and coarse matrices to the bit.
 //
 // The split: order-dependent graph work (strong neighbours, the greedy aggregation passes, the
-// per-aggregate Gram-Schmidt of the near-null modes, the smoothing filter) and every sparsity
-// pattern (P, A P, the coarse matrix, P's transpose) are built here on the host; every value of
-// every level (inverse diagonal, block norms, lambda_max, P, A P, P^T A P) is computed on the
-// device in FP64 (setup_device.cu) and stays there. Row-local host work runs on `threads` threads
+// smoothing filter) and the sparsity patterns P, A P, the coarse matrix and P's transpose are
+// built here on the host (the union patterns on the device where they fit); every value of every
+// level (inverse diagonal, block norms, lambda_max, the per-aggregate Gram-Schmidt of the
+// near-null modes, P, A P, P^T A P) is computed on the device in FP64 (setup_device.cu) and stays
+// there. Row-local host work runs on `threads` threads
 // in contiguous row chunks stitched back in row order, so the thread count never changes a bit.
 // Setup advances in whole phases; the budget counts block rows like the reference's
 // (setup.rs:191-222).
@@ -119,7 +120,8 @@ struct SetupMachine {
   SetupOptions opt;
   Phase phase = DIAGONAL;
   Bsr current;  // host pattern, device values
-  vector<double> near_null;
+  vector<double> near_null;        // the finest level's modes, on the host until uploaded
+  double* d_near_null = nullptr;    // this level's near-null modes on the device, rows x rb x 6
   vector<P3> positions;
   vector<HostLevel> levels;
   // per-level state
@@ -134,17 +136,18 @@ struct SetupMachine {
   size_t aggregates = 0;
   vector<uint32_t> member_starts, members;
   vector<P3> coarse_positions;
-  double* tentative = nullptr;  // rows x rb x 6, a pooled pinned buffer (uploaded for smoothing)
-  vector<double> coarse_null;
+  double* d_tentative = nullptr;    // T on the device, rows x rb x 6 (read by the smoothing)
+  double* d_coarse_null = nullptr;  // the next level's near-null modes, aggregates x 36
   double lambda_max = 0;
   vector<uint32_t> filter_starts, filter_cols;
   Bsr prolongator, ap, coarse;
   sf_status failure = SF_OK;
   bool cancelled = false;
   // The power iteration needs only the level operator and D^-1, so it runs on a helper thread
-  // from the end of the diagonal phase while this thread builds the strength graph, the aggregates
-  // and the tentative prolongator (host work that touches neither the device nor these buffers);
-  // the spectral phase takes its result. Declared last, so it is waited for first.
+  // from the end of the diagonal phase while this thread builds the strength graph and the
+  // aggregates (host work that touches neither the device nor these buffers); the tentative phase
+  // waits for it before its own device work, the spectral phase takes its result. Declared last,
+  // so it is waited for first.
   double *power_v = nullptr, *power_s = nullptr;
   std::future<std::pair<sf_status, double>> power;
 
@@ -152,7 +155,6 @@ struct SetupMachine {
   ~SetupMachine() {
     if (power.valid()) power.wait();
     pinned_return(norms);
-    pinned_return(tentative);
   }
 
   size_t level_index() const { return levels.size(); }
@@ -269,27 +271,35 @@ struct SetupMachine {
     // One distance per entry: the row's distances are kept while its closest one is found, and
     // each entry's verdict is marked for the fill pass.
     vector<unsigned char> strong(current.cols.size());
-    rows_parallel(rows, opt.threads, [&](size_t row) {
-      thread_local vector<double> dist;
-      const uint32_t a0 = current.starts[row], a1 = current.starts[row + 1];
-      dist.resize(a1 - a0);
-      double c = std::numeric_limits<double>::max();
-      for (uint32_t at = a0; at < a1; ++at) {
-        uint32_t col = current.cols[at];
-        if (col != row) {
-          dist[at - a0] = squared_distance(positions, row, col);
-          c = std::min(c, dist[at - a0]);
+    chunked(rows, opt.threads, [&](int, size_t r0, size_t r1) {
+      vector<double> dist;  // this chunk's rows' distances, one row at a time
+      const uint32_t* cols = current.cols.data();
+      const P3* pos = positions.data();
+      for (size_t row = r0; row < r1; ++row) {
+        const uint32_t a0 = current.starts[row], a1 = current.starts[row + 1];
+        if (dist.size() < a1 - a0) dist.resize(a1 - a0);
+        double* d = dist.data();
+        double c = std::numeric_limits<double>::max();
+        const P3& p = pos[row];
+        for (uint32_t at = a0; at < a1; ++at) {
+          const uint32_t col = cols[at];
+          if (col != row) {
+            const P3& q = pos[col];
+            const double dx = q[0] - p[0], dy = q[1] - p[1], dz = q[2] - p[2];
+            d[at - a0] = dx * dx + dy * dy + dz * dz;  // squared_distance, term for term
+            c = std::min(c, d[at - a0]);
+          }
         }
+        closest[row] = c;
+        const double limit = limit_scale * c;
+        uint32_t n = 0;
+        for (uint32_t at = a0; at < a1; ++at) {
+          const bool s = cols[at] != row && d[at - a0] <= limit;
+          strong[at] = s;
+          n += s;
+        }
+        counts[row] = n;
       }
-      closest[row] = c;
-      double limit = limit_scale * c;
-      uint32_t n = 0;
-      for (uint32_t at = a0; at < a1; ++at) {
-        const bool s = current.cols[at] != row && dist[at - a0] <= limit;
-        strong[at] = s;
-        n += s;
-      }
-      counts[row] = n;
     });
     strong_starts.assign(rows + 1, 0);
     for (size_t r = 0; r < rows; ++r) strong_starts[r + 1] = strong_starts[r] + counts[r];
@@ -380,49 +390,29 @@ struct SetupMachine {
   }
 
   // Tentative prolongator by two-pass Gram-Schmidt per aggregate (transfer.rs:19-68).
+  // setup.rs:327-386 on the device (setup_tentative: one thread per aggregate, the host loops'
+  // order and bits). The power iteration shares the stream and the solver's counters, so it is
+  // waited for first; it started at the end of the diagonal phase and has normally finished while
+  // the strength graph and the aggregates were built.
   sf_status run_tentative() {
-    size_t rb = current.rb, rows = current.rows, block = rb * MODES;
-    // Every row belongs to one aggregate, which writes its whole block row: no fill needed.
-    pinned_return(tentative);
-    tentative = (double*)pinned_acquire(rows * block * 8);
-    if (!tentative) return fail(SF_CUDA_ERROR, "cudaMallocHost failed");
-    coarse_null.assign(aggregates * 36, 0.0);
-    rows_parallel(aggregates, opt.threads, [&](size_t a) {
-      size_t count = member_starts[a + 1] - member_starts[a];
-      const uint32_t* mem = members.data() + member_starts[a];
-      size_t lrows = count * rb;
-      vector<double> local(lrows * MODES);
-      for (size_t m = 0; m < count; ++m)
-        for (size_t p = 0; p < rb; ++p)
-          for (size_t k = 0; k < MODES; ++k)
-            local[(m * rb + p) * MODES + k] = near_null[((size_t)mem[m] * rb + p) * MODES + k];
-      double* coarse = coarse_null.data() + a * 36;
-      auto column_norm = [&](size_t c) {
-        double s = 0.0;
-        for (size_t r = 0; r < lrows; ++r) s += local[r * MODES + c] * local[r * MODES + c];
-        return std::sqrt(s);
-      };
-      for (size_t c = 0; c < MODES; ++c) {
-        double original = column_norm(c);
-        for (int pass = 0; pass < 2; ++pass)
-          for (size_t prev = 0; prev < c; ++prev) {
-            double proj = 0.0;
-            for (size_t r = 0; r < lrows; ++r) proj += local[r * MODES + prev] * local[r * MODES + c];
-            coarse[prev * MODES + c] += proj;
-            for (size_t r = 0; r < lrows; ++r) local[r * MODES + c] -= proj * local[r * MODES + prev];
-          }
-        double rem = column_norm(c);
-        if (original == 0.0 || rem <= RANK_TOLERANCE * original) {
-          for (size_t r = 0; r < lrows; ++r) local[r * MODES + c] = 0.0;
-          coarse[c * MODES + c] = 0.0;
-        } else {
-          for (size_t r = 0; r < lrows; ++r) local[r * MODES + c] /= rem;
-          coarse[c * MODES + c] = rem;
-        }
-      }
-      for (size_t m = 0; m < count; ++m)
-        std::copy(local.begin() + m * block, local.begin() + (m + 1) * block, tentative + (size_t)mem[m] * block);
-    });
+    const size_t rb = current.rb, rows = current.rows;
+    if (power.valid()) power.wait();
+    uint32_t *d_starts = nullptr, *d_members = nullptr;
+    sf_status e = SF_OK;
+    if (!d_near_null) {  // the finest level's modes come from the host
+      e = upload(near_null, &d_near_null);
+      vector<double>().swap(near_null);
+    }
+    if (!e) e = upload(member_starts, &d_starts);
+    if (!e) e = upload(members, &d_members);
+    if (!e) e = dev_alloc(dev, (void**)&d_tentative, std::max<size_t>(1, rows * rb * MODES) * 8);
+    if (!e) e = dev_alloc(dev, (void**)&d_coarse_null, std::max<size_t>(1, aggregates) * 36 * 8);
+    if (!e) e = setup_tentative(dev.stream, aggregates, (int)rb, d_starts, d_members, d_near_null, d_tentative,
+                                d_coarse_null);
+    // stream-ordered frees: after the kernel that reads them
+    for (void* p : {(void*)d_starts, (void*)d_members, (void*)d_near_null}) dev_free(dev, p);
+    d_near_null = nullptr;
+    if (e) return e;
     phase = SPECTRAL;
     return SF_OK;
   }
@@ -546,7 +536,6 @@ struct SetupMachine {
     prolongator.rb = rb;
     prolongator.cb = MODES;
     uint32_t *n_starts = nullptr, *n_cols = nullptr, *agg = nullptr, *rows_of = nullptr;
-    double* t = nullptr;
     sf_status e = upload(ns, &n_starts);
     if (!e) e = upload(nc, &n_cols);
     if (!e) e = upload(aggregate, &agg);
@@ -564,9 +553,8 @@ struct SetupMachine {
       e = upload_pattern(prolongator);
     }
     size_t entries = prolongator.cols.size();
-    const size_t tentative_bytes = rows * rb * MODES * 8;
-    if (!e) e = dev_alloc(dev, (void**)&t, std::max<size_t>(1, tentative_bytes));
-    if (!e && tentative_bytes) copy_h2d(dev, t, tentative, tentative_bytes);
+    double* t = d_tentative;
+    d_tentative = nullptr;
     if (!e) e = dev_alloc(dev, (void**)&prolongator.dev, std::max<size_t>(1, entries) * rb * MODES * 8);
     if (!e) e = entry_rows(prolongator, &rows_of);
     if (!e)
@@ -575,8 +563,6 @@ struct SetupMachine {
     if (!e) e = sync("smooth");
     for (void* p : {(void*)n_starts, (void*)n_cols, (void*)agg, (void*)rows_of, (void*)t}) dev_free(dev, p);
     if (e) return e;
-    pinned_return(tentative);  // the copy above completed at the sync
-    tentative = nullptr;
     phase = PRODUCT;
     return SF_OK;
   }
@@ -677,7 +663,8 @@ struct SetupMachine {
     current = std::move(coarse);
     coarse = Bsr();
     prolongator = Bsr();
-    near_null = std::move(coarse_null);
+    d_near_null = d_coarse_null;
+    d_coarse_null = nullptr;
     positions = std::move(coarse_positions);
     pinned_return(norms);
     norms = nullptr;
@@ -690,6 +677,8 @@ struct SetupMachine {
   }
 
   void push_final(bool factored) {
+    dev_free(dev, d_near_null);  // the coarsest level's modes are not needed
+    d_near_null = nullptr;
     HostLevel lv;
     lv.a = std::move(current);
     lv.inverse_diagonal = inv;
@@ -701,51 +690,37 @@ struct SetupMachine {
   }
 
   // Dense Cholesky of the coarsest level (block.rs:307-374), then its explicit inverse
-  // L^-T L^-1, which the device applies as one matrix-vector product per cycle.
+  // L^-T L^-1, which the device applies as one matrix-vector product per cycle: both on the device
+  // in FP64 (setup_dense_inverse, the host loops' bits); the first non-positive pivot is refused.
   sf_status run_factor() {
-    size_t n = current.rows * current.rb;
-    current.vals.assign(current.cols.size() * current.rb * current.cb, 0.0);
-    if (!current.vals.empty()) copy_d2h(dev, current.vals.data(), current.dev, current.vals.size() * 8);
-    if (sf_status e = sync("coarsest level")) return e;
-    vector<double> f(n * n, 0.0);
-    for (size_t row = 0; row < current.rows; ++row)
-      for (uint32_t at = current.starts[row]; at < current.starts[row + 1]; ++at) {
-        size_t col = current.cols[at];
-        for (size_t p = 0; p < current.rb; ++p)
-          for (size_t q = 0; q < current.cb; ++q)
-            f[(row * current.rb + p) * n + col * current.cb + q] = current.block(at)[p * current.cb + q];
-      }
-    for (size_t j = 0; j < n; ++j) {
-      double sum = f[j * n + j];
-      for (size_t k = 0; k < j; ++k) sum -= f[j * n + k] * f[j * n + k];
-      if (!std::isfinite(sum) || sum <= 0.0) return fail_pd(j, sum);
-      double d = std::sqrt(sum);
-      f[j * n + j] = d;
-      rows_parallel(n - j - 1, opt.threads, [&](size_t o) {
-        size_t i = j + 1 + o;
-        double s = f[i * n + j];
-        for (size_t k = 0; k < j; ++k) s -= f[i * n + k] * f[j * n + k];
-        f[i * n + j] = s / d;
-      });
+    const size_t n = current.rows * current.rb, nn = std::max<size_t>(1, n * n) * 8;
+    double *work = nullptr, *li = nullptr, *inverse = nullptr, *pivot = nullptr;
+    unsigned long long* bad = nullptr;
+    sf_status e = dev_alloc(dev, (void**)&work, nn);
+    if (!e) e = dev_alloc(dev, (void**)&li, nn);
+    if (!e) e = dev_alloc(dev, (void**)&inverse, nn);
+    if (!e) e = dev_alloc(dev, (void**)&bad, 8);
+    if (!e) e = dev_alloc(dev, (void**)&pivot, 8);
+    unsigned long long first = ~0ull;
+    double value = 0.0;
+    if (!e) {
+      copy_h2d(dev, bad, &first, 8);
+      e = setup_dense_inverse(dev.stream, (uint32_t)current.rows, (int)current.rb, current.dev_starts, current.dev_cols,
+                              current.dev, n, work, li, inverse, bad, pivot);
     }
-    // L^-1 column by column (forward substitution on unit vectors), then A^-1 = L^-T L^-1.
-    vector<double> li(n * n, 0.0);
-    rows_parallel(n, opt.threads, [&](size_t c) {
-      for (size_t i = c; i < n; ++i) {
-        double s = i == c ? 1.0 : 0.0;
-        for (size_t k = c; k < i; ++k) s -= f[i * n + k] * li[k * n + c];
-        li[i * n + c] = s / f[i * n + i];
-      }
-    });
+    if (!e) {
+      copy_d2h(dev, &first, bad, 8);
+      copy_d2h(dev, &value, pivot, 8);
+      e = sync("coarsest factor");
+    }
+    for (void* p : {(void*)work, (void*)li, (void*)bad, (void*)pivot}) dev_free(dev, p);
+    if (!e && first != ~0ull) e = fail_pd((size_t)first, value);
+    if (e) {
+      dev_free(dev, inverse);
+      return e;
+    }
     HostLevel lv;
-    lv.coarse_inverse.assign(n * n, 0.0);
-    rows_parallel(n, opt.threads, [&](size_t i) {
-      for (size_t j = 0; j < n; ++j) {
-        double s = 0.0;
-        for (size_t k = std::max(i, j); k < n; ++k) s += li[k * n + i] * li[k * n + j];
-        lv.coarse_inverse[i * n + j] = s;
-      }
-    });
+    lv.dev_coarse_inverse = inverse;
     lv.factor_n = n;
     lv.a = std::move(current);
     lv.inverse_diagonal = inv;
@@ -760,11 +735,12 @@ struct SetupMachine {
 };
 
 SetupMachine* setup_create(DeviceSolver& solver, Bsr&& fine, vector<double>&& near_null, vector<P3>&& positions,
-                           const SetupOptions& options) {
+                           const SetupOptions& options, double* device_near_null) {
   SetupMachine* m = new SetupMachine(solver);
   m->opt = options;
   m->current = std::move(fine);
   m->near_null = std::move(near_null);
+  m->d_near_null = device_near_null;
   m->positions = std::move(positions);
   m->reach = options.reach;
   return m;

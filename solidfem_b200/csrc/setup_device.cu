@@ -23,6 +23,8 @@ namespace sf {
 
 namespace {
 
+constexpr double kRankTolerance = 1e-10;  // transfer.rs:12
+
 const int kT = 256;
 
 int grid_for(size_t n) { return (int)std::max<size_t>(1, std::min<size_t>((n + kT - 1) / kT, 148 * 32)); }
@@ -351,6 +353,169 @@ __global__ void galerkin_kernel(size_t entries, const uint32_t* __restrict__ ent
   }
 }
 
+// The tentative prolongator (setup.rs:327-386, orthonormalize_aggregate, transfer.rs:19-68): per
+// aggregate, its members' rows of the near-null modes, orthonormalised column by column with two
+// Gram-Schmidt passes against the earlier columns; a column whose remainder falls to
+// RANK_TOLERANCE of its original norm is zeroed. One thread per aggregate runs the reference's
+// loops in their order (every sum sequential over the aggregate's rows, member by member), in
+// place in T at the members' own rows, so T and the coarse near-null space (the projections and
+// remainders, 6 x 6 per aggregate) are the host loops' bits.
+__global__ void tentative_kernel(uint32_t aggregates, int rb, const uint32_t* __restrict__ member_starts,
+                                 const uint32_t* __restrict__ members, const double* __restrict__ near_null,
+                                 double* __restrict__ t, double* __restrict__ coarse) {
+  const uint32_t a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a >= aggregates) return;
+  const uint32_t m0 = member_starts[a];
+  const size_t lrows = (size_t)(member_starts[a + 1] - m0) * rb;
+  // scalar row r of the aggregate: member m0 + r / rb, component r % rb
+  auto slot = [&](size_t r) { return ((size_t)members[m0 + r / rb] * rb + r % rb) * 6; };
+  for (size_t r = 0; r < lrows; ++r) {
+    const size_t at = slot(r);
+    for (int k = 0; k < 6; ++k) t[at + k] = near_null[at + k];
+  }
+  double* c = coarse + (size_t)a * 36;
+  for (int i = 0; i < 36; ++i) c[i] = 0.0;
+  for (int col = 0; col < 6; ++col) {
+    double s = 0.0;
+    for (size_t r = 0; r < lrows; ++r) {
+      const double v = t[slot(r) + col];
+      s += v * v;
+    }
+    const double original = sqrt(s);
+    for (int pass = 0; pass < 2; ++pass)
+      for (int prev = 0; prev < col; ++prev) {
+        double proj = 0.0;
+        for (size_t r = 0; r < lrows; ++r) {
+          const size_t at = slot(r);
+          proj += t[at + prev] * t[at + col];
+        }
+        c[prev * 6 + col] += proj;
+        for (size_t r = 0; r < lrows; ++r) {
+          const size_t at = slot(r);
+          t[at + col] -= proj * t[at + prev];
+        }
+      }
+    s = 0.0;
+    for (size_t r = 0; r < lrows; ++r) {
+      const double v = t[slot(r) + col];
+      s += v * v;
+    }
+    const double rem = sqrt(s);
+    if (original == 0.0 || rem <= kRankTolerance * original) {
+      for (size_t r = 0; r < lrows; ++r) t[slot(r) + col] = 0.0;
+      c[col * 6 + col] = 0.0;
+    } else {
+      for (size_t r = 0; r < lrows; ++r) t[slot(r) + col] /= rem;
+      c[col * 6 + col] = rem;
+    }
+  }
+}
+
+// The free nodes' rigid-body modes (free_rigid_body_modes, rigid_modes.rs:36-83) about the centre
+// and scale the host summed: for free block row r (node row_node[r]) the three rows
+// [1 0 0 0 z -y], [0 1 0 -z 0 x], [0 0 1 y -x 0] of the scaled offsets, (row, mode) at 6 row + mode.
+__global__ void rigid_modes_kernel(uint32_t rows, const uint32_t* __restrict__ row_node, const double* __restrict__ nodes,
+                                   double cx, double cy, double cz, double scale, double* __restrict__ modes) {
+  const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= rows) return;
+  const double* p = nodes + (size_t)row_node[r] * 3;
+  const double x = (p[0] - cx) * scale, y = (p[1] - cy) * scale, z = (p[2] - cz) * scale;
+  const double v[18] = {1, 0, 0, 0, z, -y, 0, 1, 0, -z, 0, x, 0, 0, 1, y, -x, 0};
+  double* m = modes + (size_t)r * 18;
+  for (int i = 0; i < 18; ++i) m[i] = v[i];
+}
+
+// ------------------------------------------------------------ the coarsest level's dense factor
+// DenseCholesky (block.rs:307-374) and the explicit inverse L^-T L^-1 the cycle applies. The
+// factor is computed right-looking in panels of kPanel columns: a panel kernel finishes its
+// columns (the diagonal, then every entry below it, each summing its last terms in ascending k),
+// a trailing kernel subtracts the panel's terms from the rest of the lower triangle, again in
+// ascending k. Every entry therefore subtracts L[i][k] L[j][k] for k = 0, 1, ... in order from its
+// original value, exactly the reference's left-looking loop, so the factor has the host loops'
+// bits. Row-major n x n in device memory (the lower triangle holds the factor).
+constexpr int kPanel = 32;
+
+__global__ void dense_from_blocks_kernel(uint32_t rows, int rb, int cb, const uint32_t* __restrict__ starts,
+                                         const uint32_t* __restrict__ cols, const double* __restrict__ vals, size_t n,
+                                         double* __restrict__ f) {
+  const uint32_t row = blockIdx.x * blockDim.x + threadIdx.x;
+  if (row >= rows) return;
+  for (uint32_t at = starts[row]; at < starts[row + 1]; ++at) {
+    const size_t col = cols[at];
+    for (int p = 0; p < rb; ++p)
+      for (int q = 0; q < cb; ++q) f[((size_t)row * rb + p) * n + col * cb + q] = vals[(size_t)at * rb * cb + p * cb + q];
+  }
+}
+
+// Columns [j0, j0 + kPanel) of the factor, one block; the first non-positive pivot is recorded
+// (its column and value) and the factor stops there.
+__global__ void __launch_bounds__(1024) cholesky_panel_kernel(size_t n, size_t j0, double* __restrict__ f,
+                                                              unsigned long long* bad, double* pivot) {
+  __shared__ double d;
+  __shared__ int failed;
+  if (threadIdx.x == 0) failed = *bad != ~0ull;
+  __syncthreads();
+  if (failed) return;
+  const size_t j1 = j0 + kPanel < n ? j0 + kPanel : n;
+  for (size_t j = j0; j < j1; ++j) {
+    if (threadIdx.x == 0) {
+      double sum = f[j * n + j];
+      for (size_t k = j0; k < j; ++k) sum -= f[j * n + k] * f[j * n + k];
+      if (!isfinite(sum) || sum <= 0.0) {
+        *bad = j;
+        *pivot = sum;
+        failed = 1;
+      } else {
+        d = sqrt(sum);
+        f[j * n + j] = d;
+      }
+    }
+    __syncthreads();
+    if (failed) return;
+    for (size_t i = j + 1 + threadIdx.x; i < n; i += blockDim.x) {
+      double s = f[i * n + j];
+      for (size_t k = j0; k < j; ++k) s -= f[i * n + k] * f[j * n + k];
+      f[i * n + j] = s / d;
+    }
+    __syncthreads();
+  }
+}
+
+// The panel's terms off every entry (i, j) of the lower triangle right of it, k ascending.
+__global__ void cholesky_trailing_kernel(size_t n, size_t j0, double* __restrict__ f, const unsigned long long* bad) {
+  if (*bad != ~0ull) return;
+  const size_t j1 = j0 + kPanel;
+  const size_t m = n - j1;  // trailing size
+  const size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= m * m) return;
+  const size_t i = j1 + e / m, j = j1 + e % m;
+  if (j > i) return;
+  double s = f[i * n + j];
+  for (size_t k = j0; k < j1; ++k) s -= f[i * n + k] * f[j * n + k];
+  f[i * n + j] = s;
+}
+
+// Column c of L^-1 by forward substitution on the unit vector (the host loop's order).
+__global__ void lower_inverse_kernel(size_t n, const double* __restrict__ f, double* __restrict__ li) {
+  const size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= n) return;
+  for (size_t i = c; i < n; ++i) {
+    double s = i == c ? 1.0 : 0.0;
+    for (size_t k = c; k < i; ++k) s -= f[i * n + k] * li[k * n + c];
+    li[i * n + c] = s / f[i * n + i];
+  }
+}
+
+// A^-1 = L^-T L^-1, entry (i, j) summing k from max(i, j) up.
+__global__ void gram_inverse_kernel(size_t n, const double* __restrict__ li, double* __restrict__ out) {
+  const size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= n * n) return;
+  const size_t i = e / n, j = e % n;
+  double s = 0.0;
+  for (size_t k = i > j ? i : j; k < n; ++k) s += li[k * n + i] * li[k * n + j];
+  out[e] = s;
+}
+
 template <typename S>
 __global__ void convert_kernel(size_t n, const double* __restrict__ in, S* __restrict__ out) {
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
@@ -515,6 +680,41 @@ sf_status setup_entry_rows(cudaStream_t st, uint32_t rows, const uint32_t* start
   if (rows == 0) return SF_OK;
   entry_rows_kernel<<<grid_for(rows), kT, 0, st>>>(rows, starts, out);
   return cuda_check(cudaGetLastError(), "entry rows");
+}
+
+sf_status setup_rigid_modes(cudaStream_t st, uint32_t rows, const uint32_t* row_node, const double* nodes,
+                            const double center[3], double scale, double* modes) {
+  if (rows == 0) return SF_OK;
+  rigid_modes_kernel<<<(rows + 255) / 256, 256, 0, st>>>(rows, row_node, nodes, center[0], center[1], center[2], scale,
+                                                         modes);
+  return cuda_check(cudaGetLastError(), "rigid modes");
+}
+
+sf_status setup_dense_inverse(cudaStream_t st, uint32_t rows, int rb, const uint32_t* starts, const uint32_t* cols,
+                              const double* vals, size_t n, double* work, double* li, double* inverse,
+                              unsigned long long* bad, double* pivot) {
+  if (n == 0) return SF_OK;
+  cudaMemsetAsync(work, 0, n * n * 8, st);
+  cudaMemsetAsync(li, 0, n * n * 8, st);
+  dense_from_blocks_kernel<<<(rows + 127) / 128, 128, 0, st>>>(rows, rb, rb, starts, cols, vals, n, work);
+  for (size_t j0 = 0; j0 < n; j0 += kPanel) {
+    cholesky_panel_kernel<<<1, 1024, 0, st>>>(n, j0, work, bad, pivot);
+    if (j0 + kPanel < n) {
+      const size_t m = n - j0 - kPanel;
+      cholesky_trailing_kernel<<<(unsigned)((m * m + 255) / 256), 256, 0, st>>>(n, j0, work, bad);
+    }
+  }
+  lower_inverse_kernel<<<(unsigned)((n + 127) / 128), 128, 0, st>>>(n, work, li);
+  gram_inverse_kernel<<<(unsigned)((n * n + 255) / 256), 256, 0, st>>>(n, li, inverse);
+  return cuda_check(cudaGetLastError(), "dense inverse");
+}
+
+sf_status setup_tentative(cudaStream_t st, size_t aggregates, int rb, const uint32_t* member_starts,
+                          const uint32_t* members, const double* near_null, double* t, double* coarse) {
+  if (aggregates == 0) return SF_OK;
+  tentative_kernel<<<(unsigned)((aggregates + 127) / 128), 128, 0, st>>>((uint32_t)aggregates, rb, member_starts,
+                                                                        members, near_null, t, coarse);
+  return cuda_check(cudaGetLastError(), "tentative");
 }
 
 sf_status setup_smooth(cudaStream_t st, int rb, size_t entries, const uint32_t* entry_row, const uint32_t* p_cols,

@@ -96,7 +96,7 @@ struct HostLevel {
   Bsr p;
   bool has_factor = false;
   size_t factor_n = 0;
-  vector<double> coarse_inverse;  // the dense inverse of the coarsest level, row-major f64
+  double* dev_coarse_inverse = nullptr;  // the dense inverse of the coarsest level, row-major f64, device
   vector<uint32_t> aggregates;
 };
 
@@ -114,8 +114,11 @@ struct SetupOptions {
 // the solver. Resumable by phase, like the reference's state machine.
 struct SetupMachine;
 struct DeviceSolver;
+// The finest level's near-null modes come either from the host (`near_null`, 6 per scalar row) or,
+// when `device_near_null` is set, already on the device (owned by the solver; the setup frees it
+// once the tentative prolongator is built).
 SetupMachine* setup_create(DeviceSolver& solver, Bsr&& fine, vector<double>&& near_null, vector<P3>&& positions,
-                           const SetupOptions& options);
+                           const SetupOptions& options, double* device_near_null = nullptr);
 // Runs up to `budget` rows of work. Returns SF_OK and sets *finished, or a failure.
 sf_status setup_step(SetupMachine* machine, size_t budget, sf_cancel_fn cancel, void* user,
                      bool* finished);

@@ -2794,8 +2794,7 @@ sf_status solver_upload_hierarchy(DeviceSolver& s, const std::vector<HostLevel>&
     if (e) return e;
     L.has_factor = h.has_factor;
     if (h.has_factor) {
-      if (sf_status e = dev_alloc(s, (void**)&L.coarse_inverse, h.coarse_inverse.size() * 8)) return e;
-      copy_h2d(s, L.coarse_inverse, h.coarse_inverse.data(), h.coarse_inverse.size() * 8);
+      L.coarse_inverse = h.dev_coarse_inverse;  // made on the device by the setup, owned by this solver
     }
     // ChebyshevCoefficients (gpu/layout.rs:443-465), the recurrence of cycle.rs:578-626.
     double theta = 0.5 * (h.lambda_max + h.lambda_min);

@@ -7,6 +7,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <future>
 #include <map>
 #include <numeric>
 #include <memory>
@@ -216,8 +217,11 @@ void add_traction(const Mesh& m, const sf_boundary_face& f, const double t[3], v
   }
 }
 
-// Rigid-body modes about the free nodes' centroid (crates/solidfem-elastic/src/rigid_modes.rs:36-83).
-vector<double> rigid_modes(const vector<P3>& nodes, const vector<uint32_t>& free, size_t free_count) {
+// The frame of the free nodes' rigid-body modes (free_rigid_body_modes, rigid_modes.rs:36-83): the
+// centroid of the free nodes (summed in node order) and 1 / the largest offset from it. The modes
+// themselves are made on the device from it (setup_rigid_modes).
+void rigid_frame(const vector<P3>& nodes, const vector<uint32_t>& free, size_t free_count, double center[3],
+                 double* scale) {
   double c[3] = {0, 0, 0};
   for (size_t n = 0; n < nodes.size(); ++n)
     if (free[n] != FIXED)
@@ -228,21 +232,57 @@ vector<double> rigid_modes(const vector<P3>& nodes, const vector<uint32_t>& free
   for (size_t n = 0; n < nodes.size(); ++n)
     if (free[n] != FIXED)
       for (int a = 0; a < 3; ++a) reach = std::max(reach, std::fabs(nodes[n][a] - c[a]));
-  double scale = reach > 0.0 ? 1.0 / reach : 1.0;
-  vector<double> modes(18 * free_count, 0.0);
-  for (size_t n = 0; n < nodes.size(); ++n) {
-    if (free[n] == FIXED) continue;
-    double* m = modes.data() + 18 * (size_t)free[n];
-    double x = (nodes[n][0] - c[0]) * scale, y = (nodes[n][1] - c[1]) * scale, z = (nodes[n][2] - c[2]) * scale;
-    double rows[18] = {1, 0, 0, 0, z, -y, 0, 1, 0, -z, 0, x, 0, 0, 1, y, -x, 0};
-    std::memcpy(m, rows, sizeof(rows));
-  }
-  return modes;
+  for (int a = 0; a < 3; ++a) center[a] = c[a];
+  *scale = reach > 0.0 ? 1.0 / reach : 1.0;
 }
 
 // An allocator whose resize leaves new elements uninitialised: the pattern's large arrays are
 // written in full by the parallel pass that fills them, so a zero fill first (single-threaded,
 // and the page faults of tens of MB with it) is pure cost.
+// build_load (study.rs:696-735): nodal forces and consistent tractions into `load` (3 per node),
+// refusing a node that does not exist, a non-finite value and a face off the boundary.
+sf_status build_load(const Mesh& mesh, const Model& md, vector<double>& load) {
+  const size_t nn = mesh.nodes.size();
+  for (auto& f : md.forces) {
+    if (f.first >= nn) {
+      error_slot().node = f.first;
+      return fail(SF_NODE_OUT_OF_RANGE, "a loaded node does not exist");
+    }
+    for (double c : f.second)
+      if (!std::isfinite(c)) return fail(SF_NON_FINITE_LOAD, "a nodal force is not finite");
+    for (int a = 0; a < 3; ++a) load[3 * (size_t)f.first + a] += f.second[a];
+  }
+  if (!md.tractions.empty()) {
+    // A boundary face is fixed by its (tet, face): a per-tet mask of boundary faces, and the
+    // face's nodes compared with the mesh's own entry, decide membership in the boundary list.
+    vector<unsigned char> boundary_mask(mesh.tets.size(), 0);
+    vector<uint32_t> entry(mesh.tets.size() * 4, 0);
+    for (size_t i = 0; i < mesh.faces.size(); ++i) {
+      const sf_boundary_face& f = mesh.faces[i];
+      boundary_mask[f.tet] |= (unsigned char)(1u << f.face);
+      entry[(size_t)f.tet * 4 + f.face] = (uint32_t)i;
+    }
+    auto on_boundary = [&](const sf_boundary_face& f) {
+      if (f.tet >= mesh.tets.size() || f.face >= 4 || !(boundary_mask[f.tet] & (1u << f.face))) return false;
+      const sf_boundary_face& g = mesh.faces[entry[(size_t)f.tet * 4 + f.face]];
+      for (int i = 0; i < 6; ++i)
+        if (g.nodes[i] != f.nodes[i]) return false;
+      return true;
+    };
+    for (auto& tr : md.tractions) {
+      if (!on_boundary(tr.first)) {
+        error_slot().tet = tr.first.tet;
+        error_slot().face = tr.first.face;
+        return fail(SF_FACE_NOT_ON_BOUNDARY, "a traction face is not on the mesh boundary");
+      }
+      for (double c : tr.second)
+        if (!std::isfinite(c)) return fail(SF_NON_FINITE_LOAD, "a traction is not finite");
+      add_traction(mesh, tr.first, tr.second.data(), load);
+    }
+  }
+  return SF_OK;
+}
+
 template <typename T>
 struct NoInit : std::allocator<T> {
   template <typename U>
@@ -358,6 +398,7 @@ struct sf_builder {
   DeviceSolver solver;
   SetupMachine* setup = nullptr;
   bool setup_finished = false;
+  double* modes = nullptr;  // the finest level's near-null modes on the device, until the setup takes them
   double assembly_seconds = 0, preconditioner_seconds = 0;
   float assembly_ms = 0, setup_ms = 0;
   sf_status failure = SF_OK;
@@ -656,53 +697,34 @@ sf_status sf_builder_create(sf_model* model, const sf_study_options* options, sf
     is_fixed[n] = 1;
   }
   std::sort(md.prescribed.begin(), md.prescribed.end());
-  if (md.prescribed.empty()) {
-    if (sf_status s = check_constraints(mesh, is_fixed)) return s;
-  } else {
-    if (sf_status s = check_held_dofs(mesh, is_fixed, md.prescribed)) return s;
-  }
-  // build_load, study.rs:696-735
+  // The constraint check and the load (StudyBuilder::new's refusals, study.rs:419-474) feed
+  // neither the free numbering, the pattern nor the device set-up, so they run on a helper thread
+  // while this one builds those; a refusal is returned once both are done, with the helper's
+  // error payload, and in the reference's order (constraints, loads, prescribed values).
   vector<double> load(3 * nn, 0.0);
-  for (auto& f : md.forces) {
-    if (f.first >= nn) {
-      error_slot().node = f.first;
-      return fail(SF_NODE_OUT_OF_RANGE, "a loaded node does not exist");
+  sf_error helper_error{};
+  std::future<sf_status> checks = std::async(std::launch::async, [&]() -> sf_status {
+    sf_status st = md.prescribed.empty() ? check_constraints(mesh, is_fixed)
+                                         : check_held_dofs(mesh, is_fixed, md.prescribed);
+    if (!st) st = build_load(mesh, md, load);
+    if (st) helper_error = error_slot();
+    return st;
+  });
+  struct Join {  // the helper reads this frame's vectors: it ends before any return
+    std::future<sf_status>& f;
+    ~Join() {
+      if (f.valid()) f.wait();
     }
-    for (double c : f.second)
-      if (!std::isfinite(c)) return fail(SF_NON_FINITE_LOAD, "a nodal force is not finite");
-    for (int a = 0; a < 3; ++a) load[3 * (size_t)f.first + a] += f.second[a];
-  }
-  if (!md.tractions.empty()) {
-    // A boundary face is fixed by its (tet, face): a per-tet mask of boundary faces, and the
-    // face's nodes compared with the mesh's own entry, decide membership in the boundary list.
-    vector<unsigned char> boundary_mask(mesh.tets.size(), 0);
-    vector<uint32_t> entry(mesh.tets.size() * 4, 0);
-    for (size_t i = 0; i < mesh.faces.size(); ++i) {
-      const sf_boundary_face& f = mesh.faces[i];
-      boundary_mask[f.tet] |= (unsigned char)(1u << f.face);
-      entry[(size_t)f.tet * 4 + f.face] = (uint32_t)i;
-    }
-    auto on_boundary = [&](const sf_boundary_face& f) {
-      if (f.tet >= mesh.tets.size() || f.face >= 4 || !(boundary_mask[f.tet] & (1u << f.face))) return false;
-      const sf_boundary_face& g = mesh.faces[entry[(size_t)f.tet * 4 + f.face]];
-      for (int i = 0; i < 6; ++i)
-        if (g.nodes[i] != f.nodes[i]) return false;
-      return true;
-    };
-    for (auto& tr : md.tractions) {
-      if (!on_boundary(tr.first)) {
-        error_slot().tet = tr.first.tet;
-        error_slot().face = tr.first.face;
-        return fail(SF_FACE_NOT_ON_BOUNDARY, "a traction face is not on the mesh boundary");
-      }
-      for (double c : tr.second)
-        if (!std::isfinite(c)) return fail(SF_NON_FINITE_LOAD, "a traction is not finite");
-      add_traction(mesh, tr.first, tr.second.data(), load);
-    }
-  }
+  } join{checks};
   b->free.assign(nn, FIXED);
   for (size_t n = 0; n < nn; ++n)
     if (!is_fixed[n]) b->free[n] = (uint32_t)b->free_count++;
+  double t0 = now_seconds();
+  build_pattern(mesh, b->free, b->free_count, b->threads, b->pattern);
+  if (sf_status st = checks.get()) {
+    error_slot() = helper_error;
+    return st;
+  }
   b->rhs.reserve(3 * b->free_count);
   for (size_t n = 0; n < nn; ++n)
     if (b->free[n] != FIXED)
@@ -729,8 +751,6 @@ sf_status sf_builder_create(sf_model* model, const sf_study_options* options, sf
   for (double v : b->rhs) all_zero = all_zero && v == 0.0;
   for (auto& p : b->prescribed) all_zero = all_zero && p.second == 0.0;
   if (all_zero) return fail(SF_NO_EFFECTIVE_LOAD, "the model has no effective load");
-  double t0 = now_seconds();
-  build_pattern(mesh, b->free, b->free_count, b->threads, b->pattern);
   // Device set-up: mesh, element stiffness buffer, pattern and assembly map, system matrix.
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(SF_NO_DEVICE, "no CUDA device is visible");
@@ -947,8 +967,38 @@ static sf_status builder_assemble(sf_builder* b, uint64_t max_elements, sf_cance
       b->failure = pe;
       return pe;
     }
-    // The element stiffness buffer and the assembly map have served; free them for the solve.
     AssemblyDevice& a = b->asmdev;
+    if (b->options.preconditioner == SF_PRECONDITIONER_MULTIGRID) {
+      // The near-null modes, from the free rows' nodes while the row map is still on the device,
+      // zero at prescribed DOFs (the setup reads them at the tentative prolongator).
+      double center[3], scale = 1.0;
+      rigid_frame(b->model.mesh.nodes, b->free, b->free_count, center, &scale);
+      sf_status me = dev_alloc(s, (void**)&b->modes, std::max<size_t>(1, b->free_count) * 18 * 8);
+      if (!me) me = setup_rigid_modes(s.stream, (uint32_t)b->free_count, a.row_node, a.nodes, center, scale, b->modes);
+      if (!me && !b->prescribed.empty()) {
+        vector<uint32_t> idx;
+        for (auto& p : b->prescribed)
+          for (uint32_t k = 0; k < 6; ++k) idx.push_back((uint32_t)(p.first * 6 + k));
+        vector<double> zeros(idx.size(), 0.0);
+        uint32_t* d_idx = nullptr;
+        double* d_zero = nullptr;
+        me = dev_alloc(s, (void**)&d_idx, idx.size() * 4);
+        if (!me) me = dev_alloc(s, (void**)&d_zero, zeros.size() * 8);
+        if (!me) {
+          copy_h2d(s, d_idx, idx.data(), idx.size() * 4);
+          copy_h2d(s, d_zero, zeros.data(), zeros.size() * 8);
+          me = setup_set_values(s.stream, idx.size(), d_idx, d_zero, b->modes);
+        }
+        if (!me) me = cuda_check(cudaStreamSynchronize(s.stream), "near-null modes");
+        dev_free(s, d_idx);
+        dev_free(s, d_zero);
+      }
+      if (me) {
+        b->failure = me;
+        return me;
+      }
+    }
+    // The element stiffness buffer and the assembly map have served; free them for the solve.
     for (void* p : {(void*)a.ke, (void*)a.inc_start, (void*)a.inc, (void*)a.row_node, (void*)a.cursor})
       dev_free(s, p);
     a.ke = nullptr;
@@ -971,8 +1021,6 @@ static sf_status builder_setup(sf_builder* b, uint64_t budget, sf_cancel_fn canc
     fine.dev = (double*)s.system.vals;
     fine.dev_starts = s.system.starts;
     fine.dev_cols = s.system.cols;
-    vector<double> modes = rigid_modes(b->model.mesh.nodes, b->free, b->free_count);
-    for (auto& p : b->prescribed) std::fill(modes.begin() + p.first * 6, modes.begin() + p.first * 6 + 6, 0.0);
     vector<P3> positions;
     positions.reserve(b->free_count);
     for (size_t n = 0; n < b->free.size(); ++n)
@@ -983,7 +1031,8 @@ static sf_status builder_setup(sf_builder* b, uint64_t budget, sf_cancel_fn canc
     so.max_levels = b->options.max_levels;
     so.range = b->options.smoother_range;
     so.threads = b->threads;
-    b->setup = setup_create(s, std::move(fine), std::move(modes), std::move(positions), so);
+    b->setup = setup_create(s, std::move(fine), vector<double>(), std::move(positions), so, b->modes);
+    b->modes = nullptr;  // the setup frees it
   }
   bool finished = false;
   sf_status st = setup_step(b->setup, budget, cancel, user, &finished);

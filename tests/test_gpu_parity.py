@@ -184,3 +184,21 @@ def test_fourteen_point_assembly_and_recovery_are_bit_exact(oracle, name):
     s6, vm = ref.recover_with(sol.displacements)
     assert np.array_equal(sol.nodal_stress.view(np.uint64), s6.view(np.uint64))
     assert np.array_equal(sol.nodal_von_mises.view(np.uint64), vm.view(np.uint64))
+
+
+def test_an_invalid_material_is_refused_at_the_first_element_and_point():
+    """A material field that is not a stable solid in part of the body (nu = 0.5 past x = 6) is refused
+    during device assembly by name, at the element and integration point the reference's serial
+    assembly meets first (element.rs:83-94, ElementFault::InvalidMaterial)."""
+    mesh, model = product_model((10.0, 1.0, 1.0), (12, 3, 3), 1.0, 0.0,
+                                material=lambda p: sf.Material(200000.0, 0.5 if p[0] > 6.0 else 0.3))
+    with pytest.raises(sf.SolidfemError) as err:
+        sf.StaticStudy.new(model, mg_options(sf.Precision.DOUBLE))
+    assert err.value.status == sf.Status.ELEMENT_INVALID_MATERIAL
+    # the integration point positions, in (element, point) order, from a valid solve of the same mesh
+    _, valid = product_model((10.0, 1.0, 1.0), (12, 3, 3), 200000.0, 0.3)
+    study = sf.StaticStudy.new(valid, mg_options(sf.Precision.DOUBLE))
+    assert study.solve().kind == sf.Outcome.CONVERGED
+    pts = study.solution().point_stresses
+    first = int(np.flatnonzero(pts["position"][:, 0] > 6.0)[0])
+    assert (err.value.detail["tet"], err.value.detail["point"]) == (pts["tet"][first], pts["point"][first])

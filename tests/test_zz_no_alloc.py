@@ -85,11 +85,12 @@ def test_energy_products_refusals():
 
 
 def test_energy_products_refuse_a_short_buffer_and_keep_the_current_device():
-    """A range must lie inside one device allocation. The driver knows allocations, not a
-    sub-allocator's pieces of them (torch's caching allocator carves tensors out of larger
-    allocations), so the short buffer here is its own cudaMalloc, one entry short of two vectors."""
+    """A range must lie inside one device allocation, as the driver reports it (cuMemGetAddressRange;
+    the driver knows allocations, not a sub-allocator's pieces of them, and may round a request up).
+    y placed so its two vectors end 8 bytes past the allocation is refused; placed to end exactly at
+    the allocation's end it is accepted."""
     import torch
-    from cuda.bindings import runtime as rt
+    from cuda.bindings import driver, runtime as rt
 
     study = make_study(False)
     n = study.report()["free_dofs"]
@@ -97,18 +98,20 @@ def test_energy_products_refuse_a_short_buffer_and_keep_the_current_device():
     e = torch.zeros(2, dtype=torch.float64, device="cuda:0")
     torch.cuda.synchronize()
     before = torch.cuda.current_device()
-    err_code, short = rt.cudaMalloc((2 * n - 1) * 8)
+    err_code, buf = rt.cudaMalloc(4 * n * 8)
     assert err_code == rt.cudaError_t.cudaSuccess
     try:
+        err_code, base, size = driver.cuMemGetAddressRange(int(buf))
+        assert err_code == driver.CUresult.CUDA_SUCCESS
+        end = int(base) + int(size)
         with pytest.raises(sf.SolidfemError) as err:
-            study.energy_products(x.data_ptr(), int(short), e.data_ptr(), 2)
+            study.energy_products(x.data_ptr(), end - 2 * n * 8 + 8, e.data_ptr(), 2)
         assert err.value.status == sf.Status.INVALID_ARGUMENT
+        study.energy_products(x.data_ptr(), end - 2 * n * 8, e.data_ptr(), 2)
+        torch.cuda.synchronize()
+        assert torch.cuda.current_device() == before
     finally:
-        rt.cudaFree(short)
+        rt.cudaFree(buf)
     with pytest.raises(sf.SolidfemError) as err:
-        study.energy_products(x.data_ptr(), x[1].data_ptr(), e.data_ptr(), 1)  # overlapping x and y
+        study.energy_products(x.data_ptr(), x[1].data_ptr(), e.data_ptr(), 2)  # x's second vector is y's first
     assert err.value.status == sf.Status.INVALID_ARGUMENT
-    y = torch.zeros((2, n), dtype=torch.float64, device="cuda:0")
-    study.energy_products(x.data_ptr(), y.data_ptr(), e.data_ptr(), 2)
-    torch.cuda.synchronize()
-    assert torch.cuda.current_device() == before
