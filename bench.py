@@ -495,7 +495,7 @@ def run_serving(args):
     group = ReplicaGroup.from_env("nccl")
     device = group.local_rank
     torch.cuda.set_device(device)
-    stream = W.serving_stream(count=args.requests)
+    stream = W.serving_stream(count=args.requests, rate=args.rate)
     reqs = group.shard(stream)
     t0 = time.perf_counter()
     with concurrent.futures.ThreadPoolExecutor(max_workers=8) as pool:
@@ -563,7 +563,7 @@ def run_serving(args):
     del built
     gc.collect()
 
-    config = {"workload": f"serving stream: {len(stream)} bar/tube/plate requests, Poisson 20/s, seed 0, "
+    config = {"workload": f"serving stream: {len(stream)} bar/tube/plate requests, Poisson {args.rate:g}/s, seed 0, "
                           "10k-600k DOF log-uniform, rel. residual 1e-8, HBM budget 150 GB, "
                           "requests under 100k DOF batched",
               "build_threads": args.build_threads, "model_prep_seconds": prep,
@@ -620,6 +620,7 @@ def main():
                         "block: the 5.3M-DOF printed block")
     p.add_argument("--block-cells", type=int, default=60, help="block: hex cells per side")
     p.add_argument("--requests", type=int, default=512, help="serving: requests in the stream")
+    p.add_argument("--rate", type=float, default=20.0, help="serving: Poisson arrival rate, requests per second")
     p.add_argument("--build-threads", type=int, default=8, help="serving: host build threads")
     p.add_argument("--no-serial", action="store_true", help="serving: skip the serial FP64 comparison")
     args = p.parse_args()

@@ -227,7 +227,9 @@ sf_status setup_dense_inverse(cudaStream_t st, uint32_t rows, int rb, const uint
                               unsigned long long* bad, double* pivot);
 // The tentative prolongator of every aggregate into t (rows x rb x 6 at the members' rows) and the
 // coarse near-null space (aggregates x 36), bit-identical to the host loops (transfer.rs:19-68).
-sf_status setup_tentative(cudaStream_t st, size_t aggregates, int rb, const uint32_t* member_starts,
+// max_members: the largest aggregate's member count (its rows are staged in shared memory; an
+// aggregate of more than 200 KB of rows is refused).
+sf_status setup_tentative(cudaStream_t st, size_t aggregates, int rb, size_t max_members, const uint32_t* member_starts,
                           const uint32_t* members, const double* near_null, double* t, double* coarse);
 sf_status setup_smooth(cudaStream_t st, int rb, size_t entries, const uint32_t* entry_row, const uint32_t* p_cols,
                        const uint32_t* a_starts, const uint32_t* a_cols, const double* a_vals, const uint32_t* n_starts,

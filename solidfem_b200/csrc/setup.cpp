@@ -407,8 +407,11 @@ struct SetupMachine {
     if (!e) e = upload(members, &d_members);
     if (!e) e = dev_alloc(dev, (void**)&d_tentative, std::max<size_t>(1, rows * rb * MODES) * 8);
     if (!e) e = dev_alloc(dev, (void**)&d_coarse_null, std::max<size_t>(1, aggregates) * 36 * 8);
-    if (!e) e = setup_tentative(dev.stream, aggregates, (int)rb, d_starts, d_members, d_near_null, d_tentative,
-                                d_coarse_null);
+    size_t max_members = 0;
+    for (size_t a = 0; a < aggregates; ++a) max_members = std::max<size_t>(max_members, member_starts[a + 1] - member_starts[a]);
+    if (!e)
+      e = setup_tentative(dev.stream, aggregates, (int)rb, max_members, d_starts, d_members, d_near_null, d_tentative,
+                          d_coarse_null);
     // stream-ordered frees: after the kernel that reads them
     for (void* p : {(void*)d_starts, (void*)d_members, (void*)d_near_null}) dev_free(dev, p);
     d_near_null = nullptr;

@@ -15,6 +15,8 @@
 // doubles several times faster than one GPU thread; the products stay here.
 #include <cuda_runtime.h>
 
+#include <atomic>
+
 #include <algorithm>
 
 #include "device.h"
@@ -24,6 +26,7 @@ namespace sf {
 namespace {
 
 constexpr double kRankTolerance = 1e-10;  // transfer.rs:12
+constexpr size_t kTentativeMaxSmem = 200 * 1024;  // an aggregate's rows x 6 modes, staged whole
 
 const int kT = 256;
 
@@ -356,58 +359,60 @@ __global__ void galerkin_kernel(size_t entries, const uint32_t* __restrict__ ent
 // The tentative prolongator (setup.rs:327-386, orthonormalize_aggregate, transfer.rs:19-68): per
 // aggregate, its members' rows of the near-null modes, orthonormalised column by column with two
 // Gram-Schmidt passes against the earlier columns; a column whose remainder falls to
-// RANK_TOLERANCE of its original norm is zeroed. One thread per aggregate runs the reference's
-// loops in their order (every sum sequential over the aggregate's rows, member by member), in
-// place in T at the members' own rows, so T and the coarse near-null space (the projections and
-// remainders, 6 x 6 per aggregate) are the host loops' bits.
-__global__ void tentative_kernel(uint32_t aggregates, int rb, const uint32_t* __restrict__ member_starts,
-                                 const uint32_t* __restrict__ members, const double* __restrict__ near_null,
-                                 double* __restrict__ t, double* __restrict__ coarse) {
-  const uint32_t a = blockIdx.x * blockDim.x + threadIdx.x;
+// RANK_TOLERANCE of its original norm is zeroed. One warp per aggregate stages the aggregate's
+// rows (members in order, rb rows each, 6 modes) in shared memory; lane 0 runs every sum of the
+// reference's loops in their order (sequential over the aggregate's rows), and the lanes share the
+// element-wise updates, each of which depends only on its own entry. So T (written back at the
+// members' own rows) and the coarse near-null space (the projections and remainders, 6 x 6 per
+// aggregate) carry the host loops' bits.
+__global__ void __launch_bounds__(32) tentative_kernel(uint32_t aggregates, int rb,
+                                                       const uint32_t* __restrict__ member_starts,
+                                                       const uint32_t* __restrict__ members,
+                                                       const double* __restrict__ near_null, double* __restrict__ t,
+                                                       double* __restrict__ coarse) {
+  extern __shared__ double local[];  // lrows x 6
+  const uint32_t a = blockIdx.x;
+  const unsigned lane = threadIdx.x;
   if (a >= aggregates) return;
   const uint32_t m0 = member_starts[a];
-  const size_t lrows = (size_t)(member_starts[a + 1] - m0) * rb;
-  // scalar row r of the aggregate: member m0 + r / rb, component r % rb
-  auto slot = [&](size_t r) { return ((size_t)members[m0 + r / rb] * rb + r % rb) * 6; };
-  for (size_t r = 0; r < lrows; ++r) {
+  const uint32_t lrows = (member_starts[a + 1] - m0) * (uint32_t)rb;
+  auto slot = [&](uint32_t r) { return ((size_t)members[m0 + r / rb] * rb + r % rb) * 6; };
+  for (uint32_t r = lane; r < lrows; r += 32) {
     const size_t at = slot(r);
-    for (int k = 0; k < 6; ++k) t[at + k] = near_null[at + k];
+    for (int k = 0; k < 6; ++k) local[r * 6 + k] = near_null[at + k];
   }
+  __syncwarp();
   double* c = coarse + (size_t)a * 36;
-  for (int i = 0; i < 36; ++i) c[i] = 0.0;
-  for (int col = 0; col < 6; ++col) {
+  if (lane == 0)
+    for (int i = 0; i < 36; ++i) c[i] = 0.0;
+  auto column_norm = [&](int col) {  // lane 0's sequential sum, broadcast
     double s = 0.0;
-    for (size_t r = 0; r < lrows; ++r) {
-      const double v = t[slot(r) + col];
-      s += v * v;
-    }
-    const double original = sqrt(s);
+    if (lane == 0)
+      for (uint32_t r = 0; r < lrows; ++r) s += local[r * 6 + col] * local[r * 6 + col];
+    return __shfl_sync(0xffffffffu, sqrt(s), 0);
+  };
+  for (int col = 0; col < 6; ++col) {
+    const double original = column_norm(col);
     for (int pass = 0; pass < 2; ++pass)
       for (int prev = 0; prev < col; ++prev) {
         double proj = 0.0;
-        for (size_t r = 0; r < lrows; ++r) {
-          const size_t at = slot(r);
-          proj += t[at + prev] * t[at + col];
+        if (lane == 0) {
+          for (uint32_t r = 0; r < lrows; ++r) proj += local[r * 6 + prev] * local[r * 6 + col];
+          c[prev * 6 + col] += proj;
         }
-        c[prev * 6 + col] += proj;
-        for (size_t r = 0; r < lrows; ++r) {
-          const size_t at = slot(r);
-          t[at + col] -= proj * t[at + prev];
-        }
+        proj = __shfl_sync(0xffffffffu, proj, 0);
+        for (uint32_t r = lane; r < lrows; r += 32) local[r * 6 + col] -= proj * local[r * 6 + prev];
+        __syncwarp();
       }
-    s = 0.0;
-    for (size_t r = 0; r < lrows; ++r) {
-      const double v = t[slot(r) + col];
-      s += v * v;
-    }
-    const double rem = sqrt(s);
-    if (original == 0.0 || rem <= kRankTolerance * original) {
-      for (size_t r = 0; r < lrows; ++r) t[slot(r) + col] = 0.0;
-      c[col * 6 + col] = 0.0;
-    } else {
-      for (size_t r = 0; r < lrows; ++r) t[slot(r) + col] /= rem;
-      c[col * 6 + col] = rem;
-    }
+    const double rem = column_norm(col);
+    const bool drop = original == 0.0 || rem <= kRankTolerance * original;
+    for (uint32_t r = lane; r < lrows; r += 32) local[r * 6 + col] = drop ? 0.0 : local[r * 6 + col] / rem;
+    if (lane == 0) c[col * 6 + col] = drop ? 0.0 : rem;
+    __syncwarp();
+  }
+  for (uint32_t r = lane; r < lrows; r += 32) {
+    const size_t at = slot(r);
+    for (int k = 0; k < 6; ++k) t[at + k] = local[r * 6 + k];
   }
 }
 
@@ -709,11 +714,21 @@ sf_status setup_dense_inverse(cudaStream_t st, uint32_t rows, int rb, const uint
   return cuda_check(cudaGetLastError(), "dense inverse");
 }
 
-sf_status setup_tentative(cudaStream_t st, size_t aggregates, int rb, const uint32_t* member_starts,
+sf_status setup_tentative(cudaStream_t st, size_t aggregates, int rb, size_t max_members, const uint32_t* member_starts,
                           const uint32_t* members, const double* near_null, double* t, double* coarse) {
   if (aggregates == 0) return SF_OK;
-  tentative_kernel<<<(unsigned)((aggregates + 127) / 128), 128, 0, st>>>((uint32_t)aggregates, rb, member_starts,
-                                                                        members, near_null, t, coarse);
+  const size_t smem = max_members * (size_t)rb * 6 * sizeof(double);
+  if (smem > kTentativeMaxSmem) return fail(SF_INVALID_ARGUMENT, "an aggregate too large for the tentative kernel");
+  static std::atomic<uint64_t> opted{0};  // the opt-in above 48 KB, once per device
+  int dev = 0;
+  cudaGetDevice(&dev);
+  const uint64_t bit = dev < 64 ? 1ull << dev : 0;
+  if (smem > 48 * 1024 && (!bit || !(opted.load() & bit))) {
+    cudaFuncSetAttribute(tentative_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTentativeMaxSmem);
+    opted.fetch_or(bit);
+  }
+  tentative_kernel<<<(unsigned)aggregates, 32, smem, st>>>((uint32_t)aggregates, rb, member_starts, members, near_null,
+                                                           t, coarse);
   return cuda_check(cudaGetLastError(), "tentative");
 }
 

@@ -2578,19 +2578,30 @@ struct SellLayout {
   std::vector<uint32_t> rows, len, start;
 };
 
+// Rows by descending block count inside windows of kSellWindow rows, equal lengths in row order:
+// a counting sort per window (the order a stable sort by descending length gives).
+std::vector<uint32_t> window_order(uint32_t nrows, const uint32_t* starts) {
+  std::vector<uint32_t> order(nrows), count;
+  for (uint32_t w0 = 0; w0 < nrows; w0 += kSellWindow) {
+    const uint32_t w1 = std::min(nrows, w0 + kSellWindow);
+    uint32_t longest = 0;
+    for (uint32_t r = w0; r < w1; ++r) longest = std::max(longest, starts[r + 1] - starts[r]);
+    count.assign(longest + 2, 0);
+    for (uint32_t r = w0; r < w1; ++r) count[longest - (starts[r + 1] - starts[r]) + 1] += 1;
+    for (uint32_t k = 1; k <= longest + 1; ++k) count[k] += count[k - 1];
+    for (uint32_t r = w0; r < w1; ++r) order[w0 + count[longest - (starts[r + 1] - starts[r])]++] = r;
+  }
+  return order;
+}
+
 // Rows sorted by descending block count inside windows of kSellWindow rows (stable, so equal
 // lengths keep row order), cut into slices of 32, slice widths padded to chunks of `chunk`
 // blocks. Only this row order is host work; the blocks are placed on the device.
 SellLayout sell_layout(uint32_t nrows, const uint32_t* starts, uint32_t chunk) {
   SellLayout L;
   L.nslices = (nrows + 31) / 32;
-  std::vector<uint32_t> order(nrows);
-  for (uint32_t i = 0; i < nrows; ++i) order[i] = i;
+  std::vector<uint32_t> order = window_order(nrows, starts);
   auto rlen = [&](uint32_t r) { return starts[r + 1] - starts[r]; };
-  for (uint32_t w0 = 0; w0 < nrows; w0 += kSellWindow) {
-    uint32_t w1 = std::min(nrows, w0 + kSellWindow);
-    std::stable_sort(order.begin() + w0, order.begin() + w1, [&](uint32_t a, uint32_t b) { return rlen(a) > rlen(b); });
-  }
   L.rows.assign((size_t)L.nslices * 32, nrows);
   L.len.assign((size_t)L.nslices * 32, 0);
   L.start.assign(L.nslices + 1, 0);
@@ -2613,13 +2624,8 @@ SellLayout sell_layout(uint32_t nrows, const uint32_t* starts, uint32_t chunk) {
 SellLayout split_layout(uint32_t nrows, const uint32_t* starts, uint32_t chunk) {
   SellLayout L;
   L.nslices = (nrows + kSplitRowsPerSlice - 1) / kSplitRowsPerSlice;
-  std::vector<uint32_t> order(nrows);
-  for (uint32_t i = 0; i < nrows; ++i) order[i] = i;
+  std::vector<uint32_t> order = window_order(nrows, starts);
   auto rlen = [&](uint32_t r) { return starts[r + 1] - starts[r]; };
-  for (uint32_t w0 = 0; w0 < nrows; w0 += kSellWindow) {
-    uint32_t w1 = std::min(nrows, w0 + kSellWindow);
-    std::stable_sort(order.begin() + w0, order.begin() + w1, [&](uint32_t a, uint32_t b) { return rlen(a) > rlen(b); });
-  }
   L.rows.assign((size_t)L.nslices * 32, nrows);
   L.len.assign((size_t)L.nslices * 32, 0);
   L.start.assign(L.nslices + 1, 0);
