@@ -407,6 +407,128 @@ def run_profile(args):
     return 0
 
 
+def profile_extras(sf, torch, tol, note):
+    """The kernels the other profiled paths never launch: quadrature-point positions for a material
+    field, the degree-1 smoother's plain add, and the energy products of a row-group system product."""
+    m = sf.box_tet_mesh((0.0, 0.0, 0.0), (10.0, 1.0, 1.0), (20, 4, 4))
+    nd = m.nodes()
+    model = sf.Model(m, lambda pos: sf.Material(200000.0 if pos[0] < 5.0 else 100000.0, 0.3))
+    model.fix_nodes(np.nonzero(np.abs(nd[:, 0]) < 1e-9)[0])
+    faces = m.boundary_face_array()
+    end = np.all(np.abs(nd[faces["nodes"][:, :3], 0] - 10.0) < 1e-9, axis=1)
+    model.add_face_tractions(faces[end], (0.0, 3.0, -7.0))
+    st = sf.StaticStudy.new(model, sf.StudyOptions(
+        pcg=sf.PcgOptions(tolerance=tol or 1e-9),
+        preconditioner=sf.MultigridOptions(coarse_dofs=100, smoother_degree=1, precision=sf.Precision.DOUBLE)))
+    note("extras", st, st.solve())
+    k = st.report()["free_dofs"]
+    xs = torch.from_numpy(np.random.default_rng(1).standard_normal((2, k))).to("cuda:0")
+    ys = torch.empty_like(xs)
+    es = torch.empty(2, dtype=torch.float64, device="cuda:0")
+    torch.cuda.synchronize()
+    st.energy_products(xs.data_ptr(), ys.data_ptr(), es.data_ptr(), 2)
+    torch.cuda.synchronize()
+    return 0
+
+
+def run_profile_paths(args):
+    """Every kernel family of the library once, for a profiler's launch list (no JSON line): the gate
+    plate's study creation (mesh upload, assembly, multigrid setup), one mixed and one FP64 solve,
+    the stress recovery, the energy products and the coarse-tail cluster launch; then small studies
+    for the batched grids, the Jacobi preconditioner and prescribed displacements. `--profile-cells`
+    scales the plate (the gate plate has 100 cells a side); `--profile-iterations` and
+    `--profile-tolerance` shorten the solves, for captures that collect more than the launch times."""
+    import torch
+
+    import solidfem_b200 as sf
+
+    torch.cuda.set_device(0)
+    cells = args.profile_cells
+    tol = args.profile_tolerance
+
+    def opts(precision):
+        o = options(sf, precision, 0)
+        if tol:
+            o.pcg.tolerance = tol
+        return o
+
+    mesh = sf.box_tet_mesh((0.0, 0.0, 0.0), SIZE, (cells, cells, 2))
+    nodes = mesh.nodes()
+
+    def plate(extra=None):
+        model = sf.Model(mesh, sf.Material(YOUNGS, POISSON))
+        model.fix_nodes(np.nonzero(np.abs(nodes[:, 0]) < 1e-9)[0])
+        faces = mesh.boundary_face_array()
+        top = np.all(np.abs(nodes[faces["nodes"][:, :3], 2] - SIZE[2]) < 1e-9, axis=1)
+        model.add_face_tractions(faces[top], (0.0, 0.0, -PRESSURE))
+        if extra:
+            extra(model)
+        return model
+
+    def note(name, study, out):
+        print(f"profile {name}: {out.progress.iteration} iterations, residual {out.progress.relative_residual:.3e}, "
+              f"{study.device_timing()['step_ms']:.1f} ms", flush=True)
+
+    if args.profile_extras:
+        return profile_extras(sf, torch, tol, note)
+
+    def run(study):
+        # --profile-iterations: a few iterations of each plate solve (the stress recovery then runs on
+        # the small converged studies below)
+        return study.step(args.profile_iterations) if args.profile_iterations else study.solve()
+
+    mixed = sf.StaticStudy.new(plate(), opts(sf.Precision.MIXED))
+    note("mixed", mixed, run(mixed))
+    if not args.profile_iterations:
+        mixed.solution()
+    n = mixed.report()["free_dofs"]
+    xs = torch.from_numpy(np.random.default_rng(0).standard_normal((2, n))).to("cuda:0")
+    ys = torch.empty_like(xs)
+    es = torch.empty(2, dtype=torch.float64, device="cuda:0")
+    torch.cuda.synchronize()
+    mixed.energy_products(xs.data_ptr(), ys.data_ptr(), es.data_ptr(), 2)
+    torch.cuda.synchronize()
+    del mixed
+    gc.collect()
+    double = sf.StaticStudy.new(plate(), opts(sf.Precision.DOUBLE))
+    note("double", double, run(double))
+    del double
+    gc.collect()
+    tail_opts = opts(sf.Precision.MIXED)
+    tail_opts.coarse_tail = True
+    tail = sf.StaticStudy.new(plate(), tail_opts)
+    note("coarse tail", tail, run(tail))
+    del tail
+    gc.collect()
+
+    def small(div, precision, batchable=False, prescribe=False, jacobi=False):
+        m = sf.box_tet_mesh((0.0, 0.0, 0.0), (10.0, 1.0, 1.0), div)
+        nd = m.nodes()
+        model = sf.Model(m, sf.Material(200000.0, 0.3))
+        model.fix_nodes(np.nonzero(np.abs(nd[:, 0]) < 1e-9)[0])
+        faces = m.boundary_face_array()
+        end = np.all(np.abs(nd[faces["nodes"][:, :3], 0] - 10.0) < 1e-9, axis=1)
+        model.add_face_tractions(faces[end], (0.0, 3.0, -7.0))
+        if prescribe:
+            tip = np.nonzero(np.abs(nd[:, 0] - 10.0) < 1e-9)[0]
+            for node in tip[:4]:
+                model.prescribe_displacement(int(node), 2, -0.01)
+        pre = sf.Jacobi() if jacobi else sf.MultigridOptions(coarse_dofs=100, precision=precision)
+        return sf.StaticStudy.new(model, sf.StudyOptions(pcg=sf.PcgOptions(tolerance=tol or 1e-9), preconditioner=pre,
+                                                         batchable=batchable))
+
+    batch = [small(d, sf.Precision.MIXED, batchable=True) for d in ((24, 4, 4), (30, 5, 5), (36, 6, 6))]
+    res = sf.solve_batch(batch)
+    print("profile batch:", [r[0].progress.iteration for r in res], flush=True)
+    jacobi = small((20, 4, 4), None, jacobi=True)
+    note("jacobi", jacobi, run(jacobi))
+    prescribed = small((20, 4, 4), sf.Precision.DOUBLE, prescribe=True)
+    note("prescribed", prescribed, prescribed.solve())
+    if args.profile_iterations:
+        prescribed.solution()
+    return 0
+
+
 def percentile(values, q):
     v = sorted(values)
     if not v:
@@ -613,8 +735,16 @@ def main():
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=["mine", "reference"], default="mine")
     p.add_argument("--no-cpu-baseline", action="store_true")
-    p.add_argument("--profile", choices=["mixed", "double"], default=None,
-                   help="run one resident solve for a profiler and exit")
+    p.add_argument("--profile", choices=["mixed", "double", "paths"], default=None,
+                   help="mixed / double: two resident solves of the plate for a profiler; paths: every "
+                        "kernel family once (creation, solves, recovery, batches, Jacobi, ...); then exit")
+    p.add_argument("--profile-cells", type=int, default=100, help="paths: plate cells a side (100: the gate plate)")
+    p.add_argument("--profile-iterations", type=int, default=0,
+                   help="paths: run only this many iterations of each plate solve")
+    p.add_argument("--profile-extras", action="store_true",
+                   help="paths: only the kernels no other path launches")
+    p.add_argument("--profile-tolerance", type=float, default=None,
+                   help="paths: a looser relative residual, so each solve runs only a few iterations")
     p.add_argument("--workload", choices=["plate", "serving", "block"], default="plate",
                    help="plate: the 603k-DOF gate plate (default); serving: the mixed request stream; "
                         "block: the 5.3M-DOF printed block")
@@ -626,6 +756,8 @@ def main():
     args = p.parse_args()
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
+    if args.profile == "paths":
+        return run_profile_paths(args)
     if args.profile:
         return run_profile(args)
     if args.workload == "serving":

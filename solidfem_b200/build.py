@@ -12,6 +12,7 @@ import os
 import shutil
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
@@ -53,7 +54,7 @@ def build(verbose: bool = False, ptxas_info: bool = False) -> str:
     os.makedirs(BUILD, exist_ok=True)
     headers = [os.path.join(CSRC, h) for h in os.listdir(CSRC) if h.endswith(".h")]
     headers.append(os.path.join(HERE, "..", "include", "solidfem_b200.h"))
-    objects = []
+    objects, jobs = [], []
     for src, extra in CU_SOURCES.items():
         path = os.path.join(CSRC, src)
         obj = os.path.join(BUILD, src + ".o")
@@ -61,19 +62,21 @@ def build(verbose: bool = False, ptxas_info: bool = False) -> str:
             cmd = [NVCC, "-c", path, "-o", obj] + NVCC_COMMON + extra
             if ptxas_info:
                 cmd += ["-Xptxas", "-v"]
-            if verbose:
-                print(" ".join(cmd))
-            _run(cmd)
+            jobs.append(cmd)
         objects.append(obj)
     for src in CPP_SOURCES:
         path = os.path.join(CSRC, src)
         obj = os.path.join(BUILD, src + ".o")
         if _stale(obj, [path] + headers):
-            cmd = [CXX, "-c", path, "-o", obj] + CXX_FLAGS
+            jobs.append([CXX, "-c", path, "-o", obj] + CXX_FLAGS)
+        objects.append(obj)
+    # The translation units are independent: compile them side by side.
+    with ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 1))) as pool:
+        for cmd in jobs:
             if verbose:
                 print(" ".join(cmd))
-            _run(cmd)
-        objects.append(obj)
+        for f in [pool.submit(_run, cmd) for cmd in jobs]:
+            f.result()
     if _stale(LIB, objects):
         cmd = [NVCC, "-shared", "-o", LIB] + objects + ARCH + ["-ccbin", CXX, "-Xcompiler", "-fopenmp",
                                                               "-lgomp", "-cudart", "static"]
