@@ -22,7 +22,7 @@
 extern "C" {
 #endif
 
-#define SF_ABI_VERSION 2
+#define SF_ABI_VERSION 3
 
 /* Status codes. Named refusals mirror MeshError (crates/solidfem-mesh/src/error.rs),
  * ModelError (crates/solidfem-elastic/src/error.rs:23-119), MultigridError
@@ -112,6 +112,28 @@ sf_status sf_mesh_tets(const sf_mesh* mesh, uint32_t* out);
 /* QuadraticTetMesh::boundary_faces (quadratic.rs:89-124), ascending by sorted corners. */
 uint64_t sf_mesh_boundary_face_count(const sf_mesh* mesh);
 sf_status sf_mesh_boundary_faces(const sf_mesh* mesh, sf_boundary_face* out);
+
+/* The same meshes generated on CUDA device `device`: the nodes, ten-node tets and boundary faces
+ * are those the host builders above return, bit for bit, with the same refusals (TetMesh::new's
+ * checks, tet.rs:59-109). Edges and faces are bucketed by their smallest corner on the device in
+ * place of the host's sorts. The mesh also keeps its ten-node arrays on that device: a study built
+ * from it on the same device copies them there instead of uploading them. */
+/* box_tet_mesh + QuadraticTetMesh::from_linear (box_mesh.rs:22-80, quadratic.rs:24-124). */
+sf_status sf_box_tet_mesh_device(const double origin[3], const double size[3],
+                                 const uint64_t divisions[3], int32_t device, sf_mesh** out);
+/* TetMesh::new then QuadraticTetMesh::from_linear (tet.rs:59-109, quadratic.rs:24-124). */
+sf_status sf_mesh_from_linear_device(const double* positions, uint64_t n, const uint32_t* tets,
+                                     uint64_t ntets, int32_t device, sf_mesh** out);
+/* The demo's part mesh, build_mesh (demo/wasm/src/part.rs:135-189) over a PartGrid: ascending grid
+ * lines per axis (x_count, y_count, z_count lines), a unit box_tet_mesh of the cells, the
+ * tetrahedra whose centroid's cell lies in the hollow core dropped (wall_cells > 0: cross-section
+ * cells at least wall_cells in from every side, part.rs:114-122), the kept vertices numbered in
+ * order of first appearance and placed on their grid lines, then TetMesh::new and from_linear. */
+sf_status sf_part_tet_mesh_device(const double* x_lines, uint64_t x_count, const double* y_lines,
+                                  uint64_t y_count, const double* z_lines, uint64_t z_count,
+                                  uint64_t wall_cells, int32_t device, sf_mesh** out);
+/* The device holding the mesh's ten-node arrays, or -1 for a mesh built on the host. */
+int32_t sf_mesh_device(const sf_mesh* mesh);
 
 /* ---------------------------------------------------------------- model -------------------- */
 typedef struct sf_model sf_model;

@@ -154,6 +154,12 @@ SIGNATURES = {
     "sf_abi_version": (C.c_int32, []),
     "sf_box_tet_mesh": (C.c_int, [_P(C.c_double), _P(C.c_double), _P(C.c_uint64), _P(_V)]),
     "sf_mesh_from_linear": (C.c_int, [_P(C.c_double), C.c_uint64, _P(C.c_uint32), C.c_uint64, _P(_V)]),
+    "sf_box_tet_mesh_device": (C.c_int, [_P(C.c_double), _P(C.c_double), _P(C.c_uint64), C.c_int32, _P(_V)]),
+    "sf_mesh_from_linear_device": (C.c_int, [_P(C.c_double), C.c_uint64, _P(C.c_uint32), C.c_uint64, C.c_int32,
+                                             _P(_V)]),
+    "sf_part_tet_mesh_device": (C.c_int, [_P(C.c_double), C.c_uint64, _P(C.c_double), C.c_uint64, _P(C.c_double),
+                                          C.c_uint64, C.c_uint64, C.c_int32, _P(_V)]),
+    "sf_mesh_device": (C.c_int32, [_V]),
     "sf_mesh_destroy": (None, [_V]),
     "sf_mesh_node_count": (C.c_uint64, [_V]),
     "sf_mesh_tet_count": (C.c_uint64, [_V]),
@@ -358,21 +364,46 @@ class Mesh:
         _check(library().sf_mesh_boundary_faces(self._h, arr.ctypes.data_as(C.POINTER(BoundaryFace))))
         return arr[:n]
 
+    def device(self) -> Optional[int]:
+        """The CUDA device holding this mesh's ten-node arrays (a generated mesh), else None."""
+        d = int(library().sf_mesh_device(self._h))
+        return None if d < 0 else d
+
     @classmethod
-    def from_linear(cls, positions, tets) -> "Mesh":
-        """TetMesh::new + QuadraticTetMesh::from_linear (tet.rs:59-109, quadratic.rs:24-71)."""
+    def from_linear(cls, positions, tets, device: Optional[int] = None) -> "Mesh":
+        """TetMesh::new + QuadraticTetMesh::from_linear (tet.rs:59-109, quadratic.rs:24-71); on the
+        given CUDA device when `device` is set (the same mesh, generated there)."""
         p = np.ascontiguousarray(positions, dtype=np.float64)
         t = np.ascontiguousarray(tets, dtype=np.uint32)
         h = C.c_void_p()
-        _check(library().sf_mesh_from_linear(_dptr(p), len(p), _uptr(t), len(t), C.byref(h)))
+        if device is None:
+            _check(library().sf_mesh_from_linear(_dptr(p), len(p), _uptr(t), len(t), C.byref(h)))
+        else:
+            _check(library().sf_mesh_from_linear_device(_dptr(p), len(p), _uptr(t), len(t), int(device), C.byref(h)))
         return cls(h)
 
 
-def box_tet_mesh(origin, size, divisions) -> Mesh:
-    """box_tet_mesh (crates/solidfem-mesh/src/box_mesh.rs:22-80) upgraded to 10 nodes."""
+def box_tet_mesh(origin, size, divisions, device: Optional[int] = None) -> Mesh:
+    """box_tet_mesh (crates/solidfem-mesh/src/box_mesh.rs:22-80) upgraded to 10 nodes; generated on
+    the given CUDA device when `device` is set (the same mesh, bit for bit)."""
     h = C.c_void_p()
-    _check(library().sf_box_tet_mesh((C.c_double * 3)(*origin), (C.c_double * 3)(*size),
-                                     (C.c_uint64 * 3)(*[int(d) for d in divisions]), C.byref(h)))
+    o, sz = (C.c_double * 3)(*origin), (C.c_double * 3)(*size)
+    dv = (C.c_uint64 * 3)(*[int(d) for d in divisions])
+    if device is None:
+        _check(library().sf_box_tet_mesh(o, sz, dv, C.byref(h)))
+    else:
+        _check(library().sf_box_tet_mesh_device(o, sz, dv, int(device), C.byref(h)))
+    return Mesh(h)
+
+
+def part_tet_mesh(x_lines, y_lines, z_lines, wall_cells: int = 0, device: int = 0) -> Mesh:
+    """The demo's part mesh (demo/wasm/src/part.rs:135-189) over grid lines per axis, the hollow
+    core's cells dropped when wall_cells > 0, generated on a CUDA device."""
+    lines = [np.ascontiguousarray(v, dtype=np.float64) for v in (x_lines, y_lines, z_lines)]
+    h = C.c_void_p()
+    _check(library().sf_part_tet_mesh_device(_dptr(lines[0]), len(lines[0]), _dptr(lines[1]), len(lines[1]),
+                                             _dptr(lines[2]), len(lines[2]), int(wall_cells), int(device),
+                                             C.byref(h)))
     return Mesh(h)
 
 
@@ -1017,7 +1048,7 @@ def solve_batch(studies) -> list:
 
 
 __all__ = [
-    "FACE_DTYPE", "BoundaryFace", "Mesh", "box_tet_mesh", "Material", "ShellCore", "Quadrature", "Model", "Precision",
+    "FACE_DTYPE", "BoundaryFace", "Mesh", "box_tet_mesh", "part_tet_mesh", "Material", "ShellCore", "Quadrature", "Model", "Precision",
     "PcgOptions", "MultigridOptions", "Jacobi", "StudyOptions", "StudyBuilder", "StaticStudy", "StepOutcome",
     "Outcome", "Progress", "BuildProgress", "PointStress", "SolidfemError", "Status", "library", "SIGNATURES", "Kernel", "Solution",
     "solve_batch", "Server", "ServerOptions", "RequestResult", "System", "Recovery", "RecoveredField", "Stage",

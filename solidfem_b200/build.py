@@ -1,7 +1,7 @@
 """Builds libsolidfem_b200.so in-tree for sm_100a (B200).
 
-The CUDA sources are compiled with nvcc for compute_100a/sm_100a; assembly.cu and setup_device.cu
-additionally with -fmad=false so the FP64 stiffness and multigrid hierarchy are bit-identical to the
+The CUDA sources are compiled with nvcc for compute_100a/sm_100a; assembly.cu, setup_device.cu and
+mesh_device.cu additionally with -fmad=false so the FP64 stiffness and multigrid hierarchy are bit-identical to the
 reference's serial loops. The host
 C++ is compiled without multiply-add contraction for the same reason (setup must reproduce the
 reference's aggregates and coarse matrices to the bit). Objects go to solidfem_b200/_build/.
@@ -29,6 +29,7 @@ CU_SOURCES = {
     "solve.cu": [],
     "assembly.cu": ["-fmad=false", "-prec-div=true", "-prec-sqrt=true"],
     "setup_device.cu": ["-fmad=false", "-prec-div=true", "-prec-sqrt=true"],
+    "mesh_device.cu": ["-fmad=false", "-prec-div=true", "-prec-sqrt=true"],
 }
 CPP_SOURCES = ["mesh.cpp", "setup.cpp", "study.cpp", "server.cpp", "system.cpp"]
 CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-fopenmp", "-ffp-contract=off", "-fno-fast-math", "-Wall",

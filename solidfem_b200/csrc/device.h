@@ -122,6 +122,7 @@ struct DevLevel {
 struct DeviceSolver {
   int device = 0;
   cudaStream_t stream = nullptr;
+  std::shared_ptr<DeviceMesh> mesh_keep;  // a device-generated mesh whose arrays were copied on `stream`
   int precision = SF_PRECISION_SINGLE_STORAGE;
   bool storage_single = true, vector_single = false, flexible = false;
   bool multigrid = false;
@@ -190,6 +191,8 @@ sf_status dev_alloc(DeviceSolver& s, void** ptr, size_t bytes);
 void dev_free(DeviceSolver& s, void* ptr);
 void dev_free_all(DeviceSolver& s);
 sf_status cuda_check(cudaError_t e, const char* what);
+// Once per device: the stream-ordered pool keeps freed memory and reserves a first slab.
+void pool_setup(int device);
 
 // ------------------------------------------------------------------- setup (setup_device.cu)
 // FP64 numeric phases of the multigrid setup, bit-identical to the reference's serial loops.

@@ -7,6 +7,7 @@
 #include <cstring>
 #include <functional>
 #include <string>
+#include <memory>
 #include <vector>
 
 #include "../../include/solidfem_b200.h"
@@ -32,12 +33,22 @@ sf_status fail(sf_status status, const char* message);
 sf_error& error_slot();
 
 // ----------------------------------------------------------------------------- mesh
+// The ten-node arrays of a mesh built on a device, kept there for the studies made from it (a
+// study on the same device copies them device to device instead of uploading the host arrays).
+struct DeviceMesh {
+  int device = 0;
+  double* nodes = nullptr;   // node_count x 3
+  uint32_t* tets = nullptr;  // tet_count x 10
+  virtual ~DeviceMesh() {}
+};
+
 struct Mesh {
   vector<P3> nodes;
   vector<array<uint32_t, 10>> tets;
   vector<array<uint32_t, 4>> corners;
   size_t vertex_count = 0;
   vector<sf_boundary_face> faces;  // sorted by their sorted corners
+  std::shared_ptr<DeviceMesh> dev;  // set when the mesh was built on a device
 };
 
 sf_status build_box_mesh(const double origin[3], const double size[3], const uint64_t div[3],
@@ -45,6 +56,16 @@ sf_status build_box_mesh(const double origin[3], const double size[3], const uin
 sf_status build_linear_mesh(const double* positions, uint64_t n, const uint32_t* tets,
                             uint64_t ntets, Mesh& out);
 vector<vector<uint32_t>> face_connected_bodies(const Mesh& mesh);
+// The same meshes built on a CUDA device (mesh_device.cu), bit-identical to the host builders;
+// `out.dev` keeps the ten-node arrays on the device.
+sf_status build_box_mesh_device(const double origin[3], const double size[3], const uint64_t div[3], int device,
+                                Mesh& out);
+sf_status build_linear_mesh_device(const double* positions, uint64_t n, const uint32_t* tets, uint64_t ntets,
+                                   int device, Mesh& out);
+// The demo's part grid (demo/wasm/src/part.rs:135-189): grid lines per axis (counts[a] lines),
+// the cells of the hollow core dropped when wall_cells > 0.
+sf_status build_part_mesh_device(const double* const lines[3], const uint64_t counts[3], uint64_t wall_cells,
+                                 int device, Mesh& out);
 
 // ----------------------------------------------------------------------------- model
 enum MaterialKind { MATERIAL_UNIFORM = 0, MATERIAL_SHELL_CORE = 1, MATERIAL_CALLBACK = 2 };

@@ -439,6 +439,8 @@ struct sf_study {
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
     dev_free_all(solver);
+    if (solver.mesh_keep && solver.stream) cudaStreamSynchronize(solver.stream);
+    solver.mesh_keep.reset();
     if (solver.stream) cudaStreamDestroy(solver.stream);
   }
 };
@@ -475,6 +477,9 @@ void sf_study::orphan_recoveries() {
 
 static void release_builder_device(sf_builder* b) {
   dev_free_all(b->solver);
+  // the device-to-device copies from a generated mesh end before its arrays can be let go
+  if (b->solver.mesh_keep && b->solver.stream) cudaStreamSynchronize(b->solver.stream);
+  b->solver.mesh_keep.reset();
   if (b->solver.stream) cudaStreamDestroy(b->solver.stream);
   b->solver.stream = nullptr;
 }
@@ -546,6 +551,42 @@ sf_status sf_mesh_from_linear(const double* positions, uint64_t n, const uint32_
   *out = m.release();
   return SF_OK;
 }
+
+sf_status sf_box_tet_mesh_device(const double origin[3], const double size[3], const uint64_t divisions[3],
+                                 int32_t device, sf_mesh** out) {
+  if (!origin || !size || !divisions || !out) return fail(SF_INVALID_ARGUMENT, "null argument");
+  std::unique_ptr<sf_mesh> m(new sf_mesh);
+  if (sf_status s = build_box_mesh_device(origin, size, divisions, device, m->mesh)) return s;
+  *out = m.release();
+  return SF_OK;
+}
+
+sf_status sf_mesh_from_linear_device(const double* positions, uint64_t n, const uint32_t* tets, uint64_t ntets,
+                                     int32_t device, sf_mesh** out) {
+  if ((!positions && n) || (!tets && ntets) || !out) return fail(SF_INVALID_ARGUMENT, "null argument");
+  std::unique_ptr<sf_mesh> m(new sf_mesh);
+  if (sf_status s = build_linear_mesh_device(positions, n, tets, ntets, device, m->mesh)) return s;
+  *out = m.release();
+  return SF_OK;
+}
+
+sf_status sf_part_tet_mesh_device(const double* x_lines, uint64_t x_count, const double* y_lines, uint64_t y_count,
+                                  const double* z_lines, uint64_t z_count, uint64_t wall_cells, int32_t device,
+                                  sf_mesh** out) {
+  if (!x_lines || !y_lines || !z_lines || !out) return fail(SF_INVALID_ARGUMENT, "null argument");
+  const double* lines[3] = {x_lines, y_lines, z_lines};
+  const uint64_t counts[3] = {x_count, y_count, z_count};
+  for (int a = 0; a < 3; ++a)
+    for (uint64_t i = 0; i < counts[a]; ++i)
+      if (!std::isfinite(lines[a][i]) || (i > 0 && !(lines[a][i] > lines[a][i - 1])))
+        return fail(SF_MESH_INVALID_BOX, "grid lines must be finite and strictly ascending");
+  std::unique_ptr<sf_mesh> m(new sf_mesh);
+  if (sf_status s = build_part_mesh_device(lines, counts, wall_cells, device, m->mesh)) return s;
+  *out = m.release();
+  return SF_OK;
+}
+
+int32_t sf_mesh_device(const sf_mesh* m) { return m && m->mesh.dev ? m->mesh.dev->device : -1; }
 
 void sf_mesh_destroy(sf_mesh* m) { delete m; }
 uint64_t sf_mesh_node_count(const sf_mesh* m) { return m ? m->mesh.nodes.size() : 0; }
@@ -792,8 +833,16 @@ sf_status sf_builder_create(sf_model* model, const sf_study_options* options, sf
     release_builder_device(b.get());
     return e;
   }
-  copy_h2d(s, a.nodes, mesh.nodes.data(), nn * 24);
-  copy_h2d(s, a.tets, mesh.tets.data(), mesh.tets.size() * 40);
+  if (mesh.dev && mesh.dev->device == s.device) {
+    // a mesh generated on this device: its arrays are already here (the solver holds them until
+    // it is released, so the copies finish before they can be freed)
+    cudaMemcpyAsync(a.nodes, mesh.dev->nodes, nn * 24, cudaMemcpyDeviceToDevice, s.stream);
+    cudaMemcpyAsync(a.tets, mesh.dev->tets, mesh.tets.size() * 40, cudaMemcpyDeviceToDevice, s.stream);
+    s.mesh_keep = mesh.dev;
+  } else {
+    copy_h2d(s, a.nodes, mesh.nodes.data(), nn * 24);
+    copy_h2d(s, a.tets, mesh.tets.data(), mesh.tets.size() * 40);
+  }
   // each row's cursor starts at its node's first element
   vector<uint32_t> cursor(hp.row_node.size());
   for (size_t r = 0; r < cursor.size(); ++r) cursor[r] = hp.inc_start[hp.row_node[r]];

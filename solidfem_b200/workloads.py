@@ -2,9 +2,11 @@
 stream of mixed-size requests (Poisson arrivals).
 
 Every part is a structured hex grid split 6 tets per hex (box_tet_mesh) upgraded to Tet10; a tube
-drops the hollow cells of its box and keeps 2 cells through each wall, the way the reference's
-demo builds tubes (demo/wasm/src/part.rs:50-189). The part is clamped at x = 0 and carries a total
-force on its x = L end face, spread as a uniform traction in -z.
+is the reference demo's part grid (demo/wasm/src/part.rs:135-189) with 2 cells through each wall:
+a unit grid of the cells, the hollow core's tets dropped, the kept vertices numbered in order of
+first appearance and placed on the grid lines. Meshes are generated on a CUDA device when one is
+given (the same mesh, bit for bit), else on the host. The part is clamped at x = 0 and carries a
+total force on its x = L end face, spread as a uniform traction in -z.
 
 DOF targeting (this stream's own rule; the reference has none): the request draws a target DOF
 count, then the grid spacing is chosen so the Tet10 mesh has about that many DOFs, with at least
@@ -105,24 +107,57 @@ def _tube_layout(req: Request) -> tuple:
     return nx * h, ny * h, (nx, ny, ny)
 
 
-def build_mesh(req: Request) -> sf.Mesh:
-    """The request's Tet10 mesh."""
+TUBE_WALL_CELLS = 2
+
+
+def part_mesh_host(x_lines, y_lines, z_lines, wall_cells: int) -> sf.Mesh:
+    """The demo's part mesh (demo/wasm/src/part.rs:135-189) built on the host: a unit box_tet_mesh of
+    the cells; a tet is dropped when the cell of its centroid (summed as sum + p * 0.25 from zero,
+    then floored) lies in the hollow core (part.rs:114-122); the kept vertices are numbered in order
+    of first appearance in the kept tets and placed on their grid lines; then TetMesh::new and
+    from_linear. sf.part_tet_mesh generates the same mesh on a device."""
+    lines = [np.asarray(v, dtype=np.float64) for v in (x_lines, y_lines, z_lines)]
+    cells = tuple(len(v) - 1 for v in lines)
+    unit = sf.box_tet_mesh((0.0, 0.0, 0.0), tuple(float(c) for c in cells), cells)
+    pos = unit.nodes()[:unit.vertex_count()]
+    tets = unit.tets()[:, :4].astype(np.int64)
+    centroid = np.zeros((len(tets), 3))
+    for q in range(4):
+        centroid = centroid + pos[tets[:, q]] * 0.25
+    j, k = np.floor(centroid[:, 1]).astype(np.int64), np.floor(centroid[:, 2]).astype(np.int64)
+    hollow = ((wall_cells > 0) & (j >= wall_cells) & (j < cells[1] - wall_cells) &
+              (k >= wall_cells) & (k < cells[2] - wall_cells))
+    kept = tets[~hollow]
+    flat = kept.ravel()
+    used, first = np.unique(flat, return_index=True)
+    order = used[np.argsort(first, kind="stable")]  # vertices by first appearance
+    number = np.empty(len(pos), dtype=np.int64)
+    number[order] = np.arange(len(order))
+    grid = np.round(pos[order]).astype(np.int64)
+    positions = np.stack([lines[a][grid[:, a]] for a in range(3)], axis=1)
+    return sf.Mesh.from_linear(positions, number[kept].astype(np.uint32))
+
+
+def tube_lines(req: Request) -> tuple:
+    """Grid lines of the request's square tube (uniform cells, 2 through each wall)."""
+    length, side, (nx, ny, nz) = _tube_layout(req)
+    x = [length * i / nx for i in range(nx + 1)]
+    y = [side * j / ny for j in range(ny + 1)]
+    return x, y, list(y)
+
+
+def build_mesh(req: Request, device: int | None = None) -> sf.Mesh:
+    """The request's Tet10 mesh, generated on CUDA device `device` when it is given."""
     if req.kind == "plate":
         size = (req.length, req.width, req.thickness)
-        return sf.box_tet_mesh((0.0, 0.0, 0.0), size, _box_divisions(size, req.target_dofs, (2, 2, 2)))
+        return sf.box_tet_mesh((0.0, 0.0, 0.0), size, _box_divisions(size, req.target_dofs, (2, 2, 2)), device)
     if req.kind == "bar":
         size = (req.length, req.thickness, req.thickness)
-        return sf.box_tet_mesh((0.0, 0.0, 0.0), size, _box_divisions(size, req.target_dofs, (2, 2, 2)))
-    length, side, div = _tube_layout(req)
-    box = sf.box_tet_mesh((0.0, 0.0, 0.0), (length, side, side), div)
-    nodes, tets = box.nodes(), box.tets()[:, :4].astype(np.int64)
-    centroid = nodes[tets].mean(axis=1)
-    wall = req.thickness
-    hollow = ((centroid[:, 1] > wall) & (centroid[:, 1] < side - wall) &
-              (centroid[:, 2] > wall) & (centroid[:, 2] < side - wall))
-    kept = tets[~hollow]
-    used, inverse = np.unique(kept, return_inverse=True)
-    return sf.Mesh.from_linear(nodes[used], inverse.reshape(kept.shape).astype(np.uint32))
+        return sf.box_tet_mesh((0.0, 0.0, 0.0), size, _box_divisions(size, req.target_dofs, (2, 2, 2)), device)
+    x, y, z = tube_lines(req)
+    if device is None:
+        return part_mesh_host(x, y, z, TUBE_WALL_CELLS)
+    return sf.part_tet_mesh(x, y, z, TUBE_WALL_CELLS, device)
 
 
 def end_area(req: Request, mesh_nodes: np.ndarray) -> float:
@@ -134,9 +169,10 @@ def end_area(req: Request, mesh_nodes: np.ndarray) -> float:
     return side * side - (side - 2 * req.thickness) ** 2
 
 
-def build_model(req: Request, mesh: sf.Mesh | None = None) -> tuple:
-    """(mesh, model): clamped at x = 0, the total force as a uniform -z traction on the x = L face."""
-    mesh = mesh or build_mesh(req)
+def build_model(req: Request, mesh: sf.Mesh | None = None, device: int | None = None) -> tuple:
+    """(mesh, model): clamped at x = 0, the total force as a uniform -z traction on the x = L face;
+    the mesh generated on CUDA device `device` when it is given."""
+    mesh = mesh or build_mesh(req, device)
     nodes = mesh.nodes()
     model = sf.Model(mesh, sf.Material(req.youngs_modulus, req.poisson_ratio))
     xmax = float(nodes[:, 0].max())

@@ -26,7 +26,7 @@ def test_library_exports_every_declared_symbol():
     for name in names:
         assert hasattr(lib, name), name
         assert name in sf.SIGNATURES, name
-    assert lib.sf_abi_version() == 2
+    assert lib.sf_abi_version() == 3
 
 
 def test_status_messages():

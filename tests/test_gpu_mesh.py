@@ -1,0 +1,136 @@
+"""Meshes generated on the device (needs a B200) against the host builders, which the oracle pins
+(tests/test_capi_cpu.py): the same node coordinates to the bit, the same ten-node tets, the same
+boundary faces in the same order, and the same refusals with the same payloads
+(crates/solidfem-mesh/src/{box_mesh.rs:22-80, tet.rs:59-109, quadratic.rs:24-124},
+demo/wasm/src/part.rs:135-189). A study built from a generated mesh takes its arrays on the device
+and gives the same operator and answer as one built from the host mesh."""
+import numpy as np
+import pytest
+
+import solidfem_b200 as sf
+from solidfem_b200 import workloads as W
+from tests.helpers import mg_options
+
+pytestmark = pytest.mark.gpu
+
+
+def same_mesh(a: sf.Mesh, b: sf.Mesh):
+    assert a.vertex_count() == b.vertex_count()
+    assert np.array_equal(a.nodes().view(np.uint64), b.nodes().view(np.uint64))
+    assert np.array_equal(a.tets(), b.tets())
+    fa, fb = a.boundary_face_array(), b.boundary_face_array()
+    assert len(fa) == len(fb) and np.array_equal(fa, fb)
+
+
+@pytest.mark.parametrize("origin,size,div", [
+    ((0.0, 0.0, 0.0), (10.0, 1.0, 1.0), (12, 3, 3)),
+    ((-1.5, 0.25, 3.0), (7.3, 2.9, 1.1), (7, 5, 3)),
+    ((0.0, 0.0, 0.0), (100.0, 100.0, 0.8), (60, 60, 2)),
+    ((0.0, 0.0, 0.0), (1.0, 1.0, 1.0), (1, 1, 1)),
+])
+def test_box_mesh_matches_the_host_builder(origin, size, div):
+    dev = sf.box_tet_mesh(origin, size, div, device=0)
+    assert dev.device() == 0
+    host = sf.box_tet_mesh(origin, size, div)
+    assert host.device() is None
+    same_mesh(dev, host)
+
+
+def graded_lines(length, cells, wall=None, wall_cells=2):
+    """part.rs:57-86: a solid axis cut evenly, a tube axis with wall_cells cells across each wall
+    and as many across the hollow."""
+    if wall is None:
+        return [length * i / cells for i in range(cells + 1)]
+    inner, step = length - 2.0 * wall, wall / wall_cells
+    lines = [step * i for i in range(wall_cells + 1)]
+    lines += [wall + inner * i / wall_cells for i in range(1, wall_cells)]
+    lines += [length - wall + step * i for i in range(wall_cells + 1)]
+    return lines
+
+
+@pytest.mark.parametrize("wall_cells", [0, 2])
+def test_part_mesh_matches_its_host_restatement(wall_cells):
+    x = graded_lines(40.0, 16)
+    y = graded_lines(12.0, 0, wall=1.5, wall_cells=2) if wall_cells else graded_lines(12.0, 5)
+    z = graded_lines(9.0, 0, wall=1.2, wall_cells=2) if wall_cells else graded_lines(9.0, 4)
+    dev = sf.part_tet_mesh(x, y, z, wall_cells, device=0)
+    host = W.part_mesh_host(x, y, z, wall_cells)
+    same_mesh(dev, host)
+    if wall_cells:
+        nodes = dev.nodes()
+        assert dev.tet_count() < 6 * 16 * 6 * 6  # the hollow core's cells are gone
+        core = (nodes[:, 1] > 1.5) & (nodes[:, 1] < 10.5) & (nodes[:, 2] > 1.2) & (nodes[:, 2] < 7.8)
+        assert not core.any()
+
+
+def test_serving_parts_match_on_host_and_device():
+    seen = set()
+    for r in W.serving_stream():
+        if r.kind in seen or r.target_dofs > 80_000:
+            continue
+        seen.add(r.kind)
+        same_mesh(W.build_mesh(r, device=0), W.build_mesh(r))
+    assert seen == set(W.KINDS)
+
+
+def refusal(fn):
+    try:
+        fn()
+    except sf.SolidfemError as e:
+        return e.status, {k: e.detail.get(k) for k in ("tet", "node", "value")}
+    return None
+
+
+@pytest.mark.parametrize("case", ["out_of_range", "degenerate", "flat", "unused", "non_manifold", "non_finite"])
+def test_generated_refusals_match_the_host(case):
+    box = sf.box_tet_mesh((0.0, 0.0, 0.0), (3.0, 2.0, 1.0), (3, 2, 1))
+    pos = box.nodes()[:box.vertex_count()].copy()
+    tets = box.tets()[:, :4].astype(np.uint32).copy()
+    if case == "out_of_range":
+        tets[5, 2] = len(pos) + 7
+    elif case == "degenerate":
+        tets[4, [1, 2]] = tets[4, [2, 1]]
+    elif case == "flat":
+        pos = np.vstack([pos, [[0.0, 0.0, 0.0], [1.0, 0.0, 0.0], [0.0, 1.0, 0.0], [0.5, 0.5, 1e-14]]])
+        n = len(pos)
+        tets = np.vstack([tets, [[n - 4, n - 3, n - 2, n - 1]]]).astype(np.uint32)
+    elif case == "unused":
+        pos = np.vstack([pos, [[9.0, 9.0, 9.0]]])
+    elif case == "non_manifold":
+        tets = np.vstack([tets, tets[3:4]]).astype(np.uint32)
+    elif case == "non_finite":
+        pos[6, 1] = np.nan
+    host = refusal(lambda: sf.Mesh.from_linear(pos, tets))
+    dev = refusal(lambda: sf.Mesh.from_linear(pos, tets, device=0))
+    assert host is not None and dev is not None
+    assert dev[0] == host[0]
+    payload = {"out_of_range": ("tet", "node"), "degenerate": ("tet", "value"), "flat": ("tet", "value"),
+               "unused": ("node",), "non_manifold": (), "non_finite": ("node",)}[case]
+    for k in payload:
+        assert np.float64(dev[1][k]).tobytes() == np.float64(host[1][k]).tobytes(), (k, dev, host)
+
+
+def plate_model(mesh):
+    nodes = mesh.nodes()
+    model = sf.Model(mesh, sf.Material(2000.0, 0.35))
+    model.fix_nodes(np.nonzero(np.abs(nodes[:, 0]) < 1e-9)[0])
+    faces = mesh.boundary_face_array()
+    top = np.all(np.abs(nodes[faces["nodes"][:, :3], 2] - 0.8) < 1e-9, axis=1)
+    model.add_face_tractions(faces[top], (0.0, 0.0, -0.01))
+    return model
+
+
+def test_a_study_from_a_generated_mesh_is_the_same_study():
+    size, div = (100.0, 100.0, 0.8), (40, 40, 2)
+    host = sf.StaticStudy.new(plate_model(sf.box_tet_mesh((0, 0, 0), size, div)), mg_options(sf.Precision.MIXED))
+    dev = sf.StaticStudy.new(plate_model(sf.box_tet_mesh((0, 0, 0), size, div, device=0)),
+                             mg_options(sf.Precision.MIXED))
+    _, _, hv = host.matrix()
+    _, _, dv = dev.matrix()
+    assert np.array_equal(hv.view(np.uint64), dv.view(np.uint64))
+    # the generated mesh's arrays did not cross the host link
+    node_bytes = 24 * dev.mesh.node_count() + 40 * dev.mesh.tet_count()
+    assert dev.device_timing()["h2d_bytes"] <= host.device_timing()["h2d_bytes"] - node_bytes
+    oh, od = host.solve(), dev.solve()
+    assert oh.progress.iteration == od.progress.iteration
+    assert np.array_equal(host.displacements().view(np.uint64), dev.displacements().view(np.uint64))
