@@ -603,7 +603,10 @@ def run_block(args):
 
 def run_serving(args):
     """The serving stream (512 mixed bar / tube / plate requests, Poisson arrivals at 20/s, seed 0)
-    through the serving loop, then the same stream through serial plain FP64 GPU solves. Under
+    through the serving loop: paced at the arrivals with the models built first (meshes generated
+    on the device; the host-mesh build time is reported beside it), paced with each request's mesh
+    and model generated on the device at its arrival (inside its latency), and all submitted at
+    once; then the same stream through serial plain FP64 GPU solves. Under
     torchrun every rank serves its round-robin share of the stream on its own GPU (one server per
     GPU, no collective on the data path); rates are over all ranks, latencies pooled."""
     import concurrent.futures
@@ -619,9 +622,20 @@ def run_serving(args):
     torch.cuda.set_device(device)
     stream = W.serving_stream(count=args.requests, rate=args.rate)
     reqs = group.shard(stream)
+
+    def build_all(dev):
+        # every request's mesh and model, meshes generated on the device (dev) or on the host (None)
+        with concurrent.futures.ThreadPoolExecutor(max_workers=8) as pool:
+            return list(pool.map(lambda r: W.build_model(r, device=dev), reqs))
+
+    W.build_model(reqs[0], device=device)  # context and module load outside the clocks
     t0 = time.perf_counter()
-    with concurrent.futures.ThreadPoolExecutor(max_workers=8) as pool:
-        built = list(pool.map(W.build_model, reqs))
+    built = build_all(None)
+    prep_host = group.max(time.perf_counter() - t0)
+    del built
+    gc.collect()
+    t0 = time.perf_counter()
+    built = build_all(device)
     prep = group.max(time.perf_counter() - t0)
 
     def opts(precision):
@@ -635,16 +649,22 @@ def run_serving(args):
     gc.collect()
 
     def serve(models, paced):
+        """models None: each request's mesh and model are generated on the device when it arrives,
+        inside its latency (the latencies then run from arrival, not from submission)."""
         server = sf.Server(sf.ServerOptions(device=device, build_threads=args.build_threads))
         group.barrier()
         start = time.perf_counter()
-        ids = []
-        for r, (mesh, model) in zip(reqs, models):
+        ids, waited = [], []
+        for i, r in enumerate(reqs):
             delay = r.arrival - (time.perf_counter() - start)
             if paced and delay > 0:
                 time.sleep(delay)
+            mesh, model = models[i] if models is not None else W.build_model(r, device=device)
+            waited.append(max(0.0, time.perf_counter() - start - r.arrival) if models is None else 0.0)
             ids.append((server.submit(model, opts(sf.Precision.MIXED)), mesh.node_count()))
         results = [server.wait(rid) for rid, _ in ids]
+        for res, w in zip(results, waited):
+            res.latency_seconds += w
         makespan = time.perf_counter() - start
         stats = server.stats()
         for rid, n in ids:
@@ -676,9 +696,13 @@ def run_serving(args):
                      [f"{r.status.name}: {r.message}" for r in results if r.status != sf.Status.OK])))})
     del built
     gc.collect()
+    # each request's mesh and model generated on the device at its arrival, inside its latency
+    in_request = pooled(*serve(None, True))
+    mine["prep_in_request"] = {k: in_request[k] for k in ("solves_per_s", "makespan_s", "p50_latency_s",
+                                                           "p99_latency_s", "failed", "mean_batch_size")}
+    gc.collect()
     # the same requests all submitted at once: the loop's capacity rather than the arrival rate
-    with concurrent.futures.ThreadPoolExecutor(max_workers=8) as pool:
-        built = list(pool.map(W.build_model, reqs))
+    built = build_all(device)
     saturated = pooled(*serve(built, False))
     mine["saturated"] = {k: saturated[k] for k in ("solves_per_s", "makespan_s", "p50_latency_s", "p99_latency_s",
                                                    "failed", "mean_batch_size", "peak_reserved_gb")}
@@ -689,6 +713,7 @@ def run_serving(args):
                           "10k-600k DOF log-uniform, rel. residual 1e-8, HBM budget 150 GB, "
                           "requests under 100k DOF batched",
               "build_threads": args.build_threads, "model_prep_seconds": prep,
+              "model_prep_seconds_host_meshes": prep_host,
               "parallelism": f"replicas: {group.world} server(s), round-robin request shares"}
     if args.no_serial:
         if group.leader:
@@ -697,8 +722,7 @@ def run_serving(args):
         group.close()
         return 0
     # serial plain FP64 GPU solves of the same stream, one at a time in arrival order
-    with concurrent.futures.ThreadPoolExecutor(max_workers=8) as pool:
-        built = list(pool.map(W.build_model, reqs))
+    built = build_all(device)
     group.barrier()
     start = time.perf_counter()
     lat, serial_failed = [], 0
