@@ -669,7 +669,155 @@ sf_status check_box(const double size[3], const uint64_t div[3]) {
   return SF_OK;
 }
 
+// ------------------------------------------------------------------ consistent traction load
+// add_traction (crates/solidfem-elastic/src/loads.rs:10-41) on the device: the 6-point triangle
+// rule's measure per face and point, then per node the sum over its traction faces in list order
+// and over the points in order, starting from the node's nodal-force sum (build_load adds the
+// forces first, study.rs:696-735): the host's accumulation order, so the same bits.
+struct LoadFace {
+  uint32_t nodes[6];
+  double t[3];
+};
+
+__device__ __forceinline__ void triangle_point(int q, double* r, double* s, double* w) {
+  const double TA = 0.091576213509771, TB = 0.445948490915965;
+  const double WA = 0.109951743655322, WB = 0.223381589678011;
+  const double pts[6][3] = {{TA, TA, WA}, {1.0 - 2.0 * TA, TA, WA}, {TA, 1.0 - 2.0 * TA, WA},
+                            {TB, TB, WB}, {1.0 - 2.0 * TB, TB, WB}, {TB, 1.0 - 2.0 * TB, WB}};
+  *r = pts[q][0];
+  *s = pts[q][1];
+  *w = pts[q][2];
+}
+
+__global__ void face_measure_kernel(const LoadFace* __restrict__ faces, size_t nfaces, const double* __restrict__ pos,
+                                    double* __restrict__ measure) {
+  GRID_STRIDE(i, 6 * nfaces) {
+    const LoadFace& f = faces[i / 6];
+    const int q = (int)(i % 6);
+    double r, s, w;
+    triangle_point(q, &r, &s, &w);
+    const double l1 = 1.0 - r - s;
+    const double dr[6] = {-(4.0 * l1 - 1.0), 4.0 * r - 1.0, 0.0, 4.0 * (l1 - r), 4.0 * s, -4.0 * s};
+    const double ds[6] = {-(4.0 * l1 - 1.0), 0.0, 4.0 * s - 1.0, -4.0 * r, 4.0 * r, 4.0 * (l1 - s)};
+    double tr[3] = {0, 0, 0}, ts[3] = {0, 0, 0};
+    for (int n = 0; n < 6; ++n)
+      for (int a = 0; a < 3; ++a) {
+        const double p = pos[3 * (size_t)f.nodes[n] + a];
+        tr[a] += dr[n] * p;
+        ts[a] += ds[n] * p;
+      }
+    const double nm[3] = {tr[1] * ts[2] - tr[2] * ts[1], tr[2] * ts[0] - tr[0] * ts[2], tr[0] * ts[1] - tr[1] * ts[0]};
+    const double length = sqrt(nm[0] * nm[0] + nm[1] * nm[1] + nm[2] * nm[2]);
+    measure[i] = 0.5 * length * w;
+  }
+}
+
+__global__ void load_count_kernel(const LoadFace* __restrict__ faces, size_t nfaces, uint32_t* __restrict__ count) {
+  GRID_STRIDE(i, 6 * nfaces) atomicAdd(count + faces[i / 6].nodes[i % 6], 1u);
+}
+
+__global__ void load_fill_kernel(const LoadFace* __restrict__ faces, size_t nfaces, uint32_t* __restrict__ cursor,
+                                 uint32_t* __restrict__ entry) {
+  GRID_STRIDE(i, 6 * nfaces) entry[atomicAdd(cursor + faces[i / 6].nodes[i % 6], 1u)] = (uint32_t)i;  // 6 face + slot
+}
+
+// Node X: its force sum (or zero), then each traction face touching it in list order, each point
+// in order: load += t[a] * v[slot] * measure (loads.rs:30-38).
+__global__ void node_load_kernel(const LoadFace* __restrict__ faces, const double* __restrict__ measure,
+                                 const uint32_t* __restrict__ off, uint32_t* __restrict__ entry,
+                                 const uint32_t* __restrict__ forced, const double* __restrict__ force_sum,
+                                 uint32_t nforced, double* __restrict__ load, size_t n) {
+  GRID_STRIDE(x, n) {
+    uint32_t* e = entry + off[x];
+    const uint32_t m = off[x + 1] - off[x];
+    for (uint32_t i = 1; i < m; ++i) {  // list order: ascending face
+      const uint32_t v = e[i];
+      uint32_t j = i;
+      while (j > 0 && e[j - 1] > v) {
+        e[j] = e[j - 1];
+        --j;
+      }
+      e[j] = v;
+    }
+    double acc[3] = {0.0, 0.0, 0.0};
+    uint32_t lo = 0, hi = nforced;
+    while (lo < hi) {
+      const uint32_t mid = (lo + hi) >> 1;
+      if (forced[mid] < x)
+        lo = mid + 1;
+      else
+        hi = mid;
+    }
+    if (lo < nforced && forced[lo] == x)
+      for (int a = 0; a < 3; ++a) acc[a] = force_sum[3 * (size_t)lo + a];
+    for (uint32_t i = 0; i < m; ++i) {
+      const uint32_t face = e[i] / 6, slot = e[i] % 6;
+      const double* t = faces[face].t;
+      for (int q = 0; q < 6; ++q) {
+        double r, s, w;
+        triangle_point(q, &r, &s, &w);
+        const double l1 = 1.0 - r - s;
+        const double v[6] = {l1 * (2.0 * l1 - 1.0), r * (2.0 * r - 1.0), s * (2.0 * s - 1.0),
+                             4.0 * l1 * r, 4.0 * r * s, 4.0 * s * l1};
+        const double mq = measure[6 * (size_t)face + q];
+        for (int a = 0; a < 3; ++a) acc[a] += t[a] * v[slot] * mq;
+      }
+    }
+    for (int a = 0; a < 3; ++a) load[3 * x + a] = acc[a];
+  }
+}
+
 }  // namespace
+
+sf_status device_traction_load(const Mesh& mesh, const vector<std::pair<sf_boundary_face, array<double, 3>>>& tractions,
+                               vector<double>& load) {
+  if (!mesh.dev) return fail(SF_INVALID_ARGUMENT, "the mesh has no device arrays");
+  Build b;
+  if (sf_status s = begin(b, mesh.dev->device)) return s;
+  const size_t n = mesh.nodes.size(), nf = tractions.size();
+  // the nodal forces already summed into `load` on the host, for the nodes that carry one
+  vector<uint32_t> forced;
+  vector<double> force_sum;
+  for (size_t x = 0; x < n; ++x)
+    if (load[3 * x] != 0.0 || load[3 * x + 1] != 0.0 || load[3 * x + 2] != 0.0 || std::signbit(load[3 * x]) ||
+        std::signbit(load[3 * x + 1]) || std::signbit(load[3 * x + 2])) {
+      forced.push_back((uint32_t)x);
+      for (int a = 0; a < 3; ++a) force_sum.push_back(load[3 * x + a]);
+    }
+  vector<LoadFace> host(nf);
+  for (size_t j = 0; j < nf; ++j) {
+    for (int k = 0; k < 6; ++k) host[j].nodes[k] = tractions[j].first.nodes[k];
+    for (int a = 0; a < 3; ++a) host[j].t[a] = tractions[j].second[a];
+  }
+  LoadFace* faces = b.alloc<LoadFace>(nf);
+  double* measure = b.alloc<double>(6 * nf);
+  uint32_t* count = b.alloc<uint32_t>(n + 1);
+  uint32_t* off = b.alloc<uint32_t>(n + 1);
+  uint32_t* cursor = b.alloc<uint32_t>(n);
+  uint32_t* entry = b.alloc<uint32_t>(6 * nf);
+  uint32_t* dforced = b.alloc<uint32_t>(forced.size());
+  double* dsum = b.alloc<double>(force_sum.size());
+  double* dload = b.alloc<double>(3 * n);
+  if (b.err) return cuda_fail(b.err, "traction load");
+  cudaStream_t st = b.stream;
+  if (nf) cudaMemcpyAsync(faces, host.data(), nf * sizeof(LoadFace), cudaMemcpyHostToDevice, st);
+  if (!forced.empty()) {
+    cudaMemcpyAsync(dforced, forced.data(), forced.size() * 4, cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(dsum, force_sum.data(), force_sum.size() * 8, cudaMemcpyHostToDevice, st);
+  }
+  cudaMemsetAsync(count, 0, n * 4, st);
+  face_measure_kernel<<<grid_of(6 * nf), kT, 0, st>>>(faces, nf, mesh.dev->nodes, measure);
+  load_count_kernel<<<grid_of(6 * nf), kT, 0, st>>>(faces, nf, count);
+  scan(b, count, off, n);
+  cudaMemcpyAsync(cursor, off, n * 4, cudaMemcpyDeviceToDevice, st);
+  load_fill_kernel<<<grid_of(6 * nf), kT, 0, st>>>(faces, nf, cursor, entry);
+  node_load_kernel<<<grid_of(n), kT, 0, st>>>(faces, measure, off, entry, dforced, dsum, (uint32_t)forced.size(), dload,
+                                              n);
+  cudaMemcpyAsync(load.data(), dload, 3 * n * 8, cudaMemcpyDeviceToHost, st);
+  if (cudaError_t e = cudaStreamSynchronize(st)) return cuda_fail(e, "traction load");
+  if (cudaError_t e = cudaGetLastError()) return cuda_fail(e, "traction load");
+  return SF_OK;
+}
 
 sf_status build_box_mesh_device(const double origin[3], const double size[3], const uint64_t div[3], int device,
                                 Mesh& out) {

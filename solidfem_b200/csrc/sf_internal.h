@@ -8,6 +8,7 @@
 #include <functional>
 #include <string>
 #include <memory>
+#include <utility>
 #include <vector>
 
 #include "../../include/solidfem_b200.h"
@@ -66,6 +67,10 @@ sf_status build_linear_mesh_device(const double* positions, uint64_t n, const ui
 // the cells of the hollow core dropped when wall_cells > 0.
 sf_status build_part_mesh_device(const double* const lines[3], const uint64_t counts[3], uint64_t wall_cells,
                                  int device, Mesh& out);
+// build_load's consistent traction sums (loads.rs:10-41) on the device of a generated mesh, added
+// to the nodal-force sums already in `load`, in the host's order (the same bits).
+sf_status device_traction_load(const Mesh& mesh, const vector<std::pair<sf_boundary_face, array<double, 3>>>& tractions,
+                               vector<double>& load);
 
 // ----------------------------------------------------------------------------- model
 enum MaterialKind { MATERIAL_UNIFORM = 0, MATERIAL_SHELL_CORE = 1, MATERIAL_CALLBACK = 2 };

@@ -277,8 +277,10 @@ sf_status build_load(const Mesh& mesh, const Model& md, vector<double>& load) {
       }
       for (double c : tr.second)
         if (!std::isfinite(c)) return fail(SF_NON_FINITE_LOAD, "a traction is not finite");
-      add_traction(mesh, tr.first, tr.second.data(), load);
+      if (!mesh.dev) add_traction(mesh, tr.first, tr.second.data(), load);
     }
+    // a mesh generated on a device: the same sums, made there from its node array
+    if (mesh.dev) return device_traction_load(mesh, md.tractions, load);
   }
   return SF_OK;
 }

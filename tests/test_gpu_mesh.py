@@ -3,7 +3,8 @@
 boundary faces in the same order, and the same refusals with the same payloads
 (crates/solidfem-mesh/src/{box_mesh.rs:22-80, tet.rs:59-109, quadratic.rs:24-124},
 demo/wasm/src/part.rs:135-189). A study built from a generated mesh takes its arrays on the device
-and gives the same operator and answer as one built from the host mesh."""
+and gives the same operator and answer as one built from the host mesh; its consistent traction
+load is summed on the device (crates/solidfem-elastic/src/loads.rs:10-41) to the same bits."""
 import numpy as np
 import pytest
 
@@ -134,3 +135,39 @@ def test_a_study_from_a_generated_mesh_is_the_same_study():
     oh, od = host.solve(), dev.solve()
     assert oh.progress.iteration == od.progress.iteration
     assert np.array_equal(host.displacements().view(np.uint64), dev.displacements().view(np.uint64))
+
+
+def loaded_model(mesh):
+    """Two traction sets sharing edge nodes, forces on nodes inside and outside the loaded faces."""
+    nodes = mesh.nodes()
+    model = sf.Model(mesh, sf.Material(200000.0, 0.3))
+    model.fix_nodes(np.nonzero(np.abs(nodes[:, 0]) < 1e-9)[0])
+    faces = mesh.boundary_face_array()
+    corner = nodes[faces["nodes"][:, :3]]
+    end = np.all(np.abs(corner[:, :, 0] - 10.0) < 1e-9, axis=1)
+    top = np.all(np.abs(corner[:, :, 2] - 1.0) < 1e-9, axis=1)
+    model.add_face_tractions(faces[end], (0.0, 3.0, -7.0))
+    model.add_face_tractions(faces[top], (0.5, 0.0, -1.25))
+    tip = np.nonzero(np.abs(nodes[:, 0] - 10.0) < 1e-9)[0]
+    for node in list(tip[:3]) + [int(len(nodes) // 2)]:
+        model.add_nodal_force(int(node), (1.0, -2.0, 0.75))
+    return model
+
+
+def test_generated_traction_load_matches_the_host_and_the_oracle(oracle):
+    size, div = (10.0, 1.0, 1.0), (12, 3, 3)
+    host = sf.StaticStudy.new(loaded_model(sf.box_tet_mesh((0, 0, 0), size, div)), mg_options(sf.Precision.DOUBLE))
+    dev = sf.StaticStudy.new(loaded_model(sf.box_tet_mesh((0, 0, 0), size, div, device=0)),
+                             mg_options(sf.Precision.DOUBLE))
+    assert np.array_equal(host.rhs().view(np.uint64), dev.rhs().view(np.uint64))
+    assert np.any(dev.rhs() != 0.0)
+    # the oracle's build_load on the same model (traction faces and forces in the same order)
+    om = oracle.Mesh.box(size, div)
+    on = om.nodes()
+    end, top = oracle.faces_on_plane(om, 0, 10.0, on), oracle.faces_on_plane(om, 2, 1.0, on)
+    tip = np.nonzero(np.abs(on[:, 0] - 10.0) < 1e-9)[0]
+    forces = [(int(n), (1.0, -2.0, 0.75)) for n in list(tip[:3]) + [int(len(on) // 2)]]
+    ref = oracle.Study(om, oracle.uniform(200000.0, 0.3), oracle.default_options(precision=oracle.DOUBLE),
+                       oracle.nodes_on_plane(on, 0, 0.0), end + top,
+                       [[0.0, 3.0, -7.0]] * len(end) + [[0.5, 0.0, -1.25]] * len(top), forces=forces)
+    assert np.array_equal(ref.rhs().view(np.uint64), dev.rhs().view(np.uint64))
