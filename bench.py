@@ -418,8 +418,19 @@ def run_profile(args):
 
 
 def profile_extras(sf, torch, tol, note):
-    """The kernels the other profiled paths never launch: quadrature-point positions for a material
-    field, the degree-1 smoother's plain add, and the energy products of a row-group system product."""
+    """The kernels the other profiled paths never launch: mesh generation on the device (the gate
+    plate's box, a hollow part grid, a study's traction load from a generated mesh), quadrature-point
+    positions for a material field, the degree-1 smoother's plain add, and the energy products of a
+    row-group system product."""
+    plate = sf.box_tet_mesh((0.0, 0.0, 0.0), SIZE, DIVISIONS, 0)
+    lines = [[40.0 * i / 160 for i in range(161)], [12.0 * j / 24 for j in range(25)], [12.0 * k / 24 for k in range(25)]]
+    sf.part_tet_mesh(*lines, wall_cells=2, device=0)
+    pn = plate.nodes()
+    pm = sf.Model(plate, sf.Material(YOUNGS, POISSON))
+    pm.fix_nodes(np.nonzero(np.abs(pn[:, 0]) < 1e-9)[0])
+    pf = plate.boundary_face_array()
+    pm.add_face_tractions(pf[np.all(np.abs(pn[pf["nodes"][:, :3], 2] - SIZE[2]) < 1e-9, axis=1)], (0.0, 0.0, -PRESSURE))
+    sf.StudyBuilder(pm, options(sf, sf.Precision.MIXED, 0))  # numbering, pattern, device load
     m = sf.box_tet_mesh((0.0, 0.0, 0.0), (10.0, 1.0, 1.0), (20, 4, 4))
     nd = m.nodes()
     model = sf.Model(m, lambda pos: sf.Material(200000.0 if pos[0] < 5.0 else 100000.0, 0.3))
