@@ -767,7 +767,186 @@ __global__ void node_load_kernel(const LoadFace* __restrict__ faces, const doubl
   }
 }
 
+// ------------------------------------------------------------------ the free-node pattern
+// build_pattern on the device (assembly.rs:55-81, csr.rs:19-71): the node-to-element incidence
+// (each node's elements ascending), each free row's node and assembly cursor, and each row's
+// columns: the free numbers of the nodes of its node's elements, sorted and each kept once. A warp
+// takes a row: its candidates (10 per element) go to shared memory, a bitonic sort orders them
+// (fixed nodes, numbered 0xffffffff, sort last and are dropped), and a ballot keeps the first of
+// each run. A row with more than kPatternCap candidates sends the whole mesh back to the host build.
+constexpr int kPatternCap = 512;
+constexpr int kPatternWarps = 8;
+
+__global__ void incidence_count_kernel(const uint32_t* __restrict__ tets10, size_t n, uint32_t* __restrict__ count) {
+  GRID_STRIDE(i, n) atomicAdd(count + tets10[i], 1u);
+}
+
+__global__ void incidence_fill_kernel(const uint32_t* __restrict__ tets10, size_t n, uint32_t* __restrict__ cursor,
+                                      uint32_t* __restrict__ inc) {
+  GRID_STRIDE(i, n) inc[atomicAdd(cursor + tets10[i], 1u)] = (uint32_t)(i / 10);
+}
+
+__global__ void incidence_sort_kernel(const uint32_t* __restrict__ start, uint32_t* __restrict__ inc, size_t nodes) {
+  GRID_STRIDE(v, nodes) {
+    uint32_t* l = inc + start[v];
+    const uint32_t m = start[v + 1] - start[v];
+    for (uint32_t i = 1; i < m; ++i) {
+      const uint32_t x = l[i];
+      uint32_t j = i;
+      while (j > 0 && l[j - 1] > x) {
+        l[j] = l[j - 1];
+        --j;
+      }
+      l[j] = x;
+    }
+  }
+}
+
+__global__ void row_node_kernel(const uint32_t* __restrict__ free, const uint32_t* __restrict__ start, size_t nodes,
+                                uint32_t* __restrict__ row_node, uint32_t* __restrict__ cursor) {
+  GRID_STRIDE(v, nodes) {
+    const uint32_t f = free[v];
+    if (f != 0xffffffffu) {
+      row_node[f] = (uint32_t)v;
+      cursor[f] = start[v];  // the row's first element for the sliced assembly
+    }
+  }
+}
+
+template <bool FILL>
+__global__ void __launch_bounds__(32 * kPatternWarps) pattern_rows_kernel(
+    uint32_t rows, const uint32_t* __restrict__ row_node, const uint32_t* __restrict__ inc_start,
+    const uint32_t* __restrict__ inc, const uint32_t* __restrict__ tets10, const uint32_t* __restrict__ free,
+    const uint32_t* __restrict__ starts, uint32_t* __restrict__ out, unsigned* __restrict__ overflow) {
+  __shared__ uint32_t buf[kPatternWarps][kPatternCap];
+  const unsigned lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  uint32_t* b = buf[w];
+  for (uint32_t r = blockIdx.x * kPatternWarps + w; r < rows; r += gridDim.x * kPatternWarps) {
+    const uint32_t node = row_node[r], k0 = inc_start[node], k1 = inc_start[node + 1];
+    const uint32_t cand = 10 * (k1 - k0);
+    if (cand > (uint32_t)kPatternCap) {
+      if (lane == 0) {
+        atomicOr(overflow, 1u);
+        if (!FILL) out[r] = 0;
+      }
+      continue;
+    }
+    uint32_t p = 32;
+    while (p < cand) p <<= 1;
+    for (uint32_t i = lane; i < p; i += 32)
+      b[i] = i < cand ? free[tets10[10 * (size_t)inc[k0 + i / 10] + i % 10]] : 0xffffffffu;
+    __syncwarp();
+    for (uint32_t k = 2; k <= p; k <<= 1)
+      for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+        for (uint32_t i = lane; i < p; i += 32) {
+          const uint32_t ixj = i ^ j;
+          if (ixj > i) {
+            const uint32_t x = b[i], y = b[ixj];
+            if ((x > y) == ((i & k) == 0)) {
+              b[i] = y;
+              b[ixj] = x;
+            }
+          }
+        }
+        __syncwarp();
+      }
+    uint32_t count = 0;
+    for (uint32_t i0 = 0; i0 < p; i0 += 32) {
+      const uint32_t i = i0 + lane;
+      const uint32_t v = b[i];
+      const bool keep = v != 0xffffffffu && (i == 0 || b[i - 1] != v);
+      const unsigned m = __ballot_sync(0xffffffffu, keep);
+      if (FILL && keep) out[starts[r] + count + __popc(m & ((1u << lane) - 1u))] = v;
+      count += __popc(m);
+    }
+    if (!FILL && lane == 0) out[r] = count;
+    __syncwarp();
+  }
+}
+
 }  // namespace
+
+sf_status device_pattern(const Mesh& mesh, const vector<uint32_t>& free, size_t free_count, DevicePattern& out,
+                         vector<uint32_t>& host_starts, bool* fallback) {
+  *fallback = false;
+  if (!mesh.dev) return fail(SF_INVALID_ARGUMENT, "the mesh has no device arrays");
+  Build b;
+  if (sf_status s = begin(b, mesh.dev->device)) return s;
+  const size_t nn = mesh.nodes.size(), nt = 10 * mesh.tets.size();
+  auto keep = [&](uint32_t** p, size_t count) {
+    *p = b.alloc<uint32_t>(count, true);
+    if (*p) out.allocations.push_back({*p, std::max<size_t>(count, 1) * 4 + 64});
+  };
+  auto release = [&]() {
+    for (auto& a : out.allocations) cudaFreeAsync(a.first, b.stream);
+    out = DevicePattern();
+  };
+  keep(&out.inc_start, nn + 1);
+  keep(&out.inc, nt);
+  keep(&out.row_node, free_count);
+  keep(&out.cursor, free_count);
+  keep(&out.starts, free_count + 1);
+  uint32_t* dfree = b.alloc<uint32_t>(nn);
+  uint32_t* count = b.alloc<uint32_t>(nn);
+  uint32_t* cursor = b.alloc<uint32_t>(nn);
+  uint32_t* rows = b.alloc<uint32_t>(free_count);
+  unsigned* overflow = b.alloc<unsigned>(1);
+  if (b.err) {
+    release();
+    return cuda_fail(b.err, "pattern");
+  }
+  cudaStream_t st = b.stream;
+  cudaMemcpyAsync(dfree, free.data(), nn * 4, cudaMemcpyHostToDevice, st);
+  cudaMemsetAsync(count, 0, nn * 4, st);
+  cudaMemsetAsync(overflow, 0, 4, st);
+  incidence_count_kernel<<<grid_of(nt), kT, 0, st>>>(mesh.dev->tets, nt, count);
+  scan(b, count, out.inc_start, nn);
+  cudaMemcpyAsync(cursor, out.inc_start, nn * 4, cudaMemcpyDeviceToDevice, st);
+  incidence_fill_kernel<<<grid_of(nt), kT, 0, st>>>(mesh.dev->tets, nt, cursor, out.inc);
+  incidence_sort_kernel<<<grid_of(nn), kT, 0, st>>>(out.inc_start, out.inc, nn);
+  row_node_kernel<<<grid_of(nn), kT, 0, st>>>(dfree, out.inc_start, nn, out.row_node, out.cursor);
+  const unsigned grid = (unsigned)std::max<size_t>(1, std::min<size_t>((free_count + kPatternWarps - 1) / kPatternWarps,
+                                                                       148 * 16));
+  pattern_rows_kernel<false><<<grid, 32 * kPatternWarps, 0, st>>>((uint32_t)free_count, out.row_node, out.inc_start,
+                                                                  out.inc, mesh.dev->tets, dfree, nullptr, rows, overflow);
+  scan(b, rows, out.starts, free_count);
+  unsigned over = 0;
+  uint32_t blocks = 0;
+  cudaMemcpyAsync(&over, overflow, 4, cudaMemcpyDeviceToHost, st);
+  cudaMemcpyAsync(&blocks, out.starts + free_count, 4, cudaMemcpyDeviceToHost, st);
+  if (cudaError_t e = cudaStreamSynchronize(st)) {
+    release();
+    return cuda_fail(e, "pattern");
+  }
+  if (over || b.err) {
+    const cudaError_t err = b.err;
+    release();
+    if (err) return cuda_fail(err, "pattern");
+    *fallback = true;
+    return SF_OK;
+  }
+  out.blocks = blocks;
+  keep(&out.cols, blocks);
+  if (b.err) {
+    const cudaError_t err = b.err;
+    release();
+    return cuda_fail(err, "pattern");
+  }
+  pattern_rows_kernel<true><<<grid, 32 * kPatternWarps, 0, st>>>((uint32_t)free_count, out.row_node, out.inc_start,
+                                                                 out.inc, mesh.dev->tets, dfree, out.starts, out.cols,
+                                                                 overflow);
+  host_starts.resize(free_count + 1);
+  cudaMemcpyAsync(host_starts.data(), out.starts, (free_count + 1) * 4, cudaMemcpyDeviceToHost, st);
+  if (cudaError_t e = cudaStreamSynchronize(st)) {
+    release();
+    return cuda_fail(e, "pattern");
+  }
+  if (cudaError_t e = cudaGetLastError()) {
+    release();
+    return cuda_fail(e, "pattern");
+  }
+  return SF_OK;
+}
 
 sf_status device_traction_load(const Mesh& mesh, const vector<std::pair<sf_boundary_face, array<double, 3>>>& tractions,
                                vector<double>& load) {

@@ -67,6 +67,23 @@ sf_status build_linear_mesh_device(const double* positions, uint64_t n, const ui
 // the cells of the hollow core dropped when wall_cells > 0.
 sf_status build_part_mesh_device(const double* const lines[3], const uint64_t counts[3], uint64_t wall_cells,
                                  int device, Mesh& out);
+// build_pattern on the device of a generated mesh: the node-to-element incidence (each node's
+// elements ascending), each free row's node and assembly cursor, and the block pattern (starts and
+// sorted columns) in device arrays the caller takes over (`allocations`: pointer and bytes of each,
+// from the device's stream-ordered pool), the row starts also on the host. *fallback is set, and
+// nothing kept, when a row has too many candidate columns for the device build.
+struct DevicePattern {
+  uint32_t* inc_start = nullptr;  // node_count + 1
+  uint32_t* inc = nullptr;        // 10 x tet_count
+  uint32_t* row_node = nullptr;   // free rows
+  uint32_t* cursor = nullptr;     // free rows
+  uint32_t* starts = nullptr;     // free rows + 1
+  uint32_t* cols = nullptr;       // blocks
+  size_t blocks = 0;
+  vector<std::pair<void*, size_t>> allocations;
+};
+sf_status device_pattern(const Mesh& mesh, const vector<uint32_t>& free, size_t free_count, DevicePattern& out,
+                         vector<uint32_t>& host_starts, bool* fallback);
 // build_load's consistent traction sums (loads.rs:10-41) on the device of a generated mesh, added
 // to the nodal-force sums already in `load`, in the host's order (the same bits).
 sf_status device_traction_load(const Mesh& mesh, const vector<std::pair<sf_boundary_face, array<double, 3>>>& tractions,

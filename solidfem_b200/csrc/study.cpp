@@ -477,6 +477,20 @@ void sf_study::orphan_recoveries() {
   recoveries.clear();
 }
 
+// Frees a device-built pattern that no solver took over, on a stream of its own (no device-wide wait).
+static void release_pattern(int device, DevicePattern& dp) {
+  if (dp.allocations.empty()) return;
+  int prev = 0;
+  cudaGetDevice(&prev);
+  cudaSetDevice(device);
+  cudaStream_t st = nullptr;
+  cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+  for (auto& al : dp.allocations) cudaFreeAsync(al.first, st);
+  cudaStreamDestroy(st);
+  dp.allocations.clear();
+  cudaSetDevice(prev);
+}
+
 static void release_builder_device(sf_builder* b) {
   dev_free_all(b->solver);
   // the device-to-device copies from a generated mesh end before its arrays can be let go
@@ -763,7 +777,30 @@ sf_status sf_builder_create(sf_model* model, const sf_study_options* options, sf
   for (size_t n = 0; n < nn; ++n)
     if (!is_fixed[n]) b->free[n] = (uint32_t)b->free_count++;
   double t0 = now_seconds();
-  build_pattern(mesh, b->free, b->free_count, b->threads, b->pattern);
+  // A mesh generated on the study's device: the incidence and the pattern are built there too (the
+  // same arrays); the host build otherwise, or when a row is too wide for the device build.
+  DevicePattern dp;
+  bool host_pattern = true;
+  if (mesh.dev && mesh.dev->device == b->options.device) {
+    if (sf_status e = device_pattern(mesh, b->free, b->free_count, dp, b->pattern.starts, &host_pattern)) return e;
+    if (!host_pattern) {
+      b->pattern.cols.resize(dp.blocks);
+      if (dp.blocks &&
+          cudaMemcpy(b->pattern.cols.data(), dp.cols, dp.blocks * 4, cudaMemcpyDeviceToHost) != cudaSuccess) {
+        release_pattern(mesh.dev->device, dp);
+        return cuda_check(cudaGetLastError(), "pattern copy");
+      }
+    }
+  }
+  struct DropPattern {  // device pattern arrays not yet handed to the solver are released on a refusal
+    DevicePattern& dp;
+    int device;
+    bool armed = true;
+    ~DropPattern() {
+      if (armed) release_pattern(device, dp);
+    }
+  } drop{dp, b->options.device};
+  if (host_pattern) build_pattern(mesh, b->free, b->free_count, b->threads, b->pattern);
   if (sf_status st = checks.get()) {
     error_slot() = helper_error;
     return st;
@@ -813,23 +850,39 @@ sf_status sf_builder_create(sf_model* model, const sf_study_options* options, sf
   size_t blocks = b->pattern.cols.size();
   size_t budget = b->options.device_memory_budget;
   const HostPattern& hp = b->pattern;
-  size_t need = nn * 24 + mesh.tets.size() * 40 + mesh.tets.size() * 495 * 8 + blocks * (4 + 72) +
-                (hp.inc_start.size() + hp.inc.size() + 2 * hp.row_node.size()) * 4;
+  const size_t incidence = host_pattern ? hp.inc_start.size() + hp.inc.size() + 2 * hp.row_node.size()
+                                        : (nn + 1) + 10 * mesh.tets.size() + 2 * b->free_count;
+  size_t need = nn * 24 + mesh.tets.size() * 40 + mesh.tets.size() * 495 * 8 + blocks * (4 + 72) + incidence * 4;
   if (budget && need > budget) return fail(SF_DEVICE_MEMORY_BUDGET, "the assembly does not fit the device memory budget");
   sf_status e = SF_OK;
   if (!e) e = dev_alloc(s, (void**)&a.nodes, nn * 24);
   if (!e) e = dev_alloc(s, (void**)&a.tets, mesh.tets.size() * 40);
   if (!e) e = dev_alloc(s, (void**)&a.ke, mesh.tets.size() * 495 * 8);
-  if (!e) e = dev_alloc(s, (void**)&a.inc_start, hp.inc_start.size() * 4);
-  if (!e) e = dev_alloc(s, (void**)&a.inc, std::max<size_t>(1, hp.inc.size()) * 4);
-  if (!e) e = dev_alloc(s, (void**)&a.row_node, std::max<size_t>(1, hp.row_node.size()) * 4);
-  if (!e) e = dev_alloc(s, (void**)&a.cursor, std::max<size_t>(1, hp.row_node.size()) * 4);
-  if (!e) e = dev_alloc(s, (void**)&a.error, 8);
   s.system.rows = (uint32_t)b->free_count;
   s.system.rb = s.system.cb = 3;
   s.system.blocks = blocks;
-  if (!e) e = dev_alloc(s, (void**)&s.system.starts, (b->free_count + 1) * 4);
-  if (!e) e = dev_alloc(s, (void**)&s.system.cols, std::max<size_t>(1, blocks) * 4);
+  if (host_pattern) {
+    if (!e) e = dev_alloc(s, (void**)&a.inc_start, hp.inc_start.size() * 4);
+    if (!e) e = dev_alloc(s, (void**)&a.inc, std::max<size_t>(1, hp.inc.size()) * 4);
+    if (!e) e = dev_alloc(s, (void**)&a.row_node, std::max<size_t>(1, hp.row_node.size()) * 4);
+    if (!e) e = dev_alloc(s, (void**)&a.cursor, std::max<size_t>(1, hp.row_node.size()) * 4);
+    if (!e) e = dev_alloc(s, (void**)&s.system.starts, (b->free_count + 1) * 4);
+    if (!e) e = dev_alloc(s, (void**)&s.system.cols, std::max<size_t>(1, blocks) * 4);
+  } else {
+    // the device-built arrays become the solver's own
+    a.inc_start = dp.inc_start;
+    a.inc = dp.inc;
+    a.row_node = dp.row_node;
+    a.cursor = dp.cursor;
+    s.system.starts = dp.starts;
+    s.system.cols = dp.cols;
+    for (auto& al : dp.allocations) {
+      s.owned.push_back(al);
+      s.bytes += al.second;
+    }
+    drop.armed = false;
+  }
+  if (!e) e = dev_alloc(s, (void**)&a.error, 8);
   if (!e) e = dev_alloc(s, &s.system.vals, std::max<size_t>(1, blocks) * 72);
   if (e) {
     release_builder_device(b.get());
@@ -845,19 +898,23 @@ sf_status sf_builder_create(sf_model* model, const sf_study_options* options, sf
     copy_h2d(s, a.nodes, mesh.nodes.data(), nn * 24);
     copy_h2d(s, a.tets, mesh.tets.data(), mesh.tets.size() * 40);
   }
-  // each row's cursor starts at its node's first element
-  vector<uint32_t> cursor(hp.row_node.size());
-  for (size_t r = 0; r < cursor.size(); ++r) cursor[r] = hp.inc_start[hp.row_node[r]];
-  copy_h2d(s, a.inc_start, hp.inc_start.data(), hp.inc_start.size() * 4);
-  if (!hp.inc.empty()) copy_h2d(s, a.inc, hp.inc.data(), hp.inc.size() * 4);
-  if (!cursor.empty()) {
-    copy_h2d(s, a.row_node, hp.row_node.data(), cursor.size() * 4);
-    copy_h2d(s, a.cursor, cursor.data(), cursor.size() * 4);
+  if (host_pattern) {
+    // each row's cursor starts at its node's first element
+    vector<uint32_t> cursor(hp.row_node.size());
+    for (size_t r = 0; r < cursor.size(); ++r) cursor[r] = hp.inc_start[hp.row_node[r]];
+    copy_h2d(s, a.inc_start, hp.inc_start.data(), hp.inc_start.size() * 4);
+    if (!hp.inc.empty()) copy_h2d(s, a.inc, hp.inc.data(), hp.inc.size() * 4);
+    if (!cursor.empty()) {
+      copy_h2d(s, a.row_node, hp.row_node.data(), cursor.size() * 4);
+      copy_h2d(s, a.cursor, cursor.data(), cursor.size() * 4);
+    }
+    copy_h2d(s, s.system.starts, b->pattern.starts.data(), (b->free_count + 1) * 4);
+    copy_h2d(s, s.system.cols, b->pattern.cols.data(), blocks * 4);
+  } else {
+    s.d2h_bytes += (b->free_count + 1) * 4 + blocks * 4;  // the pattern's host copy
   }
   unsigned long long none = ~0ull;
   copy_h2d(s, a.error, &none, 8);
-  copy_h2d(s, s.system.starts, b->pattern.starts.data(), (b->free_count + 1) * 4);
-  copy_h2d(s, s.system.cols, b->pattern.cols.data(), blocks * 4);
   if ((e = make_row_groups(s, s.system, b->pattern.starts.data(), 72))) {
     release_builder_device(b.get());
     return e;

@@ -126,12 +126,15 @@ def test_a_study_from_a_generated_mesh_is_the_same_study():
     host = sf.StaticStudy.new(plate_model(sf.box_tet_mesh((0, 0, 0), size, div)), mg_options(sf.Precision.MIXED))
     dev = sf.StaticStudy.new(plate_model(sf.box_tet_mesh((0, 0, 0), size, div, device=0)),
                              mg_options(sf.Precision.MIXED))
-    _, _, hv = host.matrix()
-    _, _, dv = dev.matrix()
+    # the pattern built on the device (incidence, sorted unique columns) is the host's
+    hr, hc, hv = host.matrix()
+    dr, dc, dv = dev.matrix()
+    assert np.array_equal(hr, dr) and np.array_equal(hc, dc)
     assert np.array_equal(hv.view(np.uint64), dv.view(np.uint64))
-    # the generated mesh's arrays did not cross the host link
+    # neither the generated mesh's arrays nor the pattern and incidence crossed the host link
     node_bytes = 24 * dev.mesh.node_count() + 40 * dev.mesh.tet_count()
-    assert dev.device_timing()["h2d_bytes"] <= host.device_timing()["h2d_bytes"] - node_bytes
+    pattern_bytes = 4 * (len(hc) // 9) + 40 * dev.mesh.tet_count()
+    assert dev.device_timing()["h2d_bytes"] <= host.device_timing()["h2d_bytes"] - node_bytes - pattern_bytes
     oh, od = host.solve(), dev.solve()
     assert oh.progress.iteration == od.progress.iteration
     assert np.array_equal(host.displacements().view(np.uint64), dev.displacements().view(np.uint64))
@@ -171,3 +174,30 @@ def test_generated_traction_load_matches_the_host_and_the_oracle(oracle):
                        oracle.nodes_on_plane(on, 0, 0.0), end + top,
                        [[0.0, 3.0, -7.0]] * len(end) + [[0.5, 0.0, -1.25]] * len(top), forces=forces)
     assert np.array_equal(ref.rhs().view(np.uint64), dev.rhs().view(np.uint64))
+
+
+@pytest.mark.parametrize("precision", [sf.Precision.DOUBLE, sf.Precision.MIXED])
+def test_generated_part_and_prescribed_studies_match_the_host(precision):
+    """A hollow part (the serving stream's tube) and a model with prescribed displacements: the
+    studies from the generated meshes assemble the host's operator and give the host's answer."""
+    x = [40.0 * i / 24 for i in range(25)]
+    y = [12.0 * j / 8 for j in range(9)]
+    meshes = (sf.part_tet_mesh(x, y, y, 2, device=0), W.part_mesh_host(x, y, y, 2))
+    answers = []
+    for mesh in meshes:
+        nodes = mesh.nodes()
+        model = sf.Model(mesh, sf.Material(70000.0, 0.33))
+        model.fix_nodes(np.nonzero(np.abs(nodes[:, 0]) < 1e-9)[0])
+        faces = mesh.boundary_face_array()
+        end = np.all(np.abs(nodes[faces["nodes"][:, :3], 0] - 40.0) < 1e-9, axis=1)
+        model.add_face_tractions(faces[end], (0.0, 0.0, -2.0))
+        corner = int(np.nonzero(np.all(np.abs(nodes - [40.0, 0.0, 0.0]) < 1e-9, axis=1))[0][0])
+        model.prescribe_displacement(corner, 1, 0.001)
+        st = sf.StaticStudy.new(model, mg_options(precision))
+        out = st.solve()
+        answers.append((st.matrix(), st.rhs(), out.progress.iteration, st.displacements()))
+    (dm, dr, di, dx), (hm, hr, hi, hx) = answers
+    for a, b in zip(dm, hm):
+        assert np.array_equal(np.asarray(a).view(np.uint8), np.asarray(b).view(np.uint8))
+    assert np.array_equal(dr.view(np.uint64), hr.view(np.uint64))
+    assert di == hi and np.array_equal(dx.view(np.uint64), hx.view(np.uint64))
