@@ -563,7 +563,8 @@ def run_block(args):
     """Config 4: the 60 mm two-material printed block (60^3 hexes x 6 Tet10, 5.27M free DOFs): shell
     E 2.4 GPa nu 0.36 within 2 mm of the surface, core E 0.8 GPa nu 0.30, z = 0 clamped, 0.5 MPa
     x-shear on z = 60, mixed-precision and plain FP64 device-resident solves to 1e-8, the device FP64
-    assembly timed on its own, and the whole study end to end through the public API."""
+    assembly timed on its own, and the whole study end to end through the public API from the
+    block's description (mesh generated on the device)."""
     import torch
 
     import solidfem_b200 as sf
@@ -571,8 +572,8 @@ def run_block(args):
     torch.cuda.set_device(0)
     n = args.block_cells
 
-    def model():
-        mesh = sf.box_tet_mesh((0.0, 0.0, 0.0), (60.0, 60.0, 60.0), (n, n, n))
+    def model(device=None):
+        mesh = sf.box_tet_mesh((0.0, 0.0, 0.0), (60.0, 60.0, 60.0), (n, n, n), device)
         nodes = mesh.nodes()
         m = sf.Model(mesh, sf.ShellCore(sf.Material(2400.0, 0.36), sf.Material(800.0, 0.30), (0.0, 0.0, 0.0),
                                         (60.0, 60.0, 60.0), 2.0))
@@ -590,9 +591,11 @@ def run_block(args):
         return ms / steps, out
 
     out = {}
+    model(0)  # context and module load outside the clock
     for name, precision in (("mixed", sf.Precision.MIXED), ("fp64", sf.Precision.DOUBLE)):
-        mesh, m = model()
+        # end to end from the block's description: mesh generated on the device, model, study, solve
         t0 = time.perf_counter()
+        mesh, m = model(0)
         st = sf.StaticStudy.new(m, options(sf, precision, 0))
         res = st.solve()
         d = st.displacements()
