@@ -205,6 +205,10 @@ sf_status setup_power_step(cudaStream_t st, uint32_t rows, int rb, const uint32_
                            const double* vals, const double* inv, const double* v, double* s2);
 sf_status setup_scale(cudaStream_t st, size_t n, const double* src, double d, double* v);
 sf_status setup_entry_rows(cudaStream_t st, uint32_t rows, const uint32_t* starts, uint32_t* out);
+// The geometric strength graph (aggregate.rs:53-69): with out_starts null, each row's strong count
+// into out and its closest squared distance into closest; else the strong columns at out_starts.
+sf_status setup_strength(cudaStream_t st, uint32_t rows, const uint32_t* starts, const uint32_t* cols, const double* pos,
+                         double limit_scale, double* closest, const uint32_t* out_starts, uint32_t* out);
 // One pass of a union pattern (symbolic product): out_starts null counts each row's distinct
 // columns into out[row]; otherwise writes them, ascending, at out[out_starts[row] ..]. Columns
 // are below `width`.

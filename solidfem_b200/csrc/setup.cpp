@@ -15,6 +15,7 @@
 #include <algorithm>
 #include <atomic>
 #include <cmath>
+#include <cstdlib>
 #include <future>
 #include <limits>
 #include <memory>
@@ -110,6 +111,9 @@ double squared_distance(const vector<P3>& p, size_t a, size_t b) {
   double dx = p[b][0] - p[a][0], dy = p[b][1] - p[a][1], dz = p[b][2] - p[a][2];
   return dx * dx + dy * dy + dz * dz;
 }
+
+// Levels with at least this many block rows find their strong neighbours on the device.
+const size_t kDeviceStrengthRows = 16384;
 
 enum Phase { DIAGONAL, STRENGTH, AGGREGATE, TENTATIVE, SPECTRAL, FILTER, SMOOTH, PRODUCT, GALERKIN, FACTOR, DONE };
 
@@ -260,6 +264,45 @@ struct SetupMachine {
     if (e) return e;
     phase = STRENGTH;
     return SF_OK;
+  }
+
+  // Strong neighbours by geometry (aggregate.rs:53-69) on the device for large levels: a count
+  // pass with each row's closest distance, the starts summed here, a fill pass; the graph and the
+  // distances come back to the host for the aggregation.
+  sf_status run_strength_device() {
+    const size_t rows = current.rows;
+    double *pos = nullptr, *dclosest = nullptr;
+    uint32_t *counts = nullptr, *dstarts = nullptr, *dcols = nullptr;
+    sf_status e = dev_alloc(dev, (void**)&pos, rows * 24);
+    if (!e) e = dev_alloc(dev, (void**)&dclosest, rows * 8);
+    if (!e) e = dev_alloc(dev, (void**)&counts, rows * 4);
+    if (!e) e = dev_alloc(dev, (void**)&dstarts, (rows + 1) * 4);
+    if (!e) {
+      copy_h2d(dev, pos, positions.data(), rows * 24);
+      e = setup_strength(dev.stream, (uint32_t)rows, current.dev_starts, current.dev_cols, pos, reach * reach, dclosest,
+                         nullptr, counts);
+    }
+    closest.resize(rows);
+    strong_starts.assign(rows + 1, 0);
+    if (!e) {
+      copy_d2h(dev, closest.data(), dclosest, rows * 8);
+      copy_d2h(dev, strong_starts.data() + 1, counts, rows * 4);
+      e = sync("strength counts");
+    }
+    if (!e) {
+      for (size_t r = 0; r < rows; ++r) strong_starts[r + 1] += strong_starts[r];
+      strong_cols.resize(strong_starts[rows]);
+      copy_h2d(dev, dstarts, strong_starts.data(), (rows + 1) * 4);
+      e = dev_alloc(dev, (void**)&dcols, std::max<size_t>(1, strong_cols.size()) * 4);
+    }
+    if (!e)
+      e = setup_strength(dev.stream, (uint32_t)rows, current.dev_starts, current.dev_cols, pos, reach * reach, nullptr,
+                         dstarts, dcols);
+    if (!e && !strong_cols.empty()) copy_d2h(dev, strong_cols.data(), dcols, strong_cols.size() * 4);
+    if (!e) e = sync("strength");
+    for (void* p : {(void*)pos, (void*)dclosest, (void*)counts, (void*)dstarts, (void*)dcols}) dev_free(dev, p);
+    if (!e) phase = AGGREGATE;
+    return e;
   }
 
   // Strong neighbours by geometry (aggregate.rs:53-69), two passes so rows run in parallel.
@@ -763,7 +806,12 @@ sf_status setup_step(SetupMachine* m, size_t budget, sf_cancel_fn cancel, void* 
     sf_status s = SF_OK;
     switch (m->phase) {
       case DIAGONAL: s = m->run_diagonal(); break;
-      case STRENGTH: m->run_strength(); break;
+      case STRENGTH:
+        if (m->current.rows >= kDeviceStrengthRows && m->current.dev_starts && m->current.dev_cols)
+          s = m->run_strength_device();
+        else
+          m->run_strength();
+        break;
       case AGGREGATE: m->run_aggregate(); break;
       case TENTATIVE: s = m->run_tentative(); break;
       case SPECTRAL:

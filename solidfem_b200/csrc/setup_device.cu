@@ -681,6 +681,51 @@ sf_status setup_union_rows(cudaStream_t st, uint32_t rows, uint32_t width, const
   return cuda_check(cudaGetLastError(), "union pattern");
 }
 
+// Strong neighbours by geometry (aggregate.rs:53-69): a thread per row takes the squared distance
+// to each other column term for term (no contraction, as on the host), the row's closest one, and
+// keeps the columns within reach^2 times it. out_starts null: each row's count into out and its
+// closest distance into closest; else the strong columns in column order at out[out_starts[row]].
+__global__ void strength_kernel(uint32_t rows, const uint32_t* __restrict__ starts, const uint32_t* __restrict__ cols,
+                                const double* __restrict__ pos, double limit_scale, double* __restrict__ closest,
+                                const uint32_t* __restrict__ out_starts, uint32_t* __restrict__ out) {
+  for (uint32_t row = blockIdx.x * blockDim.x + threadIdx.x; row < rows; row += gridDim.x * blockDim.x) {
+    const double* p = pos + 3 * (size_t)row;
+    const uint32_t a0 = starts[row], a1 = starts[row + 1];
+    double c = 1.7976931348623157e308;
+    for (uint32_t at = a0; at < a1; ++at) {
+      const uint32_t col = cols[at];
+      if (col == row) continue;
+      const double* q = pos + 3 * (size_t)col;
+      const double dx = q[0] - p[0], dy = q[1] - p[1], dz = q[2] - p[2];
+      const double d = dx * dx + dy * dy + dz * dz;
+      c = d < c ? d : c;  // std::min(c, d)
+    }
+    const double limit = limit_scale * c;
+    uint32_t n = 0;
+    for (uint32_t at = a0; at < a1; ++at) {
+      const uint32_t col = cols[at];
+      if (col == row) continue;
+      const double* q = pos + 3 * (size_t)col;
+      const double dx = q[0] - p[0], dy = q[1] - p[1], dz = q[2] - p[2];
+      if (dx * dx + dy * dy + dz * dz <= limit) {
+        if (out_starts) out[out_starts[row] + n] = col;
+        ++n;
+      }
+    }
+    if (!out_starts) {
+      closest[row] = c;
+      out[row] = n;
+    }
+  }
+}
+
+sf_status setup_strength(cudaStream_t st, uint32_t rows, const uint32_t* starts, const uint32_t* cols, const double* pos,
+                         double limit_scale, double* closest, const uint32_t* out_starts, uint32_t* out) {
+  if (rows == 0) return SF_OK;
+  strength_kernel<<<grid_for(rows), kT, 0, st>>>(rows, starts, cols, pos, limit_scale, closest, out_starts, out);
+  return cuda_check(cudaGetLastError(), "strength");
+}
+
 sf_status setup_entry_rows(cudaStream_t st, uint32_t rows, const uint32_t* starts, uint32_t* out) {
   if (rows == 0) return SF_OK;
   entry_rows_kernel<<<grid_for(rows), kT, 0, st>>>(rows, starts, out);
