@@ -186,7 +186,11 @@ __global__ void point_positions_kernel(const double* __restrict__ nodes, const u
 // place in each; lane j then walks them in order for block j of the row and, where an element
 // also holds the block's column node, adds that element's (a, b) block. Each block therefore
 // sums its elements in ascending order, the order of the reference's element loop
-// (assembly.rs:87-130); no per-block list of contributions exists.
+// (assembly.rs:87-130); no per-block list of contributions exists. A row sums only its blocks on
+// and above the diagonal and writes each off-diagonal one's mirror (column, row) as its
+// transpose: an element's (b, a) block is the transpose of its (a, b) block to the bit (the
+// reference mirrors the value), so the mirror's sum over the same elements in the same order is
+// that transpose, and every element block is read once.
 constexpr int kGatherWarps = 8;
 constexpr int kGatherStage = 32;
 
@@ -204,14 +208,27 @@ __global__ void __launch_bounds__(32 * kGatherWarps)
   for (uint32_t r = blockIdx.x * kGatherWarps + warp; r < rows; r += gridDim.x * kGatherWarps) {
     const uint32_t node = row_node[r], k0 = cursor[r], k1 = inc_start[node + 1];
     const uint32_t b0 = starts[r], nb = starts[r + 1] - b0;
+    // the row's first block on or above the diagonal (columns ascend)
+    uint32_t lo = 0, hi = nb;
+    while (lo < hi) {
+      const uint32_t mid = (lo + hi) >> 1;
+      if (cols[b0 + mid] < r)
+        lo = mid + 1;
+      else
+        hi = mid;
+    }
+    const uint32_t upper = lo;
     uint32_t k_end = k0;
-    for (uint32_t jb = 0; jb < nb; jb += 32) {
+    for (uint32_t jb = upper; jb < nb; jb += 32) {
       const uint32_t j = jb + lane;
       const bool live = j < nb;
       const uint32_t col_node = live ? row_node[cols[b0 + j]] : 0xffffffffu;
+      // a row's first slice starts its blocks from zero (the values were zeroed at allocation)
+      // without reading them; later slices resume from the stored sums
+      const bool resume = k0 != inc_start[node];
       double v[9];
 #pragma unroll
-      for (int q = 0; q < 9; ++q) v[q] = live ? vals[(size_t)(b0 + j) * 9 + q] : 0.0;
+      for (int q = 0; q < 9; ++q) v[q] = live && resume ? vals[(size_t)(b0 + j) * 9 + q] : 0.0;
       uint32_t k = k0;
       for (;;) {
         // stage the next elements below `end` (they are ascending: the first at or past `end`
@@ -260,9 +277,27 @@ __global__ void __launch_bounds__(32 * kGatherWarps)
         if (count < 32) break;
       }
       k_end = k;
-      if (live)
+      if (live) {
 #pragma unroll
         for (int q = 0; q < 9; ++q) vals[(size_t)(b0 + j) * 9 + q] = v[q];
+        const uint32_t col = cols[b0 + j];
+        if (col != r) {
+          // the mirror block (col, r) in row col: the transpose
+          uint32_t mlo = starts[col], mhi = starts[col + 1];
+          while (mlo < mhi) {
+            const uint32_t mid = (mlo + mhi) >> 1;
+            if (cols[mid] < r)
+              mlo = mid + 1;
+            else
+              mhi = mid;
+          }
+          if (mlo < starts[col + 1] && cols[mlo] == r)
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+#pragma unroll
+              for (int q = 0; q < 3; ++q) vals[(size_t)mlo * 9 + q * 3 + i] = v[i * 3 + q];
+        }
+      }
     }
     if (lane == 0) cursor[r] = k_end;
   }
