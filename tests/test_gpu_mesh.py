@@ -201,3 +201,54 @@ def test_generated_part_and_prescribed_studies_match_the_host(precision):
         assert np.array_equal(np.asarray(a).view(np.uint8), np.asarray(b).view(np.uint8))
     assert np.array_equal(dr.view(np.uint64), hr.view(np.uint64))
     assert di == hi and np.array_equal(dx.view(np.uint64), hx.view(np.uint64))
+
+
+def umbrella(k=30):
+    """A vertex at the origin shared by 2k tetrahedra (a ring of k points, one apex above and one
+    below): 10 x 2k candidate columns for its row, more than the device pattern build sorts in
+    shared memory, so the study falls back to the host build."""
+    ring = [(np.cos(2 * np.pi * i / k), np.sin(2 * np.pi * i / k), 0.0) for i in range(k)]
+    pos = np.array([(0.0, 0.0, 0.0)] + ring + [(0.0, 0.0, 1.0), (0.0, 0.0, -1.0)])
+    top, bottom = k + 1, k + 2
+    tets = []
+    for i in range(k):
+        a, b = 1 + i, 1 + (i + 1) % k
+        for t in ((0, a, b, top), (0, b, a, bottom)):
+            p = pos[list(t)]
+            if np.linalg.det(p[1:] - p[0]) < 0:
+                t = (t[0], t[2], t[1], t[3])
+            tets.append(t)
+    return pos, np.array(tets, dtype=np.uint32)
+
+
+def test_a_row_too_wide_for_the_device_pattern_takes_the_host_build():
+    pos, tets = umbrella()
+    matrices = []
+    for device in (0, None):
+        mesh = sf.Mesh.from_linear(pos, tets, device=device)
+        nodes = mesh.nodes()
+        model = sf.Model(mesh, sf.Material(1000.0, 0.3))
+        model.fix_nodes(np.nonzero(nodes[:, 2] < -0.99)[0].tolist() + [1, 1 + len(pos) // 3])
+        model.add_nodal_force(len(pos) - 2, (0.0, 0.0, 1.0))
+        st = sf.StaticStudy.new(model, sf.StudyOptions(pcg=sf.PcgOptions(tolerance=1e-10)))
+        st.solve()
+        matrices.append((st.matrix(), st.displacements()))
+    (dm, dx), (hm, hx) = matrices
+    for a, b in zip(dm, hm):
+        assert np.array_equal(np.asarray(a).view(np.uint8), np.asarray(b).view(np.uint8))
+    assert np.array_equal(dx.view(np.uint64), hx.view(np.uint64))
+
+
+def test_a_refusal_after_the_device_pattern_releases_it():
+    """A generated mesh whose model has no load is refused after its pattern was built on the
+    device; the refusal is the host's, and the device keeps working (repeated, nothing leaks)."""
+    mesh = sf.box_tet_mesh((0, 0, 0), (10.0, 1.0, 1.0), (40, 4, 4), device=0)
+    nodes = mesh.nodes()
+    for _ in range(5):
+        model = sf.Model(mesh, sf.Material(200000.0, 0.3))
+        model.fix_nodes(np.nonzero(np.abs(nodes[:, 0]) < 1e-9)[0])
+        with pytest.raises(sf.SolidfemError) as e:
+            sf.StaticStudy.new(model, mg_options(sf.Precision.MIXED))
+        assert e.value.status == sf.Status.NO_EFFECTIVE_LOAD
+    model = plate_model(sf.box_tet_mesh((0, 0, 0), (100.0, 100.0, 0.8), (20, 20, 2), device=0))
+    assert sf.StaticStudy.new(model, mg_options(sf.Precision.MIXED)).solve().kind == sf.Outcome.CONVERGED
