@@ -600,6 +600,15 @@ sf_status from_linear(Build& b, double* pos, size_t n, uint32_t* corners, size_t
   mirror->device = b.device;
   mirror->nodes = b.alloc<double>(3 * nodes, true);
   mirror->tets = b.alloc<uint32_t>(10 * ntets, true);
+  // On an early return the mirror frees its arrays on a stream of its own: the build's kernels
+  // that write them must have finished first (declared after `mirror`, so it runs before).
+  struct Drain {
+    cudaStream_t st;
+    bool armed = true;
+    ~Drain() {
+      if (armed) cudaStreamSynchronize(st);
+    }
+  } drain{st};
   if (b.err) return cuda_fail(b.err, "mesh build");
   cudaMemcpyAsync(mirror->nodes, pos, n * 24, cudaMemcpyDeviceToDevice, st);
   midside_kernel<<<grid_of(n), kT, 0, st>>>(off, eoff, other, mirror->nodes, n);
@@ -643,6 +652,7 @@ sf_status from_linear(Build& b, double* pos, size_t n, uint32_t* corners, size_t
   if (cudaError_t e = cudaGetLastError()) return cuda_fail(e, "mesh kernels");
   mirror->stream = nullptr;
   out.dev = mirror;
+  drain.armed = false;  // the copies above synchronized the stream
   return SF_OK;
 }
 
