@@ -167,11 +167,11 @@ extern thread_local std::vector<LaunchRecord>* g_recorder;
 // Stream-ordered copies that count the bytes crossing the host-device link.
 inline void copy_h2d(const DeviceSolver& s, void* dst, const void* src, size_t bytes) {
   cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s.stream);
-  s.h2d_bytes += bytes;
+  __atomic_fetch_add(&s.h2d_bytes, bytes, __ATOMIC_RELAXED);  // setup's helper thread copies too
 }
 inline void copy_d2h(const DeviceSolver& s, void* dst, const void* src, size_t bytes) {
   cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, s.stream);
-  s.d2h_bytes += bytes;
+  __atomic_fetch_add(&s.d2h_bytes, bytes, __ATOMIC_RELAXED);
 }
 // Pinned host memory that is never freed (freeing pinned memory synchronizes the device):
 // pooled buffers, and 512-byte slots for per-study state.

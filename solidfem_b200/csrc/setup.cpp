@@ -479,20 +479,35 @@ struct SetupMachine {
       double n0 = norm2(pinned, dofs);
       for (size_t i = 0; i < dofs; ++i) pinned[i] /= n0;
       copy_h2d(dev, v, pinned, dofs * 8);
+      // Each iterate comes back in chunks, each with an event: the host's serial sum of squares
+      // (norm2's order) starts on the first chunk while the rest are still in flight.
+      constexpr int kChunks = 8;
+      cudaEvent_t landed[kChunks];
+      for (int c = 0; c < kChunks; ++c) cudaEventCreateWithFlags(&landed[c], cudaEventDisableTiming);
+      const size_t chunk = (dofs + kChunks - 1) / kChunks;
       for (int it = 0; it < POWER_ITERATIONS && !e; ++it) {
         e = setup_power_step(dev.stream, (uint32_t)rows, (int)rb, current.dev_starts, current.dev_cols, current.dev,
                              inv, v, s2);
-        if (!e) {
-          copy_d2h(dev, pinned, s2, dofs * 8);
-          e = sync("power iteration");
+        for (int c = 0; c < kChunks && !e; ++c) {
+          const size_t at = std::min(dofs, c * chunk), len = std::min(dofs, at + chunk) - at;
+          if (len) copy_d2h(dev, pinned + at, s2 + at, len * 8);
+          cudaEventRecord(landed[c], dev.stream);
+        }
+        double sum = 0.0;
+        for (int c = 0; c < kChunks && !e; ++c) {
+          e = cuda_check(cudaEventSynchronize(landed[c]), "power iteration");
+          const size_t at = std::min(dofs, c * chunk), end = std::min(dofs, at + chunk);
+          for (size_t i = at; i < end; ++i) sum += pinned[i] * pinned[i];
         }
         if (!e) {
-          double n = norm2(pinned, dofs);
+          double n = std::sqrt(sum);  // norm2 (block.rs:398-404), the same serial sum
           lm = n;
           e = setup_scale(dev.stream, dofs, s2, n, v);
         }
       }
       if (!e) e = sync("power iteration");
+      else cudaStreamSynchronize(dev.stream);
+      for (int c = 0; c < kChunks; ++c) cudaEventDestroy(landed[c]);
     }
     pinned_return(pinned);  // every copy from it completed at the syncs
     return {e, lm};

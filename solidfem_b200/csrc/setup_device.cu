@@ -140,34 +140,43 @@ __global__ void scale_kernel(size_t n, const double* __restrict__ src, double d,
 }
 
 // s2 = D^-1 (A v) for one block row per thread, in the order of setup.rs:404-432.
+// One power step s2 = D^-1 (A v) (setup.rs:390-449). Lane p of a team of N lanes owns component
+// p of a block row: its sum runs over the row's blocks in column order and, inside a block, over
+// q in order, one running sum, as the reference's serial loop; the team's N sums then meet by
+// shuffles for D^-1 y, again summed in q order. A warp holds 32 / N teams (10 rows of 3, 5 of
+// 6), so a block's N value rows are read by N neighbouring lanes.
 template <int N>
 __global__ void power_step_kernel(uint32_t rows, const uint32_t* __restrict__ starts, const uint32_t* __restrict__ cols,
                                   const double* __restrict__ vals, const double* __restrict__ inv,
                                   const double* __restrict__ v, double* __restrict__ s2) {
-  for (uint32_t row = blockIdx.x * blockDim.x + threadIdx.x; row < rows; row += gridDim.x * blockDim.x) {
-    double y[N];
+  constexpr uint32_t kTeams = 32 / N;
+  const uint32_t lane = threadIdx.x & 31, team = lane / N, p = lane - team * N;
+  const bool on = team < kTeams;
+  const uint32_t warps = blockDim.x >> 5;
+  const uint32_t warp0 = blockIdx.x * warps + (threadIdx.x >> 5);
+  for (uint32_t base = warp0 * kTeams; base < rows; base += gridDim.x * warps * kTeams) {
+    const uint32_t row = base + team;
+    const bool live = on && row < rows;
+    double y = 0.0;
+    if (live) {
+      for (uint32_t at = starts[row]; at < starts[row + 1]; ++at) {
+        const double* b = vals + (size_t)at * N * N + (size_t)p * N;
+        const double* x = v + (size_t)cols[at] * N;
+        double sum = y;
 #pragma unroll
-    for (int p = 0; p < N; ++p) y[p] = 0.0;
-    for (uint32_t at = starts[row]; at < starts[row + 1]; ++at) {
-      const double* b = vals + (size_t)at * N * N;
-      const double* x = v + (size_t)cols[at] * N;
-      double xv[N];
-#pragma unroll
-      for (int q = 0; q < N; ++q) xv[q] = x[q];
-#pragma unroll
-      for (int p = 0; p < N; ++p) {
-        double sum = y[p];
-#pragma unroll
-        for (int q = 0; q < N; ++q) sum += b[p * N + q] * xv[q];
-        y[p] = sum;
+        for (int q = 0; q < N; ++q) sum += b[q] * x[q];
+        y = sum;
       }
     }
-    const double* d = inv + (size_t)row * N * N;
+    const uint32_t first = team * N;
+    double yq[N];
 #pragma unroll
-    for (int p = 0; p < N; ++p) {
+    for (int q = 0; q < N; ++q) yq[q] = __shfl_sync(0xffffffffu, y, (first + q) & 31);
+    if (live) {
+      const double* d = inv + (size_t)row * N * N + (size_t)p * N;
       double sum = 0.0;
 #pragma unroll
-      for (int q = 0; q < N; ++q) sum += d[p * N + q] * y[q];
+      for (int q = 0; q < N; ++q) sum += d[q] * yq[q];
       s2[(size_t)row * N + p] = sum;
     }
   }
@@ -651,9 +660,9 @@ sf_status setup_power_step(cudaStream_t st, uint32_t rows, int rb, const uint32_
                            const double* vals, const double* inv, const double* v, double* s2) {
   if (rows == 0) return SF_OK;
   if (rb == 3)
-    power_step_kernel<3><<<grid_for(rows), kT, 0, st>>>(rows, starts, cols, vals, inv, v, s2);
+    power_step_kernel<3><<<grid_for((size_t)rows * 32 / 10), kT, 0, st>>>(rows, starts, cols, vals, inv, v, s2);
   else
-    power_step_kernel<6><<<grid_for(rows), kT, 0, st>>>(rows, starts, cols, vals, inv, v, s2);
+    power_step_kernel<6><<<grid_for((size_t)rows * 32 / 5), kT, 0, st>>>(rows, starts, cols, vals, inv, v, s2);
   return cuda_check(cudaGetLastError(), "power step");
 }
 
