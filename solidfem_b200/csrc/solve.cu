@@ -2057,9 +2057,10 @@ void launch_bsr_lpr(const DevBsr& m, const V* x, V* y, const V* b, const int* st
   launch_body<bsr_kernel<S, V, RB, CB, LPR, OP>>(sh.grid, sh.threads, sh.smem, st, A, x, y, b, status);
 }
 
-// The SELL-32 products run in blocks of two warps: at ~110 registers a thread an SM holds 18
-// warps, which blocks of eight fill only to 16 (measured on the gate plate: the finest Chebyshev
-// step 41.7 -> 40.8 us, the mixed solve 184.3 -> 182.9 ms, same bits; FP64 unchanged).
+// The SELL-32 and split-row products run in blocks of two warps: at ~110 registers a thread an SM
+// holds 18 warps, which blocks of eight fill only to 16 (the finest Chebyshev step 41.7 -> 40.8
+// us), and level 1's ~2,000 slices spread evenly over the SMs instead of two eight-warp blocks on
+// some and one on others (mixed solve 182.5 -> 181.7 ms); same bits, FP64 unchanged.
 constexpr int kSellThreads = 64;
 inline int sell_threads() { return kSellThreads; }
 inline int sell_grid(uint32_t nslices) {
@@ -2094,9 +2095,9 @@ void launch_bsr(const DevBsr& m, const V* x, V* y, const V* b, const int* status
 template <typename S, typename V, int OP>
 void launch_split(const DevBsr& m, const V* x, V* y, const V* b, const int* status, cudaStream_t st) {
   if (m.cb == 3)
-    launch_body<split_kernel<S, V, 3, OP>>(grid_for_slices(m.nslices), kThreads, 0, st, sell_of<S>(m), x, y, b, status);
+    launch_body<split_kernel<S, V, 3, OP>>(sell_grid(m.nslices), sell_threads(), 0, st, sell_of<S>(m), x, y, b, status);
   else
-    launch_body<split_kernel<S, V, 6, OP>>(grid_for_slices(m.nslices), kThreads, 0, st, sell_of<S>(m), x, y, b, status);
+    launch_body<split_kernel<S, V, 6, OP>>(sell_grid(m.nslices), sell_threads(), 0, st, sell_of<S>(m), x, y, b, status);
 }
 
 template <typename S, typename V, int RB, int OP>
@@ -2133,7 +2134,7 @@ void launch_cheb_step(const DevLevel& L, const V* d_old, V* d_new, V* r, V* x, V
                       const int* status, cudaStream_t st) {
   if constexpr (RB == 6) {
     if (L.a.split) {
-      launch_body<split_cheb_kernel<S, V>>(grid_for_slices(L.a.nslices), kThreads, 0, st, sell_of<S>(L.a),
+      launch_body<split_cheb_kernel<S, V>>(sell_grid(L.a.nslices), sell_threads(), 0, st, sell_of<S>(L.a),
                                            (const S*)L.dinv, d_old, d_new, r, x, outer, (V)keep, (V)step, status);
       return;
     }
@@ -2165,7 +2166,7 @@ void launch_start_rb(const DevBsr& m, const V* x, const V* b, const StartArgs<S,
                      cudaStream_t st) {
   if constexpr (RB == 6) {
     if (m.split) {
-      launch_body<split_start_kernel<S, V, CB, OP>>(grid_for_slices(m.nslices), kThreads, 0, st, sell_of<S>(m), x, b,
+      launch_body<split_start_kernel<S, V, CB, OP>>(sell_grid(m.nslices), sell_threads(), 0, st, sell_of<S>(m), x, b,
                                                     a, status);
       return;
     }
