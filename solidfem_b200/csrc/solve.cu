@@ -2057,10 +2057,12 @@ void launch_bsr_lpr(const DevBsr& m, const V* x, V* y, const V* b, const int* st
   launch_body<bsr_kernel<S, V, RB, CB, LPR, OP>>(sh.grid, sh.threads, sh.smem, st, A, x, y, b, status);
 }
 
-// The SELL-32 and split-row products run in blocks of two warps: at ~110 registers a thread an SM
-// holds 18 warps, which blocks of eight fill only to 16 (the finest Chebyshev step 41.7 -> 40.8
-// us), and level 1's ~2,000 slices spread evenly over the SMs instead of two eight-warp blocks on
-// some and one on others (mixed solve 182.5 -> 181.7 ms); same bits, FP64 unchanged.
+// The SELL-32 and split-row products run in blocks of two warps. The resident warps per SM do not
+// change (at ~110 registers each scheduler's quarter of the register file holds four warps), but
+// finer blocks even out the end of the grid: the SMs that finish early take the last slices two
+// warps at a time (the finest Chebyshev step 41.7 -> 40.8 us), and level 1's ~2,000 slices spread
+// evenly instead of two eight-warp blocks on some SMs and one on others (mixed solve 182.5 ->
+// 181.7 ms). Same bits; FP64 unchanged.
 constexpr int kSellThreads = 64;
 inline int sell_threads() { return kSellThreads; }
 inline int sell_grid(uint32_t nslices) {
