@@ -1,5 +1,6 @@
 """The serving loop (sf_server) on a small mixed stream (needs a B200): every request's answer in
-the mix equals its answer alone in the same operator layout, one answer of each part kind matches
+the mix equals its answer alone in the same operator layout (also with the requests' meshes
+generated on the device), one answer of each part kind matches
 the oracle's FP64 solve, a request cancelled in the middle of a batch leaves the others' answers
 unchanged, and the memory budget holds.
 """
@@ -47,10 +48,10 @@ def solo_answers(reqs, batch_max_dofs=BATCH_MAX_DOFS):
     return out
 
 
-def serve(reqs, server_options, cancel_index=None):
+def serve(reqs, server_options, cancel_index=None, device=None):
     server = sf.Server(server_options)
     try:
-        models = [W.build_model(r) for r in reqs]
+        models = [W.build_model(r, device=device) for r in reqs]
         start = time.perf_counter()
         ids = []
         for r, (mesh, model) in zip(reqs, models):
@@ -98,6 +99,22 @@ def test_served_answers_equal_solo_answers():
         else:  # solved on its own stream exactly as alone
             assert np.array_equal(a.view(np.uint64), s.view(np.uint64)), (r.index, r.kind, d)
         assert res.latency_seconds >= res.solve_seconds >= 0.0
+
+
+def test_served_answers_from_device_meshes_equal_solo_host_answers():
+    """The serving bench generates each request's mesh on the device: the device mesh, pattern and
+    traction load give the host-mesh answers (unbatched to the bit, batched within the mix bar)."""
+    reqs = stream()
+    solo = solo_answers(reqs)
+    results, answers, stats, _ = serve(reqs, sf.ServerOptions(batch_max_dofs=BATCH_MAX_DOFS, build_threads=3),
+                                       device=0)
+    assert stats["completed"] == len(reqs)
+    for r, res, a, s in zip(reqs, results, answers, solo):
+        assert res.status == sf.Status.OK and res.outcome.kind == sf.Outcome.CONVERGED
+        if res.batched:
+            assert rel(a, s) <= MIX_BAR, (r.index, r.kind, rel(a, s))
+        else:
+            assert np.array_equal(a.view(np.uint64), s.view(np.uint64)), (r.index, r.kind, rel(a, s))
 
 
 def oracle_answer(O, req):
