@@ -503,14 +503,17 @@ struct Build {
   }
 };
 
-void scan(Build& b, const uint32_t* in, uint32_t* out, size_t n) {
+// Returns false (b.err set) when its scratch could not be allocated: the caller must not launch
+// anything that reads `out`.
+bool scan(Build& b, const uint32_t* in, uint32_t* out, size_t n) {
   const size_t nb = std::max<size_t>(1, (n + 1023) / 1024);
   uint32_t* sums = b.alloc<uint32_t>(nb);
-  if (b.err) return;
+  if (b.err) return false;
   if (n) scan_blocks_kernel<<<(unsigned)nb, 1024, 0, b.stream>>>(in, out, sums, n);
   else cudaMemsetAsync(sums, 0, sizeof(uint32_t), b.stream);
   scan_sums_kernel<<<1, 1024, 0, b.stream>>>(sums, n ? nb : 0, out + n);
   if (n) scan_add_kernel<<<grid_of(n), kT, 0, b.stream>>>(out, sums, n);
+  return true;
 }
 
 struct DeviceMeshOwner : DeviceMesh {
@@ -526,6 +529,14 @@ struct DeviceMeshOwner : DeviceMesh {
     cudaSetDevice(prev);
   }
 };
+
+sf_status cuda_fail(cudaError_t e, const char* what);
+
+// A scan whose scratch allocation failed: wait for the work already queued, report the failure.
+sf_status scan_failed(Build& b) {
+  cudaStreamSynchronize(b.stream);
+  return cuda_fail(b.err, "scan");
+}
 
 sf_status cuda_fail(cudaError_t e, const char* what) {
   char msg[200];
@@ -584,11 +595,11 @@ sf_status from_linear(Build& b, double* pos, size_t n, uint32_t* corners, size_t
   if (b.err) return cuda_fail(b.err, "mesh build");
   cudaMemsetAsync(count, 0, n * 4, st);
   edge_count_kernel<<<grid_of(6 * ntets), kT, 0, st>>>(corners, ntets, count);
-  scan(b, count, off, n);
+  if (!scan(b, count, off, n)) return scan_failed(b);
   cudaMemcpyAsync(cursor, off, n * 4, cudaMemcpyDeviceToDevice, st);
   edge_fill_kernel<<<grid_of(6 * ntets), kT, 0, st>>>(corners, ntets, cursor, other);
   edge_unique_kernel<<<grid_of(n), kT, 0, st>>>(off, other, ucount, n);
-  scan(b, ucount, eoff, n);
+  if (!scan(b, ucount, eoff, n)) return scan_failed(b);
   uint32_t edges = 0;
   cudaMemcpyAsync(&edges, eoff + n, 4, cudaMemcpyDeviceToHost, st);
   if (cudaError_t e = cudaStreamSynchronize(st)) return cuda_fail(e, "mesh edges");
@@ -623,11 +634,11 @@ sf_status from_linear(Build& b, double* pos, size_t n, uint32_t* corners, size_t
   if (b.err) return cuda_fail(b.err, "mesh build");
   cudaMemsetAsync(fcount, 0, n * 4, st);
   face_count_kernel<<<grid_of(4 * ntets), kT, 0, st>>>(corners, ntets, fcount);
-  scan(b, fcount, foff, n);
+  if (!scan(b, fcount, foff, n)) return scan_failed(b);
   cudaMemcpyAsync(cursor, foff, n * 4, cudaMemcpyDeviceToDevice, st);
   face_fill_kernel<<<grid_of(4 * ntets), kT, 0, st>>>(corners, ntets, cursor, rest, item);
   face_bucket_kernel<<<grid_of(n), kT, 0, st>>>(foff, rest, item, single, checks, n);
-  scan(b, single, soff, n);
+  if (!scan(b, single, soff, n)) return scan_failed(b);
   uint32_t nfaces = 0;
   unsigned int manifold = 0;
   cudaMemcpyAsync(&nfaces, soff + n, 4, cudaMemcpyDeviceToHost, st);
@@ -910,7 +921,11 @@ sf_status device_pattern(const Mesh& mesh, const vector<uint32_t>& free, size_t 
   cudaMemsetAsync(count, 0, nn * 4, st);
   cudaMemsetAsync(overflow, 0, 4, st);
   incidence_count_kernel<<<grid_of(nt), kT, 0, st>>>(mesh.dev->tets, nt, count);
-  scan(b, count, out.inc_start, nn);
+  if (!scan(b, count, out.inc_start, nn)) {
+    const sf_status e = scan_failed(b);
+    release();
+    return e;
+  }
   cudaMemcpyAsync(cursor, out.inc_start, nn * 4, cudaMemcpyDeviceToDevice, st);
   incidence_fill_kernel<<<grid_of(nt), kT, 0, st>>>(mesh.dev->tets, nt, cursor, out.inc);
   incidence_sort_kernel<<<grid_of(nn), kT, 0, st>>>(out.inc_start, out.inc, nn);
@@ -919,7 +934,11 @@ sf_status device_pattern(const Mesh& mesh, const vector<uint32_t>& free, size_t 
                                                                        148 * 16));
   pattern_rows_kernel<false><<<grid, 32 * kPatternWarps, 0, st>>>((uint32_t)free_count, out.row_node, out.inc_start,
                                                                   out.inc, mesh.dev->tets, dfree, nullptr, rows, overflow);
-  scan(b, rows, out.starts, free_count);
+  if (!scan(b, rows, out.starts, free_count)) {
+    const sf_status e = scan_failed(b);
+    release();
+    return e;
+  }
   unsigned over = 0;
   uint32_t blocks = 0;
   cudaMemcpyAsync(&over, overflow, 4, cudaMemcpyDeviceToHost, st);
@@ -997,7 +1016,7 @@ sf_status device_traction_load(const Mesh& mesh, const vector<std::pair<sf_bound
   cudaMemsetAsync(count, 0, n * 4, st);
   face_measure_kernel<<<grid_of(6 * nf), kT, 0, st>>>(faces, nf, mesh.dev->nodes, measure);
   load_count_kernel<<<grid_of(6 * nf), kT, 0, st>>>(faces, nf, count);
-  scan(b, count, off, n);
+  if (!scan(b, count, off, n)) return scan_failed(b);
   cudaMemcpyAsync(cursor, off, n * 4, cudaMemcpyDeviceToDevice, st);
   load_fill_kernel<<<grid_of(6 * nf), kT, 0, st>>>(faces, nf, cursor, entry);
   node_load_kernel<<<grid_of(n), kT, 0, st>>>(faces, measure, off, entry, dforced, dsum, (uint32_t)forced.size(), dload,
@@ -1058,7 +1077,7 @@ sf_status build_part_mesh_device(const double* const lines[3], const uint64_t co
   box_vertices_kernel<<<grid_of(nv), kT, 0, b.stream>>>(unit, upos, nv);
   PartCells g{cells[1], cells[2], wall_cells};
   part_keep_kernel<<<grid_of(nt), kT, 0, b.stream>>>(unit, g, upos, keep, nt);
-  scan(b, keep, at, nt);
+  if (!scan(b, keep, at, nt)) return scan_failed(b);
   uint32_t kept_count = 0;
   cudaMemcpyAsync(&kept_count, at + nt, 4, cudaMemcpyDeviceToHost, b.stream);
   if (cudaError_t e = cudaStreamSynchronize(b.stream)) return cuda_fail(e, "part cells");
@@ -1072,7 +1091,7 @@ sf_status build_part_mesh_device(const double* const lines[3], const uint64_t co
   cudaMemsetAsync(mark, 0, 4 * (size_t)kept_count * 4, b.stream);
   part_compact_kernel<<<grid_of(nt), kT, 0, b.stream>>>(unit, keep, at, kept, first, nt);
   part_mark_kernel<<<grid_of(nv), kT, 0, b.stream>>>(first, mark, nv);
-  scan(b, mark, rank, 4 * (size_t)kept_count);
+  if (!scan(b, mark, rank, 4 * (size_t)kept_count)) return scan_failed(b);
   uint32_t used = 0;
   cudaMemcpyAsync(&used, rank + 4 * (size_t)kept_count, 4, cudaMemcpyDeviceToHost, b.stream);
   if (cudaError_t e = cudaStreamSynchronize(b.stream)) return cuda_fail(e, "part vertices");
