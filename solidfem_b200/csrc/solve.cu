@@ -717,11 +717,12 @@ __device__ __forceinline__ void sell_rows(const SellOp<S>& A, const V* __restric
     for (int p = 0; p < RB; ++p) acc[p] = mag[p] = V(0);
     const uint32_t base = A.start[s];
     // One chunk of U blocks per step: its columns in one vector load, its values in NV 16-byte
-    // vector loads (each a contiguous 512 bytes across the warp). The loads of chunk k+1 are
+    // vector loads (each a contiguous 512 bytes across the warp). The values of chunk k+1 are
     // issued before chunk k's x gathers and FMAs, so a chunk's stream latency hides behind the
-    // previous chunk's gathers. The FMAs run in column order, so the row's sum keeps its
-    // sequential order.
-    uint32_t cn[U];
+    // previous chunk's gathers; the columns run one chunk further ahead (chunk k+2), so the x
+    // gathers of a chunk never wait on the DRAM load of its own columns. The FMAs run in column
+    // order, so the row's sum keeps its sequential order.
+    uint32_t cn[U], cf[U];
     S vn[U * LEN];
     if (n > 0) {
       load_cols<U>(A.cols + base + lane * U, cn);
@@ -729,6 +730,7 @@ __device__ __forceinline__ void sell_rows(const SellOp<S>& A, const V* __restric
 #pragma unroll
       for (int q = 0; q < NV; ++q) Vec16<S>::split(__ldcs(vp + 32 * q), vn + q * VEC);
     }
+    if (U < n) load_cols<U>(A.cols + base + 32 * U + lane * U, cf);
     for (uint32_t k0 = 0; k0 < n; k0 += U) {
       uint32_t c[U];
       S v[U * LEN];
@@ -738,10 +740,12 @@ __device__ __forceinline__ void sell_rows(const SellOp<S>& A, const V* __restric
       for (int i = 0; i < U * LEN; ++i) v[i] = vn[i];
       if (k0 + U < n) {
         const uint32_t q1 = base + 32 * (k0 + U);
-        load_cols<U>(A.cols + q1 + lane * U, cn);
+#pragma unroll
+        for (int u = 0; u < U; ++u) cn[u] = cf[u];
         const W* vp = reinterpret_cast<const W*>(A.vals + (size_t)q1 * LEN) + lane;
 #pragma unroll
         for (int q = 0; q < NV; ++q) Vec16<S>::split(__ldcs(vp + 32 * q), vn + q * VEC);
+        if (k0 + 2 * U < n) load_cols<U>(A.cols + q1 + 32 * U + lane * U, cf);
       }
       V xv[U][CB];
 #pragma unroll
@@ -902,7 +906,8 @@ __device__ __forceinline__ void split_rows(const SellOp<S>& A, const V* __restri
     V acc = V(0);
     const uint32_t base = A.start[s];
     const uint32_t* cp = A.cols + (size_t)(base >> 5) * kSplitRowsPerSlice + (size_t)m * U;
-    uint32_t cn[U];
+    // Values one chunk ahead, columns two (as in sell_rows).
+    uint32_t cn[U], cf[U];
     S vn[U * CB];
     if (n > 0) {
       load_cols_shared<U>(cp, cn);
@@ -910,6 +915,7 @@ __device__ __forceinline__ void split_rows(const SellOp<S>& A, const V* __restri
 #pragma unroll
       for (int q = 0; q < NV; ++q) Vec16<S>::split(__ldcs(vp + 32 * q), vn + q * VEC);
     }
+    if (U < n) load_cols_shared<U>(cp + (size_t)kSplitRowsPerSlice * U, cf);
     for (uint32_t k0 = 0; k0 < n; k0 += U) {
       uint32_t c[U];
       S v[U * CB];
@@ -918,10 +924,12 @@ __device__ __forceinline__ void split_rows(const SellOp<S>& A, const V* __restri
 #pragma unroll
       for (int i = 0; i < U * CB; ++i) v[i] = vn[i];
       if (k0 + U < n) {
-        load_cols_shared<U>(cp + (size_t)kSplitRowsPerSlice * (k0 + U), cn);
+#pragma unroll
+        for (int u = 0; u < U; ++u) cn[u] = cf[u];
         const W* vp = reinterpret_cast<const W*>(A.vals + ((size_t)base + 32 * (k0 + U)) * CB) + lane;
 #pragma unroll
         for (int q = 0; q < NV; ++q) Vec16<S>::split(__ldcs(vp + 32 * q), vn + q * VEC);
+        if (k0 + 2 * U < n) load_cols_shared<U>(cp + (size_t)kSplitRowsPerSlice * (k0 + 2 * U), cf);
       }
       V xv[U][CB];
 #pragma unroll
