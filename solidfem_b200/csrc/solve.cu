@@ -696,8 +696,29 @@ __device__ __forceinline__ void load_cols(const uint32_t* p, uint32_t (&c)[U]) {
   }
 }
 
-template <typename S, typename V, int RB, int CB, bool MAG, class Epi>
-__device__ __forceinline__ void sell_rows(const SellOp<S>& A, const V* __restrict__ x, Epi& epi) {
+// The row walks test their kernel's gate (the status word) only after the first slice's row map
+// has been requested, so the status load and the row-map loads travel together instead of one
+// after the other. The operator arrays are never written by a solve kernel, and a closed gate
+// ends the walk before any x gather, epilogue load or store. The row-map loads are volatile so
+// the compiler keeps them ahead of the gate's branch.
+__device__ __forceinline__ uint32_t ld_early(const uint32_t* p) {
+  uint32_t v;
+  asm volatile("ld.global.nc.u32 %0, [%1];" : "=r"(v) : "l"(p));
+  return v;
+}
+
+struct StatusGate {
+  const int* status;
+  __device__ __forceinline__ bool operator()() const { return *status == ST_ACTIVE; }
+};
+struct OpenGate {
+  __device__ __forceinline__ bool operator()() const { return true; }
+};
+
+// Returns the gate: false when the kernel must end (uniform over the grid, so a body may still
+// reduce across its blocks after a true return).
+template <typename S, typename V, int RB, int CB, bool MAG, class Epi, class Gate>
+__device__ __forceinline__ bool sell_rows(const SellOp<S>& A, const V* __restrict__ x, Epi& epi, const Gate& gate) {
   constexpr int LEN = RB * CB;
   constexpr int U = sell_chunk_blocks(LEN, (int)sizeof(S));
   constexpr int VEC = 16 / (int)sizeof(S);
@@ -706,16 +727,21 @@ __device__ __forceinline__ void sell_rows(const SellOp<S>& A, const V* __restric
   typedef typename Vec16<S>::type W;
   const uint32_t lane = threadIdx.x & 31;
   const uint32_t warps = blockDim.x >> 5;
+  bool open = false;
   for (uint32_t s = blockIdx.x * warps + (threadIdx.x >> 5); s < A.nslices; s += gridDim.x * warps) {
     const uint32_t slot = s * 32 + lane;
-    const uint32_t row = A.rows[slot];
-    const uint32_t n = A.len[slot];
+    const uint32_t row = ld_early(A.rows + slot);
+    const uint32_t n = ld_early(A.len + slot);
+    const uint32_t base = ld_early(A.start + s);
+    if (!open) {
+      if (!gate()) return false;
+      open = true;
+    }
     const bool live = row < A.nrows;
     epi.pre(row, live);
     V acc[RB], mag[RB];
 #pragma unroll
     for (int p = 0; p < RB; ++p) acc[p] = mag[p] = V(0);
-    const uint32_t base = A.start[s];
     // One chunk of U blocks per step: its columns in one vector load, its values in NV 16-byte
     // vector loads (each a contiguous 512 bytes across the warp). The values of chunk k+1 are
     // issued before chunk k's x gathers and FMAs, so a chunk's stream latency hides behind the
@@ -767,6 +793,7 @@ __device__ __forceinline__ void sell_rows(const SellOp<S>& A, const V* __restric
     }
     epi.post(row, live, n, acc, mag);
   }
+  return open || gate();
 }
 
 template <typename V, int RB, int OP>
@@ -794,9 +821,8 @@ struct SellAxpy {
 template <typename S, typename V, int RB, int CB, int OP>
 __device__ __forceinline__ void sell_kernel(SellOp<S> A, const V* __restrict__ x, V* __restrict__ y,
                                                         const V* __restrict__ b, const int* __restrict__ status) {
-  if (*status != ST_ACTIVE) return;
   SellAxpy<V, RB, OP> epi{y, b, {}};
-  sell_rows<S, V, RB, CB, false>(A, x, epi);
+  sell_rows<S, V, RB, CB, false>(A, x, epi, StatusGate{status});
 }
 
 // The fused Chebyshev step of cheb_step_kernel, one thread per row.
@@ -841,7 +867,6 @@ __device__ __forceinline__ void sell_cheb_kernel(SellOp<S> A, const S* __restric
                                                              const V* __restrict__ d_old, V* __restrict__ d_new,
                                                              V* __restrict__ r, V* __restrict__ x, V* __restrict__ outer,
                                                              V keep, V step, const int* __restrict__ status) {
-  if (*status != ST_ACTIVE) return;
   SellCheb<S, V, RB> epi;
   epi.dinv = dinv;
   epi.d_old = d_old;
@@ -851,7 +876,7 @@ __device__ __forceinline__ void sell_cheb_kernel(SellOp<S> A, const S* __restric
   epi.outer = outer;
   epi.keep = keep;
   epi.step = step;
-  sell_rows<S, V, RB, RB, false>(A, d_old, epi);
+  sell_rows<S, V, RB, RB, false>(A, d_old, epi, StatusGate{status});
 }
 
 // ------------------------------------------------------------ split rows: one thread per scalar row
@@ -887,8 +912,8 @@ __device__ __forceinline__ void load_cols_shared(const uint32_t* p, uint32_t (&c
   }
 }
 
-template <typename S, typename V, int CB, class Epi>
-__device__ __forceinline__ void split_rows(const SellOp<S>& A, const V* __restrict__ x, Epi& epi) {
+template <typename S, typename V, int CB, class Epi, class Gate>
+__device__ __forceinline__ bool split_rows(const SellOp<S>& A, const V* __restrict__ x, Epi& epi, const Gate& gate) {
   constexpr int U = sell_chunk_blocks(CB, (int)sizeof(S));
   constexpr int VEC = 16 / (int)sizeof(S);
   constexpr int NV = U * CB / VEC;
@@ -897,14 +922,19 @@ __device__ __forceinline__ void split_rows(const SellOp<S>& A, const V* __restri
   const uint32_t lane = threadIdx.x & 31;
   const uint32_t m = lane / 6, part = lane - 6 * m;
   const uint32_t warps = blockDim.x >> 5;
+  bool open = false;  // the gate, tested after the first slice's row map is requested (sell_rows)
   for (uint32_t s = blockIdx.x * warps + (threadIdx.x >> 5); s < A.nslices; s += gridDim.x * warps) {
     const uint32_t slot = s * 32 + lane;
-    const uint32_t row = A.rows[slot];
-    const uint32_t n = A.len[slot];
+    const uint32_t row = ld_early(A.rows + slot);
+    const uint32_t n = ld_early(A.len + slot);
+    const uint32_t base = ld_early(A.start + s);
+    if (!open) {
+      if (!gate()) return false;
+      open = true;
+    }
     const bool live = row < A.nrows;
     epi.pre(row, part, live);
     V acc = V(0);
-    const uint32_t base = A.start[s];
     const uint32_t* cp = A.cols + (size_t)(base >> 5) * kSplitRowsPerSlice + (size_t)m * U;
     // Values one chunk ahead, columns two (as in sell_rows).
     uint32_t cn[U], cf[U];
@@ -951,6 +981,7 @@ __device__ __forceinline__ void split_rows(const SellOp<S>& A, const V* __restri
     }
     epi.post(row, part, live, acc);
   }
+  return open || gate();
 }
 
 template <typename V, int OP>
@@ -975,9 +1006,8 @@ struct SplitAxpy {
 template <typename S, typename V, int CB, int OP>
 __device__ __forceinline__ void split_kernel(SellOp<S> A, const V* __restrict__ x, V* __restrict__ y,
                                              const V* __restrict__ b, const int* __restrict__ status) {
-  if (*status != ST_ACTIVE) return;
   SplitAxpy<V, OP> epi{y, b, V(0)};
-  split_rows<S, V, CB>(A, x, epi);
+  split_rows<S, V, CB>(A, x, epi, StatusGate{status});
 }
 
 // The fused Chebyshev step with split rows. z = D^-1 r couples a block row's six components:
@@ -1021,7 +1051,6 @@ __device__ __forceinline__ void split_cheb_kernel(SellOp<S> A, const S* __restri
                                                   const V* __restrict__ d_old, V* __restrict__ d_new,
                                                   V* __restrict__ r, V* __restrict__ x, V* __restrict__ outer,
                                                   V keep, V step, const int* __restrict__ status) {
-  if (*status != ST_ACTIVE) return;
   SplitCheb<S, V> epi;
   epi.dinv = dinv;
   epi.d_old = d_old;
@@ -1031,7 +1060,7 @@ __device__ __forceinline__ void split_cheb_kernel(SellOp<S> A, const S* __restri
   epi.outer = outer;
   epi.keep = keep;
   epi.step = step;
-  split_rows<S, V, 6>(A, d_old, epi);
+  split_rows<S, V, 6>(A, d_old, epi, StatusGate{status});
 }
 
 // ------------------------------------------------------------ the coarse tail: one cluster launch
@@ -1599,11 +1628,10 @@ struct SellStart {
 template <typename S, typename V, int RB, int CB, int OP>
 __device__ __forceinline__ void sell_start_kernel(SellOp<S> A, const V* __restrict__ x, const V* __restrict__ b,
                                                   StartArgs<S, V> a, const int* __restrict__ status) {
-  if (*status != ST_ACTIVE) return;
   SellStart<S, V, RB, OP> epi;
   epi.a = a;
   epi.b = b;
-  sell_rows<S, V, RB, CB, false>(A, x, epi);
+  sell_rows<S, V, RB, CB, false>(A, x, epi, StatusGate{status});
 }
 
 // Split rows (lane 6 m + p: scalar row p of block row m); the six values of a block row meet by
@@ -1630,12 +1658,11 @@ struct SplitStart {
 template <typename S, typename V, int CB, int OP>
 __device__ __forceinline__ void split_start_kernel(SellOp<S> A, const V* __restrict__ x, const V* __restrict__ b,
                                                    StartArgs<S, V> a, const int* __restrict__ status) {
-  if (*status != ST_ACTIVE) return;
   SplitStart<S, V, OP> epi;
   epi.a = a;
   epi.b = b;
   epi.in = V(0);
-  split_rows<S, V, CB>(A, x, epi);
+  split_rows<S, V, CB>(A, x, epi, StatusGate{status});
 }
 
 // Row groups (LPR lanes per row): after the butterfly every lane holds the whole row.
@@ -1697,12 +1724,11 @@ struct SellDot {
 __device__ __forceinline__ void sell_pcg_spmv_dot_kernel(SellOp<double> A, const double* __restrict__ p,
                                                                       double* __restrict__ ap, double* partials,
                                                                       PcgState* st) {
-  if (st->status != ST_ACTIVE) return;
   SellDot epi;
   epi.p = p;
   epi.ap = ap;
   epi.local = 0.0;
-  sell_rows<double, double, 3, 3, false>(A, p, epi);
+  if (!sell_rows<double, double, 3, 3, false>(A, p, epi, StatusGate{&st->status})) return;
   double v[1] = {epi.local}, total[1];
   if (finish_partials<1>(v, partials, &st->tickets[0], total) && threadIdx.x == 0) {
     double curvature = total[0];
@@ -1741,16 +1767,21 @@ struct SellCheck {
   }
 };
 
+// The true-residual check runs only in its mode (the pcg_* kernels' MODE_CHECK test).
+struct CheckGate {
+  const PcgState* st;
+  __device__ __forceinline__ bool operator()() const { return st->status == ST_ACTIVE && st->mode == MODE_CHECK; }
+};
+
 __device__ __forceinline__ void sell_pcg_check_kernel(SellOp<double> A, const double* __restrict__ x,
                                                                    const double* __restrict__ b, double* __restrict__ r,
                                                                    double* partials, PcgState* st) {
-  if (st->status != ST_ACTIVE || st->mode != MODE_CHECK) return;
   SellCheck epi;
   epi.b = b;
   epi.r = r;
   epi.res2 = 0.0;
   epi.bound2 = 0.0;
-  sell_rows<double, double, 3, 3, true>(A, x, epi);
+  if (!sell_rows<double, double, 3, 3, true>(A, x, epi, CheckGate{st})) return;
   double v[2] = {epi.res2, epi.bound2}, total[2];
   if (finish_partials<2>(v, partials, &st->tickets[2], total) && threadIdx.x == 0) {
     double rel = sqrt(total[0]) / st->rhs_norm;
@@ -3335,7 +3366,7 @@ __global__ void __launch_bounds__(kThreads) sell_energy_kernel(SellOp<double> A,
   epi.p = x + off;
   epi.ap = y + off;
   epi.local = 0.0;
-  sell_rows<double, double, 3, 3, false>(A, x + off, epi);
+  sell_rows<double, double, 3, 3, false>(A, x + off, epi, OpenGate{});
   energy_finish(epi.local, scratch, energy);
 }
 
