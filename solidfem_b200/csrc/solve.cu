@@ -283,8 +283,44 @@ __host__ __device__ __forceinline__ uint32_t slot_bytes(const Op<S>& A) {
 // epi.post(row, live, sums[RB], mag[RB], lane) after the team's fixed butterfly, in every lane.
 // With MAG it also sums |a_ij x_j| per row (the rounding floor of pcg.rs:246-248). A group is
 // staged one grid-stride step ahead (double buffer), its descriptor two steps ahead.
-template <typename S, typename V, int RB, int CB, int LPR, bool MAG, class Epi>
-__device__ __forceinline__ void run_groups(const Op<S>& A, const V* __restrict__ x, char* wbase, Epi& epi) {
+// Gates: the row walks (run_groups, sell_rows, split_rows) test their kernel's gate (the status
+// word) only after their first operator loads have been requested, so the status load and those
+// loads travel together instead of one after the other. The operator arrays are never written by
+// a solve kernel, and a closed gate ends the walk before any x gather, epilogue load or store.
+// sell_rows' and split_rows' row-map loads are volatile so the compiler keeps them ahead of the
+// gate's branch.
+__device__ __forceinline__ uint32_t ld_early(const uint32_t* p) {
+  uint32_t v;
+  asm volatile("ld.global.nc.u32 %0, [%1];" : "=r"(v) : "l"(p));
+  return v;
+}
+
+// load() reads the gate's word(s); open() tests them. run_groups issues the load before its first
+// operator loads and tests it after them; gate() does both at once.
+struct StatusGate {
+  const int* status;
+  __device__ __forceinline__ int load() const { return *status; }
+  __device__ __forceinline__ static bool open(int w) { return w == ST_ACTIVE; }
+  __device__ __forceinline__ bool operator()() const { return open(load()); }
+};
+struct OpenGate {
+  __device__ __forceinline__ int load() const { return 0; }
+  __device__ __forceinline__ static bool open(int) { return true; }
+  __device__ __forceinline__ bool operator()() const { return true; }
+};
+
+// The true-residual check runs only in its mode.
+struct CheckGate {
+  const PcgState* st;
+  __device__ __forceinline__ int2 load() const { return make_int2(st->status, st->mode); }
+  __device__ __forceinline__ static bool open(int2 w) { return w.x == ST_ACTIVE && w.y == MODE_CHECK; }
+  __device__ __forceinline__ bool operator()() const { return open(load()); }
+};
+
+// Returns the gate (uniform over the grid: a body may still reduce across its blocks after true).
+template <typename S, typename V, int RB, int CB, int LPR, bool MAG, class Epi, class Gate>
+__device__ __forceinline__ bool run_groups(const Op<S>& A, const V* __restrict__ x, char* wbase, Epi& epi,
+                                           const Gate& gate) {
   constexpr int LEN = RB * CB;
   constexpr int TEAMS = 32 / LPR;
   const int lane = threadIdx.x & 31;
@@ -309,10 +345,17 @@ __device__ __forceinline__ void run_groups(const Op<S>& A, const V* __restrict__
     }
   };
   const uint4 none = make_uint4(0, 0, 0, 0);
+  // The gate's load goes first (the staging asm below is a compiler memory barrier) and is tested
+  // once the first group's staging is in flight; a closed gate drains the copies and ends.
+  const auto word = gate.load();
   uint4 cur = g < A.ngroups ? A.groups[g] : none;
   uint4 nxt = g + nw < A.ngroups ? A.groups[g + nw] : none;
   if (g < A.ngroups) issue(cur, 0);
   cp_async_commit();
+  if (!Gate::open(word)) {
+    cp_async_wait_all();
+    return false;
+  }
   for (int k = 0; g < A.ngroups; ++k, g += nw) {
     const int slot = k & 1;
     const bool has_next = g + nw < A.ngroups;
@@ -383,6 +426,7 @@ __device__ __forceinline__ void run_groups(const Op<S>& A, const V* __restrict__
     nxt = after;
   }
   cp_async_wait_all();
+  return true;
 }
 
 template <typename V, int RB>
@@ -434,11 +478,10 @@ struct EpiAxpy {
 template <typename S, typename V, int RB, int CB, int LPR, int OP>
 __device__ __forceinline__ void bsr_kernel(Op<S> A, const V* __restrict__ x, V* __restrict__ y,
                                                        const V* __restrict__ b, const int* __restrict__ status) {
-  if (*status != ST_ACTIVE) return;
   extern __shared__ __align__(16) char smem[];
   char* wbase = smem + (threadIdx.x >> 5) * 2 * slot_bytes(A);
   EpiAxpy<V, RB, LPR, OP> epi{y, b, {}};
-  run_groups<S, V, RB, CB, LPR, false>(A, x, wbase, epi);
+  run_groups<S, V, RB, CB, LPR, false>(A, x, wbase, epi, StatusGate{status});
 }
 
 // One Chebyshev step fused with its product (cycle.rs:611-650): ad = A d_old; r -= ad;
@@ -504,7 +547,6 @@ __device__ __forceinline__ void cheb_step_kernel(Op<S> A, const S* __restrict__ 
                                                              V* __restrict__ d_new, V* __restrict__ r, V* __restrict__ x,
                                                              V* __restrict__ outer, V keep, V step,
                                                              const int* __restrict__ status) {
-  if (*status != ST_ACTIVE) return;
   extern __shared__ __align__(16) char smem[];
   char* wbase = smem + (threadIdx.x >> 5) * 2 * slot_bytes(A);
   EpiCheb<S, V, RB, LPR> epi;
@@ -516,7 +558,7 @@ __device__ __forceinline__ void cheb_step_kernel(Op<S> A, const S* __restrict__ 
   epi.outer = outer;
   epi.keep = keep;
   epi.step = step;
-  run_groups<S, V, RB, RB, LPR, false>(A, d_old, wbase, epi);
+  run_groups<S, V, RB, RB, LPR, false>(A, d_old, wbase, epi, StatusGate{status});
 }
 
 // The smoother's start from a zero guess (cycle.rs:591-610): r = b; d = (D^-1 b) / theta; x = d.
@@ -695,25 +737,6 @@ __device__ __forceinline__ void load_cols(const uint32_t* p, uint32_t (&c)[U]) {
     for (int u = 0; u < U; ++u) c[u] = __ldcs(p + u);
   }
 }
-
-// The row walks test their kernel's gate (the status word) only after the first slice's row map
-// has been requested, so the status load and the row-map loads travel together instead of one
-// after the other. The operator arrays are never written by a solve kernel, and a closed gate
-// ends the walk before any x gather, epilogue load or store. The row-map loads are volatile so
-// the compiler keeps them ahead of the gate's branch.
-__device__ __forceinline__ uint32_t ld_early(const uint32_t* p) {
-  uint32_t v;
-  asm volatile("ld.global.nc.u32 %0, [%1];" : "=r"(v) : "l"(p));
-  return v;
-}
-
-struct StatusGate {
-  const int* status;
-  __device__ __forceinline__ bool operator()() const { return *status == ST_ACTIVE; }
-};
-struct OpenGate {
-  __device__ __forceinline__ bool operator()() const { return true; }
-};
 
 // Returns the gate: false when the kernel must end (uniform over the grid, so a body may still
 // reduce across its blocks after a true return).
@@ -1692,13 +1715,12 @@ struct EpiStart {
 template <typename S, typename V, int RB, int CB, int LPR, int OP>
 __device__ __forceinline__ void bsr_start_kernel(Op<S> A, const V* __restrict__ x, const V* __restrict__ b,
                                                  StartArgs<S, V> a, const int* __restrict__ status) {
-  if (*status != ST_ACTIVE) return;
   extern __shared__ __align__(16) char smem[];
   char* wbase = smem + (threadIdx.x >> 5) * 2 * slot_bytes(A);
   EpiStart<S, V, RB, LPR, OP> epi;
   epi.a = a;
   epi.b = b;
-  run_groups<S, V, RB, CB, LPR, false>(A, x, wbase, epi);
+  run_groups<S, V, RB, CB, LPR, false>(A, x, wbase, epi, StatusGate{status});
 }
 
 struct SellDot {
@@ -1767,12 +1789,6 @@ struct SellCheck {
   }
 };
 
-// The true-residual check runs only in its mode (the pcg_* kernels' MODE_CHECK test).
-struct CheckGate {
-  const PcgState* st;
-  __device__ __forceinline__ bool operator()() const { return st->status == ST_ACTIVE && st->mode == MODE_CHECK; }
-};
-
 __device__ __forceinline__ void sell_pcg_check_kernel(SellOp<double> A, const double* __restrict__ x,
                                                                    const double* __restrict__ b, double* __restrict__ r,
                                                                    double* partials, PcgState* st) {
@@ -1828,14 +1844,13 @@ struct EpiDot {
 template <int LPR>
 __device__ __forceinline__ void pcg_spmv_dot_kernel(Op<double> A, const double* __restrict__ p,
                                                                  double* __restrict__ ap, double* partials, PcgState* st) {
-  if (st->status != ST_ACTIVE) return;
   extern __shared__ __align__(16) char smem[];
   char* wbase = smem + (threadIdx.x >> 5) * 2 * slot_bytes(A);
   EpiDot<LPR> epi;
   epi.p = p;
   epi.ap = ap;
   epi.local = 0.0;
-  run_groups<double, double, 3, 3, LPR, false>(A, p, wbase, epi);
+  if (!run_groups<double, double, 3, 3, LPR, false>(A, p, wbase, epi, StatusGate{&st->status})) return;
   double v[1] = {epi.local}, total[1];
   if (finish_partials<1>(v, partials, &st->tickets[0], total) && threadIdx.x == 0) {
     double curvature = total[0];
@@ -1926,7 +1941,6 @@ template <int LPR>
 __device__ __forceinline__ void pcg_check_kernel(Op<double> A, const double* __restrict__ x,
                                                               const double* __restrict__ b, double* __restrict__ r,
                                                               double* partials, PcgState* st) {
-  if (st->status != ST_ACTIVE || st->mode != MODE_CHECK) return;
   extern __shared__ __align__(16) char smem[];
   char* wbase = smem + (threadIdx.x >> 5) * 2 * slot_bytes(A);
   EpiCheck<LPR> epi;
@@ -1935,7 +1949,7 @@ __device__ __forceinline__ void pcg_check_kernel(Op<double> A, const double* __r
   epi.starts = A.starts;
   epi.res2 = 0.0;
   epi.bound2 = 0.0;
-  run_groups<double, double, 3, 3, LPR, true>(A, x, wbase, epi);
+  if (!run_groups<double, double, 3, 3, LPR, true>(A, x, wbase, epi, CheckGate{st})) return;
   double v[2] = {epi.res2, epi.bound2}, total[2];
   if (finish_partials<2>(v, partials, &st->tickets[2], total) && threadIdx.x == 0) {
     double rel = sqrt(total[0]) / st->rhs_norm;
@@ -3382,7 +3396,7 @@ __global__ void __launch_bounds__(kThreads) energy_kernel(Op<double> A, const do
   epi.p = x + off;
   epi.ap = y + off;
   epi.local = 0.0;
-  run_groups<double, double, 3, 3, LPR, false>(A, x + off, wbase, epi);
+  run_groups<double, double, 3, 3, LPR, false>(A, x + off, wbase, epi, OpenGate{});
   energy_finish(epi.local, scratch, energy);
 }
 
