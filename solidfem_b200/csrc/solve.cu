@@ -278,11 +278,6 @@ __host__ __device__ __forceinline__ uint32_t slot_bytes(const Op<S>& A) {
   return A.vbuf + A.cbuf + A.sbuf;
 }
 
-// Walks this warp's row groups. Per row (one team of LPR lanes each) it calls epi.pre(row, live,
-// lane) before the row's blocks are read, so the epilogue's own loads overlap the gathers, and
-// epi.post(row, live, sums[RB], mag[RB], lane) after the team's fixed butterfly, in every lane.
-// With MAG it also sums |a_ij x_j| per row (the rounding floor of pcg.rs:246-248). A group is
-// staged one grid-stride step ahead (double buffer), its descriptor two steps ahead.
 // Gates: the row walks (run_groups, sell_rows, split_rows) test their kernel's gate (the status
 // word) only after their first operator loads have been requested, so the status load and those
 // loads travel together instead of one after the other. The operator arrays are never written by
@@ -317,6 +312,11 @@ struct CheckGate {
   __device__ __forceinline__ bool operator()() const { return open(load()); }
 };
 
+// Walks this warp's row groups. Per row (one team of LPR lanes each) it calls epi.pre(row, live,
+// lane) before the row's blocks are read, so the epilogue's own loads overlap the gathers, and
+// epi.post(row, live, sums[RB], mag[RB], lane) after the team's fixed butterfly, in every lane.
+// With MAG it also sums |a_ij x_j| per row (the rounding floor of pcg.rs:246-248). A group is
+// staged one grid-stride step ahead (double buffer), its descriptor two steps ahead.
 // Returns the gate (uniform over the grid: a body may still reduce across its blocks after true).
 template <typename S, typename V, int RB, int CB, int LPR, bool MAG, class Epi, class Gate>
 __device__ __forceinline__ bool run_groups(const Op<S>& A, const V* __restrict__ x, char* wbase, Epi& epi,
